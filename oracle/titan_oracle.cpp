@@ -1,0 +1,1159 @@
+// ============================================================================
+// ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of TITAN's plasma time step (`Setka::Go`,
+// TITAN/source/Setka_physics.cpp:1484-2278) on flat arrays. Only tests/,
+// __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it, and
+// only as the checker / the timed CPU baseline — never as the product path.
+//
+// Parity pin: the Riemann solver below (`o_chlld`) is checked bit-for-bit
+// against the reference's own Phys_param::chlld compiled unmodified from the
+// reference tree (oracle/Makefile `ref`, tests/test_oracle_ref.py and the
+// golden vectors in tests/golden/). The step driver, reconstruction,
+// geometry and sources are restatements of the cited reference functions;
+// the reference's driver cannot be compiled here (it needs Boost, CGAL,
+// Eigen and missing mesh files), so those parts are pinned through the
+// reference solver plus invariants (conservation, Test_geometr checks).
+//
+// Floating point: compiled with -ffp-contract=off so that every expression is
+// evaluated in the same order and rounding as the reference's x86-64 build.
+// ============================================================================
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// Constants restated from TITAN/source/Header.h:96-104.
+const double kPi = 3.14159265358979323846;
+const double kCpi4 = 4.0 * kPi;
+const double kSpi4 = std::sqrt(kCpi4);
+const double kEpsB = 1E-4;
+const double kMeDmp = (1.0 / 1836.15);
+// Literal 8*pi used by the energy update, Setka_physics.cpp:1927-1929.
+const double kC8Pi = 25.13274122871834590768;
+
+inline double sq(double x) { return x * x; }
+inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+// std::min / std::max semantics (first argument wins ties and NaN on the left)
+inline double mn(double a, double b) { return (b < a) ? b : a; }
+inline double mx(double a, double b) { return (a < b) ? b : a; }
+
+}  // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// Layout shared with the Python side (tests/oracle_lib.py mirrors it).
+// State: SoA [NV][ncell], NV = 10: rho, Vx, Vy, Vz, p, Bx, By, Bz, Q, rho_He.
+// H fields (frozen neutral fluids, Bera sources): SoA [5*nh][ncell] in the
+// order rho_Hk, Vx_Hk, Vy_Hk, Vz_Hk, p_Hk for k = 1..nh.
+// ---------------------------------------------------------------------------
+struct OMesh {
+    int64_t nnode, ncell, nface;
+    const int32_t* cell_nodes;   // ncell*8
+    const int32_t* cell_faces;   // ncell*6, the cell's `grans` order
+    const int8_t* cell_type;     // ncell, Type_cell (Cell.h:5-11)
+    const uint8_t* cell_tvd;     // ncell, Cell::is_TVD
+    const int32_t* face_nodes;   // nface*4, nodes around the quad
+    const int32_t* face_cells;   // nface*2, cells[0], cells[1] (-1 when absent)
+    const int8_t* face_type;     // nface, Type_Gran (Gran.h:5-10)
+    const int8_t* face_surf;     // nface, Type_Gran_surf (Gran.h:12-17)
+    const int8_t* face_method;   // nface, n_state (policy 0)
+    const int32_t* face_bc;      // nface, row of bc_vals for hard faces, else -1
+    const double* bc_vals;       // nbc*10, fixed face values (Init_physics)
+    const double* node_amp;      // nnode, radial velocity amplitude (ALE), may be null
+    const double* node_phase;    // nnode, phase (ALE), may be null
+};
+
+struct OParams {
+    double gamma;         // Phys_param::gamma
+    double KFL;           // Courant number
+    double velosity_inf;  // Phys_param::Velosity_inf (soft-boundary fix-up)
+    double omega;         // angular frequency of the prescribed node motion
+    double par_a_2, par_n_H_LISM, par_Kn;  // charge exchange (Phys_param.h:111-114)
+    double beta_switch;   // policy 1: HLLD where b^2/(2p) > beta_switch, else HLLC
+    int32_t move;         // Phys_param::move_setka
+    int32_t soft_fixups;  // Outer_Soft fix-ups of Setka_gran_snos.cpp:27-45 (1) or plain copy (0)
+    int32_t method_policy;  // 0: face_method array; 1: beta switch per face per step
+    int32_t npassive;     // 0 or 2 (Q, rho_He carried as passive scalars)
+    int32_t nh;           // number of frozen H fluids feeding the Bera sources (0 = none)
+    int32_t TS_hard, contact_hard;
+    int32_t pad;
+};
+
+struct OStepInfo {
+    int64_t steps_done;
+    int64_t err_code;     // 0 ok; >0: first failure kind
+    int64_t err_index;    // cell or face index of the failure
+    int64_t n_rho_floor, n_p_floor;
+};
+
+enum { NV = 10 };
+
+// ---------------------------------------------------------------------------
+// get_bazis, TITAN/source/Help_funk.cpp:219-232 (Eigen dot / cross / normalized)
+// ---------------------------------------------------------------------------
+static void o_bazis(const double n[3], double t[3], double m[3]) {
+    double a[3] = {1.0, 0.0, 0.0};
+    if (std::abs(n[0] * a[0] + n[1] * a[1] + n[2] * a[2]) > 0.9) {
+        a[0] = 0.0;
+        a[1] = 1.0;
+        a[2] = 0.0;
+    }
+    double c[3] = {a[1] * n[2] - a[2] * n[1], a[2] * n[0] - a[0] * n[2], a[0] * n[1] - a[1] * n[0]};
+    double z = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+    if (z > 0.0) {
+        double s = std::sqrt(z);
+        t[0] = c[0] / s;
+        t[1] = c[1] / s;
+        t[2] = c[2] / s;
+    } else {
+        t[0] = c[0];
+        t[1] = c[1];
+        t[2] = c[2];
+    }
+    m[0] = n[1] * t[2] - n[2] * t[1];
+    m[1] = n[2] * t[0] - n[0] * t[2];
+    m[2] = n[0] * t[1] - n[1] * t[0];
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solver family, restating Phys_param::chlld
+// (TITAN/source/Phys_param.cpp:882-1878): n_state 0 Lax, 1 HLL, 2 HLLC,
+// 3 HLLD, in the frame of a face moving with normal speed w. Returns 0, or a
+// nonzero code where the reference prints an error and exits.
+// ---------------------------------------------------------------------------
+int o_chlld(int n_state, const double* nrm, double w, const double* q1, const double* q2,
+            int null_bn, int n_disc, int nk, const double* kl, const double* kr, double* qout,
+            double* kout, double* ds, int left_ydar, int contact, double gamma) {
+    const double g1 = gamma - 1.0;
+    double wv = w;
+    const double r1 = q1[0], u1 = q1[1], v1 = q1[2], w1 = q1[3], p1 = q1[4];
+    const double bx1 = q1[5] / kSpi4, by1 = q1[6] / kSpi4, bz1 = q1[7] / kSpi4;
+    const double r2 = q2[0], u2 = q2[1], v2 = q2[2], w2 = q2[3], p2 = q2[4];
+    const double bx2 = q2[5] / kSpi4, by2 = q2[6] / kSpi4, bz2 = q2[7] / kSpi4;
+    const double ro = (r2 + r1) / 2.0;
+    const double ap = (p2 + p1) / 2.0;
+
+    double n[3] = {nrm[0], nrm[1], nrm[2]}, t[3], m[3];
+    o_bazis(n, t, m);
+
+    double vL[3], vR[3], bL[3], bR[3];
+    vL[0] = n[0] * u1 + n[1] * v1 + n[2] * w1;
+    vL[1] = t[0] * u1 + t[1] * v1 + t[2] * w1;
+    vL[2] = m[0] * u1 + m[1] * v1 + m[2] * w1;
+    vR[0] = n[0] * u2 + n[1] * v2 + n[2] * w2;
+    vR[1] = t[0] * u2 + t[1] * v2 + t[2] * w2;
+    vR[2] = m[0] * u2 + m[1] * v2 + m[2] * w2;
+    bL[0] = n[0] * bx1 + n[1] * by1 + n[2] * bz1;
+    bL[1] = t[0] * bx1 + t[1] * by1 + t[2] * bz1;
+    bL[2] = m[0] * bx1 + m[1] * by1 + m[2] * bz1;
+    bR[0] = n[0] * bx2 + n[1] * by2 + n[2] * bz2;
+    bR[1] = t[0] * bx2 + t[1] * by2 + t[2] * bz2;
+    bR[2] = m[0] * bx2 + m[1] * by2 + m[2] * bz2;
+
+    // fast magnetosonic speeds (:977-1002)
+    const double aaL = bL[0] / std::sqrt(r1);
+    const double b2L = dot3(bL, bL);
+    const double b21 = b2L / r1;
+    const double cL = std::sqrt(gamma * p1 / r1);
+    double qp = std::sqrt(b21 + cL * (cL + 2.0 * aaL));
+    double qm = std::sqrt(b21 + cL * (cL - 2.0 * aaL));
+    const double cfL = (qp + qm) / 2.0;
+    const double ptL = p1 + b2L / 2.0;
+
+    const double aaR = bR[0] / std::sqrt(r2);
+    const double b2R = dot3(bR, bR);
+    const double b22 = b2R / r2;
+    const double cR = std::sqrt(gamma * p2 / r2);
+    qp = std::sqrt(b22 + cR * (cR + 2.0 * aaR));
+    qm = std::sqrt(b22 + cR * (cR - 2.0 * aaR));
+    const double cfR = (qp + qm) / 2.0;
+    const double ptR = p2 + b2R / 2.0;
+
+    const double aC = (aaL + aaR) / 2.0;
+    const double b2o = (b22 + b21) / 2.0;
+    const double cC = std::sqrt(gamma * ap / ro);
+    qp = std::sqrt(b2o + cC * (cC + 2.0 * aC));
+    qm = std::sqrt(b2o + cC * (cC - 2.0 * aC));
+    const double cfC = (qp + qm) / 2.0;
+    const double vC1 = (vL[0] + vR[0]) / 2.0;
+
+    // wave-speed estimate by n_disc (:1006-1037)
+    double SL = 0.0, SR = 0.0;
+    if (left_ydar) n_disc = 2;
+    if (n_disc == 0) {
+        SL = mn(vL[0] - cfL, vR[0] - cfR);
+        SR = mx(vL[0] + cfL, vR[0] + cfR);
+    } else if (n_disc == 1) {
+        SL = mn(vL[0] - cfL, vC1 - cfC);
+        SR = mx(vR[0] + cfR, vC1 + cfC);
+    } else if (n_disc == 2) {
+        const double SL_1 = mn(vL[0] - cfL, vC1 - cfC);
+        const double SR_1 = mx(vR[0] + cfR, vC1 + cfC);
+        const double SL_2 = mn(vL[0] - cfL, vR[0] - cfR);
+        const double SR_2 = mx(vL[0] + cfL, vR[0] + cfR);
+        const double oo = 0.6;
+        const double oo1 = 1.0 - oo;
+        SL = oo * SL_1 + oo1 * SL_2;
+        SR = oo * SR_1 + oo1 * SR_2;
+    } else if (n_disc == 3) {
+        SL = mn(vL[0], vR[0]) - mx(cfL, cfR);
+        SR = mx(vL[0], vR[0]) + mx(cfL, cfR);
+    }
+    ds[2] = SR;
+    ds[0] = SL;
+
+    const double suR = SR - vR[0];
+    const double suL = SL - vL[0];
+    const double SM = (suR * r2 * vR[0] - ptR + ptL - suL * r1 * vL[0]) / (suR * r2 - suL * r1);
+    ds[1] = SM;
+    if (contact) wv = SM;
+
+    if (n_state == 0) {  // Lax speeds override after dsl/dsr were recorded (:1053-1059)
+        const double TR0 = std::fabs(vL[0] + vR[0]) / 2.0 + cfC;
+        SR = TR0;
+        SL = -TR0;
+    }
+
+    const double upt1 = (sq(u1) + sq(v1) + sq(w1)) / 2.0;
+    const double sbv1 = u1 * bx1 + v1 * by1 + w1 * bz1;
+    const double upt2 = (sq(u2) + sq(v2) + sq(w2)) / 2.0;
+    const double sbv2 = u2 * bx2 + v2 * by2 + w2 * bz2;
+    const double e1 = p1 / g1 + r1 * upt1 + b2L / 2.0;
+    const double e2 = p2 / g1 + r2 * upt2 + b2R / 2.0;
+
+    double FL[8], FR[8], UL[8], UR[8], UZ[8];
+    FL[0] = r1 * vL[0];
+    FL[1] = r1 * vL[0] * vL[0] + ptL - sq(bL[0]);
+    FL[2] = r1 * vL[0] * vL[1] - bL[0] * bL[1];
+    FL[3] = r1 * vL[0] * vL[2] - bL[0] * bL[2];
+    FL[4] = (e1 + ptL) * vL[0] - bL[0] * sbv1;
+    FL[5] = 0.0;
+    FL[6] = vL[0] * bL[1] - vL[1] * bL[0];
+    FL[7] = vL[0] * bL[2] - vL[2] * bL[0];
+    FR[0] = r2 * vR[0];
+    FR[1] = r2 * vR[0] * vR[0] + ptR - sq(bR[0]);
+    FR[2] = r2 * vR[0] * vR[1] - bR[0] * bR[1];
+    FR[3] = r2 * vR[0] * vR[2] - bR[0] * bR[2];
+    FR[4] = (e2 + ptR) * vR[0] - bR[0] * sbv2;
+    FR[5] = 0.0;
+    FR[6] = vR[0] * bR[1] - vR[1] * bR[0];
+    FR[7] = vR[0] * bR[2] - vR[2] * bR[0];
+    UL[0] = r1;
+    UL[4] = e1;
+    UR[0] = r2;
+    UR[4] = e2;
+    for (int i = 0; i < 3; ++i) {
+        UL[i + 1] = r1 * vL[i];
+        UL[i + 5] = bL[i];
+        UR[i + 1] = r2 * vR[i];
+        UR[i + 5] = bR[i];
+    }
+    for (int k = 0; k < 8; ++k) UZ[k] = (SR * UR[k] - SL * UL[k] + FL[k] - FR[k]) / (SR - SL);
+
+    // passive scalars (konvect)
+    double FLk[4], FRk[4], UZk[4];
+    for (int i = 0; i < nk; ++i) {
+        FLk[i] = kl[i] * vL[0];
+        FRk[i] = kr[i] * vR[0];
+        UZk[i] = (SR * kr[i] - SL * kl[i] + FLk[i] - FRk[i]) / (SR - SL);
+    }
+    if (null_bn) UZ[5] = 0.0;
+
+    double qv[3], qb[3];
+    double SN, wbn;
+
+    if (n_state <= 1) {  // Lax / HLL (:1133-1257)
+        double dq[8], FW[8], FWk[4];
+        for (int k = 0; k < 8; ++k) dq[k] = UR[k] - UL[k];
+        if (left_ydar) wv = SL;
+        double TL = SL, TR = SR;
+        if (SL > wv || left_ydar) {
+            TL = 0.0;
+            for (int k = 0; k < 8; ++k) FW[k] = wv * UL[k];
+            for (int k = 0; k < nk; ++k) FWk[k] = wv * kl[k];
+        } else if (SL <= wv && wv <= SR) {
+            for (int k = 0; k < 8; ++k) FW[k] = wv * UZ[k];
+            for (int k = 0; k < nk; ++k) FWk[k] = wv * UZk[k];
+        } else if (SR < wv) {
+            TR = 0.0;
+            for (int k = 0; k < 8; ++k) FW[k] = wv * UR[k];
+            for (int k = 0; k < nk; ++k) FWk[k] = wv * kr[k];
+        } else {
+            return 1;
+        }
+        const double a = TR * TL;
+        const double b = TR - TL;
+        qout[0] = (TR * FL[0] - TL * FR[0] + a * dq[0]) / b - FW[0];
+        qout[4] = (TR * FL[4] - TL * FR[4] + a * dq[4]) / b - FW[4];
+        for (int k = 0; k < nk; ++k)
+            kout[k] = (TR * FLk[k] - TL * FRk[k] + a * (kr[k] - kl[k])) / b - FWk[k];
+        for (int k = 1; k < 4; ++k) qv[k - 1] = (TR * FL[k] - TL * FR[k] + a * dq[k]) / b - FW[k];
+        for (int k = 5; k < 8; ++k) qb[k - 5] = (TR * FL[k] - TL * FR[k] + a * dq[k]) / b - FW[k];
+        SN = mx(std::fabs(SL), std::fabs(SR));
+        if (wv >= SR)
+            wbn = wv * bR[0];
+        else if (wv <= SL)
+            wbn = wv * bL[0];
+        else
+            wbn = wv * (bL[0] + bR[0]) / 2.0;
+    } else if (n_state == 2) {  // HLLC (:1258-1475)
+        const double suRm = suR / (SR - SM);
+        const double suLm = suL / (SL - SM);
+        const double rzR = r2 * suRm;
+        const double rzL = r1 * suLm;
+        const double ptz =
+            (suR * r2 * ptL - suL * r1 * ptR + r1 * r2 * suR * suL * (vR[0] - vL[0])) / (suR * r2 - suL * r1);
+        double vzR[3], vzL[3], bzR[3], bzL[3];
+        vzR[0] = SM;
+        vzL[0] = SM;
+        bzR[0] = UZ[5];
+        bzL[0] = UZ[5];
+        vzR[1] = vR[1] + UZ[5] * (bR[1] - UZ[6]) / suR / r2;
+        vzR[2] = vR[2] + UZ[5] * (bR[2] - UZ[7]) / suR / r2;
+        vzL[1] = vL[1] + UZ[5] * (bL[1] - UZ[6]) / suL / r1;
+        vzL[2] = vL[2] + UZ[5] * (bL[2] - UZ[7]) / suL / r1;
+        bzR[1] = UZ[6];
+        bzR[2] = UZ[7];
+        bzL[1] = bzR[1];
+        bzL[2] = bzR[2];
+        const double sbvz = (UZ[5] * UZ[1] + UZ[6] * UZ[2] + UZ[7] * UZ[3]) / UZ[0];
+        const double ezR = e2 * suRm + (ptz * SM - ptR * vR[0] + UZ[5] * (sbv2 - sbvz)) / (SR - SM);
+        const double ezL = e1 * suLm + (ptz * SM - ptL * vL[0] + UZ[5] * (sbv1 - sbvz)) / (SL - SM);
+        if (std::fabs(UZ[5]) <= kEpsB) {
+            vzR[1] = vR[1];
+            vzR[2] = vR[2];
+            vzL[1] = vL[1];
+            vzL[2] = vL[2];
+            bzR[1] = bR[1] * suRm;
+            bzR[2] = bR[2] * suRm;
+            bzL[1] = bL[1] * suLm;
+            bzL[2] = bL[2] * suLm;
+        }
+        double UZL[8], UZR[8], UZLk[4], UZRk[4];
+        for (int k = 0; k < nk; ++k) {
+            UZLk[k] = kl[k] * suLm;
+            UZRk[k] = kr[k] * suRm;
+        }
+        UZL[0] = rzL;
+        UZL[4] = ezL;
+        UZR[0] = rzR;
+        UZR[4] = ezR;
+        for (int i = 0; i < 3; ++i) {
+            UZL[i + 1] = vzL[i] * rzL;
+            UZL[i + 5] = bzL[i];
+            UZR[i + 1] = vzR[i] * rzR;
+            UZR[i + 5] = bzR[i];
+        }
+        if (left_ydar) wv = SL;
+        if (SL >= wv || left_ydar) {
+            qout[0] = FL[0] - wv * UL[0];
+            qout[4] = FL[4] - wv * UL[4];
+            for (int k = 0; k < nk; ++k) kout[k] = FLk[k] - wv * kl[k];
+            for (int k = 1; k < 4; ++k) qv[k - 1] = FL[k] - wv * UL[k];
+            for (int k = 5; k < 8; ++k) qb[k - 5] = FL[k] - wv * UL[k];
+        } else if (SL <= wv && SM >= wv) {
+            qout[0] = FL[0] + SL * (rzL - r1) - wv * UZL[0];
+            qout[4] = FL[4] + SL * (ezL - e1) - wv * UZL[4];
+            for (int k = 0; k < nk; ++k) kout[k] = FLk[k] + SL * (UZLk[k] - kl[k]) - wv * UZLk[k];
+            for (int k = 1; k < 4; ++k) qv[k - 1] = FL[k] + SL * (UZL[k] - UL[k]) - wv * UZL[k];
+            for (int k = 5; k < 8; ++k) qb[k - 5] = FL[k] + SL * (UZL[k] - UL[k]) - wv * UZL[k];
+        } else if (SM <= wv && SR > wv) {
+            qout[0] = FR[0] + SR * (rzR - r2) - wv * UZR[0];
+            qout[4] = FR[4] + SR * (ezR - e2) - wv * UZR[4];
+            for (int k = 0; k < nk; ++k) kout[k] = FRk[k] + SR * (UZRk[k] - kr[k]) - wv * UZRk[k];
+            for (int k = 1; k < 4; ++k) qv[k - 1] = FR[k] + SR * (UZR[k] - UR[k]) - wv * UZR[k];
+            for (int k = 5; k < 8; ++k) qb[k - 5] = FR[k] + SR * (UZR[k] - UR[k]) - wv * UZR[k];
+        } else if (SR <= wv) {
+            qout[0] = FR[0] - wv * UR[0];
+            qout[4] = FR[4] - wv * UR[4];
+            for (int k = 0; k < nk; ++k) kout[k] = FRk[k] - wv * kr[k];
+            for (int k = 1; k < 4; ++k) qv[k - 1] = FR[k] - wv * UR[k];
+            for (int k = 5; k < 8; ++k) qb[k - 5] = FR[k] - wv * UR[k];
+        } else {
+            return 2;
+        }
+        SN = mx(std::fabs(SL), std::fabs(SR));
+        if (wv > SR)
+            wbn = wv * bR[0];
+        else if (wv < SL)
+            wbn = wv * bL[0];
+        else
+            wbn = wv * (bL[0] + bR[0]) / 2.0;
+    } else if (n_state == 3) {  // HLLD (:1476-1870)
+        const double ptz =
+            (suR * r2 * ptL - suL * r1 * ptR + r1 * r2 * suR * suL * (vR[0] - vL[0])) / (suR * r2 - suL * r1);
+        double vzL[3], vzR[3], vzzL[3], vzzR[3], bzL[3], bzR[3], bzzL[3], bzzR[3];
+        vzL[0] = SM;
+        vzR[0] = SM;
+        vzzL[0] = SM;
+        vzzR[0] = SM;
+        const double suRm = suR / (SR - SM);
+        const double suLm = suL / (SL - SM);
+        const double rzR = r2 * suRm;
+        const double rzL = r1 * suLm;
+        double qzL[4], qzR[4];
+        for (int k = 0; k < nk; ++k) {
+            qzL[k] = kl[k] * suLm;
+            qzR[k] = kr[k] * suRm;
+        }
+        const double bn = UZ[5];
+        const double bn2 = bn * bn;
+        bzL[0] = bn;
+        bzR[0] = bn;
+        bzzL[0] = bn;
+        bzzR[0] = bn;
+        double tvR, tbR, tvL, tbL;
+        const double ttR = r2 * suR * (SR - SM) - bn2;
+        if (std::fabs(ttR) < 0.000000001) {
+            tvR = 0.0;
+            tbR = 0.0;
+        } else {
+            tvR = (SM - vR[0]) / ttR;
+            tbR = (r2 * suR * suR - bn2) / ttR;
+        }
+        const double ttL = r1 * suL * (SL - SM) - bn2;
+        if (std::fabs(ttL) < 0.000000001) {
+            tvL = 0.0;
+            tbL = 0.0;
+        } else {
+            tvL = (SM - vL[0]) / ttL;
+            tbL = (r1 * suL * suL - bn2) / ttL;
+        }
+        vzL[1] = vL[1] - bn * bL[1] * tvL;
+        vzL[2] = vL[2] - bn * bL[2] * tvL;
+        vzR[1] = vR[1] - bn * bR[1] * tvR;
+        vzR[2] = vR[2] - bn * bR[2] * tvR;
+        bzL[1] = bL[1] * tbL;
+        bzL[2] = bL[2] * tbL;
+        bzR[1] = bR[1] * tbR;
+        bzR[2] = bR[2] * tbR;
+        const double sbvL = bzL[0] * vzL[0] + bzL[1] * vzL[1] + bzL[2] * vzL[2];
+        const double sbvR = bzR[0] * vzR[0] + bzR[1] * vzR[1] + bzR[2] * vzR[2];
+        const double ezR = e2 * suRm + (ptz * SM - ptR * vR[0] + bn * (sbv2 - sbvR)) / (SR - SM);
+        const double ezL = e1 * suLm + (ptz * SM - ptL * vL[0] + bn * (sbv1 - sbvL)) / (SL - SM);
+        const double rzRs = std::sqrt(rzR);
+        const double rzLs = std::sqrt(rzL);
+        const double rzss = rzRs + rzLs;
+        const double rzps = rzRs * rzLs;
+        double SZL = SM - std::fabs(bn) / rzLs;
+        double SZR = SM + std::fabs(bn) / rzRs;
+        double sbn;
+        int ibn;
+        if (std::fabs(bn) > kEpsB) {
+            sbn = std::fabs(bn) / bn;
+            ibn = 1;
+        } else {
+            sbn = 0.0;
+            ibn = 0;
+            SZL = SM;
+            SZR = SM;
+        }
+        vzzL[1] = (rzLs * vzL[1] + rzRs * vzR[1] + sbn * (bzR[1] - bzL[1])) / rzss;
+        vzzL[2] = (rzLs * vzL[2] + rzRs * vzR[2] + sbn * (bzR[2] - bzL[2])) / rzss;
+        vzzR[1] = vzzL[1];
+        vzzR[2] = vzzL[2];
+        bzzL[1] = (rzLs * bzR[1] + rzRs * bzL[1] + sbn * rzps * (vzR[1] - vzL[1])) / rzss;
+        bzzL[2] = (rzLs * bzR[2] + rzRs * bzL[2] + sbn * rzps * (vzR[2] - vzL[2])) / rzss;
+        bzzR[1] = bzzL[1];
+        bzzR[2] = bzzL[2];
+        const double sbzz = bzzL[0] * vzzL[0] + bzzL[1] * vzzL[1] + bzzL[2] * vzzL[2];
+        const double ezzR = ezR + rzRs * sbn * (sbvR - sbzz);
+        const double ezzL = ezL - rzLs * sbn * (sbvL - sbzz);
+        double UZL[8], UZR[8], UZZL[8], UZZR[8];
+        UZL[0] = rzL;
+        UZL[4] = ezL;
+        UZR[0] = rzR;
+        UZR[4] = ezR;
+        UZZL[0] = rzL;
+        UZZL[4] = ezzL;
+        UZZR[0] = rzR;
+        UZZR[4] = ezzR;
+        for (int i = 0; i < 3; ++i) {
+            UZL[i + 1] = vzL[i] * rzL;
+            UZL[i + 5] = bzL[i];
+            UZR[i + 1] = vzR[i] * rzR;
+            UZR[i + 5] = bzR[i];
+            UZZL[i + 1] = vzzL[i] * rzL;
+            UZZL[i + 5] = bzzL[i];
+            UZZR[i + 1] = vzzR[i] * rzR;
+            UZZR[i + 5] = bzzR[i];
+        }
+        int j_ccs = -1;
+        if (left_ydar) wv = SL;
+        if (SL >= wv || left_ydar) {  // zone 1
+            qout[0] = FL[0] - wv * UL[0];
+            qout[4] = FL[4] - wv * UL[4];
+            for (int k = 1; k < 4; ++k) qv[k - 1] = FL[k] - wv * UL[k];
+            for (int k = 5; k < 8; ++k) qb[k - 5] = FL[k] - wv * UL[k];
+            for (int k = 0; k < nk; ++k) kout[k] = FLk[k] - wv * kl[k];
+            j_ccs = 1;
+        } else if (SL <= wv && SZL >= wv) {  // zone 2
+            for (int k : {0, 4}) qout[k] = FL[k] + SL * (UZL[k] - UL[k]) - wv * UZL[k];
+            for (int k = 0; k < nk; ++k) kout[k] = FLk[k] + SL * (qzL[k] - kl[k]) - wv * qzL[k];
+            for (int k = 1; k < 4; ++k) qv[k - 1] = FL[k] + SL * (UZL[k] - UL[k]) - wv * UZL[k];
+            for (int k = 5; k < 8; ++k) qb[k - 5] = FL[k] + SL * (UZL[k] - UL[k]) - wv * UZL[k];
+            j_ccs = 2;
+        }
+        if (ibn == 1) {
+            if (SZL <= wv && SM >= wv) {  // zone 3
+                for (int k : {0, 4})
+                    qout[k] = FL[k] + SZL * (UZZL[k] - UZL[k]) + SL * (UZL[k] - UL[k]) - wv * UZZL[k];
+                for (int k = 0; k < nk; ++k)
+                    kout[k] = FLk[k] + SZL * (qzL[k] - qzL[k]) + SL * (qzL[k] - kl[k]) - wv * qzL[k];
+                for (int k = 1; k < 4; ++k)
+                    qv[k - 1] = FL[k] + SZL * (UZZL[k] - UZL[k]) + SL * (UZL[k] - UL[k]) - wv * UZZL[k];
+                for (int k = 5; k < 8; ++k)
+                    qb[k - 5] = FL[k] + SZL * (UZZL[k] - UZL[k]) + SL * (UZL[k] - UL[k]) - wv * UZZL[k];
+                j_ccs = 3;
+            } else if (SM <= wv && SZR >= wv) {  // zone 4
+                for (int k : {0, 4})
+                    qout[k] = FR[k] + SZR * (UZZR[k] - UZR[k]) + SR * (UZR[k] - UR[k]) - wv * UZZR[k];
+                for (int k = 0; k < nk; ++k)
+                    kout[k] = FRk[k] + SZR * (qzR[k] - qzR[k]) + SR * (qzR[k] - kr[k]) - wv * qzR[k];
+                for (int k = 1; k < 4; ++k)
+                    qv[k - 1] = FR[k] + SZR * (UZZR[k] - UZR[k]) + SR * (UZR[k] - UR[k]) - wv * UZZR[k];
+                for (int k = 5; k < 8; ++k)
+                    qb[k - 5] = FR[k] + SZR * (UZZR[k] - UZR[k]) + SR * (UZR[k] - UR[k]) - wv * UZZR[k];
+                j_ccs = 4;
+            }
+        }
+        if (SZR <= wv && SR >= wv) {  // zone 5
+            for (int k : {0, 4}) qout[k] = FR[k] + SR * (UZR[k] - UR[k]) - wv * UZR[k];
+            for (int k = 0; k < nk; ++k) kout[k] = FRk[k] + SR * (qzR[k] - kr[k]) - wv * qzR[k];
+            for (int k = 1; k < 4; ++k) qv[k - 1] = FR[k] + SR * (UZR[k] - UR[k]) - wv * UZR[k];
+            for (int k = 5; k < 8; ++k) qb[k - 5] = FR[k] + SR * (UZR[k] - UR[k]) - wv * UZR[k];
+            j_ccs = 5;
+        } else if (SR <= wv) {  // zone 6
+            qout[0] = FR[0] - wv * UR[0];
+            qout[4] = FR[4] - wv * UR[4];
+            for (int k = 0; k < nk; ++k) kout[k] = FRk[k] - wv * kr[k];
+            for (int k = 1; k < 4; ++k) qv[k - 1] = FR[k] - wv * UR[k];
+            for (int k = 5; k < 8; ++k) qb[k - 5] = FR[k] - wv * UR[k];
+            j_ccs = 6;
+        }
+        if (j_ccs == -1) return 3;
+        SN = mx(std::fabs(SL), std::fabs(SR));
+        if (wv > SR)
+            wbn = wv * bR[0];
+        else if (wv < SL)
+            wbn = wv * bL[0];
+        else
+            wbn = wv * (bL[0] + bR[0]) / 2.0;
+    } else {
+        return 4;
+    }
+    // normal-B flux (Powell form) and rotation back with the sqrt(4 pi) rescale
+    qb[0] = -SN * (bR[0] - bL[0]) - wbn;
+    if (null_bn) qb[0] = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        qout[i + 1] = n[i] * qv[0] + t[i] * qv[1] + m[i] * qv[2];
+        qout[i + 5] = n[i] * qb[0] + t[i] * qb[1] + m[i] * qb[2];
+        qout[i + 5] = kSpi4 * qout[i + 5];
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Geometry, restating Setka::Calculating_measure (Setka.cpp:2465-2502):
+// cell centres (Cell.cpp:909-930) -> face centre / area / oriented normal
+// (Gran.cpp:112-218) -> cell volume, method 1 (Cell.cpp:958-1001).
+// Outputs: cc[3*ncell], vol[ncell], fc[3*nface], fn[3*nface], fa[nface].
+// ---------------------------------------------------------------------------
+static double tri_area(const double* a, const double* b, const double* c) {
+    const double v1x = b[0] - a[0], v1y = b[1] - a[1], v1z = b[2] - a[2];
+    const double v2x = c[0] - a[0], v2y = c[1] - a[1], v2z = c[2] - a[2];
+    const double cx = v1y * v2z - v1z * v2y;
+    const double cy = v1z * v2x - v1x * v2z;
+    const double cz = v1x * v2y - v1y * v2x;
+    return 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+}
+
+static double tet_vol(const double* a, const double* b, const double* c, const double* d) {
+    const double abx = b[0] - a[0], aby = b[1] - a[1], abz = b[2] - a[2];
+    const double acx = c[0] - a[0], acy = c[1] - a[1], acz = c[2] - a[2];
+    const double adx = d[0] - a[0], ady = d[1] - a[1], adz = d[2] - a[2];
+    const double cx = aby * acz - abz * acy;
+    const double cy = abz * acx - abx * acz;
+    const double cz = abx * acy - aby * acx;
+    const double dp = cx * adx + cy * ady + cz * adz;
+    return std::abs(dp) / 6.0;
+}
+
+void oracle_geometry(const OMesh* M, const double* xyz, double* cc, double* vol, double* fc,
+                     double* fn, double* fa) {
+    const int64_t nc = M->ncell, nf = M->nface;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < nc; ++c) {
+        double x = 0.0, y = 0.0, z = 0.0;
+        for (int k = 0; k < 8; ++k) {
+            const double* p = xyz + 3 * (int64_t)M->cell_nodes[8 * c + k];
+            x += p[0];
+            y += p[1];
+            z += p[2];
+        }
+        cc[3 * c + 0] = x / 8;
+        cc[3 * c + 1] = y / 8;
+        cc[3 * c + 2] = z / 8;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < nf; ++f) {
+        const double* P[4];
+        for (int k = 0; k < 4; ++k) P[k] = xyz + 3 * (int64_t)M->face_nodes[4 * f + k];
+        double xc = 0.0, yc = 0.0, zc = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            xc += P[k][0];
+            yc += P[k][1];
+            zc += P[k][2];
+        }
+        xc /= 4;
+        yc /= 4;
+        zc /= 4;
+        fc[3 * f + 0] = xc;
+        fc[3 * f + 1] = yc;
+        fc[3 * f + 2] = zc;
+        double S = 0.0;
+        S += tri_area(P[0], P[1], P[2]);
+        S += tri_area(P[0], P[3], P[2]);
+        fa[f] = S;
+        const double x1 = (P[0][0] + P[1][0]) / 2.0, y1 = (P[0][1] + P[1][1]) / 2.0, z1 = (P[0][2] + P[1][2]) / 2.0;
+        const double x2 = (P[1][0] + P[2][0]) / 2.0, y2 = (P[1][1] + P[2][1]) / 2.0, z2 = (P[1][2] + P[2][2]) / 2.0;
+        const double x3 = (P[2][0] + P[3][0]) / 2.0, y3 = (P[2][1] + P[3][1]) / 2.0, z3 = (P[2][2] + P[3][2]) / 2.0;
+        const double ax = x2 - x1, ay = y2 - y1, az = z2 - z1;
+        const double bx = x3 - x1, by = y3 - y1, bz = z3 - z1;
+        double n1 = ay * bz - az * by;
+        double n2 = az * bx - ax * bz;
+        double n3 = ax * by - ay * bx;
+        const double nn = std::sqrt(n1 * n1 + n2 * n2 + n3 * n3);
+        n1 /= nn;
+        n2 /= nn;
+        n3 /= nn;
+        const double* c0 = cc + 3 * (int64_t)M->face_cells[2 * f];
+        if (n1 * (c0[0] - xc) + n2 * (c0[1] - yc) + n3 * (c0[2] - zc) > 0.0) {
+            n1 = -n1;
+            n2 = -n2;
+            n3 = -n3;
+        }
+        fn[3 * f + 0] = n1;
+        fn[3 * f + 1] = n2;
+        fn[3 * f + 2] = n3;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < nc; ++c) {
+        double V = 0.0;
+        const double* C = cc + 3 * c;
+        for (int s = 0; s < 6; ++s) {
+            const int32_t* fnd = M->face_nodes + 4 * (int64_t)M->cell_faces[6 * c + s];
+            const double* P0 = xyz + 3 * (int64_t)fnd[0];
+            const double* P1 = xyz + 3 * (int64_t)fnd[1];
+            const double* P2 = xyz + 3 * (int64_t)fnd[2];
+            const double* P3 = xyz + 3 * (int64_t)fnd[3];
+            V += tet_vol(C, P0, P1, P2);
+            V += tet_vol(C, P0, P3, P2);
+        }
+        vol[c] = V;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Spherical <-> Cartesian vector helpers, TITAN/source/Help_funk.cpp:75-135.
+// ---------------------------------------------------------------------------
+static double o_polar_angle(double x, double y) {
+    if (std::fabs(x) + std::fabs(y) < 0.000001) return 0.0;
+    if (x < 0) return std::atan(y / x) + 1.0 * kPi;
+    if (x > 0 && y >= 0) return std::atan(y / x);
+    if (x > 0 && y < 0) return std::atan(y / x) + 2.0 * kPi;
+    if (y > 0 && x >= 0 && x <= 0) return kPi / 2.0;
+    if (y < 0 && x >= 0 && x <= 0) return 3.0 * kPi / 2.0;
+    return 0.0;
+}
+
+static void o_spherical(double z, double x, double y, double Vz, double Vx, double Vy, double& Vr,
+                        double& Vphi, double& Vtheta) {
+    const double r = std::sqrt(x * x + y * y + z * z);
+    const double th = std::acos(z / r);
+    const double ph = o_polar_angle(x, y);
+    Vr = Vx * std::sin(th) * std::cos(ph) + Vy * std::sin(th) * std::sin(ph) + Vz * std::cos(th);
+    Vtheta = Vx * std::cos(th) * std::cos(ph) + Vy * std::cos(th) * std::sin(ph) - Vz * std::sin(th);
+    Vphi = -Vx * std::sin(ph) + Vy * std::cos(ph);
+}
+
+static void o_cartesian(double z, double x, double y, double Vr, double Vphi, double Vtheta, double& Vz,
+                        double& Vx, double& Vy) {
+    const double r = std::sqrt(x * x + y * y + z * z);
+    const double th = std::acos(z / r);
+    const double ph = o_polar_angle(x, y);
+    Vx = Vr * std::sin(th) * std::cos(ph) + Vtheta * std::cos(th) * std::cos(ph) - Vphi * std::sin(ph);
+    Vy = Vr * std::sin(th) * std::sin(ph) + Vtheta * std::cos(th) * std::sin(ph) + Vphi * std::cos(ph);
+    Vz = Vr * std::cos(th) - Vtheta * std::sin(th);
+}
+
+// First-order interior reconstruction of one side, Setka_gran_snos.cpp:737-907
+// (cells[0]) and :909-1069 (cells[1]): Zone_1 cells are scaled radially from
+// the cell centre to the face centre; other cells are copied.
+static void o_snos_side(const double* st, int64_t nc, int64_t c, int ctype, const double* cc, const double* G,
+                        double gamma, double* out) {
+    for (int k = 0; k < NV; ++k) out[k] = st[k * nc + c];
+    if (ctype != 1) return;
+    const double* Ac = cc + 3 * c;
+    const double r1 = std::sqrt(Ac[0] * Ac[0] + Ac[1] * Ac[1] + Ac[2] * Ac[2]);
+    const double rr = std::sqrt(G[0] * G[0] + G[1] * G[1] + G[2] * G[2]);
+    const double the1 = std::acos(G[2] / rr);
+    for (int ik = 0; ik < 2; ++ik) {  // ik 0: velocity, 1: magnetic field
+        const int i1 = ik == 0 ? 1 : 5;
+        const double AX = st[(i1 + 0) * nc + c], AY = st[(i1 + 1) * nc + c], AZ = st[(i1 + 2) * nc + c];
+        double VA0, VA1, VA2;
+        if (the1 > kPi / 9 && the1 < 8 * kPi / 9) {
+            o_spherical(Ac[2], Ac[0], Ac[1], AZ, AX, AY, VA0, VA1, VA2);
+            if (ik == 1) {
+                VA0 = VA0 * (sq(r1 / rr));
+                VA1 = VA1 * ((r1) / (rr));
+                VA2 = VA2 * ((r1) / (rr));
+            }
+            o_cartesian(G[2], G[0], G[1], VA0, VA1, VA2, out[i1 + 2], out[i1 + 0], out[i1 + 1]);
+        } else {
+            o_spherical(Ac[0], Ac[1], Ac[2], AX, AY, AZ, VA0, VA1, VA2);
+            if (ik == 1) {
+                VA0 = VA0 * (sq(r1 / rr));
+                VA1 = VA1 * ((r1) / (rr));
+                VA2 = VA2 * ((r1) / (rr));
+            }
+            o_cartesian(G[0], G[1], G[2], VA0, VA1, VA2, out[i1 + 0], out[i1 + 1], out[i1 + 2]);
+        }
+    }
+    out[0] = st[0 * nc + c] * sq(r1) / sq(rr);
+    out[8] = st[8 * nc + c] * sq(r1) / sq(rr);
+    out[9] = st[9 * nc + c] * sq(r1) / sq(rr);
+    out[4] = st[4 * nc + c] * std::pow(r1, 2.0 * gamma) / std::pow(rr, 2.0 * gamma);
+}
+
+// Per-face flux, restating Setka::Culc_Gran_Potok (Setka_physics.cpp:2280-2571)
+// for the plasma: reconstruction, solver choice, chlld, local dt, flux*area,
+// Powell PdivB. Writes 11 values per face: rho, Vx, Vy, Vz, p(energy), Bx,
+// By, Bz, divB, Q, rho_He (all times area); returns the dt candidate.
+static double o_face(const OMesh* M, const OParams* P, const double* st, const double* cc, const double* fc,
+                     const double* fn, const double* fa, const double* xyz1, const double* xyz2,
+                     int64_t f, double time, double* out, int* err) {
+    const int64_t nc = M->ncell;
+    const double area = fa[f];
+    const double* n = fn + 3 * f;
+    double w = 0.0;
+    if (P->move) {  // Gran::culc_velosity, Gran.cpp:571-589
+        double ddot = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            const int64_t nd = M->face_nodes[4 * f + k];
+            double dx[3];
+            for (int j = 0; j < 3; ++j) dx[j] = xyz2[3 * nd + j] - xyz1[3 * nd + j];
+            ddot = ddot + (dx[0] * n[0] + dx[1] * n[1] + dx[2] * n[2]);
+        }
+        w = ddot / 4.0 / time;
+    }
+    double loc_time = 10000000.0;
+    const int type = M->face_type[f];
+    const int64_t A = M->face_cells[2 * f];
+    const int64_t B = M->face_cells[2 * f + 1];
+    double dist = 0.0;
+    double L[NV], R[NV];
+    if (type == 0) {
+        const double dx = cc[3 * A] - cc[3 * B], dy = cc[3 * A + 1] - cc[3 * B + 1], dz = cc[3 * A + 2] - cc[3 * B + 2];
+        dist = std::sqrt(dx * dx + dy * dy + dz * dz) / 2.0;
+        o_snos_side(st, nc, A, M->cell_type[A], cc, fc + 3 * f, P->gamma, L);
+        o_snos_side(st, nc, B, M->cell_type[B], cc, fc + 3 * f, P->gamma, R);
+    } else {
+        // boundary faces, Setka_gran_snos.cpp:7-65; plasma_condition (Phys_param.cpp:203-206):
+        // Inner_Hard 2, Outer_Hard 2, Outer_Soft 1
+        for (int k = 0; k < NV; ++k) L[k] = st[k * nc + A];
+        if (type == 3) {
+            if (P->soft_fixups) {
+                if (n[0] < -0.95) {
+                    if (L[1] > P->velosity_inf / 7.0) L[1] = P->velosity_inf / 5.0;
+                } else {
+                    if (L[1] * n[0] + L[2] * n[1] + L[3] * n[2] < 0.0) {
+                        L[1] = 0.1 * n[0];
+                        L[2] = 0.1 * n[1];
+                        L[3] = 0.1 * n[2];
+                    }
+                }
+            }
+            for (int k = 0; k < NV; ++k) R[k] = L[k];
+        } else {
+            const int32_t row = M->face_bc[f];
+            if (row < 0) {
+                *err = 5;
+                return loc_time;
+            }
+            for (int k = 0; k < NV; ++k) R[k] = M->bc_vals[(int64_t)NV * row + k];
+        }
+    }
+    int method;
+    if (P->method_policy == 1) {
+        const double bb = ((L[5] * L[5] + L[6] * L[6] + L[7] * L[7]) + (R[5] * R[5] + R[6] * R[6] + R[7] * R[7])) / 2.0;
+        const double pp = (L[4] + R[4]) / 2.0;
+        method = (bb / kCpi4 / (2.0 * pp) > P->beta_switch) ? 3 : 2;
+    } else {
+        method = M->face_method[f];
+    }
+    const int surf = M->face_surf[f];
+    const int left_ydar = (surf == 1 && P->TS_hard) ? 1 : 0;
+    const int contact = (surf == 2 && P->contact_hard) ? 1 : 0;
+    const int nk = P->npassive;
+    double q[8], kq[2] = {0.0, 0.0}, ds[3];
+    const int rc = o_chlld(method, n, w, L, R, 0, 0, nk, L + 8, R + 8, q, kq, ds, left_ydar, contact, P->gamma);
+    if (rc) *err = 10 + rc;
+    if (type == 0) {
+        const double dnt = P->KFL * dist / (mx(std::fabs(ds[0]), std::fabs(ds[2])) + std::fabs(w));
+        if (dnt < loc_time) loc_time = mn(loc_time, dnt);
+    }
+    for (int k = 0; k < 8; ++k) out[k] = q[k] * area;
+    out[8] = 0.5 * (n[0] * (L[5] + R[5]) + n[1] * (L[6] + R[6]) + n[2] * (L[7] + R[7])) * area;
+    out[9] = kq[0] * area;
+    out[10] = kq[1] * area;
+    return loc_time;
+}
+
+// Bera multi-fluid charge-exchange sources for the plasma, restating
+// Setka::Calc_sourse_MF_Bera (Setka_physics.cpp:766-1258) without pickup ions,
+// with U_bera / Um_bera / UE_bera (:746-762), determ_zone (:1427-1482) and
+// Phys_param::Plasma_components_1 (Phys_param.cpp:628-665). Returns m_x, m_y,
+// m_z, E scaled by n_H_LISM / Kn.
+static void o_bera(const OParams* P, const double* prim /*NV*/, int ctype, const double* H /*5*nh*/, double* S) {
+    const double rho = prim[0], p = prim[4], Q = prim[8], rho_He = prim[9];
+    int zone;
+    if (Q / rho < 50.0)
+        zone = (ctype == 1) ? 1 : 2;
+    else
+        zone = (ctype == 4) ? 4 : 3;
+    const int zone_ = zone - 1;  // Calc_sourse_MF_Bera passes zone - 1
+    const int al = (zone_ <= 2) ? 2 : 1;
+    double rho_p = -(kMeDmp * al * rho_He + 4.0 * (-rho + rho_He)) / (4.0 * (1.0 + kMeDmp));
+    double T_p = 8.0 * (1.0 + kMeDmp) * p / (8.0 * rho - (7.0 - al + (-1.0 + al) * kMeDmp) * rho_He);
+    if (rho_p <= 1e-8) rho_p = 1e-8;
+    if (T_p <= 1e-8) T_p = 1e-8;
+    if (T_p > 1e5) T_p = 1e5;
+    const double Vp[3] = {prim[1], prim[2], prim[3]};
+    double mxs = 0.0, mys = 0.0, mzs = 0.0, Es = 0.0;
+    for (int h = 0; h < P->nh; ++h) {
+        const double rho_h = H[5 * h + 0];
+        const double Vh[3] = {H[5 * h + 1], H[5 * h + 2], H[5 * h + 3]};
+        const double T_h = 2.0 * H[5 * h + 4] / mx(rho_h, 1e-9);
+        const double d[3] = {Vp[0] - Vh[0], Vp[1] - Vh[1], Vp[2] - Vh[2]};
+        const double uu = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        // (V2 - V1) has the same norm bitwise, so U is symmetric
+        const double U_ph = std::sqrt((4.0 / kPi) * (T_p + T_h) + sq(uu));
+        const double U_hp = std::sqrt((4.0 / kPi) * (T_h + T_p) + sq(uu));
+        const double Um_ph = std::sqrt((16.0 / kPi) * T_p + (9.0 * kPi / 4.0) * T_h + 4.0 * sq(uu));
+        const double Um_hp = std::sqrt((16.0 / kPi) * T_h + (9.0 * kPi / 4.0) * T_p + 4.0 * sq(uu));
+        const double UE_ph = std::sqrt((4.0 / kPi) * T_p + (64.0 / 9.0 / kPi) * T_h + sq(uu));
+        const double UE_hp = std::sqrt((4.0 / kPi) * T_h + (64.0 / 9.0 / kPi) * T_p + sq(uu));
+        const double sig_ph = sq(1.0 - P->par_a_2 * std::log(U_ph));
+        const double sig_hp = sq(1.0 - P->par_a_2 * std::log(U_hp));
+        const double k_hp = sig_hp * rho_p * rho_h;
+        const double k_ph = sig_ph * rho_p * rho_h;
+        double Hm_hp[3], Hm_ph[3];
+        for (int j = 0; j < 3; ++j) {
+            Hm_hp[j] = k_hp * (U_hp * Vp[j] + T_p / Um_hp * (Vp[j] - Vh[j]));
+            Hm_ph[j] = k_ph * (U_ph * Vh[j] - T_h / Um_ph * (Vp[j] - Vh[j]));
+        }
+        const double vp2 = Vp[0] * Vp[0] + Vp[1] * Vp[1] + Vp[2] * Vp[2];
+        const double vh2 = Vh[0] * Vh[0] + Vh[1] * Vh[1] + Vh[2] * Vh[2];
+        const double vpd = Vp[0] * d[0] + Vp[1] * d[1] + Vp[2] * d[2];
+        const double vhd = Vh[0] * d[0] + Vh[1] * d[1] + Vh[2] * d[2];
+        const double HE_hp = k_hp * (0.5 * U_hp * vp2 + T_p / Um_hp * vpd + 3.0 / 4.0 * T_p * UE_hp);
+        const double HE_ph = k_ph * (0.5 * U_ph * vh2 - T_h / Um_ph * vhd + 3.0 / 4.0 * T_h * UE_ph);
+        mxs += (-Hm_hp[0] + Hm_ph[0]);
+        mys += (-Hm_hp[1] + Hm_ph[1]);
+        mzs += (-Hm_hp[2] + Hm_ph[2]);
+        Es += (-HE_hp + HE_ph);
+    }
+    const double ddp = (P->par_n_H_LISM / P->par_Kn);
+    S[0] = mxs * ddp;
+    S[1] = mys * ddp;
+    S[2] = mzs * ddp;
+    S[3] = Es * ddp;
+}
+
+// Conservative update of one cell, restating Setka_physics.cpp:1671-2028
+// (plasma): flux gather in the cell's face order with sign by cells[0],
+// Powell terms, ALE volume ratio, sources, Zone_2 dissipation, floors.
+static void o_cell(const OMesh* M, const OParams* P, const double* st, double* st2, const double* H,
+                   const double* S_ext, const double* fl, const double* vol1, const double* vol2, int64_t c,
+                   double time, int* err, int64_t* nrf, int64_t* npf) {
+    const int64_t nc = M->ncell;
+    const double Volume = vol1[c];
+    const double Volume2 = vol2[c];
+    double PO[11];
+    for (int k = 0; k < 11; ++k) PO[k] = 0.0;
+    for (int s = 0; s < 6; ++s) {
+        const int64_t f = M->cell_faces[6 * c + s];
+        const double sign = (M->face_cells[2 * f] != c) ? -1.0 : 1.0;
+        for (int k = 0; k < 11; ++k) PO[k] += sign * fl[11 * f + k];
+    }
+    double prim[NV];
+    for (int k = 0; k < NV; ++k) prim[k] = st[k * nc + c];
+    double S[4] = {0.0, 0.0, 0.0, 0.0};
+    if (S_ext) {
+        for (int k = 0; k < 4; ++k) S[k] = S_ext[4 * c + k];
+    } else if (P->nh > 0) {
+        double Hc[20];
+        for (int k = 0; k < 5 * P->nh; ++k) Hc[k] = H[(int64_t)k * nc + c];
+        o_bera(P, prim, M->cell_type[c], Hc, S);
+    }
+    const double g1 = P->gamma - 1.0;
+    const double rho = prim[0], vx = prim[1], vy = prim[2], vz = prim[3], p = prim[4];
+    const double bx = prim[5], by = prim[6], bz = prim[7], Q = prim[8], rho_He = prim[9];
+    const double dsk = vx * bx + vy * by + vz * bz;
+    double rho3 = rho * Volume / Volume2 - time * PO[0] / Volume2;
+    bool rho_null = false;
+    double Q3 = 0.0, rho_He3 = 0.0;
+    if (rho3 < 1e-7) {
+        rho_null = true;
+        rho3 = 0.1;
+        Q3 = Q / rho * rho3;
+        rho_He3 = 0.0;
+        (*nrf)++;
+    }
+    if (P->npassive) {
+        Q3 = Q * Volume / Volume2 - time * PO[9] / Volume2;
+        rho_He3 = rho_He * Volume / Volume2 - time * PO[10] / Volume2;
+    } else {
+        Q3 = 0.0;
+        rho_He3 = 0.0;
+    }
+    if (rho_He3 < 0.0) rho_He3 = 0.0;
+    double u3, v3, w3, bx3, by3, bz3, p3;
+    if (!rho_null) {
+        u3 = (rho * vx * Volume / Volume2 - time * (PO[1] + (bx / kCpi4) * PO[8]) / Volume2 + time * S[0]) / rho3;
+        v3 = (rho * vy * Volume / Volume2 - time * (PO[2] + (by / kCpi4) * PO[8]) / Volume2 + time * S[1]) / rho3;
+        w3 = (rho * vz * Volume / Volume2 - time * (PO[3] + (bz / kCpi4) * PO[8]) / Volume2 + time * S[2]) / rho3;
+        bx3 = bx * Volume / Volume2 - time * (PO[5] + vx * PO[8]) / Volume2;
+        by3 = by * Volume / Volume2 - time * (PO[6] + vy * PO[8]) / Volume2;
+        bz3 = bz * Volume / Volume2 - time * (PO[7] + vz * PO[8]) / Volume2;
+        p3 = (((p / g1 + 0.5 * rho * (vx * vx + vy * vy + vz * vz) + (bx * bx + by * by + bz * bz) / kC8Pi) * Volume /
+                   Volume2 -
+               time * (PO[4] + (dsk / kCpi4) * PO[8]) / Volume2 + time * S[3]) -
+              0.5 * rho3 * (u3 * u3 + v3 * v3 + w3 * w3) - (bx3 * bx3 + by3 * by3 + bz3 * bz3) / kC8Pi) *
+             g1;
+        if (M->cell_type[c] == 2) {  // Zone_2 effective magnetic dissipation, :1932-1947
+            const double tau = 1.0;
+            const double bx4 = bx3 - time * bx3 / tau;
+            const double by4 = by3 - time * by3 / tau;
+            const double bz4 = bz3 - time * bz3 / tau;
+            const double p4 =
+                p3 + (time / tau - sq(time / tau)) * (g1) * (bx3 * bx3 + by3 * by3 + bz3 * bz3) / (4.0 * kPi);
+            bx3 = bx4;
+            by3 = by4;
+            bz3 = bz4;
+            p3 = p4;
+        }
+    } else {
+        u3 = vx;
+        v3 = vy;
+        w3 = vz;
+        bx3 = bx;
+        by3 = by;
+        bz3 = bz;
+        p3 = rho3 / 2.0;
+    }
+    if (std::isnan(rho3) || std::fpclassify(rho3) == FP_SUBNORMAL || std::isnan(Q3) ||
+        std::fpclassify(Q3) == FP_SUBNORMAL)
+        *err = 20;
+    if (p3 < 0.00000001) {
+        p3 = 0.000001;
+        (*npf)++;
+    }
+    if (rho_He3 > rho3) rho_He3 = rho3 * 0.1;
+    st2[0 * nc + c] = rho3;
+    st2[1 * nc + c] = u3;
+    st2[2 * nc + c] = v3;
+    st2[3 * nc + c] = w3;
+    st2[4 * nc + c] = p3;
+    if (M->cell_tvd[c]) {
+        st2[5 * nc + c] = bx3;
+        st2[6 * nc + c] = by3;
+        st2[7 * nc + c] = bz3;
+    } else {
+        st2[5 * nc + c] = bx;
+        st2[6 * nc + c] = by;
+        st2[7 * nc + c] = bz;
+    }
+    st2[8 * nc + c] = Q3;
+    st2[9 * nc + c] = rho_He3;
+}
+
+// Prescribed radial node motion (the synthetic ALE mesh motion):
+// x' = x + dt * amp_i * sin(omega * t + phase_i) * x / |x|.
+void oracle_move_nodes(const OMesh* M, const OParams* P, const double* xyz1, double* xyz2, double t,
+                       double time) {
+    const int64_t nn = M->nnode;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nn; ++i) {
+        const double x = xyz1[3 * i], y = xyz1[3 * i + 1], z = xyz1[3 * i + 2];
+        const double amp = M->node_amp ? M->node_amp[i] : 0.0;
+        if (amp == 0.0) {
+            xyz2[3 * i] = x;
+            xyz2[3 * i + 1] = y;
+            xyz2[3 * i + 2] = z;
+            continue;
+        }
+        const double r = std::sqrt(x * x + y * y + z * z);
+        const double v = amp * std::sin(P->omega * t + M->node_phase[i]);
+        const double s = time * v / r;
+        xyz2[3 * i] = x + s * x;
+        xyz2[3 * i + 1] = y + s * y;
+        xyz2[3 * i + 2] = z + s * z;
+    }
+}
+
+// Flux of every face at layer `xyz1` (and node displacement to `xyz2` when
+// moving). fl: 11*nface. Returns the dt candidate (min over Us faces).
+double oracle_face_fluxes(const OMesh* M, const OParams* P, const double* st, const double* xyz1,
+                          const double* xyz2, double time, double* fl, int* err_out) {
+    const int64_t nc = M->ncell, nf = M->nface;
+    std::vector<double> cc(3 * nc), vol(nc), fc(3 * nf), fn(3 * nf), fa(nf);
+    oracle_geometry(M, xyz1, cc.data(), vol.data(), fc.data(), fn.data(), fa.data());
+    double loc = 100000000.0;
+    int err = 0;
+#pragma omp parallel for schedule(static) reduction(min : loc)
+    for (int64_t f = 0; f < nf; ++f) {
+        int e = 0;
+        const double d = o_face(M, P, st, cc.data(), fc.data(), fn.data(), fa.data(), xyz1, xyz2, f, time,
+                                fl + 11 * f, &e);
+        if (d < loc) loc = d;
+        if (e) {
+#pragma omp critical
+            if (!err) err = e;
+        }
+    }
+    *err_out = err;
+    return loc;
+}
+
+// Bera sources for every cell (m_x, m_y, m_z, E): S[4*ncell].
+void oracle_sources(const OMesh* M, const OParams* P, const double* st, const double* H, double* S) {
+    const int64_t nc = M->ncell;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < nc; ++c) {
+        double prim[NV], Hc[20];
+        for (int k = 0; k < NV; ++k) prim[k] = st[k * nc + c];
+        for (int k = 0; k < 5 * P->nh; ++k) Hc[k] = H[(int64_t)k * nc + c];
+        o_bera(P, prim, M->cell_type[c], Hc, S + 4 * c);
+    }
+}
+
+// `nsteps` steps of Setka::Go's plasma loop (Setka_physics.cpp:1589-2028).
+//   state  [NV*ncell]   in/out (primitive variables)
+//   xyz    [3*nnode]    in/out node coordinates (moved when P->move)
+//   H      [5*nh*ncell] frozen neutral fluids (may be null when nh == 0)
+//   S_ext  [4*ncell]    external sources (overrides Bera when non-null)
+//   clock  [2]          in/out: {dt of the next step, physical time t}
+// The first step of a run uses the dt the caller passes (the reference starts
+// with 1e-5, :1582-1583); each step's CFL minimum is applied on the next step.
+int oracle_go(const OMesh* M, const OParams* P, double* state, double* xyz, const double* H, const double* S_ext,
+              int64_t nsteps, double* clock, OStepInfo* info) {
+    const int64_t nc = M->ncell, nf = M->nface, nn = M->nnode;
+    std::vector<double> st2(NV * nc), xyz2(3 * nn), fl(11 * nf);
+    std::vector<double> cc1(3 * nc), vol1(nc), fc1(3 * nf), fn1(3 * nf), fa1(nf);
+    std::vector<double> cc2(3 * nc), vol2(nc), fc2(3 * nf), fn2(3 * nf), fa2(nf);
+    double time = clock[0], tphys = clock[1];
+    info->err_code = 0;
+    info->n_rho_floor = 0;
+    info->n_p_floor = 0;
+    oracle_geometry(M, xyz, cc1.data(), vol1.data(), fc1.data(), fn1.data(), fa1.data());
+    for (int64_t step = 0; step < nsteps; ++step) {
+        const double* X2 = xyz;
+        const double* V2 = vol1.data();
+        if (P->move) {
+            oracle_move_nodes(M, P, xyz, xyz2.data(), tphys, time);
+            oracle_geometry(M, xyz2.data(), cc2.data(), vol2.data(), fc2.data(), fn2.data(), fa2.data());
+            X2 = xyz2.data();
+            V2 = vol2.data();
+        }
+        double loc = 100000000.0;
+        int err = 0;
+#pragma omp parallel for schedule(static) reduction(min : loc)
+        for (int64_t f = 0; f < nf; ++f) {
+            int e = 0;
+            const double d = o_face(M, P, state, cc1.data(), fc1.data(), fn1.data(), fa1.data(), xyz, X2, f, time,
+                                    fl.data() + 11 * f, &e);
+            if (d < loc) loc = d;
+            if (e) {
+#pragma omp critical
+                if (!err) {
+                    err = e;
+                    info->err_index = f;
+                }
+            }
+        }
+        int64_t nrf = 0, npf = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nrf, npf)
+        for (int64_t c = 0; c < nc; ++c) {
+            int e = 0;
+            o_cell(M, P, state, st2.data(), H, S_ext, fl.data(), vol1.data(), V2, c, time, &e, &nrf, &npf);
+            if (e) {
+#pragma omp critical
+                if (!err) {
+                    err = e;
+                    info->err_index = c;
+                }
+            }
+        }
+        info->n_rho_floor += nrf;
+        info->n_p_floor += npf;
+        std::memcpy(state, st2.data(), sizeof(double) * NV * nc);
+        if (P->move) {
+            std::memcpy(xyz, xyz2.data(), sizeof(double) * 3 * nn);
+            cc1.swap(cc2);
+            vol1.swap(vol2);
+            fc1.swap(fc2);
+            fn1.swap(fn2);
+            fa1.swap(fa2);
+        }
+        tphys += time;
+        time = loc;
+        info->steps_done = step + 1;
+        if (err) {
+            info->err_code = err;
+            break;
+        }
+    }
+    clock[0] = time;
+    clock[1] = tphys;
+    return (int)info->err_code;
+}
+
+int oracle_chlld(int n_state, const double* nrm, double w, const double* q1, const double* q2, int null_bn,
+                 int n_disc, int nk, const double* kl, const double* kr, double* qout, double* kout, double* ds,
+                 int left_ydar, int contact, double gamma) {
+    return o_chlld(n_state, nrm, w, q1, q2, null_bn, n_disc, nk, kl, kr, qout, kout, ds, left_ydar, contact,
+                   gamma);
+}
+
+void oracle_chlld_batch(int64_t n, const int* n_state, const double* nrm, const double* w, const double* q1,
+                        const double* q2, double* qout, double* ds, double gamma, int* rc) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        double dummy = 0.0;
+        rc[i] = o_chlld(n_state[i], nrm + 3 * i, w[i], q1 + 8 * i, q2 + 8 * i, 0, 0, 0, &dummy, &dummy,
+                        qout + 8 * i, &dummy, ds + 3 * i, 0, 0, gamma);
+    }
+}
+
+int oracle_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,170 @@
+"""ctypes bindings for the oracle (test infrastructure only).
+
+* ``oracle/liboracle.so``         — the CPU restatement of the plasma step
+  (oracle/titan_oracle.cpp), built by ``make -C oracle``.
+* ``oracle/_ref/libtitan_ref.so`` — the reference's own Riemann solver
+  (TITAN/source/Phys_param.cpp compiled unmodified), built by
+  ``make -C oracle ref`` where the reference tree is present.
+
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+import this module; the shipped library never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+REF_SO = os.path.join(ORACLE_DIR, "_ref", "libtitan_ref.so")
+REF_RUN = os.path.join(ORACLE_DIR, "_ref", "run")
+
+D = ctypes.POINTER(ctypes.c_double)
+I32 = ctypes.POINTER(ctypes.c_int32)
+I8 = ctypes.POINTER(ctypes.c_int8)
+U8 = ctypes.POINTER(ctypes.c_uint8)
+
+NV = 10
+
+
+def _p(a, t=D):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+class OMesh(ctypes.Structure):
+    _fields_ = [
+        ("nnode", ctypes.c_int64), ("ncell", ctypes.c_int64), ("nface", ctypes.c_int64),
+        ("cell_nodes", I32), ("cell_faces", I32), ("cell_type", I8), ("cell_tvd", U8),
+        ("face_nodes", I32), ("face_cells", I32), ("face_type", I8), ("face_surf", I8),
+        ("face_method", I8), ("face_bc", I32), ("bc_vals", D), ("node_amp", D), ("node_phase", D),
+    ]
+
+
+class OParams(ctypes.Structure):
+    _fields_ = [
+        ("gamma", ctypes.c_double), ("KFL", ctypes.c_double), ("velosity_inf", ctypes.c_double),
+        ("omega", ctypes.c_double), ("par_a_2", ctypes.c_double), ("par_n_H_LISM", ctypes.c_double),
+        ("par_Kn", ctypes.c_double), ("beta_switch", ctypes.c_double),
+        ("move", ctypes.c_int32), ("soft_fixups", ctypes.c_int32), ("method_policy", ctypes.c_int32),
+        ("npassive", ctypes.c_int32), ("nh", ctypes.c_int32), ("TS_hard", ctypes.c_int32),
+        ("contact_hard", ctypes.c_int32), ("pad", ctypes.c_int32),
+    ]
+
+
+class OStepInfo(ctypes.Structure):
+    _fields_ = [("steps_done", ctypes.c_int64), ("err_code", ctypes.c_int64), ("err_index", ctypes.c_int64),
+                ("n_rho_floor", ctypes.c_int64), ("n_p_floor", ctypes.c_int64)]
+
+
+_oracle = None
+_ref = None
+
+
+def build_oracle(ref: bool = False) -> None:
+    """Build the oracle (and, when asked and the reference tree exists, the reference solver)."""
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR, "all"], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "ref"], check=True)
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        lib = ctypes.CDLL(ORACLE_SO)
+        lib.oracle_chlld.argtypes = [ctypes.c_int, D, ctypes.c_double, D, D, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, D, D, D, D, D, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        lib.oracle_chlld.restype = ctypes.c_int
+        lib.oracle_chlld_batch.argtypes = [ctypes.c_int64, I32, D, D, D, D, D, D, ctypes.c_double, I32]
+        lib.oracle_geometry.argtypes = [ctypes.POINTER(OMesh), D, D, D, D, D, D]
+        lib.oracle_go.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D, D, D,
+                                  ctypes.c_int64, D, ctypes.POINTER(OStepInfo)]
+        lib.oracle_go.restype = ctypes.c_int
+        lib.oracle_face_fluxes.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D, D,
+                                           ctypes.c_double, D, ctypes.POINTER(ctypes.c_int)]
+        lib.oracle_face_fluxes.restype = ctypes.c_double
+        lib.oracle_sources.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D, D]
+        lib.oracle_move_nodes.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D,
+                                          ctypes.c_double, ctypes.c_double]
+        lib.oracle_num_threads.restype = ctypes.c_int
+        _oracle = lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    """The reference's compiled Phys_param (raises if it was not built)."""
+    global _ref
+    if _ref is None:
+        lib = ctypes.CDLL(REF_SO)
+        lib.titan_ref_init.argtypes = [ctypes.c_char_p]
+        lib.titan_ref_init.restype = ctypes.c_int
+        rc = lib.titan_ref_init(REF_RUN.encode())
+        if rc != 0:
+            raise RuntimeError(f"titan_ref_init failed: {rc}")
+        lib.titan_ref_chlld.argtypes = [ctypes.c_int, D, ctypes.c_double, D, D, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, D, D, D, D, D, ctypes.c_int, ctypes.c_int]
+        lib.titan_ref_set_gamma.argtypes = [ctypes.c_double]
+        lib.titan_ref_plasma_components_1.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                      ctypes.c_double, D]
+        _ref = lib
+    return _ref
+
+
+def chlld(lib_kind: str, n_state, nrm, w, q1, q2, *, null_bn=0, n_disc=0, kl=(), kr=(), left_ydar=0,
+          contact=0, gamma=5.0 / 3.0):
+    """One Riemann-solver call through the oracle ('oracle') or the reference ('ref').
+
+    Returns (flux[8], konvect[nk], ds[3] = (dsl, dsc, dsr), rc)."""
+    nrm = np.ascontiguousarray(nrm, dtype=np.float64)
+    q1 = np.ascontiguousarray(q1, dtype=np.float64)
+    q2 = np.ascontiguousarray(q2, dtype=np.float64)
+    nk = len(kl)
+    kla = np.ascontiguousarray(kl if nk else [0.0], dtype=np.float64)
+    kra = np.ascontiguousarray(kr if nk else [0.0], dtype=np.float64)
+    out = np.zeros(8)
+    kout = np.zeros(max(nk, 1))
+    ds = np.zeros(3)
+    if lib_kind == "ref":
+        r = ref()
+        r.titan_ref_set_gamma(gamma)
+        r.titan_ref_chlld(int(n_state), _p(nrm), float(w), _p(q1), _p(q2), int(null_bn), int(n_disc), nk,
+                          _p(kla), _p(kra), _p(out), _p(kout), _p(ds), int(left_ydar), int(contact))
+        rc = 0
+    else:
+        rc = oracle().oracle_chlld(int(n_state), _p(nrm), float(w), _p(q1), _p(q2), int(null_bn), int(n_disc),
+                                   nk, _p(kla), _p(kra), _p(out), _p(kout), _p(ds), int(left_ydar),
+                                   int(contact), float(gamma))
+    return out, kout[:nk], ds, rc
+
+
+def random_riemann_cases(n: int, seed: int, *, weak_bn_frac=0.15, x_normal_frac=0.15):
+    """Seeded random face problems covering every HLLD zone and both get_bazis branches."""
+    rng = np.random.default_rng(seed)
+    q1 = np.empty((n, 8))
+    q2 = np.empty((n, 8))
+    for q in (q1, q2):
+        q[:, 0] = np.exp(rng.normal(0.0, 1.0, n))
+        q[:, 1:4] = rng.normal(0.0, 1.0, (n, 3))
+        q[:, 4] = np.exp(rng.normal(0.0, 1.0, n))
+        q[:, 5:8] = rng.normal(0.0, 2.0, (n, 3))
+    nrm = rng.normal(size=(n, 3))
+    k = int(n * x_normal_frac)
+    nrm[:k] = np.array([1.0, 0.0, 0.0]) + 0.05 * rng.normal(size=(k, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    # make some faces carry (almost) no normal field: |B_n| below epsb
+    kb = int(n * weak_bn_frac)
+    for q in (q1, q2):
+        bn = np.sum(q[k:k + kb, 5:8] * nrm[k:k + kb], axis=1, keepdims=True)
+        q[k:k + kb, 5:8] -= bn * nrm[k:k + kb]
+    w = rng.normal(0.0, 1.5, n)
+    w[rng.random(n) < 0.3] = 0.0
+    return nrm, w, q1, q2

@@ -1,0 +1,186 @@
+/*
+ * titan_b200.h — C ABI of the B200 (sm_100a) plasma time step of TITAN.
+ *
+ * Drop-in replacement for the two OpenMP loops of
+ *   void Setka::Go(bool is_inner_area, size_t steps, short metod)
+ *        (TITAN/source/Setka.h:221, body TITAN/source/Setka_physics.cpp:1484-2278)
+ * i.e. the per-face flux loop
+ *   double Setka::Culc_Gran_Potok(Gran*, unsigned short now, short metod, string&, const double& time)
+ *        (TITAN/source/Setka.h:223, TITAN/source/Setka_physics.cpp:2280-2571)
+ * with its reconstruction Setka::Snos_on_Gran (TITAN/source/Setka_gran_snos.cpp:3-1075)
+ * and Riemann solver Phys_param::chlld (TITAN/source/Phys_param.h:240-251,
+ * TITAN/source/Phys_param.cpp:882-1878), the per-cell conservative update with
+ * the charge-exchange sources Setka::Calc_sourse_MF_Bera
+ * (TITAN/source/Setka_physics.cpp:766-1258), the CFL reduction and the
+ * geometry refresh Setka::Calculating_measure (TITAN/source/Setka.cpp:2465-2502).
+ *
+ * Conventions (all arrays are host memory owned by the caller and copied at
+ * the call; nothing is retained after a call returns):
+ *   - indices are 0-based (the reference's `number` minus 1);
+ *   - cell state is SoA [TITAN_NV][ncell]: rho, Vx, Vy, Vz, p, Bx, By, Bz, Q,
+ *     rho_He — the names of Cell::parameters (TITAN/source/Cell.h:36), B in
+ *     Gaussian units as the reference stores it;
+ *   - every call returns a titan_status; on failure titan_last_error() gives a
+ *     message. The library never exits the process (the reference's
+ *     convention is print + exit(-1)).
+ * One host thread per context; calls on a context are synchronous.
+ */
+#ifndef TITAN_B200_H
+#define TITAN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TITAN_NV 10
+
+typedef enum titan_status {
+    TITAN_OK = 0,
+    TITAN_EINVAL = -1,      /* bad argument */
+    TITAN_EMESH = -2,       /* mesh fails a consistency check (Setka::Test_geometr rules) */
+    TITAN_ENONFINITE = -3,  /* NaN / subnormal produced (the reference's Error 9851234578) */
+    TITAN_ECUDA = -4,       /* CUDA runtime error */
+    TITAN_ETIMEOUT = -5,    /* a bounded device wait gave up */
+    TITAN_ENOMEM = -6,      /* device allocation failed */
+    TITAN_ESOLVER = -7      /* Riemann solver found no admissible wave region */
+} titan_status;
+
+/* Type_Gran (TITAN/source/Gran.h:5-10) */
+enum { TITAN_FACE_US = 0, TITAN_FACE_INNER_HARD = 1, TITAN_FACE_OUTER_HARD = 2, TITAN_FACE_OUTER_SOFT = 3 };
+/* Type_Gran_surf (TITAN/source/Gran.h:12-17) */
+enum { TITAN_SURF_US = 0, TITAN_SURF_TS = 1, TITAN_SURF_HP = 2, TITAN_SURF_BS = 3 };
+/* Type_Cell (TITAN/source/Cell.h:5-11) */
+enum { TITAN_CELL_NONE = 0, TITAN_CELL_ZONE_1 = 1, TITAN_CELL_ZONE_2 = 2, TITAN_CELL_ZONE_3 = 3, TITAN_CELL_ZONE_4 = 4 };
+/* n_state of Phys_param::chlld */
+enum { TITAN_LAX = 0, TITAN_HLL = 1, TITAN_HLLC = 2, TITAN_HLLD = 3 };
+
+/* Flattened Setka: All_Yzel / All_Cell / All_Gran (TITAN/source/Setka.h:8-322). */
+typedef struct titan_mesh {
+    int64_t nnode, ncell, nface, nbc;
+    const double*  node_xyz;    /* [nnode*3]  Yzel::coord[0] */
+    const int32_t* cell_nodes;  /* [ncell*8]  Cell::yzels */
+    const int32_t* cell_faces;  /* [ncell*6]  Cell::grans, order kept (flux gather order) */
+    const int8_t*  cell_type;   /* [ncell]    Cell::type */
+    const uint8_t* cell_tvd;    /* [ncell]    Cell::is_TVD (B frozen where 0) */
+    const int32_t* face_nodes;  /* [nface*4]  Gran::yzels, around the quad */
+    const int32_t* face_cells;  /* [nface*2]  Gran::cells; -1 when the face has one cell */
+    const int8_t*  face_type;   /* [nface]    Gran::type */
+    const int8_t*  face_surf;   /* [nface]    Gran::type2 */
+    const int32_t* face_bc;     /* [nface]    row of bc_vals for hard boundary faces, else -1 */
+    const double*  bc_vals;     /* [nbc*TITAN_NV] fixed face values (Gran::parameters) */
+    const double*  node_amp;    /* [nnode] or NULL: prescribed radial node speed amplitude */
+    const double*  node_phase;  /* [nnode] or NULL: its phase */
+} titan_mesh;
+
+/* Phys_param settings that the step reads (TITAN/source/Phys_param.h:95-160). */
+typedef struct titan_params {
+    double gamma;          /* adiabatic index (5/3) */
+    double KFL;            /* Courant number */
+    double velosity_inf;   /* Velosity_inf, used by the Outer_Soft outflow fix-up */
+    double omega;          /* angular frequency of the prescribed node motion */
+    double par_a_2;        /* charge-exchange cross-section parameter */
+    double par_n_H_LISM;   /* n_H at infinity */
+    double par_Kn;         /* Knudsen number */
+    double beta_switch;    /* method_policy 1: HLLD where B^2/(8 pi p) > beta_switch, else HLLC */
+    int32_t move;          /* move_setka: ALE step with prescribed node motion */
+    int32_t soft_fixups;   /* Outer_Soft outflow fix-ups (1, as the reference) or plain copy (0) */
+    int32_t method_policy; /* 0: per-face n_state from titan_set_face_method; 1: beta switch */
+    int32_t npassive;      /* 0, or 2 to carry Q and rho_He through the contact */
+    int32_t nh;            /* frozen neutral fluids for the Bera sources (0..4) */
+    int32_t TS_hard;       /* left_ydar on TS faces */
+    int32_t contact_hard;  /* face speed = contact speed on HP faces */
+    int32_t flux_precision;/* 64: all-FP64; 32: FP32 Riemann flux, FP64 accumulation/update/dt */
+} titan_params;
+
+typedef struct titan_step_info {
+    int64_t steps_done;      /* steps completed by this call */
+    int64_t err_index;       /* original-numbering face/cell index of the first failure, or -1 */
+    int64_t n_rho_floor;     /* cells where rho < 1e-7 was reset (Setka_physics.cpp:1784-1794) */
+    int64_t n_p_floor;       /* cells where p < 1e-8 was reset (Setka_physics.cpp:1981-2001) */
+    int32_t status;          /* titan_status of the step loop */
+    int32_t err_kind;        /* 0, 11-14 solver region/branch, 20 non-finite density */
+    double  dt_next;         /* CFL dt that the next step will use */
+    double  t;               /* accumulated physical time */
+    double  gpu_ms;          /* device time of this call's step loop (CUDA events) */
+} titan_step_info;
+
+typedef struct titan_ctx titan_ctx;
+
+const char* titan_version(void);
+/* Message of the last failing call on this thread. */
+const char* titan_last_error(void);
+
+/* Validates and uploads the mesh: space-filling-curve renumbering of cells,
+ * faces and nodes (bit-exact and invertible), device geometry of layer 0. */
+int titan_create(const titan_mesh* mesh, const titan_params* params, titan_ctx** out);
+int titan_destroy(titan_ctx* ctx);
+
+/* Per-face solver choice (Gran::Get_method, TITAN/source/Gran.cpp:3-14) as
+ * data: n_state per face in original numbering. */
+int titan_set_face_method(titan_ctx* ctx, const int8_t* n_state);
+
+/* Cell::parameters[now] for all cells, SoA [TITAN_NV][ncell], original order. */
+int titan_upload_state(titan_ctx* ctx, const double* state);
+int titan_download_state(titan_ctx* ctx, double* state);
+
+/* Frozen neutral fluids for the Bera sources: SoA [5*nh][ncell] with
+ * rho_Hk, Vx_Hk, Vy_Hk, Vz_Hk, p_Hk for k = 1..nh. */
+int titan_upload_hfluids(titan_ctx* ctx, const double* h);
+
+/* External plasma sources SoA [4][ncell] (m_x, m_y, m_z, E; the closure or a
+ * Monte-Carlo table). They replace the Bera sources; NULL switches back. */
+int titan_set_sources(titan_ctx* ctx, const double* src);
+
+/* `nsteps` steps of the plasma loop of Setka::Go. dt_inout: in, dt of the
+ * first step (the reference starts with 1e-5); out, the CFL dt of the next
+ * step. t_inout: accumulated physical time (drives the node motion). */
+int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout, titan_step_info* info);
+
+/* Node coordinates [nnode*3] and geometry of the current layer (original numbering). */
+int titan_download_nodes(titan_ctx* ctx, double* xyz);
+int titan_download_geometry(titan_ctx* ctx, double* cell_center, double* cell_volume, double* face_center,
+                            double* face_normal, double* face_area);
+
+/* Face fluxes of the last step [nface*11], original numbering: Prho, PVx, PVy,
+ * PVz, Pp (energy), PBx, PBy, PBz, PdivB, PQ, Prho_He — the Gran::parameters
+ * "P*" values of Culc_Gran_Potok (flux times area). */
+int titan_download_face_fluxes(titan_ctx* ctx, double* flux);
+
+/* The space-filling-curve renumbering titan_create applies, computed on the
+ * host alone (no device needed): new index -> original index for cells, faces
+ * and nodes. No reference counterpart: Setka::Renumerate
+ * (TITAN/source/Setka.cpp:443-465) numbers objects in construction order. */
+int titan_sfc_renumber(int64_t nnode, int64_t ncell, int64_t nface, const double* node_xyz,
+                       const int32_t* cell_nodes, const int32_t* face_cells, int32_t* cell_new2old,
+                       int32_t* face_new2old, int32_t* node_new2old);
+
+/* Permutations chosen at upload: new index -> original index. */
+int titan_get_permutation(titan_ctx* ctx, int32_t* cell_new2old, int32_t* face_new2old, int32_t* node_new2old);
+
+/* Stateless batch of Phys_param::chlld calls on the device, host buffers.
+ * q1/q2 [n*8] (rho,u,v,w,p,Bx,By,Bz), nrm [n*3], w [n], n_state [n].
+ * flags: bit0 null_bn, bit1 left_ydar, bit2 contact, bits 4-5 n_disc.
+ * precision 64 or 32. Outputs flux [n*8], ds [n*3] = (dsl, dsc, dsr), rc [n]. */
+int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, const double* w, const double* q1,
+                        const double* q2, int32_t flags, int32_t precision, double gamma, double* flux,
+                        double* ds, int32_t* rc);
+
+/* The CUDA stream of the context (cudaStream_t), for event timing by callers. */
+void* titan_stream(titan_ctx* ctx);
+
+/* Per-kernel timing: when on, titan_step records CUDA events around every
+ * kernel (no CUDA graph) and accumulates device milliseconds per kernel. */
+int titan_set_profiling(titan_ctx* ctx, int32_t on);
+/* Up to `cap` entries: names (static strings), total ms and launch counts. */
+int titan_kernel_times(titan_ctx* ctx, const char** names, double* total_ms, int64_t* launches, int32_t cap);
+
+/* Bytes of device memory the context holds. */
+int64_t titan_device_bytes(titan_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TITAN_B200_H */

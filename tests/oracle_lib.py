@@ -168,3 +168,72 @@ def random_riemann_cases(n: int, seed: int, *, weak_bn_frac=0.15, x_normal_frac=
     w = rng.normal(0.0, 1.5, n)
     w[rng.random(n) < 0.3] = 0.0
     return nrm, w, q1, q2
+
+
+class OracleRun:
+    """The oracle's step loop (oracle_go) on a mesh dict of titan_c-_b200.mesh."""
+
+    def __init__(self, mesh: dict, params: dict):
+        self._keep = {}
+
+        def keep(name, a, dt):
+            arr = None if a is None else np.ascontiguousarray(a, dtype=dt)
+            self._keep[name] = arr
+            return arr
+
+        self.xyz = np.ascontiguousarray(mesh["node_xyz"], dtype=np.float64).copy()
+        m = OMesh()
+        m.nnode, m.ncell, m.nface = self.xyz.shape[0], mesh["cell_nodes"].shape[0], mesh["face_nodes"].shape[0]
+        m.cell_nodes = _p(keep("cn", mesh["cell_nodes"], np.int32), I32)
+        m.cell_faces = _p(keep("cf", mesh["cell_faces"], np.int32), I32)
+        m.cell_type = _p(keep("ct", mesh["cell_type"], np.int8), I8)
+        m.cell_tvd = _p(keep("cv", mesh["cell_tvd"], np.uint8), U8)
+        m.face_nodes = _p(keep("fn", mesh["face_nodes"], np.int32), I32)
+        m.face_cells = _p(keep("fc", mesh["face_cells"], np.int32), I32)
+        m.face_type = _p(keep("ft", mesh["face_type"], np.int8), I8)
+        m.face_surf = _p(keep("fs", mesh["face_surf"], np.int8), I8)
+        self.face_method = keep("fm", np.full(m.nface, 0, dtype=np.int8), np.int8)
+        self.face_method[:] = np.where(mesh["face_surf"] != 0, 3, 0)   # Gran::Get_method
+        m.face_method = _p(self.face_method, I8)
+        m.face_bc = _p(keep("fb", mesh["face_bc"], np.int32), I32)
+        bc = keep("bc", mesh["bc_vals"], np.float64)
+        m.bc_vals = _p(bc) if bc.shape[0] else None
+        m.node_amp = _p(keep("amp", mesh.get("node_amp"), np.float64))
+        m.node_phase = _p(keep("ph", mesh.get("node_phase"), np.float64))
+        self.mesh = m
+        p = OParams()
+        for k, _ in OParams._fields_:
+            if k != "pad":
+                setattr(p, k, params[k])
+        self.params = p
+        self.ncell = m.ncell
+        self.clock = np.array([1e-5, 0.0])
+        self.hf = None
+        self.src = None
+
+    def set_face_method(self, ns):
+        self.face_method[:] = np.asarray(ns, dtype=np.int8)
+
+    def go(self, state: np.ndarray, steps: int) -> OStepInfo:
+        """Advances `state` ([10, C], modified in place) by `steps` steps."""
+        assert state.flags.c_contiguous and state.dtype == np.float64
+        info = OStepInfo()
+        oracle().oracle_go(ctypes.byref(self.mesh), ctypes.byref(self.params), _p(state), _p(self.xyz),
+                           _p(self.hf), _p(self.src), int(steps), _p(self.clock), ctypes.byref(info))
+        return info
+
+    def geometry(self, xyz=None):
+        xyz = self.xyz if xyz is None else np.ascontiguousarray(xyz)
+        nc, nf = self.mesh.ncell, self.mesh.nface
+        cc, vol = np.empty((nc, 3)), np.empty(nc)
+        fc, fn, fa = np.empty((nf, 3)), np.empty((nf, 3)), np.empty(nf)
+        oracle().oracle_geometry(ctypes.byref(self.mesh), _p(xyz), _p(cc), _p(vol), _p(fc), _p(fn), _p(fa))
+        return dict(cell_center=cc, cell_volume=vol, face_center=fc, face_normal=fn, face_area=fa)
+
+    def face_fluxes(self, state: np.ndarray, time: float = 1e-5):
+        """Face fluxes (11 per face) of `state` at the current nodes (stationary w)."""
+        fl = np.empty((self.mesh.nface, 11))
+        err = ctypes.c_int(0)
+        dtn = oracle().oracle_face_fluxes(ctypes.byref(self.mesh), ctypes.byref(self.params), _p(state),
+                                          _p(self.xyz), _p(self.xyz), float(time), _p(fl), ctypes.byref(err))
+        return fl, dtn, err.value

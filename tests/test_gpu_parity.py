@@ -1,0 +1,221 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the reference.
+
+FP64: bit-exact where the arithmetic is the reference's (Riemann solver,
+geometry, update); the bar written into every comparison is 1e-12 relative per
+cell per step, and the tests also report whether the match is exact.
+FP32 flux: relative L1 error against the FP64 oracle below 1e-4.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+
+
+def rel_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = np.maximum(np.abs(b), 1e-300)
+    return float(np.max(np.abs(a - b) / np.maximum(scale, 1e-12 * np.max(np.abs(b)))))
+
+
+@pytest.fixture(scope="module")
+def T(titan, built_lib):
+    return titan
+
+
+def test_riemann_batch_fp64_matches_reference_golden(T):
+    g = np.load(ol.ROOT + "/tests/golden/chlld_golden.npz")
+    flags = (g["null_bn"] | (g["left_ydar"] << 1) | (g["contact"] << 2) | (g["n_disc"] << 4)).astype(int)
+    for fl in np.unique(flags):
+        sel = flags == fl
+        flux, ds, rc = T.chlld(g["n_state"][sel], g["nrm"][sel], g["w"][sel], g["q1"][sel], g["q2"][sel],
+                               flags=int(fl), precision=64)
+        assert np.all(rc == 0)
+        np.testing.assert_array_equal(flux, g["flux"][sel])
+        np.testing.assert_array_equal(ds, g["ds"][sel])
+
+
+def test_riemann_batch_fp64_matches_oracle_random(T, oracle_lib):
+    nrm, w, q1, q2 = ol.random_riemann_cases(4096, seed=5)
+    for ns in range(4):
+        flux, ds, rc = T.chlld(ns, nrm, w, q1, q2, precision=64)
+        ref_flux = np.empty_like(flux)
+        ref_ds = np.empty_like(ds)
+        for i in range(0, 4096, 17):
+            out, _, d, _ = ol.chlld("oracle", ns, nrm[i], w[i], q1[i], q2[i])
+            ref_flux[i], ref_ds[i] = out, d
+        idx = np.arange(0, 4096, 17)
+        np.testing.assert_array_equal(flux[idx], ref_flux[idx])
+        np.testing.assert_array_equal(ds[idx], ref_ds[idx])
+
+
+def test_riemann_batch_fp32_error(T):
+    nrm, w, q1, q2 = ol.random_riemann_cases(20000, seed=6, weak_bn_frac=0.0)
+    for ns in (2, 3):
+        f64, _, rc64 = T.chlld(ns, nrm, w, q1, q2, precision=64)
+        f32, _, rc32 = T.chlld(ns, nrm, w, q1, q2, precision=32)
+        ok = (rc64 == 0) & (rc32 == 0)
+        l1 = np.abs(f32[ok] - f64[ok]).sum() / np.abs(f64[ok]).sum()
+        assert l1 < 1e-4, l1
+
+
+def _pair(T, mesh, params, method=None, hf=None):
+    gpu = T.PlasmaStep(mesh, params)
+    run = ol.OracleRun(mesh, params)
+    if method is not None:
+        gpu.set_face_method(method)
+        run.set_face_method(method)
+    if hf is not None:
+        gpu.upload_hfluids(hf)
+        run.hf = np.ascontiguousarray(hf)
+    return gpu, run
+
+
+def test_geometry_matches_oracle(T, oracle_lib):
+    m = T.mesh.shell_mesh(8, 6)
+    gpu, run = _pair(T, m, T.problems.params())
+    a, b = gpu.geometry(), run.geometry()
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    gpu.close()
+
+
+def test_state_roundtrip_is_bitexact(T):
+    m = T.mesh.shell_mesh(8, 5)
+    gpu = T.PlasmaStep(m, T.problems.params(npassive=2))
+    rng = np.random.default_rng(1)
+    st = rng.standard_normal((10, m["cell_nodes"].shape[0]))
+    gpu.upload_state(st)
+    back = gpu.download_state()
+    assert np.array_equal(back.view(np.uint64), st.view(np.uint64))
+    gpu.close()
+
+
+@pytest.mark.parametrize("steps", [1, 7])
+def test_brio_wu_cube_steps_match_oracle(T, oracle_lib, steps):
+    m, p, st, meth = T.problems.brio_wu_cube(16)
+    gpu, run = _pair(T, m, p, meth)
+    gpu.upload_state(st)
+    s_or = np.ascontiguousarray(st.copy())
+    info = gpu.go(steps)
+    oi = run.go(s_or, steps)
+    assert info["steps_done"] == steps and oi.err_code == 0
+    s_gpu = gpu.download_state()
+    e = rel_err(s_gpu[:8], s_or[:8])
+    assert e <= REL, e
+    assert gpu.dt == run.clock[0]
+    assert gpu.t == run.clock[1]
+    gpu.close()
+
+
+def test_brio_wu_face_fluxes_match_oracle(T, oracle_lib):
+    m, p, st, meth = T.problems.brio_wu_cube(10)
+    gpu, run = _pair(T, m, p, meth)
+    gpu.upload_state(st)
+    gpu.go(1)
+    fl_gpu = gpu.face_fluxes()
+    fl_or, dtn, err = run.face_fluxes(np.ascontiguousarray(st))
+    assert err == 0
+    np.testing.assert_array_equal(fl_gpu[:, :9], fl_or[:, :9])
+    assert gpu.dt == dtn
+    gpu.close()
+
+
+@pytest.mark.parametrize("features", [
+    dict(move=False, zones=False, npassive=0, nh=0),
+    dict(move=True, zones=False, npassive=0, nh=0),
+    dict(move=True, zones=True, npassive=2, nh=0),
+    dict(move=False, zones=True, npassive=2, nh=4),
+    dict(move=True, zones=True, npassive=2, nh=4),
+])
+def test_heliosphere_shell_steps_match_oracle(T, oracle_lib, features):
+    m, p, st, hf = T.problems.heliosphere_shell(nq=8, nlayer=6, **features)
+    gpu, run = _pair(T, m, p, hf=hf)
+    gpu.upload_state(st)
+    s_or = np.ascontiguousarray(st.copy())
+    gpu.go(5)
+    oi = run.go(s_or, 5)
+    assert oi.err_code == 0
+    s_gpu = gpu.download_state()
+    ns = 8 + p["npassive"]
+    e = rel_err(s_gpu[:ns], s_or[:ns])
+    assert e <= REL, e
+    np.testing.assert_array_equal(gpu.nodes(), run.xyz)
+    assert abs(gpu.dt - run.clock[0]) <= REL * run.clock[0]
+    gpu.close()
+
+
+def test_per_step_parity_over_a_run(T, oracle_lib):
+    """Re-synchronise the oracle to the GPU state every step: per-step error <= 1e-12."""
+    m, p, st, hf = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, zones=True, npassive=2)
+    gpu, run = _pair(T, m, p)
+    gpu.upload_state(st)
+    worst = 0.0
+    for k in range(20):
+        before = np.ascontiguousarray(gpu.download_state())
+        run.xyz[:] = gpu.nodes()
+        run.clock[:] = (gpu.dt, gpu.t)
+        gpu.go(1)
+        run.go(before, 1)
+        worst = max(worst, rel_err(gpu.download_state()[:10], before[:10]))
+    assert worst <= REL, worst
+    gpu.close()
+
+
+def test_fp32_flux_step_error_against_fp64_oracle(T, oracle_lib):
+    m, p, st, _ = T.problems.heliosphere_shell(nq=12, nlayer=8, move=True)
+    p32 = dict(p, flux_precision=32)
+    gpu = T.PlasmaStep(m, p32)
+    run = ol.OracleRun(m, p)
+    gpu.upload_state(st)
+    s_or = np.ascontiguousarray(st.copy())
+    gpu.go(50)
+    run.go(s_or, 50)
+    s = gpu.download_state()
+    for k, name in [(0, "rho"), (4, "p")]:
+        l1 = np.abs(s[k] - s_or[k]).sum() / np.abs(s_or[k]).sum()
+        assert l1 < 1e-4, (name, l1)
+    b32 = np.linalg.norm(s[5:8], axis=0)
+    b64 = np.linalg.norm(s_or[5:8], axis=0)
+    assert np.abs(b32 - b64).sum() / b64.sum() < 1e-4
+    gpu.close()
+
+
+def test_graph_and_eager_paths_agree(T):
+    m, p, st, meth = T.problems.brio_wu_cube(8)
+    a = T.PlasmaStep(m, p)
+    b = T.PlasmaStep(m, p)
+    for g in (a, b):
+        g.set_face_method(meth)
+        g.upload_state(st)
+    b.set_profiling(True)
+    a.go(6)
+    b.go(6)
+    assert np.array_equal(a.download_state(), b.download_state())
+    kt = b.kernel_times()
+    assert kt["face_flux_fp64"][1] == 6 and kt["cell_update"][1] == 6
+    a.close()
+    b.close()
+
+
+def test_nonfinite_input_is_reported_and_context_recovers(T):
+    """A NaN density made on the host: the step reports it, nothing faults, and
+    the same context steps normally once a good state is uploaded."""
+    m, p, st, meth = T.problems.brio_wu_cube(6)
+    g = T.PlasmaStep(m, p)
+    g.set_face_method(meth)
+    bad = st.copy()
+    bad[0, 17] = np.nan
+    g.upload_state(bad)
+    with pytest.raises(T.TitanError) as e:
+        g.go(3)
+    assert e.value.code in (-3, -7)
+    assert g.last_info["steps_done"] < 3
+    g.upload_state(st)
+    g.go(2)
+    assert np.all(np.isfinite(g.download_state()))
+    g.close()

@@ -1,0 +1,74 @@
+// FP64 translation unit: geometry, FP64 face flux, cell update, permutations.
+// Built with -fmad=false so that double-precision expressions round exactly as
+// the reference's x86-64 build (no fused multiply-add contraction).
+#include "launch.h"
+#include "step_kernels.cuh"
+
+namespace titan {
+
+cudaError_t launch_move_nodes(const MeshView& M, const Params& P, const double* xyz1, double* xyz2,
+                              const DevStatus* st, cudaStream_t s) {
+    move_nodes_kernel<<<blocks_for(M.nnode, kGeomBlock), kGeomBlock, 0, s>>>(M, P, xyz1, xyz2, st);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_geometry(const MeshView& M, const Layer& L, cudaStream_t s) {
+    cell_geometry_kernel<<<blocks_for(M.ncell, kGeomBlock), kGeomBlock, 0, s>>>(M, L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_face_geometry(const MeshView& M, const Layer& L, cudaStream_t s) {
+    face_geometry_kernel<<<blocks_for(M.nface, kGeomBlock), kGeomBlock, 0, s>>>(M, L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, cudaStream_t s) {
+    const unsigned int g = blocks_for(a.M.nface, kFaceBlock);
+    if (nk == 0 && !move) face_flux_kernel<double, double, 0, false><<<g, kFaceBlock, 0, s>>>(a);
+    else if (nk == 0 && move) face_flux_kernel<double, double, 0, true><<<g, kFaceBlock, 0, s>>>(a);
+    else if (nk == 2 && !move) face_flux_kernel<double, double, 2, false><<<g, kFaceBlock, 0, s>>>(a);
+    else if (nk == 2 && move) face_flux_kernel<double, double, 2, true><<<g, kFaceBlock, 0, s>>>(a);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+template <typename FT, int NK, bool MOVE>
+static void cell_update_src(const CellArgs& a, int src, unsigned int g, cudaStream_t s) {
+    if (src == 0) cell_update_kernel<FT, NK, MOVE, 0><<<g, kCellBlock, 0, s>>>(a);
+    else if (src == 1) cell_update_kernel<FT, NK, MOVE, 1><<<g, kCellBlock, 0, s>>>(a);
+    else cell_update_kernel<FT, NK, MOVE, 2><<<g, kCellBlock, 0, s>>>(a);
+}
+
+template <typename FT>
+static cudaError_t cell_update_ft(const CellArgs& a, int nk, bool move, int src, cudaStream_t s) {
+    const unsigned int g = blocks_for(a.M.ncell, kCellBlock);
+    if (nk == 0 && !move) cell_update_src<FT, 0, false>(a, src, g, s);
+    else if (nk == 0 && move) cell_update_src<FT, 0, true>(a, src, g, s);
+    else if (nk == 2 && !move) cell_update_src<FT, 2, false>(a, src, g, s);
+    else if (nk == 2 && move) cell_update_src<FT, 2, true>(a, src, g, s);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, cudaStream_t s) {
+    return flux_fp32 ? cell_update_ft<float>(a, nk, move, src, s) : cell_update_ft<double>(a, nk, move, src, s);
+}
+
+cudaError_t launch_gather(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s) {
+    gather_fields_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, perm, n, nfields);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s) {
+    scatter_fields_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, perm, n, nfields);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_riemann_batch_fp64(long long n, const signed char* ns, const double* nrm, const double* w,
+                                      const double* q1, const double* q2, double* flux, double* ds, int* rc,
+                                      int flags, double gamma, cudaStream_t s) {
+    riemann_batch_kernel<double><<<blocks_for(n, 128), 128, 0, s>>>(n, ns, nrm, w, q1, q2, flux, ds, rc, flags, gamma);
+    return cudaGetLastError();
+}
+
+}  // namespace titan

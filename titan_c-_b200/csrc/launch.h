@@ -1,0 +1,33 @@
+// Host-callable launchers of the step kernels (implemented in kernels_fp64.cu,
+// built with -fmad=false, and kernels_fp32.cu, built with contraction on).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "step_types.h"
+
+namespace titan {
+
+constexpr int kFaceBlock = 128;
+constexpr int kCellBlock = 256;
+constexpr int kGeomBlock = 256;
+
+cudaError_t launch_move_nodes(const MeshView& M, const Params& P, const double* xyz1, double* xyz2,
+                              const DevStatus* st, cudaStream_t s);
+cudaError_t launch_cell_geometry(const MeshView& M, const Layer& L, cudaStream_t s);
+cudaError_t launch_face_geometry(const MeshView& M, const Layer& L, cudaStream_t s);
+cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, cudaStream_t s);
+cudaError_t launch_face_flux_fp32(const FaceArgs& a, int nk, bool move, cudaStream_t s);
+// flux_fp32: the flux buffer holds floats
+cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, cudaStream_t s);
+cudaError_t launch_gather(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s);
+cudaError_t launch_scatter(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s);
+cudaError_t launch_riemann_batch_fp64(long long n, const signed char* ns, const double* nrm, const double* w,
+                                      const double* q1, const double* q2, double* flux, double* ds, int* rc,
+                                      int flags, double gamma, cudaStream_t s);
+cudaError_t launch_riemann_batch_fp32(long long n, const signed char* ns, const double* nrm, const double* w,
+                                      const double* q1, const double* q2, double* flux, double* ds, int* rc,
+                                      int flags, double gamma, cudaStream_t s);
+
+inline unsigned int blocks_for(long long n, int bs) { return (unsigned int)((n + bs - 1) / bs); }
+
+}  // namespace titan

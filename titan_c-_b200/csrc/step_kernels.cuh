@@ -1,0 +1,663 @@
+// Kernels of one explicit plasma time step on the SFC-renumbered mesh.
+//
+//   move_nodes      prescribed radial node motion (ALE), x' = x + dt*v(t)
+//   cell_geometry   cell centre (mean of 8 nodes) and volume (12 tetrahedra)
+//   face_geometry   face centre, area (2 triangles), oriented normal, half
+//                   centre distance
+//   face_flux<R>    reconstruction + Riemann flux in precision R, flux*area,
+//                   Powell PdivB, CFL candidate -> warp/block min -> atomicMin
+//   cell_update     deterministic gather of the 6 face fluxes in the cell's
+//                   own face order (no atomics), conservative update with the
+//                   ALE volume ratio, sources, Zone_2 dissipation, floors; the
+//                   last block rolls the CFL dt over to the next step
+//
+// The arithmetic restates TITAN's Setka::Go plasma loops
+// (TITAN/source/Setka_physics.cpp:1589-2028), Setka::Culc_Gran_Potok (:2280-2571),
+// Setka::Snos_on_Gran (Setka_gran_snos.cpp:3-180, :737-1071), the geometry of
+// Gran::Culc_measure / Cell::Culc_center / Cell::Culc_volume (Gran.cpp:112-218,
+// Cell.cpp:909-1007) and Gran::culc_velosity (Gran.cpp:571-589), in the same
+// expression order, so the FP64 instantiation (compiled with -fmad=false)
+// reproduces the reference's rounding.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "riemann.cuh"
+#include "step_types.h"
+
+namespace titan {
+
+__device__ __forceinline__ void record_error(DevStatus* st, int kind, int index) {
+    if (atomicCAS(&st->err_kind, 0, kind) == 0) st->err_index = index;
+}
+
+// ---------------------------------------------------------------------------
+// Node motion (ALE): the synthetic radial motion of the heliosphere shell.
+// ---------------------------------------------------------------------------
+static __global__ void move_nodes_kernel(MeshView M, Params P, const double* __restrict__ xyz1, double* __restrict__ xyz2,
+                                  const DevStatus* __restrict__ st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M.nnode) return;
+    const int nn = M.nnode;
+    const double x = xyz1[i], y = xyz1[nn + i], z = xyz1[2 * nn + i];
+    const double amp = M.node_amp ? M.node_amp[i] : 0.0;
+    if (amp == 0.0) {
+        xyz2[i] = x;
+        xyz2[nn + i] = y;
+        xyz2[2 * nn + i] = z;
+        return;
+    }
+    const double time = st->dt, t = st->t;
+    const double r = sqrt(x * x + y * y + z * z);
+    const double v = amp * sin(P.omega * t + M.node_phase[i]);
+    const double s = time * v / r;
+    xyz2[i] = x + s * x;
+    xyz2[nn + i] = y + s * y;
+    xyz2[2 * nn + i] = z + s * z;
+}
+
+__device__ __forceinline__ double tri_area(double ax, double ay, double az, double bx, double by, double bz,
+                                           double cx, double cy, double cz) {
+    const double v1x = bx - ax, v1y = by - ay, v1z = bz - az;
+    const double v2x = cx - ax, v2y = cy - ay, v2z = cz - az;
+    const double x = v1y * v2z - v1z * v2y;
+    const double y = v1z * v2x - v1x * v2z;
+    const double z = v1x * v2y - v1y * v2x;
+    return 0.5 * sqrt(x * x + y * y + z * z);
+}
+
+__device__ __forceinline__ double tet_vol(const double* a, const double* b, const double* c, const double* d) {
+    const double abx = b[0] - a[0], aby = b[1] - a[1], abz = b[2] - a[2];
+    const double acx = c[0] - a[0], acy = c[1] - a[1], acz = c[2] - a[2];
+    const double adx = d[0] - a[0], ady = d[1] - a[1], adz = d[2] - a[2];
+    const double x = aby * acz - abz * acy;
+    const double y = abz * acx - abx * acz;
+    const double z = abx * acy - aby * acx;
+    return fabs(x * adx + y * ady + z * adz) / 6.0;
+}
+
+__device__ __forceinline__ void load_node(const double* xyz, int nn, int i, double* p) {
+    p[0] = xyz[i];
+    p[1] = xyz[nn + i];
+    p[2] = xyz[2 * nn + i];
+}
+
+// Cell centre (Cell.cpp:909-930) and volume by method 1 (Cell.cpp:958-1001).
+static __global__ void cell_geometry_kernel(MeshView M, Layer L) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= M.ncell) return;
+    const int nc = M.ncell, nn = M.nnode;
+    double x = 0.0, y = 0.0, z = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int i = M.cell_nodes[k * nc + c];
+        x += L.xyz[i];
+        y += L.xyz[nn + i];
+        z += L.xyz[2 * nn + i];
+    }
+    const double C[3] = {x / 8, y / 8, z / 8};
+    L.cc[c] = C[0];
+    L.cc[nc + c] = C[1];
+    L.cc[2 * nc + c] = C[2];
+    double V = 0.0;
+    const int nf = M.nface;
+    for (int s = 0; s < 6; ++s) {
+        const int f = M.cell_faces[s * nc + c] & 0x7fffffff;
+        double P0[3], P1[3], P2[3], P3[3];
+        load_node(L.xyz, nn, M.face_nodes[f], P0);
+        load_node(L.xyz, nn, M.face_nodes[nf + f], P1);
+        load_node(L.xyz, nn, M.face_nodes[2 * nf + f], P2);
+        load_node(L.xyz, nn, M.face_nodes[3 * nf + f], P3);
+        V += tet_vol(C, P0, P1, P2);
+        V += tet_vol(C, P0, P3, P2);
+    }
+    L.vol[c] = V;
+}
+
+// Face centre, area, normal oriented from cells[0] to cells[1] (Gran.cpp:112-218)
+// and half the centre distance used by the CFL estimate (Setka_physics.cpp:2298-2307).
+static __global__ void face_geometry_kernel(MeshView M, Layer L) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= M.nface) return;
+    const int nf = M.nface, nn = M.nnode, nc = M.ncell;
+    double P[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) load_node(L.xyz, nn, M.face_nodes[k * nf + f], P[k]);
+    double xc = 0.0, yc = 0.0, zc = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        xc += P[k][0];
+        yc += P[k][1];
+        zc += P[k][2];
+    }
+    xc /= 4;
+    yc /= 4;
+    zc /= 4;
+    L.fc[f] = xc;
+    L.fc[nf + f] = yc;
+    L.fc[2 * nf + f] = zc;
+    double S = 0.0;
+    S += tri_area(P[0][0], P[0][1], P[0][2], P[1][0], P[1][1], P[1][2], P[2][0], P[2][1], P[2][2]);
+    S += tri_area(P[0][0], P[0][1], P[0][2], P[3][0], P[3][1], P[3][2], P[2][0], P[2][1], P[2][2]);
+    L.fa[f] = S;
+    const double x1 = (P[0][0] + P[1][0]) / 2.0, y1 = (P[0][1] + P[1][1]) / 2.0, z1 = (P[0][2] + P[1][2]) / 2.0;
+    const double x2 = (P[1][0] + P[2][0]) / 2.0, y2 = (P[1][1] + P[2][1]) / 2.0, z2 = (P[1][2] + P[2][2]) / 2.0;
+    const double x3 = (P[2][0] + P[3][0]) / 2.0, y3 = (P[2][1] + P[3][1]) / 2.0, z3 = (P[2][2] + P[3][2]) / 2.0;
+    const double ax = x2 - x1, ay = y2 - y1, az = z2 - z1;
+    const double bx = x3 - x1, by = y3 - y1, bz = z3 - z1;
+    double n1 = ay * bz - az * by;
+    double n2 = az * bx - ax * bz;
+    double n3 = ax * by - ay * bx;
+    const double nrm = sqrt(n1 * n1 + n2 * n2 + n3 * n3);
+    n1 /= nrm;
+    n2 /= nrm;
+    n3 /= nrm;
+    const int c0 = M.face_c0[f];
+    const double c0x = L.cc[c0], c0y = L.cc[nc + c0], c0z = L.cc[2 * nc + c0];
+    if (n1 * (c0x - xc) + n2 * (c0y - yc) + n3 * (c0z - zc) > 0.0) {
+        n1 = -n1;
+        n2 = -n2;
+        n3 = -n3;
+    }
+    L.fn[f] = n1;
+    L.fn[nf + f] = n2;
+    L.fn[2 * nf + f] = n3;
+    const int c1 = M.face_c1[f];
+    double d = 0.0;
+    if (c1 >= 0) {
+        const double dx = c0x - L.cc[c1], dy = c0y - L.cc[nc + c1], dz = c0z - L.cc[2 * nc + c1];
+        d = sqrt(dx * dx + dy * dy + dz * dz) / 2.0;
+    }
+    L.fd[f] = d;
+}
+
+// ---------------------------------------------------------------------------
+// Reconstruction helpers (first order), Setka_gran_snos.cpp:737-1071.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double polar_angle(double x, double y) {
+    if (fabs(x) + fabs(y) < 0.000001) return 0.0;
+    if (x < 0) return atan(y / x) + 1.0 * kPi;
+    if (x > 0 && y >= 0) return atan(y / x);
+    if (x > 0 && y < 0) return atan(y / x) + 2.0 * kPi;
+    if (y > 0 && x >= 0 && x <= 0) return kPi / 2.0;
+    if (y < 0 && x >= 0 && x <= 0) return 3.0 * kPi / 2.0;
+    return 0.0;
+}
+
+// Cartesian -> (r, phi, theta) components (Help_funk.cpp:121-135)
+__device__ __forceinline__ void to_spherical(double z, double x, double y, double Vz, double Vx, double Vy,
+                                             double& Vr, double& Vphi, double& Vtheta) {
+    const double r = sqrt(x * x + y * y + z * z);
+    const double th = acos(z / r);
+    const double ph = polar_angle(x, y);
+    const double sth = sin(th), cth = cos(th), sph = sin(ph), cph = cos(ph);
+    Vr = Vx * sth * cph + Vy * sth * sph + Vz * cth;
+    Vtheta = Vx * cth * cph + Vy * cth * sph - Vz * sth;
+    Vphi = -Vx * sph + Vy * cph;
+}
+
+// (r, phi, theta) -> Cartesian components (Help_funk.cpp:107-119)
+__device__ __forceinline__ void to_cartesian(double z, double x, double y, double Vr, double Vphi, double Vtheta,
+                                             double& Vz, double& Vx, double& Vy) {
+    const double r = sqrt(x * x + y * y + z * z);
+    const double th = acos(z / r);
+    const double ph = polar_angle(x, y);
+    const double sth = sin(th), cth = cos(th), sph = sin(ph), cph = cos(ph);
+    Vx = Vr * sth * cph + Vtheta * cth * cph - Vphi * sph;
+    Vy = Vr * sth * sph + Vtheta * cth * sph + Vphi * cph;
+    Vz = Vr * cth - Vtheta * sth;
+}
+
+// Zone_1 cells are carried radially from the cell centre to the face centre:
+// rho, Q, rho_He ~ r^-2, p ~ r^-2gamma, B_r ~ r^-2, B_t ~ r^-1, velocity
+// direction rotated (Setka_gran_snos.cpp:744-873).
+static __device__ __noinline__ void zone1_scale(double* s, double ax, double ay, double az, double gx, double gy, double gz,
+                                         double gamma) {
+    const double r1 = sqrt(ax * ax + ay * ay + az * az);
+    const double rr = sqrt(gx * gx + gy * gy + gz * gz);
+    const double the1 = acos(gz / rr);
+    const bool band = (the1 > kPi / 9 && the1 < 8 * kPi / 9);
+#pragma unroll
+    for (int ik = 0; ik < 2; ++ik) {
+        const int i1 = ik == 0 ? 1 : 5;
+        const double X = s[i1], Y = s[i1 + 1], Z = s[i1 + 2];
+        double A0, A1, A2;
+        if (band)
+            to_spherical(az, ax, ay, Z, X, Y, A0, A1, A2);
+        else
+            to_spherical(ax, ay, az, X, Y, Z, A0, A1, A2);
+        if (ik == 1) {
+            A0 = A0 * ((r1 / rr) * (r1 / rr));
+            A1 = A1 * ((r1) / (rr));
+            A2 = A2 * ((r1) / (rr));
+        }
+        if (band)
+            to_cartesian(gz, gx, gy, A0, A1, A2, s[i1 + 2], s[i1], s[i1 + 1]);
+        else
+            to_cartesian(gx, gy, gz, A0, A1, A2, s[i1], s[i1 + 1], s[i1 + 2]);
+    }
+    s[0] = s[0] * (r1 * r1) / (rr * rr);
+    s[8] = s[8] * (r1 * r1) / (rr * rr);
+    s[9] = s[9] * (r1 * r1) / (rr * rr);
+    s[4] = s[4] * pow(r1, 2.0 * gamma) / pow(rr, 2.0 * gamma);
+}
+
+
+
+// Stored flux values per face: rho, m_x, m_y, m_z, E, B_x, B_y, B_z, divB
+// (+ Q, rho_He), padded to a 16-byte multiple.
+template <typename FT, int NK>
+struct FluxLayout {
+    static constexpr int n = 9 + NK;
+    static constexpr int stride = (sizeof(FT) == 8) ? ((n + 1) & ~1) : ((n + 3) & ~3);
+};
+
+template <typename R, typename FT, int NK, bool MOVE>
+__global__ void __launch_bounds__(128) face_flux_kernel(FaceArgs a) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    double contrib = 100000000.0;  // identity of the min (Setka_physics.cpp:1607)
+    if (f < a.M.nface && a.st->err_kind == 0) {
+        const MeshView& M = a.M;
+        const Params& P = a.P;
+        const int nf = M.nface, nc = M.ncell;
+        const int type = M.face_type[f];
+        const int c0 = M.face_c0[f];
+        const double n[3] = {a.L1.fn[f], a.L1.fn[nf + f], a.L1.fn[2 * nf + f]};
+        const double area = a.L1.fa[f];
+        double w = 0.0;
+        if (MOVE) {
+            const double time = a.st->dt;
+            const int nn = M.nnode;
+            double ddot = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int i = M.face_nodes[k * nf + f];
+                const double dx = a.xyz2[i] - a.L1.xyz[i];
+                const double dy = a.xyz2[nn + i] - a.L1.xyz[nn + i];
+                const double dz = a.xyz2[2 * nn + i] - a.L1.xyz[2 * nn + i];
+                ddot = ddot + (dx * n[0] + dy * n[1] + dz * n[2]);
+            }
+            w = ddot / 4.0 / time;
+        }
+        constexpr int NS = 8 + NK;
+        double Ls[NV], Rs[NV];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) Ls[k] = a.state[k * nc + c0];
+#pragma unroll
+        for (int k = NS; k < NV; ++k) Ls[k] = 0.0;
+        if (type == 0) {
+            const int c1 = M.face_c1[f];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) Rs[k] = a.state[k * nc + c1];
+#pragma unroll
+            for (int k = NS; k < NV; ++k) Rs[k] = 0.0;
+            const double gx = a.L1.fc[f], gy = a.L1.fc[nf + f], gz = a.L1.fc[2 * nf + f];
+            if (M.cell_type[c0] == 1)
+                zone1_scale(Ls, a.L1.cc[c0], a.L1.cc[nc + c0], a.L1.cc[2 * nc + c0], gx, gy, gz, P.gamma);
+            if (M.cell_type[c1] == 1)
+                zone1_scale(Rs, a.L1.cc[c1], a.L1.cc[nc + c1], a.L1.cc[2 * nc + c1], gx, gy, gz, P.gamma);
+        } else if (type == 3) {
+            // Outer_Soft: copy the interior cell, with the reference's outflow fix-ups
+            if (P.soft_fixups) {
+                if (n[0] < -0.95) {
+                    if (Ls[1] > P.velosity_inf / 7.0) Ls[1] = P.velosity_inf / 5.0;
+                } else if (Ls[1] * n[0] + Ls[2] * n[1] + Ls[3] * n[2] < 0.0) {
+                    Ls[1] = 0.1 * n[0];
+                    Ls[2] = 0.1 * n[1];
+                    Ls[3] = 0.1 * n[2];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < NV; ++k) Rs[k] = Ls[k];
+        } else {
+            // Inner_Hard / Outer_Hard: fixed face values
+            const int row = M.face_bc[f];
+#pragma unroll
+            for (int k = 0; k < NV; ++k) Rs[k] = M.bc_vals[k * M.nbc + row];
+        }
+        int method;
+        if (P.method_policy == 1) {
+            const double bb = ((Ls[5] * Ls[5] + Ls[6] * Ls[6] + Ls[7] * Ls[7]) +
+                               (Rs[5] * Rs[5] + Rs[6] * Rs[6] + Rs[7] * Rs[7])) / 2.0;
+            const double pp = (Ls[4] + Rs[4]) / 2.0;
+            method = (bb / (4.0 * kPi) / (2.0 * pp) > P.beta_switch) ? 3 : 2;
+        } else {
+            method = M.face_method[f];
+        }
+        const int surf = M.face_surf[f];
+        RiemannFlags fl;
+        fl.null_bn = false;
+        fl.n_disc = 0;
+        fl.left_ydar = (surf == 1 && P.TS_hard);
+        fl.contact = (surf == 2 && P.contact_hard);
+        R qL[8], qR[8], kl[NK > 0 ? NK : 1], kr[NK > 0 ? NK : 1], q[8], kq[NK > 0 ? NK : 1], nr[3];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            qL[k] = R(Ls[k]);
+            qR[k] = R(Rs[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+            kl[k] = R(Ls[8 + k]);
+            kr[k] = R(Rs[8 + k]);
+        }
+        nr[0] = R(n[0]);
+        nr[1] = R(n[1]);
+        nr[2] = R(n[2]);
+        R dsl, dsc, dsr;
+        const int rc = riemann_flux<R, NK>(method, nr, R(w), qL, qR, kl, kr, q, kq, dsl, dsc, dsr, fl, R(P.gamma));
+        if (rc) record_error(a.st, 10 + rc, f);
+        if (type == 0) {
+            const double dist = a.L1.fd[f];
+            const double dnt = P.KFL * dist / (rmax(fabs(double(dsl)), fabs(double(dsr))) + fabs(w));
+            contrib = 10000000.0;
+            if (dnt < contrib) contrib = dnt;
+        } else {
+            contrib = 10000000.0;
+        }
+        using L = FluxLayout<FT, NK>;
+        FT out[L::stride];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) out[k] = FT(double(q[k]) * area);
+        out[8] = FT(0.5 * (n[0] * (Ls[5] + Rs[5]) + n[1] * (Ls[6] + Rs[6]) + n[2] * (Ls[7] + Rs[7])) * area);
+#pragma unroll
+        for (int k = 0; k < NK; ++k) out[9 + k] = FT(double(kq[k]) * area);
+#pragma unroll
+        for (int k = L::n; k < L::stride; ++k) out[k] = FT(0);
+        FT* dst = reinterpret_cast<FT*>(a.flux) + size_t(f) * L::stride;
+        if (sizeof(FT) == 8) {
+#pragma unroll
+            for (int k = 0; k < L::stride; k += 2)
+                reinterpret_cast<double2*>(dst)[k / 2] = make_double2(double(out[k]), double(out[k + 1]));
+        } else {
+#pragma unroll
+            for (int k = 0; k < L::stride; k += 4)
+                reinterpret_cast<float4*>(dst)[k / 4] =
+                    make_float4(float(out[k]), float(out[k + 1]), float(out[k + 2]), float(out[k + 3]));
+        }
+    }
+    // CFL minimum: warp shuffle, then shared memory across the block, then one
+    // atomicMin on the ordered bit pattern (all candidates are >= 0).
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) contrib = fmin(contrib, __shfl_xor_sync(0xffffffffu, contrib, o));
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = contrib;
+    __syncthreads();
+    if (wid == 0) {
+        double v = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 100000000.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0 && v < 100000000.0)
+            atomicMin(&a.st->dt_next_bits, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+
+
+// Bera charge-exchange sources of the plasma (Setka_physics.cpp:766-1258,
+// no pickup ions), returning m_x, m_y, m_z, E times n_H_LISM / Kn.
+static __device__ __noinline__ void bera_sources(const Params& P, const double* prim, int ctype, const double* H, int nc,
+                                          int c, double* S) {
+    const double rho = prim[0], p = prim[4], Q = prim[8], rho_He = prim[9];
+    int zone;
+    if (Q / rho < 50.0)
+        zone = (ctype == 1) ? 1 : 2;
+    else
+        zone = (ctype == 4) ? 4 : 3;
+    const int al = (zone - 1 <= 2) ? 2 : 1;  // Plasma_components_1 receives zone - 1
+    double rho_p = -(kMeDmp * al * rho_He + 4.0 * (-rho + rho_He)) / (4.0 * (1.0 + kMeDmp));
+    double T_p = 8.0 * (1.0 + kMeDmp) * p / (8.0 * rho - (7.0 - al + (-1.0 + al) * kMeDmp) * rho_He);
+    if (rho_p <= 1e-8) rho_p = 1e-8;
+    if (T_p <= 1e-8) T_p = 1e-8;
+    if (T_p > 1e5) T_p = 1e5;
+    const double Vp0 = prim[1], Vp1 = prim[2], Vp2 = prim[3];
+    double mxs = 0.0, mys = 0.0, mzs = 0.0, Es = 0.0;
+    for (int h = 0; h < P.nh; ++h) {
+        const double rho_h = H[(5 * h + 0) * nc + c];
+        const double Vh0 = H[(5 * h + 1) * nc + c], Vh1 = H[(5 * h + 2) * nc + c], Vh2 = H[(5 * h + 3) * nc + c];
+        const double T_h = 2.0 * H[(5 * h + 4) * nc + c] / rmax(rho_h, 1e-9);
+        const double d0 = Vp0 - Vh0, d1 = Vp1 - Vh1, d2 = Vp2 - Vh2;
+        const double uu = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        const double U_ph = sqrt((4.0 / kPi) * (T_p + T_h) + uu * uu);
+        const double U_hp = sqrt((4.0 / kPi) * (T_h + T_p) + uu * uu);
+        const double Um_ph = sqrt((16.0 / kPi) * T_p + (9.0 * kPi / 4.0) * T_h + 4.0 * (uu * uu));
+        const double Um_hp = sqrt((16.0 / kPi) * T_h + (9.0 * kPi / 4.0) * T_p + 4.0 * (uu * uu));
+        const double UE_ph = sqrt((4.0 / kPi) * T_p + (64.0 / 9.0 / kPi) * T_h + uu * uu);
+        const double UE_hp = sqrt((4.0 / kPi) * T_h + (64.0 / 9.0 / kPi) * T_p + uu * uu);
+        const double a_ph = 1.0 - P.par_a_2 * log(U_ph);
+        const double a_hp = 1.0 - P.par_a_2 * log(U_hp);
+        const double k_hp = (a_hp * a_hp) * rho_p * rho_h;
+        const double k_ph = (a_ph * a_ph) * rho_p * rho_h;
+        const double t_hp = T_p / Um_hp, t_ph = T_h / Um_ph;
+        const double Hm_hp0 = k_hp * (U_hp * Vp0 + t_hp * d0);
+        const double Hm_hp1 = k_hp * (U_hp * Vp1 + t_hp * d1);
+        const double Hm_hp2 = k_hp * (U_hp * Vp2 + t_hp * d2);
+        const double Hm_ph0 = k_ph * (U_ph * Vh0 - t_ph * d0);
+        const double Hm_ph1 = k_ph * (U_ph * Vh1 - t_ph * d1);
+        const double Hm_ph2 = k_ph * (U_ph * Vh2 - t_ph * d2);
+        const double vp2 = Vp0 * Vp0 + Vp1 * Vp1 + Vp2 * Vp2;
+        const double vh2 = Vh0 * Vh0 + Vh1 * Vh1 + Vh2 * Vh2;
+        const double vpd = Vp0 * d0 + Vp1 * d1 + Vp2 * d2;
+        const double vhd = Vh0 * d0 + Vh1 * d1 + Vh2 * d2;
+        const double HE_hp = k_hp * (0.5 * U_hp * vp2 + t_hp * vpd + 3.0 / 4.0 * T_p * UE_hp);
+        const double HE_ph = k_ph * (0.5 * U_ph * vh2 - t_ph * vhd + 3.0 / 4.0 * T_h * UE_ph);
+        mxs += (-Hm_hp0 + Hm_ph0);
+        mys += (-Hm_hp1 + Hm_ph1);
+        mzs += (-Hm_hp2 + Hm_ph2);
+        Es += (-HE_hp + HE_ph);
+    }
+    const double ddp = (P.par_n_H_LISM / P.par_Kn);
+    S[0] = mxs * ddp;
+    S[1] = mys * ddp;
+    S[2] = mzs * ddp;
+    S[3] = Es * ddp;
+}
+
+template <typename FT, int NK, bool MOVE, int SRC>
+__global__ void __launch_bounds__(256) cell_update_kernel(CellArgs a) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = a.st->err_kind == 0;
+    if (c < a.M.ncell && ok) {
+        const MeshView& M = a.M;
+        const int nc = M.ncell;
+        const double time = a.st->dt;
+        const double Volume = a.vol1[c];
+        const double Volume2 = MOVE ? a.vol2[c] : Volume;
+        using L = FluxLayout<FT, NK>;
+        double PO[9 + NK];
+#pragma unroll
+        for (int k = 0; k < 9 + NK; ++k) PO[k] = 0.0;
+        const FT* fx = reinterpret_cast<const FT*>(a.flux);
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            const int fs = M.cell_faces[s * nc + c];
+            const int f = fs & 0x7fffffff;
+            const double sign = (fs < 0) ? -1.0 : 1.0;
+            const FT* src = fx + size_t(f) * L::stride;
+            FT v[L::stride];
+            if (sizeof(FT) == 8) {
+#pragma unroll
+                for (int k = 0; k < L::stride; k += 2) {
+                    const double2 t = __ldg(reinterpret_cast<const double2*>(src) + k / 2);
+                    v[k] = FT(t.x);
+                    v[k + 1] = FT(t.y);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < L::stride; k += 4) {
+                    const float4 t = __ldg(reinterpret_cast<const float4*>(src) + k / 4);
+                    v[k] = FT(t.x);
+                    v[k + 1] = FT(t.y);
+                    v[k + 2] = FT(t.z);
+                    v[k + 3] = FT(t.w);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 9 + NK; ++k) PO[k] += sign * double(v[k]);
+        }
+        double prim[NV];
+#pragma unroll
+        for (int k = 0; k < 8 + NK; ++k) prim[k] = a.state[k * nc + c];
+#pragma unroll
+        for (int k = 8 + NK; k < NV; ++k) prim[k] = 0.0;
+        double S[4] = {0.0, 0.0, 0.0, 0.0};
+        if (SRC == 1) {
+            bera_sources(a.P, prim, M.cell_type[c], a.hfl, nc, c, S);
+        } else if (SRC == 2) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) S[k] = a.src[k * nc + c];
+        }
+        const double g1 = a.P.gamma - 1.0;
+        const double cpi4 = 4.0 * kPi;
+        const double rho = prim[0], vx = prim[1], vy = prim[2], vz = prim[3], p = prim[4];
+        const double bx = prim[5], by = prim[6], bz = prim[7], Q = prim[8], rho_He = prim[9];
+        const double dsk = vx * bx + vy * by + vz * bz;
+        double rho3 = rho * Volume / Volume2 - time * PO[0] / Volume2;
+        bool rho_null = false;
+        if (rho3 < 1e-7) {
+            rho_null = true;
+            rho3 = 0.1;
+            atomicAdd(&a.st->n_rho_floor, 1ull);
+        }
+        double Q3 = 0.0, rho_He3 = 0.0;
+        if (NK > 0) {
+            Q3 = Q * Volume / Volume2 - time * PO[9] / Volume2;
+            rho_He3 = rho_He * Volume / Volume2 - time * PO[9 + (NK > 1 ? 1 : 0)] / Volume2;
+        }
+        if (rho_He3 < 0.0) rho_He3 = 0.0;
+        double u3, v3, w3, bx3, by3, bz3, p3;
+        if (!rho_null) {
+            u3 = (rho * vx * Volume / Volume2 - time * (PO[1] + (bx / cpi4) * PO[8]) / Volume2 + time * S[0]) / rho3;
+            v3 = (rho * vy * Volume / Volume2 - time * (PO[2] + (by / cpi4) * PO[8]) / Volume2 + time * S[1]) / rho3;
+            w3 = (rho * vz * Volume / Volume2 - time * (PO[3] + (bz / cpi4) * PO[8]) / Volume2 + time * S[2]) / rho3;
+            bx3 = bx * Volume / Volume2 - time * (PO[5] + vx * PO[8]) / Volume2;
+            by3 = by * Volume / Volume2 - time * (PO[6] + vy * PO[8]) / Volume2;
+            bz3 = bz * Volume / Volume2 - time * (PO[7] + vz * PO[8]) / Volume2;
+            p3 = (((p / g1 + 0.5 * rho * (vx * vx + vy * vy + vz * vz) + (bx * bx + by * by + bz * bz) / kC8Pi) *
+                       Volume / Volume2 -
+                   time * (PO[4] + (dsk / cpi4) * PO[8]) / Volume2 + time * S[3]) -
+                  0.5 * rho3 * (u3 * u3 + v3 * v3 + w3 * w3) - (bx3 * bx3 + by3 * by3 + bz3 * bz3) / kC8Pi) *
+                 g1;
+            if (M.cell_type[c] == 2) {  // Zone_2 effective magnetic dissipation, tau = 1
+                const double tau = 1.0;
+                const double bx4 = bx3 - time * bx3 / tau;
+                const double by4 = by3 - time * by3 / tau;
+                const double bz4 = bz3 - time * bz3 / tau;
+                const double p4 = p3 + (time / tau - (time / tau) * (time / tau)) * (g1) *
+                                           (bx3 * bx3 + by3 * by3 + bz3 * bz3) / (4.0 * kPi);
+                bx3 = bx4;
+                by3 = by4;
+                bz3 = bz4;
+                p3 = p4;
+            }
+        } else {
+            u3 = vx;
+            v3 = vy;
+            w3 = vz;
+            bx3 = bx;
+            by3 = by;
+            bz3 = bz;
+            p3 = rho3 / 2.0;
+        }
+        if (isnan(rho3) || (rho3 != 0.0 && fabs(rho3) < 2.2250738585072014e-308) || isnan(Q3) ||
+            (Q3 != 0.0 && fabs(Q3) < 2.2250738585072014e-308))
+            record_error(a.st, 20, c);
+        if (p3 < 0.00000001) {
+            p3 = 0.000001;
+            atomicAdd(&a.st->n_p_floor, 1ull);
+        }
+        if (rho_He3 > rho3) rho_He3 = rho3 * 0.1;
+        double* o = a.state2;
+        o[c] = rho3;
+        o[nc + c] = u3;
+        o[2 * nc + c] = v3;
+        o[3 * nc + c] = w3;
+        o[4 * nc + c] = p3;
+        const bool tvd = M.cell_tvd[c] != 0;
+        o[5 * nc + c] = tvd ? bx3 : bx;
+        o[6 * nc + c] = tvd ? by3 : by;
+        o[7 * nc + c] = tvd ? bz3 : bz;
+        if (NK > 0) {
+            o[8 * nc + c] = Q3;
+            if (NK > 1) o[9 * nc + c] = rho_He3;
+        }
+    }
+    // Last block to finish rolls the clock: t += dt, dt = CFL minimum of this
+    // step's faces (applied on the next step, Setka_physics.cpp:1606-1607).
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int prev = atomicAdd(&a.st->block_counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        DevStatus* st = a.st;
+        const unsigned long long bits = atomicAdd(&st->dt_next_bits, 0ull);
+        if (st->err_kind == 0) {
+            st->t += st->dt;
+            st->dt = __longlong_as_double((long long)bits);
+            st->steps_done += 1ull;
+        }
+        st->dt_next_bits = (unsigned long long)__double_as_longlong(100000000.0);
+        st->block_counter = 0u;
+        __threadfence();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Permutation kernels for upload/download (SoA fields of length n).
+// dst[k][i] = src[k][perm[i]]  (gather)   /   dst[k][perm[i]] = src[k][i] (scatter)
+// ---------------------------------------------------------------------------
+static __global__ void gather_fields_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                     const int* __restrict__ perm, int n, int nfields) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = perm[i];
+    for (int k = 0; k < nfields; ++k) dst[size_t(k) * n + i] = src[size_t(k) * n + j];
+}
+
+static __global__ void scatter_fields_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                      const int* __restrict__ perm, int n, int nfields) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = perm[i];
+    for (int k = 0; k < nfields; ++k) dst[size_t(k) * n + j] = src[size_t(k) * n + i];
+}
+
+// Stateless batched Riemann solver (parity checks against the reference
+// solver and FP32 error measurements). AoS inputs, as the reference's qqq.
+template <typename R>
+__global__ void riemann_batch_kernel(long long n, const signed char* __restrict__ ns, const double* __restrict__ nrm,
+                                     const double* __restrict__ w, const double* __restrict__ q1,
+                                     const double* __restrict__ q2, double* __restrict__ flux,
+                                     double* __restrict__ ds, int* __restrict__ rc, int flags, double gamma) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    R a[8], b[8], q[8], nr[3], dummy[1], ko[1];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        a[k] = R(q1[8 * i + k]);
+        b[k] = R(q2[8 * i + k]);
+    }
+    nr[0] = R(nrm[3 * i]);
+    nr[1] = R(nrm[3 * i + 1]);
+    nr[2] = R(nrm[3 * i + 2]);
+    RiemannFlags fl;
+    fl.null_bn = (flags & 1) != 0;
+    fl.left_ydar = (flags & 2) != 0;
+    fl.contact = (flags & 4) != 0;
+    fl.n_disc = (flags >> 4) & 3;
+    R dsl, dsc, dsr;
+    rc[i] = riemann_flux<R, 0>(ns[i], nr, R(w[i]), a, b, dummy, dummy, q, ko, dsl, dsc, dsr, fl, R(gamma));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) flux[8 * i + k] = double(q[k]);
+    ds[3 * i] = double(dsl);
+    ds[3 * i + 1] = double(dsc);
+    ds[3 * i + 2] = double(dsr);
+}
+
+}  // namespace titan

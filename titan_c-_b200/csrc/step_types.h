@@ -1,0 +1,82 @@
+// Plain data shared by the host side and the kernels of the plasma step.
+#pragma once
+#include <cstdint>
+
+namespace titan {
+
+constexpr int NV = 10;             // rho, Vx, Vy, Vz, p, Bx, By, Bz, Q, rho_He
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kC8Pi = 25.13274122871834590768;  // literal of Setka_physics.cpp:1927
+constexpr double kMeDmp = (1.0 / 1836.15);
+
+// Device status word shared by all kernels of a context.
+struct DevStatus {
+    int err_kind;                 // 0 ok; first failure kind (see titan_b200.h)
+    int err_index;                // renumbered index of the failing face/cell
+    unsigned long long n_rho_floor;
+    unsigned long long n_p_floor;
+    unsigned long long steps_done;
+    unsigned int block_counter;   // last-block-done counter of cell_update
+    unsigned int pad;
+    unsigned long long dt_next_bits;  // running CFL minimum (as ordered bits)
+    double dt;                    // dt of the current step ("time" in Setka::Go)
+    double t;                     // physical time accumulated
+};
+
+struct Params {
+    double gamma, KFL, velosity_inf, omega, par_a_2, par_n_H_LISM, par_Kn, beta_switch;
+    int move, soft_fixups, method_policy, npassive, nh, TS_hard, contact_hard, src_mode;
+};
+
+struct MeshView {
+    int ncell, nface, nnode, nbc;
+    const int* face_c0;           // [nface] cells[0]
+    const int* face_c1;           // [nface] cells[1] or -1
+    const signed char* face_type; // Type_Gran
+    const signed char* face_surf; // Type_Gran_surf
+    const signed char* face_method;
+    const int* face_bc;           // row into bc_vals or -1
+    const double* bc_vals;        // [NV][nbc]
+    const int* face_nodes;        // [4][nface]
+    const int* cell_faces;        // [6][ncell], bit 31 set when the cell is cells[1]
+    const int* cell_nodes;        // [8][ncell]
+    const signed char* cell_type; // Type_cell
+    const unsigned char* cell_tvd;
+    const double* node_amp;       // [nnode] or null
+    const double* node_phase;     // [nnode] or null
+};
+
+struct Layer {  // geometry of one time layer (the reference's [2] arrays)
+    double* xyz;   // [3][nnode]
+    double* cc;    // [3][ncell]
+    double* vol;   // [ncell]
+    double* fc;    // [3][nface]
+    double* fn;    // [3][nface]
+    double* fa;    // [nface]
+    double* fd;    // [nface] half distance between the two cell centres
+};
+
+struct FaceArgs {
+    MeshView M;
+    Params P;
+    Layer L1;                    // geometry at the current layer
+    const double* xyz2;          // node coordinates at the next layer (ALE)
+    const double* state;         // [NV][ncell] current layer
+    void* flux;                  // [nface][NFS] (double or float)
+    DevStatus* st;
+};
+
+struct CellArgs {
+    MeshView M;
+    Params P;
+    const double* vol1;
+    const double* vol2;
+    const double* state;   // [NV][ncell] current
+    double* state2;        // [NV][ncell] next
+    const void* flux;
+    const double* hfl;     // [5*nh][ncell] frozen neutral fluids (Bera sources)
+    const double* src;     // [4][ncell] external sources (m_x, m_y, m_z, E)
+    DevStatus* st;
+};
+
+}  // namespace titan

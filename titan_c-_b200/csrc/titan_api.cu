@@ -1,0 +1,794 @@
+// Host side of the C ABI declared in include/titan_b200.h: mesh validation and
+// SFC renumbering, device buffers, the step loop (CUDA-graph captured), and
+// the state / geometry / flux transfers in the caller's original numbering.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/titan_b200.h"
+#include "launch.h"
+#include "renumber.h"
+
+using namespace titan;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return fail(e_ == cudaErrorMemoryAllocation ? TITAN_ENOMEM : TITAN_ECUDA,                \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                         \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t n, int64_t* total) {
+    *p = nullptr;
+    if (n == 0) return cudaSuccess;
+    *total += int64_t(n * sizeof(T));
+    return cudaMalloc((void**)p, n * sizeof(T));
+}
+
+template <typename T>
+cudaError_t dput(T* d, const std::vector<T>& h, cudaStream_t s) {
+    if (h.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+}  // namespace
+
+struct KernelClock {
+    double ms = 0.0;
+    int64_t launches = 0;
+};
+
+struct titan_ctx {
+    int64_t ncell = 0, nface = 0, nnode = 0, nbc = 0;
+    titan_params prm{};
+    Params P{};
+    int ns = 8;  // state fields stored on the device (8 + npassive)
+    bool fp32 = false;
+    cudaStream_t stream = nullptr;
+    int64_t dev_bytes = 0;
+
+    Renumbering R;
+    int32_t* d_cell_n2o = nullptr;
+    int32_t* d_node_n2o = nullptr;
+
+    // mesh (renumbered)
+    int32_t *d_face_c0 = nullptr, *d_face_c1 = nullptr, *d_face_bc = nullptr, *d_face_nodes = nullptr;
+    int8_t *d_face_type = nullptr, *d_face_surf = nullptr, *d_face_method = nullptr;
+    double* d_bc_vals = nullptr;
+    int32_t *d_cell_faces = nullptr, *d_cell_nodes = nullptr;
+    int8_t* d_cell_type = nullptr;
+    uint8_t* d_cell_tvd = nullptr;
+    double *d_node_amp = nullptr, *d_node_phase = nullptr;
+
+    Layer layer[2]{};
+    int cur = 0;
+    double* d_state[2] = {nullptr, nullptr};
+    int scur = 0;
+    void* d_flux = nullptr;
+    int flux_stride = 0;
+    size_t flux_elem = 8;
+    double* d_hfl = nullptr;
+    double* d_src = nullptr;
+    bool use_src = false;
+    double* d_stage = nullptr;  // NV*max(ncell, nnode) staging for transfers
+    DevStatus* d_status = nullptr;
+    DevStatus* h_status = nullptr;  // pinned
+
+    // CUDA graph of two steps (the buffer ping-pong has period two)
+    cudaGraphExec_t graph = nullptr;
+    int graph_cur = -1, graph_scur = -1;
+
+    bool profiling = false;
+    std::map<std::string, KernelClock> clocks;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+
+    MeshView view() const {
+        MeshView M;
+        M.ncell = (int)ncell;
+        M.nface = (int)nface;
+        M.nnode = (int)nnode;
+        M.nbc = (int)nbc;
+        M.face_c0 = d_face_c0;
+        M.face_c1 = d_face_c1;
+        M.face_type = d_face_type;
+        M.face_surf = d_face_surf;
+        M.face_method = d_face_method;
+        M.face_bc = d_face_bc;
+        M.bc_vals = d_bc_vals;
+        M.face_nodes = d_face_nodes;
+        M.cell_faces = d_cell_faces;
+        M.cell_nodes = d_cell_nodes;
+        M.cell_type = d_cell_type;
+        M.cell_tvd = d_cell_tvd;
+        M.node_amp = d_node_amp;
+        M.node_phase = d_node_phase;
+        return M;
+    }
+};
+
+namespace {
+
+// Runs `fn` (which launches one kernel on ctx->stream); when profiling, times
+// it with CUDA events under `name`.
+template <typename F>
+cudaError_t timed(titan_ctx* ctx, const char* name, F fn) {
+    if (!ctx->profiling) return fn();
+    cudaEventRecord(ctx->ev[0], ctx->stream);
+    cudaError_t e = fn();
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+    cudaEventSynchronize(ctx->ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    KernelClock& k = ctx->clocks[name];
+    k.ms += ms;
+    k.launches += 1;
+    return e;
+}
+
+// Enqueue one step; flips the layer and state buffers.
+cudaError_t enqueue_step(titan_ctx* ctx) {
+    const MeshView M = ctx->view();
+    const bool move = ctx->prm.move != 0;
+    const int nxt = ctx->cur ^ 1;
+    cudaError_t e = cudaSuccess;
+    if (move) {
+        e = timed(ctx, "move_nodes", [&] {
+            return launch_move_nodes(M, ctx->P, ctx->layer[ctx->cur].xyz, ctx->layer[nxt].xyz, ctx->d_status,
+                                     ctx->stream);
+        });
+        if (e) return e;
+        e = timed(ctx, "cell_geometry", [&] { return launch_cell_geometry(M, ctx->layer[nxt], ctx->stream); });
+        if (e) return e;
+        e = timed(ctx, "face_geometry", [&] { return launch_face_geometry(M, ctx->layer[nxt], ctx->stream); });
+        if (e) return e;
+    }
+    FaceArgs fa;
+    fa.M = M;
+    fa.P = ctx->P;
+    fa.L1 = ctx->layer[ctx->cur];
+    fa.xyz2 = move ? ctx->layer[nxt].xyz : ctx->layer[ctx->cur].xyz;
+    fa.state = ctx->d_state[ctx->scur];
+    fa.flux = ctx->d_flux;
+    fa.st = ctx->d_status;
+    const int nk = ctx->prm.npassive;
+    if (ctx->fp32)
+        e = timed(ctx, "face_flux_fp32", [&] { return launch_face_flux_fp32(fa, nk, move, ctx->stream); });
+    else
+        e = timed(ctx, "face_flux_fp64", [&] { return launch_face_flux_fp64(fa, nk, move, ctx->stream); });
+    if (e) return e;
+    CellArgs ca;
+    ca.M = M;
+    ca.P = ctx->P;
+    ca.vol1 = ctx->layer[ctx->cur].vol;
+    ca.vol2 = move ? ctx->layer[nxt].vol : ctx->layer[ctx->cur].vol;
+    ca.state = ctx->d_state[ctx->scur];
+    ca.state2 = ctx->d_state[ctx->scur ^ 1];
+    ca.flux = ctx->d_flux;
+    ca.hfl = ctx->d_hfl;
+    ca.src = ctx->d_src;
+    ca.st = ctx->d_status;
+    const int src = ctx->use_src ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
+    e = timed(ctx, "cell_update", [&] { return launch_cell_update(ca, ctx->fp32, nk, move, src, ctx->stream); });
+    if (e) return e;
+    ctx->scur ^= 1;
+    if (move) ctx->cur = nxt;
+    return cudaSuccess;
+}
+
+void drop_graph(titan_ctx* ctx) {
+    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+    ctx->graph_cur = ctx->graph_scur = -1;
+}
+
+// Captures two steps into a CUDA graph starting from the current buffer phase.
+cudaError_t capture_two_steps(titan_ctx* ctx) {
+    drop_graph(ctx);
+    const int c0 = ctx->cur, s0 = ctx->scur;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e) return e;
+    cudaError_t e1 = enqueue_step(ctx);
+    cudaError_t e2 = e1 ? e1 : enqueue_step(ctx);
+    e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->cur = c0;
+    ctx->scur = s0;
+    if (e2) {
+        if (g) cudaGraphDestroy(g);
+        return e2;
+    }
+    if (e) return e;
+    e = cudaGraphInstantiate(&ctx->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e) return e;
+    ctx->graph_cur = c0;
+    ctx->graph_scur = s0;
+    return cudaSuccess;
+}
+
+std::string validate(const titan_mesh* m, const titan_params* p) {
+    char buf[256];
+    if (m->ncell <= 0 || m->nface <= 0 || m->nnode <= 0) return "empty mesh";
+    if (m->ncell >= (1LL << 31) - 1 || m->nface >= (1LL << 31) - 1 || m->nnode >= (1LL << 31) - 1)
+        return "mesh too large for 32-bit indices";
+    if (!m->node_xyz || !m->cell_nodes || !m->cell_faces || !m->cell_type || !m->cell_tvd || !m->face_nodes ||
+        !m->face_cells || !m->face_type || !m->face_surf || !m->face_bc)
+        return "null mesh array";
+    if ((m->node_amp == nullptr) != (m->node_phase == nullptr)) return "node_amp and node_phase go together";
+    if (p->move && !m->node_amp) return "move requires node_amp / node_phase";
+    if (p->npassive != 0 && p->npassive != 2) return "npassive must be 0 or 2";
+    if (p->nh < 0 || p->nh > 4) return "nh must be 0..4";
+    if (p->flux_precision != 64 && p->flux_precision != 32) return "flux_precision must be 64 or 32";
+    if (!(p->gamma > 1.0)) return "gamma must exceed 1";
+    for (int64_t i = 0; i < 3 * m->nnode; ++i)
+        if (!std::isfinite(m->node_xyz[i])) return "non-finite node coordinate";
+    for (int64_t c = 0; c < m->ncell; ++c) {
+        for (int k = 0; k < 8; ++k) {
+            const int32_t v = m->cell_nodes[8 * c + k];
+            if (v < 0 || v >= m->nnode) {
+                snprintf(buf, sizeof buf, "cell %lld: node index out of range", (long long)c);
+                return buf;
+            }
+        }
+        for (int s = 0; s < 6; ++s) {
+            const int32_t f = m->cell_faces[6 * c + s];
+            if (f < 0 || f >= m->nface) {
+                snprintf(buf, sizeof buf, "cell %lld: face index out of range", (long long)c);
+                return buf;
+            }
+            if (m->face_cells[2 * f] != c && m->face_cells[2 * f + 1] != c) {
+                snprintf(buf, sizeof buf, "cell %lld lists face %d which does not list it", (long long)c, f);
+                return buf;
+            }
+        }
+        if (m->cell_type[c] < 0 || m->cell_type[c] > 4) return "cell_type out of range";
+    }
+    for (int64_t f = 0; f < m->nface; ++f) {
+        for (int k = 0; k < 4; ++k) {
+            const int32_t v = m->face_nodes[4 * f + k];
+            if (v < 0 || v >= m->nnode) {
+                snprintf(buf, sizeof buf, "face %lld: node index out of range", (long long)f);
+                return buf;
+            }
+        }
+        const int32_t c0 = m->face_cells[2 * f], c1 = m->face_cells[2 * f + 1];
+        const int t = m->face_type[f];
+        if (c0 < 0 || c0 >= m->ncell) {
+            snprintf(buf, sizeof buf, "face %lld: cells[0] out of range", (long long)f);
+            return buf;
+        }
+        if (t < 0 || t > 3) return "face_type out of range";
+        if (m->face_surf[f] < 0 || m->face_surf[f] > 3) return "face_surf out of range";
+        if (t == 0 && (c1 < 0 || c1 >= m->ncell)) {
+            snprintf(buf, sizeof buf, "interior face %lld needs two cells", (long long)f);
+            return buf;
+        }
+        if (t != 0 && c1 != -1) {
+            snprintf(buf, sizeof buf, "boundary face %lld must have one cell", (long long)f);
+            return buf;
+        }
+        if (t == 1 || t == 2) {
+            const int32_t r = m->face_bc[f];
+            if (r < 0 || r >= m->nbc || !m->bc_vals) {
+                snprintf(buf, sizeof buf, "hard boundary face %lld has no fixed values", (long long)f);
+                return buf;
+            }
+        }
+    }
+    return "";
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* titan_version(void) { return "titan-b200 0.1 (sm_100a)"; }
+
+const char* titan_last_error(void) { return g_err.c_str(); }
+
+int titan_destroy(titan_ctx* ctx) {
+    if (!ctx) return TITAN_OK;
+    drop_graph(ctx);
+    void* ptrs[] = {ctx->d_cell_n2o, ctx->d_node_n2o, ctx->d_face_c0, ctx->d_face_c1, ctx->d_face_bc,
+                    ctx->d_face_nodes, ctx->d_face_type, ctx->d_face_surf, ctx->d_face_method, ctx->d_bc_vals,
+                    ctx->d_cell_faces, ctx->d_cell_nodes, ctx->d_cell_type, ctx->d_cell_tvd, ctx->d_node_amp,
+                    ctx->d_node_phase, ctx->d_state[0], ctx->d_state[1], ctx->d_flux, ctx->d_hfl, ctx->d_src,
+                    ctx->d_stage, ctx->d_status};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (int l = 0; l < 2; ++l) {
+        Layer& L = ctx->layer[l];
+        void* lp[] = {L.xyz, L.cc, L.vol, L.fc, L.fn, L.fa, L.fd};
+        for (void* p : lp)
+            if (p) cudaFree(p);
+    }
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return TITAN_OK;
+}
+
+int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
+    if (!m || !p || !out) return fail(TITAN_EINVAL, "null argument");
+    *out = nullptr;
+    const std::string v = validate(m, p);
+    if (!v.empty()) return fail(TITAN_EMESH, v);
+
+    titan_ctx* ctx = new titan_ctx();
+    ctx->ncell = m->ncell;
+    ctx->nface = m->nface;
+    ctx->nnode = m->nnode;
+    ctx->nbc = m->nbc;
+    ctx->prm = *p;
+    ctx->fp32 = p->flux_precision == 32;
+    ctx->ns = 8 + p->npassive;
+    Params& P = ctx->P;
+    P.gamma = p->gamma;
+    P.KFL = p->KFL;
+    P.velosity_inf = p->velosity_inf;
+    P.omega = p->omega;
+    P.par_a_2 = p->par_a_2;
+    P.par_n_H_LISM = p->par_n_H_LISM;
+    P.par_Kn = p->par_Kn;
+    P.beta_switch = p->beta_switch;
+    P.move = p->move;
+    P.soft_fixups = p->soft_fixups;
+    P.method_policy = p->method_policy;
+    P.npassive = p->npassive;
+    P.nh = p->nh;
+    P.TS_hard = p->TS_hard;
+    P.contact_hard = p->contact_hard;
+    P.src_mode = 0;
+
+    auto bail = [&](int code) {
+        titan_destroy(ctx);
+        return code;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e) return bail(fail(TITAN_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)));
+    cudaEventCreate(&ctx->ev[0]);
+    cudaEventCreate(&ctx->ev[1]);
+
+    // --- renumbering and remapped host arrays ---
+    ctx->R = sfc_renumber(m->nnode, m->ncell, m->nface, m->node_xyz, m->cell_nodes, m->face_cells);
+    const Renumbering& R = ctx->R;
+    const int64_t nc = m->ncell, nf = m->nface, nn = m->nnode;
+    std::vector<int32_t> face_c0(nf), face_c1(nf), face_bc(nf), face_nodes(4 * nf);
+    std::vector<int8_t> face_type(nf), face_surf(nf), face_method(nf);
+    for (int64_t f = 0; f < nf; ++f) {
+        const int32_t o = R.face_n2o[f];
+        face_c0[f] = R.cell_o2n[m->face_cells[2 * o]];
+        const int32_t c1 = m->face_cells[2 * o + 1];
+        face_c1[f] = c1 >= 0 ? R.cell_o2n[c1] : -1;
+        face_type[f] = m->face_type[o];
+        face_surf[f] = m->face_surf[o];
+        face_method[f] = m->face_surf[o] != TITAN_SURF_US ? TITAN_HLLD : TITAN_LAX;  // Gran::Get_method
+        face_bc[f] = m->face_bc[o];
+        for (int k = 0; k < 4; ++k) face_nodes[k * nf + f] = R.node_o2n[m->face_nodes[4 * o + k]];
+    }
+    std::vector<int32_t> cell_faces(6 * nc), cell_nodes(8 * nc);
+    std::vector<int8_t> cell_type(nc);
+    std::vector<uint8_t> cell_tvd(nc);
+    for (int64_t c = 0; c < nc; ++c) {
+        const int32_t o = R.cell_n2o[c];
+        for (int s = 0; s < 6; ++s) {
+            const int32_t fo = m->cell_faces[6 * o + s];
+            int32_t fnew = R.face_o2n[fo];
+            if (m->face_cells[2 * fo] != o) fnew |= (int32_t)0x80000000;  // sign -1 in the gather
+            cell_faces[s * nc + c] = fnew;
+        }
+        for (int k = 0; k < 8; ++k) cell_nodes[k * nc + c] = R.node_o2n[m->cell_nodes[8 * o + k]];
+        cell_type[c] = m->cell_type[o];
+        cell_tvd[c] = m->cell_tvd[o];
+    }
+    std::vector<double> xyz(3 * nn), amp, phase;
+    for (int64_t i = 0; i < nn; ++i) {
+        const int32_t o = R.node_n2o[i];
+        for (int k = 0; k < 3; ++k) xyz[k * nn + i] = m->node_xyz[3 * o + k];
+    }
+    if (m->node_amp) {
+        amp.resize(nn);
+        phase.resize(nn);
+        for (int64_t i = 0; i < nn; ++i) {
+            amp[i] = m->node_amp[R.node_n2o[i]];
+            phase[i] = m->node_phase[R.node_n2o[i]];
+        }
+    }
+    std::vector<double> bc(TITAN_NV * std::max<int64_t>(m->nbc, 1), 0.0);
+    for (int64_t r = 0; r < m->nbc; ++r)
+        for (int k = 0; k < TITAN_NV; ++k) bc[k * m->nbc + r] = m->bc_vals[TITAN_NV * r + k];
+
+    // --- device buffers ---
+    int64_t& tot = ctx->dev_bytes;
+#define DA(ptr, n)                                                                                     \
+    do {                                                                                               \
+        cudaError_t e_ = dalloc(&(ptr), (n), &tot);                                                    \
+        if (e_) return bail(fail(TITAN_ENOMEM, std::string("cudaMalloc ") + #ptr + ": " + cudaGetErrorString(e_))); \
+    } while (0)
+    DA(ctx->d_cell_n2o, nc);
+    DA(ctx->d_node_n2o, nn);
+    DA(ctx->d_face_c0, nf);
+    DA(ctx->d_face_c1, nf);
+    DA(ctx->d_face_bc, nf);
+    DA(ctx->d_face_nodes, 4 * nf);
+    DA(ctx->d_face_type, nf);
+    DA(ctx->d_face_surf, nf);
+    DA(ctx->d_face_method, nf);
+    DA(ctx->d_bc_vals, bc.size());
+    DA(ctx->d_cell_faces, 6 * nc);
+    DA(ctx->d_cell_nodes, 8 * nc);
+    DA(ctx->d_cell_type, nc);
+    DA(ctx->d_cell_tvd, nc);
+    if (m->node_amp) {
+        DA(ctx->d_node_amp, nn);
+        DA(ctx->d_node_phase, nn);
+    }
+    const int nlayers = p->move ? 2 : 1;
+    for (int l = 0; l < nlayers; ++l) {
+        Layer& L = ctx->layer[l];
+        DA(L.xyz, 3 * nn);
+        DA(L.cc, 3 * nc);
+        DA(L.vol, nc);
+        DA(L.fc, 3 * nf);
+        DA(L.fn, 3 * nf);
+        DA(L.fa, nf);
+        DA(L.fd, nf);
+    }
+    if (!p->move) ctx->layer[1] = ctx->layer[0];
+    DA(ctx->d_state[0], (size_t)ctx->ns * nc);
+    DA(ctx->d_state[1], (size_t)ctx->ns * nc);
+    {
+        const int n = 9 + p->npassive;
+        ctx->flux_elem = ctx->fp32 ? 4 : 8;
+        ctx->flux_stride = ctx->fp32 ? ((n + 3) & ~3) : ((n + 1) & ~1);
+        char* fp = nullptr;
+        DA(fp, (size_t)nf * ctx->flux_stride * ctx->flux_elem);
+        ctx->d_flux = fp;
+    }
+    if (p->nh > 0) DA(ctx->d_hfl, (size_t)5 * p->nh * nc);
+    DA(ctx->d_stage, (size_t)TITAN_NV * std::max(nc, nn));
+    DA(ctx->d_status, 1);
+#undef DA
+    e = cudaMallocHost((void**)&ctx->h_status, sizeof(DevStatus));
+    if (e) return bail(fail(TITAN_ENOMEM, "cudaMallocHost status"));
+
+    cudaStream_t s = ctx->stream;
+    int rc = TITAN_OK;
+    auto put = [&](auto* d, const auto& h) {
+        if (rc) return;
+        cudaError_t e_ = dput(d, h, s);
+        if (e_) rc = fail(TITAN_ECUDA, cudaGetErrorString(e_));
+    };
+    put(ctx->d_cell_n2o, R.cell_n2o);
+    put(ctx->d_node_n2o, R.node_n2o);
+    put(ctx->d_face_c0, face_c0);
+    put(ctx->d_face_c1, face_c1);
+    put(ctx->d_face_bc, face_bc);
+    put(ctx->d_face_nodes, face_nodes);
+    put(ctx->d_face_type, face_type);
+    put(ctx->d_face_surf, face_surf);
+    put(ctx->d_face_method, face_method);
+    put(ctx->d_bc_vals, bc);
+    put(ctx->d_cell_faces, cell_faces);
+    put(ctx->d_cell_nodes, cell_nodes);
+    put(ctx->d_cell_type, cell_type);
+    put(ctx->d_cell_tvd, cell_tvd);
+    put(ctx->layer[0].xyz, xyz);
+    if (m->node_amp) {
+        put(ctx->d_node_amp, amp);
+        put(ctx->d_node_phase, phase);
+    }
+    if (rc) return bail(rc);
+    e = cudaMemsetAsync(ctx->d_state[0], 0, sizeof(double) * ctx->ns * nc, s);
+    if (!e) e = cudaMemsetAsync(ctx->d_state[1], 0, sizeof(double) * ctx->ns * nc, s);
+    if (!e) e = cudaMemsetAsync(ctx->d_status, 0, sizeof(DevStatus), s);
+    const MeshView M = ctx->view();
+    if (!e) e = launch_cell_geometry(M, ctx->layer[0], s);
+    if (!e) e = launch_face_geometry(M, ctx->layer[0], s);
+    if (!e) e = cudaStreamSynchronize(s);
+    if (e) return bail(fail(TITAN_ECUDA, std::string("create: ") + cudaGetErrorString(e)));
+    *out = ctx;
+    return TITAN_OK;
+}
+
+int titan_set_face_method(titan_ctx* ctx, const int8_t* ns) {
+    if (!ctx || !ns) return fail(TITAN_EINVAL, "null argument");
+    std::vector<int8_t> h(ctx->nface);
+    for (int64_t f = 0; f < ctx->nface; ++f) {
+        const int8_t v = ns[ctx->R.face_n2o[f]];
+        if (v < 0 || v > 3) return fail(TITAN_EINVAL, "n_state must be 0..3");
+        h[f] = v;
+    }
+    CK(cudaMemcpyAsync(ctx->d_face_method, h.data(), h.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TITAN_OK;
+}
+
+int titan_upload_state(titan_ctx* ctx, const double* state) {
+    if (!ctx || !state) return fail(TITAN_EINVAL, "null argument");
+    const int64_t nc = ctx->ncell;
+    CK(cudaMemcpyAsync(ctx->d_stage, state, sizeof(double) * ctx->ns * nc, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_gather(ctx->d_stage, ctx->d_state[ctx->scur], ctx->d_cell_n2o, (int)nc, ctx->ns, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TITAN_OK;
+}
+
+int titan_download_state(titan_ctx* ctx, double* state) {
+    if (!ctx || !state) return fail(TITAN_EINVAL, "null argument");
+    const int64_t nc = ctx->ncell;
+    CK(launch_scatter(ctx->d_state[ctx->scur], ctx->d_stage, ctx->d_cell_n2o, (int)nc, ctx->ns, ctx->stream));
+    CK(cudaMemcpyAsync(state, ctx->d_stage, sizeof(double) * ctx->ns * nc, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = ctx->ns; k < TITAN_NV; ++k) std::memset(state + k * nc, 0, sizeof(double) * nc);
+    return TITAN_OK;
+}
+
+int titan_upload_hfluids(titan_ctx* ctx, const double* h) {
+    if (!ctx || !h) return fail(TITAN_EINVAL, "null argument");
+    if (ctx->prm.nh <= 0) return fail(TITAN_EINVAL, "context was created with nh = 0");
+    const int64_t nc = ctx->ncell;
+    const int nfields = 5 * ctx->prm.nh;
+    for (int k0 = 0; k0 < nfields; k0 += TITAN_NV) {
+        const int nk = std::min(TITAN_NV, nfields - k0);
+        CK(cudaMemcpyAsync(ctx->d_stage, h + (size_t)k0 * nc, sizeof(double) * nk * nc, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(launch_gather(ctx->d_stage, ctx->d_hfl + (size_t)k0 * nc, ctx->d_cell_n2o, (int)nc, nk, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TITAN_OK;
+}
+
+int titan_set_sources(titan_ctx* ctx, const double* src) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    drop_graph(ctx);
+    if (!src) {
+        ctx->use_src = false;
+        return TITAN_OK;
+    }
+    const int64_t nc = ctx->ncell;
+    if (!ctx->d_src) {
+        int64_t dummy = 0;
+        CK(dalloc(&ctx->d_src, (size_t)4 * nc, &dummy));
+        ctx->dev_bytes += dummy;
+    }
+    CK(cudaMemcpyAsync(ctx->d_stage, src, sizeof(double) * 4 * nc, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_gather(ctx->d_stage, ctx->d_src, ctx->d_cell_n2o, (int)nc, 4, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->use_src = true;
+    return TITAN_OK;
+}
+
+int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout, titan_step_info* info) {
+    if (!ctx || !dt_inout || nsteps < 0) return fail(TITAN_EINVAL, "bad argument");
+    const double t0 = t_inout ? *t_inout : 0.0;
+    if (!(*dt_inout > 0.0) || !std::isfinite(*dt_inout)) return fail(TITAN_EINVAL, "dt must be positive");
+    DevStatus init{};
+    init.dt = *dt_inout;
+    init.t = t0;
+    init.dt_next_bits = 0x4197D78400000000ull;  // bits of 1e8, the identity of the CFL minimum
+    cudaStream_t s = ctx->stream;
+    std::memcpy(ctx->h_status, &init, sizeof(DevStatus));
+    CK(cudaMemcpyAsync(ctx->d_status, ctx->h_status, sizeof(DevStatus), cudaMemcpyHostToDevice, s));
+    CK(cudaEventRecord(ctx->ev[0], s));
+    int64_t done = 0;
+    if (ctx->profiling) {
+        drop_graph(ctx);
+        for (; done < nsteps; ++done) CK(enqueue_step(ctx));
+    } else {
+        // The graph holds two steps; its pointers are fixed for one buffer phase.
+        if (nsteps >= 2 && (ctx->graph == nullptr || ctx->graph_cur != ctx->cur || ctx->graph_scur != ctx->scur))
+            CK(capture_two_steps(ctx));
+        for (; done + 2 <= nsteps; done += 2) CK(cudaGraphLaunch(ctx->graph, s));
+        for (; done < nsteps; ++done) {
+            // The graph's two-step period leaves the buffers in the captured
+            // phase; a final odd step runs eagerly.
+            CK(enqueue_step(ctx));
+        }
+    }
+    CK(cudaEventRecord(ctx->ev[1], s));
+    CK(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    const DevStatus& st = *ctx->h_status;
+    *dt_inout = st.dt;
+    if (t_inout) *t_inout = st.t;
+    int status = TITAN_OK;
+    if (st.err_kind != 0) status = st.err_kind >= 20 ? TITAN_ENONFINITE : TITAN_ESOLVER;
+    if (info) {
+        info->steps_done = (int64_t)st.steps_done;
+        info->n_rho_floor = (int64_t)st.n_rho_floor;
+        info->n_p_floor = (int64_t)st.n_p_floor;
+        info->status = status;
+        info->err_kind = st.err_kind;
+        info->err_index = -1;
+        if (st.err_kind != 0) {
+            const int idx = st.err_index;
+            if (st.err_kind >= 20)
+                info->err_index = (idx >= 0 && idx < ctx->ncell) ? ctx->R.cell_n2o[idx] : -1;
+            else
+                info->err_index = (idx >= 0 && idx < ctx->nface) ? ctx->R.face_n2o[idx] : -1;
+        }
+        info->dt_next = st.dt;
+        info->t = st.t;
+        info->gpu_ms = ms;
+    }
+    if (status != TITAN_OK) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "step failed: kind %d at renumbered index %d after %llu steps", st.err_kind,
+                 st.err_index, (unsigned long long)st.steps_done);
+        return fail(status, buf);
+    }
+    return TITAN_OK;
+}
+
+int titan_download_nodes(titan_ctx* ctx, double* xyz) {
+    if (!ctx || !xyz) return fail(TITAN_EINVAL, "null argument");
+    const int64_t nn = ctx->nnode;
+    std::vector<double> h(3 * nn);
+    CK(cudaMemcpyAsync(h.data(), ctx->layer[ctx->cur].xyz, sizeof(double) * 3 * nn, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int64_t i = 0; i < nn; ++i)
+        for (int k = 0; k < 3; ++k) xyz[3 * (int64_t)ctx->R.node_n2o[i] + k] = h[k * nn + i];
+    return TITAN_OK;
+}
+
+int titan_download_geometry(titan_ctx* ctx, double* cc, double* vol, double* fc, double* fn, double* fa) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    const int64_t nc = ctx->ncell, nf = ctx->nface;
+    const Layer& L = ctx->layer[ctx->cur];
+    std::vector<double> hcc(3 * nc), hvol(nc), hfc(3 * nf), hfn(3 * nf), hfa(nf);
+    CK(cudaMemcpyAsync(hcc.data(), L.cc, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(hvol.data(), L.vol, sizeof(double) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(hfc.data(), L.fc, sizeof(double) * 3 * nf, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(hfn.data(), L.fn, sizeof(double) * 3 * nf, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(hfa.data(), L.fa, sizeof(double) * nf, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int64_t c = 0; c < nc; ++c) {
+        const int64_t o = ctx->R.cell_n2o[c];
+        if (cc)
+            for (int k = 0; k < 3; ++k) cc[3 * o + k] = hcc[k * nc + c];
+        if (vol) vol[o] = hvol[c];
+    }
+    for (int64_t f = 0; f < nf; ++f) {
+        const int64_t o = ctx->R.face_n2o[f];
+        for (int k = 0; k < 3; ++k) {
+            if (fc) fc[3 * o + k] = hfc[k * nf + f];
+            if (fn) fn[3 * o + k] = hfn[k * nf + f];
+        }
+        if (fa) fa[o] = hfa[f];
+    }
+    return TITAN_OK;
+}
+
+int titan_download_face_fluxes(titan_ctx* ctx, double* flux) {
+    if (!ctx || !flux) return fail(TITAN_EINVAL, "null argument");
+    const int64_t nf = ctx->nface;
+    const int stride = ctx->flux_stride;
+    std::vector<char> raw((size_t)nf * stride * ctx->flux_elem);
+    CK(cudaMemcpyAsync(raw.data(), ctx->d_flux, raw.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int n = 9 + ctx->prm.npassive;
+    for (int64_t f = 0; f < nf; ++f) {
+        double* dst = flux + 11 * (int64_t)ctx->R.face_n2o[f];
+        for (int k = 0; k < 11; ++k) {
+            double v = 0.0;
+            if (k < n) {
+                if (ctx->fp32)
+                    v = reinterpret_cast<const float*>(raw.data())[(size_t)f * stride + k];
+                else
+                    v = reinterpret_cast<const double*>(raw.data())[(size_t)f * stride + k];
+            }
+            dst[k] = v;
+        }
+    }
+    return TITAN_OK;
+}
+
+int titan_sfc_renumber(int64_t nnode, int64_t ncell, int64_t nface, const double* xyz, const int32_t* cell_nodes,
+                       const int32_t* face_cells, int32_t* cells, int32_t* faces, int32_t* nodes) {
+    if (nnode <= 0 || ncell <= 0 || nface <= 0 || !xyz || !cell_nodes || !face_cells)
+        return fail(TITAN_EINVAL, "bad argument");
+    for (int64_t i = 0; i < 8 * ncell; ++i)
+        if (cell_nodes[i] < 0 || cell_nodes[i] >= nnode) return fail(TITAN_EMESH, "cell node index out of range");
+    for (int64_t f = 0; f < nface; ++f)
+        if (face_cells[2 * f] < 0 || face_cells[2 * f] >= ncell) return fail(TITAN_EMESH, "cells[0] out of range");
+    const Renumbering R = sfc_renumber(nnode, ncell, nface, xyz, cell_nodes, face_cells);
+    if (cells) std::memcpy(cells, R.cell_n2o.data(), sizeof(int32_t) * ncell);
+    if (faces) std::memcpy(faces, R.face_n2o.data(), sizeof(int32_t) * nface);
+    if (nodes) std::memcpy(nodes, R.node_n2o.data(), sizeof(int32_t) * nnode);
+    return TITAN_OK;
+}
+
+int titan_get_permutation(titan_ctx* ctx, int32_t* cells, int32_t* faces, int32_t* nodes) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    if (cells) std::memcpy(cells, ctx->R.cell_n2o.data(), sizeof(int32_t) * ctx->ncell);
+    if (faces) std::memcpy(faces, ctx->R.face_n2o.data(), sizeof(int32_t) * ctx->nface);
+    if (nodes) std::memcpy(nodes, ctx->R.node_n2o.data(), sizeof(int32_t) * ctx->nnode);
+    return TITAN_OK;
+}
+
+int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, const double* w, const double* q1,
+                        const double* q2, int32_t flags, int32_t precision, double gamma, double* flux,
+                        double* ds, int32_t* rc) {
+    if (n < 0 || (n > 0 && (!n_state || !nrm || !w || !q1 || !q2 || !flux || !ds || !rc)))
+        return fail(TITAN_EINVAL, "bad argument");
+    if (precision != 64 && precision != 32) return fail(TITAN_EINVAL, "precision must be 64 or 32");
+    if (n == 0) return TITAN_OK;
+    signed char* dns = nullptr;
+    double *dn = nullptr, *dw = nullptr, *d1 = nullptr, *d2 = nullptr, *df = nullptr, *dd = nullptr;
+    int* drc = nullptr;
+    int64_t tot = 0;
+    cudaError_t e = cudaSuccess;
+    if (!e) e = dalloc(&dns, n, &tot);
+    if (!e) e = dalloc(&dn, 3 * n, &tot);
+    if (!e) e = dalloc(&dw, n, &tot);
+    if (!e) e = dalloc(&d1, 8 * n, &tot);
+    if (!e) e = dalloc(&d2, 8 * n, &tot);
+    if (!e) e = dalloc(&df, 8 * n, &tot);
+    if (!e) e = dalloc(&dd, 3 * n, &tot);
+    if (!e) e = dalloc(&drc, n, &tot);
+    if (!e) e = cudaMemcpy(dns, n_state, n, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(dn, nrm, sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(dw, w, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d1, q1, sizeof(double) * 8 * n, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d2, q2, sizeof(double) * 8 * n, cudaMemcpyHostToDevice);
+    if (!e)
+        e = precision == 64 ? launch_riemann_batch_fp64(n, dns, dn, dw, d1, d2, df, dd, drc, flags, gamma, 0)
+                            : launch_riemann_batch_fp32(n, dns, dn, dw, d1, d2, df, dd, drc, flags, gamma, 0);
+    if (!e) e = cudaMemcpy(flux, df, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost);
+    if (!e) e = cudaMemcpy(ds, dd, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost);
+    if (!e) e = cudaMemcpy(rc, drc, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    void* ps[] = {dns, dn, dw, d1, d2, df, dd, drc};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (e) return fail(TITAN_ECUDA, std::string("riemann_batch: ") + cudaGetErrorString(e));
+    return TITAN_OK;
+}
+
+void* titan_stream(titan_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int titan_set_profiling(titan_ctx* ctx, int32_t on) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    ctx->profiling = on != 0;
+    if (on) ctx->clocks.clear();
+    return TITAN_OK;
+}
+
+int titan_kernel_times(titan_ctx* ctx, const char** names, double* total_ms, int64_t* launches, int32_t cap) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    // names point into the map's keys: valid until profiling is switched on again
+    int i = 0;
+    for (auto& kv : ctx->clocks) {
+        if (i >= cap) break;
+        if (names) names[i] = kv.first.c_str();
+        if (total_ms) total_ms[i] = kv.second.ms;
+        if (launches) launches[i] = kv.second.launches;
+        ++i;
+    }
+    return i;
+}
+
+int64_t titan_device_bytes(titan_ctx* ctx) { return ctx ? ctx->dev_bytes : 0; }
+
+}  // extern "C"

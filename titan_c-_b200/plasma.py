@@ -1,0 +1,186 @@
+"""Python view of the C ABI, shaped like the reference's plasma loop.
+
+``PlasmaStep`` owns one titan context: the flattened mesh (Setka's All_Cell /
+All_Gran / All_Yzel), the cell state (Cell::parameters) and the step loop of
+Setka::Go (TITAN/source/Setka_physics.cpp:1484-2278). ``chlld`` is the batched
+form of Phys_param::chlld (TITAN/source/Phys_param.cpp:882-1878) on the GPU.
+Errors surface as TitanError carrying the C status code.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import native as N
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class PlasmaStep:
+    """One B200 context for a mesh; `go(steps)` advances the plasma."""
+
+    def __init__(self, mesh: dict, params: dict):
+        L = N.lib()
+        self._keep = {}
+
+        def keep(name, a, dt):
+            arr = None if a is None else np.ascontiguousarray(a, dtype=dt)
+            self._keep[name] = arr
+            return arr
+
+        xyz = keep("xyz", mesh["node_xyz"], np.float64)
+        cn = keep("cn", mesh["cell_nodes"], np.int32)
+        cf = keep("cf", mesh["cell_faces"], np.int32)
+        ct = keep("ct", mesh["cell_type"], np.int8)
+        cv = keep("cv", mesh["cell_tvd"], np.uint8)
+        fnd = keep("fn", mesh["face_nodes"], np.int32)
+        fcl = keep("fc", mesh["face_cells"], np.int32)
+        ft = keep("ft", mesh["face_type"], np.int8)
+        fs = keep("fs", mesh["face_surf"], np.int8)
+        fb = keep("fb", mesh["face_bc"], np.int32)
+        bc = keep("bc", mesh["bc_vals"], np.float64)
+        amp = keep("amp", mesh.get("node_amp"), np.float64)
+        ph = keep("ph", mesh.get("node_phase"), np.float64)
+        self.ncell = cn.shape[0]
+        self.nface = fnd.shape[0]
+        self.nnode = xyz.shape[0]
+        m = N.TitanMesh()
+        m.nnode, m.ncell, m.nface, m.nbc = self.nnode, self.ncell, self.nface, bc.shape[0]
+        m.node_xyz, m.cell_nodes, m.cell_faces = N.ptr(xyz), N.ptr(cn, N.I32), N.ptr(cf, N.I32)
+        m.cell_type, m.cell_tvd = N.ptr(ct, N.I8), N.ptr(cv, N.U8)
+        m.face_nodes, m.face_cells = N.ptr(fnd, N.I32), N.ptr(fcl, N.I32)
+        m.face_type, m.face_surf, m.face_bc = N.ptr(ft, N.I8), N.ptr(fs, N.I8), N.ptr(fb, N.I32)
+        m.bc_vals = N.ptr(bc) if bc.shape[0] else None
+        m.node_amp, m.node_phase = N.ptr(amp), N.ptr(ph)
+        p = N.TitanParams()
+        for k, _ in N.TitanParams._fields_:
+            setattr(p, k, params[k])
+        self.params = dict(params)
+        ctx = ctypes.c_void_p()
+        N.check(L.titan_create(ctypes.byref(m), ctypes.byref(p), ctypes.byref(ctx)))
+        self._ctx = ctx
+        self._lib = L
+        self._keep.clear()  # the library copied everything
+        self.dt = 1e-5      # Setka::Go starts with time = 1e-5 (Setka_physics.cpp:1582)
+        self.t = 0.0
+        self.last_info = None
+
+    # -- context management ------------------------------------------------
+    def close(self):
+        if getattr(self, "_ctx", None) is not None and self._ctx.value:
+            self._lib.titan_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    # -- data --------------------------------------------------------------
+    def set_face_method(self, n_state: np.ndarray):
+        a = np.ascontiguousarray(n_state, dtype=np.int8)
+        N.check(self._lib.titan_set_face_method(self._ctx, N.ptr(a, N.I8)))
+
+    def upload_state(self, state: np.ndarray):
+        a = np.ascontiguousarray(state, dtype=np.float64)
+        assert a.shape == (N.NV, self.ncell)
+        N.check(self._lib.titan_upload_state(self._ctx, N.ptr(a)))
+
+    def download_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty((N.NV, self.ncell)) if out is None else out
+        N.check(self._lib.titan_download_state(self._ctx, N.ptr(out)))
+        return out
+
+    def upload_hfluids(self, h: np.ndarray):
+        a = np.ascontiguousarray(h, dtype=np.float64)
+        N.check(self._lib.titan_upload_hfluids(self._ctx, N.ptr(a)))
+
+    def set_sources(self, s: np.ndarray | None):
+        a = None if s is None else np.ascontiguousarray(s, dtype=np.float64)
+        N.check(self._lib.titan_set_sources(self._ctx, N.ptr(a)))
+
+    def go(self, steps: int) -> dict:
+        """`steps` plasma steps; dt and t carry over between calls like Setka::Go's loop."""
+        dt = ctypes.c_double(self.dt)
+        t = ctypes.c_double(self.t)
+        info = N.TitanStepInfo()
+        rc = self._lib.titan_step(self._ctx, int(steps), ctypes.byref(dt), ctypes.byref(t), ctypes.byref(info))
+        self.last_info = {k: getattr(info, k) for k, _ in N.TitanStepInfo._fields_}
+        if rc == N.TITAN_OK:
+            self.dt, self.t = dt.value, t.value
+        N.check(rc)
+        return self.last_info
+
+    def nodes(self) -> np.ndarray:
+        out = np.empty((self.nnode, 3))
+        N.check(self._lib.titan_download_nodes(self._ctx, N.ptr(out)))
+        return out
+
+    def geometry(self):
+        cc = np.empty((self.ncell, 3))
+        vol = np.empty(self.ncell)
+        fc = np.empty((self.nface, 3))
+        fn = np.empty((self.nface, 3))
+        fa = np.empty(self.nface)
+        N.check(self._lib.titan_download_geometry(self._ctx, N.ptr(cc), N.ptr(vol), N.ptr(fc), N.ptr(fn),
+                                                  N.ptr(fa)))
+        return dict(cell_center=cc, cell_volume=vol, face_center=fc, face_normal=fn, face_area=fa)
+
+    def face_fluxes(self) -> np.ndarray:
+        out = np.empty((self.nface, 11))
+        N.check(self._lib.titan_download_face_fluxes(self._ctx, N.ptr(out)))
+        return out
+
+    def permutation(self):
+        c = np.empty(self.ncell, dtype=np.int32)
+        f = np.empty(self.nface, dtype=np.int32)
+        n = np.empty(self.nnode, dtype=np.int32)
+        N.check(self._lib.titan_get_permutation(self._ctx, N.ptr(c, N.I32), N.ptr(f, N.I32), N.ptr(n, N.I32)))
+        return c, f, n
+
+    def stream(self) -> int:
+        return int(self._lib.titan_stream(self._ctx) or 0)
+
+    def set_profiling(self, on: bool):
+        N.check(self._lib.titan_set_profiling(self._ctx, int(on)))
+
+    def kernel_times(self) -> dict:
+        cap = 16
+        names = (ctypes.c_char_p * cap)()
+        ms = np.zeros(cap)
+        cnt = np.zeros(cap, dtype=np.int64)
+        n = self._lib.titan_kernel_times(self._ctx, names, N.ptr(ms), N.ptr(cnt, N.I64), cap)
+        return {names[i].decode(): (float(ms[i]), int(cnt[i])) for i in range(n)}
+
+    def device_bytes(self) -> int:
+        return int(self._lib.titan_device_bytes(self._ctx))
+
+
+def chlld(n_state, nrm, w, q1, q2, *, flags: int = 0, precision: int = 64, gamma: float = 5.0 / 3.0):
+    """Batched Phys_param::chlld on the GPU. Returns (flux [n,8], ds [n,3], rc [n])."""
+    q1 = np.ascontiguousarray(q1, dtype=np.float64)
+    q2 = np.ascontiguousarray(q2, dtype=np.float64)
+    n = q1.shape[0]
+    ns = np.ascontiguousarray(np.broadcast_to(np.asarray(n_state, dtype=np.int8), (n,)))
+    nrm = np.ascontiguousarray(nrm, dtype=np.float64)
+    w = np.ascontiguousarray(np.broadcast_to(np.asarray(w, dtype=np.float64), (n,)))
+    flux = np.empty((n, 8))
+    ds = np.empty((n, 3))
+    rc = np.empty(n, dtype=np.int32)
+    N.check(N.lib().titan_riemann_batch(n, N.ptr(ns, N.I8), N.ptr(nrm), N.ptr(w), N.ptr(q1), N.ptr(q2), flags,
+                                        precision, gamma, N.ptr(flux), N.ptr(ds), N.ptr(rc, N.I32)))
+    return flux, ds, rc

@@ -134,6 +134,12 @@ def run_ours(args, rank, world):
     F = m["face_nodes"].shape[0]
     step = pkg.PlasmaStep(m, p)
     step.upload_state(st)
+    if args.tuning == "auto":
+        tuning = step.autotune(reps=3)
+    else:
+        fv, cv = (int(x) for x in args.tuning.split(","))
+        step.set_tuning(fv, cv)
+        tuning = step.tuning()
     kernels_per_step = 5 if p["move"] else 2
     flux_name = "face_flux_fp32" if args.flux == 32 else "face_flux_fp64"
 
@@ -169,7 +175,7 @@ def run_ours(args, rank, world):
     # end to end through the C ABI with pinned host buffers
     host = torch.empty((10, C), dtype=torch.float64, pin_memory=True).numpy()
     host[:] = step.download_state()
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = max(3, min(args.steps, 20))
     barrier()
     t0 = time.perf_counter()
     ev0.record(stream)
@@ -200,7 +206,7 @@ def run_ours(args, rank, world):
         "data": "synthetic (seeded heliosphere-like shell; no external data)",
         "config": {"workload": f"heliosphere shell 6x{args.nq}x{args.nq}x{args.nlayer} = {C} cells, {F} faces, "
                                f"ALE, HLLD/HLLC, FP{args.flux} flux", "cells": C, "faces": F,
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "tuning": tuning,
                    "l2": "inputs larger than L2 (state 141 MB + face data 0.5 GB), no flush"},
         "face_fluxes_per_s": world * F * args.steps / (ms / 1e3),
         "e2e": {"value": world * C * e2e_steps / e2e_wall, "unit": UNIT,
@@ -265,13 +271,14 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nq", type=int, default=96)
     ap.add_argument("--nlayer", type=int, default=40)
     ap.add_argument("--flux", type=int, default=64, choices=[64, 32])
     ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--tuning", default="auto", help="auto, or 'face_variant,cell_variant'")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     args = ap.parse_args()
     if args.impl == "reference":

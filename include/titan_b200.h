@@ -167,6 +167,18 @@ int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, con
                         const double* q2, int32_t flags, int32_t precision, double gamma, double* flux,
                         double* ds, int32_t* rc);
 
+/* Launch-shape autotuner (no reference counterpart: the reference's OpenMP
+ * loops have no launch shapes). Times every face-flux variant (threads per
+ * block x minimum resident blocks per SM) and every cell-update block size on
+ * this context's mesh and state, `reps` launches each, and keeps the fastest.
+ * Call after titan_upload_state. With a cache file, a line for the same mesh
+ * size and step options is reused instead of timing, and new results are
+ * appended. The device status is reset, so call it between runs. */
+int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path);
+int titan_set_tuning(titan_ctx* ctx, int32_t face_variant, int32_t cell_variant);
+int titan_get_tuning(titan_ctx* ctx, int32_t* face_variant, int32_t* cell_variant, int32_t* face_block,
+                     int32_t* face_min_blocks, int32_t* cell_block);
+
 /* The CUDA stream of the context (cudaStream_t), for event timing by callers. */
 void* titan_stream(titan_ctx* ctx);
 

@@ -76,8 +76,8 @@ def _pair(T, mesh, params, method=None, hf=None):
 
 
 def test_geometry_matches_oracle(T, oracle_lib):
-    m = T.mesh.shell_mesh(8, 6)
-    gpu, run = _pair(T, m, T.problems.params())
+    m, p, _, _ = T.problems.heliosphere_shell(nq=8, nlayer=6, move=False)
+    gpu, run = _pair(T, m, p)
     a, b = gpu.geometry(), run.geometry()
     for k in a:
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
@@ -85,8 +85,8 @@ def test_geometry_matches_oracle(T, oracle_lib):
 
 
 def test_state_roundtrip_is_bitexact(T):
-    m = T.mesh.shell_mesh(8, 5)
-    gpu = T.PlasmaStep(m, T.problems.params(npassive=2))
+    m, p, _, _ = T.problems.heliosphere_shell(nq=8, nlayer=5, npassive=2)
+    gpu = T.PlasmaStep(m, p)
     rng = np.random.default_rng(1)
     st = rng.standard_normal((10, m["cell_nodes"].shape[0]))
     gpu.upload_state(st)
@@ -219,3 +219,43 @@ def test_nonfinite_input_is_reported_and_context_recovers(T):
     g.go(2)
     assert np.all(np.isfinite(g.download_state()))
     g.close()
+
+
+def test_every_launch_shape_gives_identical_results(T):
+    m, p, st, hf = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, zones=True, npassive=2)
+    outs = []
+    for fv in range(6):
+        for cv in range(3):
+            if cv and fv:
+                continue
+            g = T.PlasmaStep(m, p)
+            g.set_tuning(fv, cv)
+            g.upload_state(st)
+            g.go(4)
+            outs.append(g.download_state())
+            g.close()
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+
+
+def test_autotune_picks_a_shape_and_caches_it(T, tmp_path):
+    m, p, st, meth = T.problems.brio_wu_cube(16)
+    cache = str(tmp_path / "tune.txt")
+    g = T.PlasmaStep(m, p)
+    g.set_face_method(meth)
+    g.upload_state(st)
+    t1 = g.autotune(reps=2, cache=cache)
+    assert 0 <= t1["face_variant"] < 6 and 0 <= t1["cell_variant"] < 3
+    assert open(cache).read().count("|") == 1
+    g2 = T.PlasmaStep(m, p)
+    g2.upload_state(st)
+    assert g2.autotune(reps=2, cache=cache) == t1          # served from the cache
+    # tuning resets the device status: stepping afterwards still matches a fresh context
+    g.go(3)
+    g3 = T.PlasmaStep(m, p)
+    g3.set_face_method(meth)
+    g3.upload_state(st)
+    g3.go(3)
+    assert np.array_equal(g.download_state(), g3.download_state())
+    for x in (g, g2, g3):
+        x.close()

@@ -22,36 +22,67 @@ cudaError_t launch_face_geometry(const MeshView& M, const Layer& L, cudaStream_t
     return cudaGetLastError();
 }
 
-cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, cudaStream_t s) {
-    const unsigned int g = blocks_for(a.M.nface, kFaceBlock);
-    if (nk == 0 && !move) face_flux_kernel<double, double, 0, false><<<g, kFaceBlock, 0, s>>>(a);
-    else if (nk == 0 && move) face_flux_kernel<double, double, 0, true><<<g, kFaceBlock, 0, s>>>(a);
-    else if (nk == 2 && !move) face_flux_kernel<double, double, 2, false><<<g, kFaceBlock, 0, s>>>(a);
-    else if (nk == 2 && move) face_flux_kernel<double, double, 2, true><<<g, kFaceBlock, 0, s>>>(a);
-    else return cudaErrorInvalidValue;
+template <typename R, int NK, bool MOVE>
+static cudaError_t face_flux_variant(const FaceArgs& a, int v, cudaStream_t s) {
+    switch (v) {
+#define TITAN_FACE_CASE(i)                                                                              \
+    case i: {                                                                                         \
+        constexpr FaceVariant fv = kFaceVariant[i];                                                   \
+        face_flux_kernel<R, R, NK, MOVE, fv.block, fv.min_blocks>                                     \
+            <<<blocks_for(a.M.nface, fv.block), fv.block, 0, s>>>(a);                                 \
+        break;                                                                                        \
+    }
+        TITAN_FACE_CASE(0)
+        TITAN_FACE_CASE(1)
+        TITAN_FACE_CASE(2)
+        TITAN_FACE_CASE(3)
+        TITAN_FACE_CASE(4)
+        TITAN_FACE_CASE(5)
+#undef TITAN_FACE_CASE
+        default:
+            return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
+}
+
+cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s) {
+    if (nk == 0 && !move) return face_flux_variant<double, 0, false>(a, variant, s);
+    if (nk == 0 && move) return face_flux_variant<double, 0, true>(a, variant, s);
+    if (nk == 2 && !move) return face_flux_variant<double, 2, false>(a, variant, s);
+    if (nk == 2 && move) return face_flux_variant<double, 2, true>(a, variant, s);
+    return cudaErrorInvalidValue;
+}
+
+template <typename FT, int NK, bool MOVE, int BS>
+static void cell_update_src(const CellArgs& a, int src, cudaStream_t s) {
+    const unsigned int g = blocks_for(a.M.ncell, BS);
+    if (src == 0) cell_update_kernel<FT, NK, MOVE, 0, BS><<<g, BS, 0, s>>>(a);
+    else if (src == 1) cell_update_kernel<FT, NK, MOVE, 1, BS><<<g, BS, 0, s>>>(a);
+    else cell_update_kernel<FT, NK, MOVE, 2, BS><<<g, BS, 0, s>>>(a);
 }
 
 template <typename FT, int NK, bool MOVE>
-static void cell_update_src(const CellArgs& a, int src, unsigned int g, cudaStream_t s) {
-    if (src == 0) cell_update_kernel<FT, NK, MOVE, 0><<<g, kCellBlock, 0, s>>>(a);
-    else if (src == 1) cell_update_kernel<FT, NK, MOVE, 1><<<g, kCellBlock, 0, s>>>(a);
-    else cell_update_kernel<FT, NK, MOVE, 2><<<g, kCellBlock, 0, s>>>(a);
-}
-
-template <typename FT>
-static cudaError_t cell_update_ft(const CellArgs& a, int nk, bool move, int src, cudaStream_t s) {
-    const unsigned int g = blocks_for(a.M.ncell, kCellBlock);
-    if (nk == 0 && !move) cell_update_src<FT, 0, false>(a, src, g, s);
-    else if (nk == 0 && move) cell_update_src<FT, 0, true>(a, src, g, s);
-    else if (nk == 2 && !move) cell_update_src<FT, 2, false>(a, src, g, s);
-    else if (nk == 2 && move) cell_update_src<FT, 2, true>(a, src, g, s);
+static cudaError_t cell_update_variant(const CellArgs& a, int src, int v, cudaStream_t s) {
+    if (v == 0) cell_update_src<FT, NK, MOVE, kCellBlock[0]>(a, src, s);
+    else if (v == 1) cell_update_src<FT, NK, MOVE, kCellBlock[1]>(a, src, s);
+    else if (v == 2) cell_update_src<FT, NK, MOVE, kCellBlock[2]>(a, src, s);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
-cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, cudaStream_t s) {
-    return flux_fp32 ? cell_update_ft<float>(a, nk, move, src, s) : cell_update_ft<double>(a, nk, move, src, s);
+template <typename FT>
+static cudaError_t cell_update_ft(const CellArgs& a, int nk, bool move, int src, int v, cudaStream_t s) {
+    if (nk == 0 && !move) return cell_update_variant<FT, 0, false>(a, src, v, s);
+    if (nk == 0 && move) return cell_update_variant<FT, 0, true>(a, src, v, s);
+    if (nk == 2 && !move) return cell_update_variant<FT, 2, false>(a, src, v, s);
+    if (nk == 2 && move) return cell_update_variant<FT, 2, true>(a, src, v, s);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, int variant,
+                               cudaStream_t s) {
+    return flux_fp32 ? cell_update_ft<float>(a, nk, move, src, variant, s)
+                     : cell_update_ft<double>(a, nk, move, src, variant, s);
 }
 
 cudaError_t launch_gather(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s) {

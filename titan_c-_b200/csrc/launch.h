@@ -7,18 +7,27 @@
 
 namespace titan {
 
-constexpr int kFaceBlock = 128;
-constexpr int kCellBlock = 256;
 constexpr int kGeomBlock = 256;
+
+// Launch shapes the autotuner chooses from: threads per block and the minimum
+// resident blocks per SM requested from the register allocator.
+struct FaceVariant {
+    int block, min_blocks;
+};
+constexpr int kFaceVariants = 6;
+constexpr FaceVariant kFaceVariant[kFaceVariants] = {{128, 1}, {128, 3}, {128, 4}, {256, 2}, {64, 8}, {128, 5}};
+constexpr int kCellVariants = 3;
+constexpr int kCellBlock[kCellVariants] = {256, 128, 512};
 
 cudaError_t launch_move_nodes(const MeshView& M, const Params& P, const double* xyz1, double* xyz2,
                               const DevStatus* st, cudaStream_t s);
 cudaError_t launch_cell_geometry(const MeshView& M, const Layer& L, cudaStream_t s);
 cudaError_t launch_face_geometry(const MeshView& M, const Layer& L, cudaStream_t s);
-cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, cudaStream_t s);
-cudaError_t launch_face_flux_fp32(const FaceArgs& a, int nk, bool move, cudaStream_t s);
+cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s);
+cudaError_t launch_face_flux_fp32(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s);
 // flux_fp32: the flux buffer holds floats
-cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, cudaStream_t s);
+cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, int variant,
+                               cudaStream_t s);
 cudaError_t launch_gather(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s);
 cudaError_t launch_scatter(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s);
 cudaError_t launch_riemann_batch_fp64(long long n, const signed char* ns, const double* nrm, const double* w,

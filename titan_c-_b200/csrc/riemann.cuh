@@ -6,14 +6,19 @@
 // get_bazis (TITAN/source/Help_funk.cpp:219-232), with the Powell-form normal
 // B flux -SN*(bR-bL) - w*bn and the sqrt(4*pi) Gaussian rescale of B.
 //
-// The arithmetic is written so that, in double precision and compiled without
-// FMA contraction (the FP64 translation unit uses -fmad=false), every value
-// rounds exactly as the reference's x86-64 build does: same expression trees,
-// same branch order (including the HLLD zone-5 overwrite when |bn| <= epsb and
-// the Lax speeds that replace SL/SR after dsl/dsr were recorded). The single
-// precision instantiation runs the same algorithm in float.
+// Every value is written with the reference's expression tree, so that in
+// double precision, compiled without FMA contraction (the FP64 translation
+// unit uses -fmad=false), it rounds exactly as the reference's x86-64 build.
+// The evaluation ORDER differs where that saves work on the GPU: the HLLC and
+// HLLD wave region ("zone") is decided first from the wave speeds, replaying
+// the reference's sequence of tests (including the HLLD zone-5 overwrite at
+// ties and when |bn| <= epsb), and only the star states that region needs are
+// formed; the averaged-state speed is formed only for the estimates that use
+// it. The single precision instantiation runs the same algorithm in float.
 #pragma once
+#ifdef __CUDACC__
 #include <cuda_runtime.h>
+#endif
 #include <math.h>
 
 namespace titan {
@@ -22,7 +27,7 @@ template <typename R>
 struct RConst;
 template <>
 struct RConst<double> {
-    // sqrt(4*pi) rounded to double, as TITAN/source/Header.h:99 computes it
+    // sqrt(4*pi) rounded to double, the value TITAN/source/Header.h:99 computes
     static __device__ __forceinline__ double spi4() { return 3.5449077018110318; }
     static __device__ __forceinline__ double epsb() { return 1E-4; }
     static __device__ __forceinline__ double tt_eps() { return 0.000000001; }
@@ -74,6 +79,27 @@ struct RiemannFlags {
     int n_disc;
 };
 
+// Flux F and conserved vector U of one side in the face frame.
+template <typename R>
+__device__ __forceinline__ void side_flux(R r, const R v[3], const R b[3], R pt, R e, R sbv, R F[8], R U[8]) {
+    F[0] = r * v[0];
+    F[1] = r * v[0] * v[0] + pt - b[0] * b[0];
+    F[2] = r * v[0] * v[1] - b[0] * b[1];
+    F[3] = r * v[0] * v[2] - b[0] * b[2];
+    F[4] = (e + pt) * v[0] - b[0] * sbv;
+    F[5] = R(0);
+    F[6] = v[0] * b[1] - v[1] * b[0];
+    F[7] = v[0] * b[2] - v[2] * b[0];
+    U[0] = r;
+    U[1] = r * v[0];
+    U[2] = r * v[1];
+    U[3] = r * v[2];
+    U[4] = e;
+    U[5] = b[0];
+    U[6] = b[1];
+    U[7] = b[2];
+}
+
 // Returns 0 on success; 1/2/3 where the reference would abort (no admissible
 // wave region, i.e. NaN speeds) for the HLL/HLLC/HLLD branches, 4 for a bad
 // n_state. q1/q2: rho, u, v, w, p, Bx, By, Bz (Gaussian B). qout: 8 fluxes.
@@ -89,8 +115,6 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
     const R bx1 = q1[5] / spi4, by1 = q1[6] / spi4, bz1 = q1[7] / spi4;
     const R r2 = q2[0], u2 = q2[1], v2 = q2[2], w2 = q2[3], p2 = q2[4];
     const R bx2 = q2[5] / spi4, by2 = q2[6] / spi4, bz2 = q2[7] / spi4;
-    const R ro = (r2 + r1) / R(2);
-    const R ap = (p2 + p1) / R(2);
 
     R n[3] = {nrm[0], nrm[1], nrm[2]}, t[3], m[3];
     face_basis(n, t, m);
@@ -109,7 +133,7 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
     bR[1] = t[0] * bx2 + t[1] * by2 + t[2] * bz2;
     bR[2] = m[0] * bx2 + m[1] * by2 + m[2] * bz2;
 
-    // fast magnetosonic speeds of the two states and of their average
+    // fast magnetosonic speeds of the two states
     const R aaL = bL[0] / sqrt(r1);
     const R b2L = bL[0] * bL[0] + bL[1] * bL[1] + bL[2] * bL[2];
     const R b21 = b2L / r1;
@@ -128,16 +152,22 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
     const R cfR = (qp + qm) / R(2);
     const R ptR = p2 + b2R / R(2);
 
-    const R aC = (aaL + aaR) / R(2);
-    const R b2o = (b22 + b21) / R(2);
-    const R cC = sqrt(gamma * ap / ro);
-    qp = sqrt(b2o + cC * (cC + R(2) * aC));
-    qm = sqrt(b2o + cC * (cC - R(2) * aC));
-    const R cfC = (qp + qm) / R(2);
+    const int n_disc = fl.left_ydar ? 2 : fl.n_disc;
+    // speed of the averaged state: only the n_disc 1/2 estimates and Lax use it
+    R cfC = R(0);
+    if (n_state == 0 || n_disc == 1 || n_disc == 2) {
+        const R ro = (r2 + r1) / R(2);
+        const R ap = (p2 + p1) / R(2);
+        const R aC = (aaL + aaR) / R(2);
+        const R b2o = (b22 + b21) / R(2);
+        const R cC = sqrt(gamma * ap / ro);
+        const R qpc = sqrt(b2o + cC * (cC + R(2) * aC));
+        const R qmc = sqrt(b2o + cC * (cC - R(2) * aC));
+        cfC = (qpc + qmc) / R(2);
+    }
     const R vC1 = (vL[0] + vR[0]) / R(2);
 
     R SL = R(0), SR = R(0);
-    const int n_disc = fl.left_ydar ? 2 : fl.n_disc;
     if (n_disc == 0) {
         SL = rmin(vL[0] - cfL, vR[0] - cfR);
         SR = rmax(vL[0] + cfL, vR[0] + cfR);
@@ -172,229 +202,142 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
         SL = -TR0;
     }
 
-    const R upt1 = (u1 * u1 + v1 * v1 + w1 * w1) / R(2);
+    // energies and v.B of the two states (original Cartesian frame)
     const R sbv1 = u1 * bx1 + v1 * by1 + w1 * bz1;
-    const R upt2 = (u2 * u2 + v2 * v2 + w2 * w2) / R(2);
     const R sbv2 = u2 * bx2 + v2 * by2 + w2 * bz2;
-    const R e1 = p1 / g1 + r1 * upt1 + b2L / R(2);
-    const R e2 = p2 / g1 + r2 * upt2 + b2R / R(2);
+    auto energy1 = [&]() { return p1 / g1 + r1 * ((u1 * u1 + v1 * v1 + w1 * w1) / R(2)) + b2L / R(2); };
+    auto energy2 = [&]() { return p2 / g1 + r2 * ((u2 * u2 + v2 * v2 + w2 * w2) / R(2)) + b2R / R(2); };
 
-    R FL[8], FR[8], UL[8], UR[8], UZ[8];
-    FL[0] = r1 * vL[0];
-    FL[1] = r1 * vL[0] * vL[0] + ptL - bL[0] * bL[0];
-    FL[2] = r1 * vL[0] * vL[1] - bL[0] * bL[1];
-    FL[3] = r1 * vL[0] * vL[2] - bL[0] * bL[2];
-    FL[4] = (e1 + ptL) * vL[0] - bL[0] * sbv1;
-    FL[5] = R(0);
-    FL[6] = vL[0] * bL[1] - vL[1] * bL[0];
-    FL[7] = vL[0] * bL[2] - vL[2] * bL[0];
-    FR[0] = r2 * vR[0];
-    FR[1] = r2 * vR[0] * vR[0] + ptR - bR[0] * bR[0];
-    FR[2] = r2 * vR[0] * vR[1] - bR[0] * bR[1];
-    FR[3] = r2 * vR[0] * vR[2] - bR[0] * bR[2];
-    FR[4] = (e2 + ptR) * vR[0] - bR[0] * sbv2;
-    FR[5] = R(0);
-    FR[6] = vR[0] * bR[1] - vR[1] * bR[0];
-    FR[7] = vR[0] * bR[2] - vR[2] * bR[0];
-    UL[0] = r1;
-    UL[4] = e1;
-    UR[0] = r2;
-    UR[4] = e2;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        UL[i + 1] = r1 * vL[i];
-        UL[i + 5] = bL[i];
-        UR[i + 1] = r2 * vR[i];
-        UR[i + 5] = bR[i];
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) UZ[k] = (SR * UR[k] - SL * UL[k] + FL[k] - FR[k]) / (SR - SL);
-
-    R FLk[NK > 0 ? NK : 1], FRk[NK > 0 ? NK : 1], UZk[NK > 0 ? NK : 1];
+    R FLk[NK > 0 ? NK : 1], FRk[NK > 0 ? NK : 1];
 #pragma unroll
     for (int i = 0; i < NK; ++i) {
         FLk[i] = kl[i] * vL[0];
         FRk[i] = kr[i] * vR[0];
-        UZk[i] = (SR * kr[i] - SL * kl[i] + FLk[i] - FRk[i]) / (SR - SL);
     }
-    if (fl.null_bn) UZ[5] = R(0);
 
-    R qv[3], qb[3];
-    R SN, wbn;
-
-    if (n_state <= 1) {
-        R FW[8], FWk[NK > 0 ? NK : 1];
+    R out[8];
+    if (n_state <= 1) {  // Lax / HLL
+        const R e1 = energy1(), e2 = energy2();
+        R FL[8], FR[8], UL[8], UR[8], UZ[8];
+        side_flux(r1, vL, bL, ptL, e1, sbv1, FL, UL);
+        side_flux(r2, vR, bR, ptR, e2, sbv2, FR, UR);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) UZ[k] = (SR * UR[k] - SL * UL[k] + FL[k] - FR[k]) / (SR - SL);
+        if (fl.null_bn) UZ[5] = R(0);
+        R UZk[NK > 0 ? NK : 1];
+#pragma unroll
+        for (int i = 0; i < NK; ++i) UZk[i] = (SR * kr[i] - SL * kl[i] + FLk[i] - FRk[i]) / (SR - SL);
         if (fl.left_ydar) wv = SL;
         R TL = SL, TR = SR;
+        const R* Uw;
+        const R* Kw;
         if (SL > wv || fl.left_ydar) {
             TL = R(0);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) FW[k] = wv * UL[k];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) FWk[k] = wv * kl[k];
+            Uw = UL;
+            Kw = kl;
         } else if (SL <= wv && wv <= SR) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) FW[k] = wv * UZ[k];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) FWk[k] = wv * UZk[k];
+            Uw = UZ;
+            Kw = UZk;
         } else if (SR < wv) {
             TR = R(0);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) FW[k] = wv * UR[k];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) FWk[k] = wv * kr[k];
+            Uw = UR;
+            Kw = kr;
         } else {
             return 1;
         }
         const R a = TR * TL;
         const R b = TR - TL;
-        qout[0] = (TR * FL[0] - TL * FR[0] + a * (UR[0] - UL[0])) / b - FW[0];
-        qout[4] = (TR * FL[4] - TL * FR[4] + a * (UR[4] - UL[4])) / b - FW[4];
 #pragma unroll
-        for (int k = 0; k < NK; ++k) kout[k] = (TR * FLk[k] - TL * FRk[k] + a * (kr[k] - kl[k])) / b - FWk[k];
+        for (int k = 0; k < 8; ++k) out[k] = (TR * FL[k] - TL * FR[k] + a * (UR[k] - UL[k])) / b - wv * Uw[k];
 #pragma unroll
-        for (int k = 1; k < 4; ++k) qv[k - 1] = (TR * FL[k] - TL * FR[k] + a * (UR[k] - UL[k])) / b - FW[k];
-#pragma unroll
-        for (int k = 5; k < 8; ++k) qb[k - 5] = (TR * FL[k] - TL * FR[k] + a * (UR[k] - UL[k])) / b - FW[k];
-        SN = rmax(fabs(SL), fabs(SR));
-        if (wv >= SR)
-            wbn = wv * bR[0];
-        else if (wv <= SL)
-            wbn = wv * bL[0];
-        else
-            wbn = wv * (bL[0] + bR[0]) / R(2);
-    } else if (n_state == 2) {
-        const R suRm = suR / (SR - SM);
-        const R suLm = suL / (SL - SM);
-        const R rzR = r2 * suRm;
-        const R rzL = r1 * suLm;
-        const R ptz = (suR * r2 * ptL - suL * r1 * ptR + r1 * r2 * suR * suL * (vR[0] - vL[0])) /
-                      (suR * r2 - suL * r1);
-        R vzR1 = vR[1] + UZ[5] * (bR[1] - UZ[6]) / suR / r2;
-        R vzR2 = vR[2] + UZ[5] * (bR[2] - UZ[7]) / suR / r2;
-        R vzL1 = vL[1] + UZ[5] * (bL[1] - UZ[6]) / suL / r1;
-        R vzL2 = vL[2] + UZ[5] * (bL[2] - UZ[7]) / suL / r1;
-        R bzR1 = UZ[6], bzR2 = UZ[7], bzL1 = UZ[6], bzL2 = UZ[7];
-        const R sbvz = (UZ[5] * UZ[1] + UZ[6] * UZ[2] + UZ[7] * UZ[3]) / UZ[0];
-        const R ezR = e2 * suRm + (ptz * SM - ptR * vR[0] + UZ[5] * (sbv2 - sbvz)) / (SR - SM);
-        const R ezL = e1 * suLm + (ptz * SM - ptL * vL[0] + UZ[5] * (sbv1 - sbvz)) / (SL - SM);
-        if (fabs(UZ[5]) <= RConst<R>::epsb()) {
-            vzR1 = vR[1];
-            vzR2 = vR[2];
-            vzL1 = vL[1];
-            vzL2 = vL[2];
-            bzR1 = bR[1] * suRm;
-            bzR2 = bR[2] * suRm;
-            bzL1 = bL[1] * suLm;
-            bzL2 = bL[2] * suLm;
-        }
-        R UZL[8], UZR[8];
-        UZL[0] = rzL;
-        UZL[4] = ezL;
-        UZR[0] = rzR;
-        UZR[4] = ezR;
-        UZL[1] = SM * rzL;
-        UZL[2] = vzL1 * rzL;
-        UZL[3] = vzL2 * rzL;
-        UZR[1] = SM * rzR;
-        UZR[2] = vzR1 * rzR;
-        UZR[3] = vzR2 * rzR;
-        UZL[5] = UZ[5];
-        UZL[6] = bzL1;
-        UZL[7] = bzL2;
-        UZR[5] = UZ[5];
-        UZR[6] = bzR1;
-        UZR[7] = bzR2;
+        for (int k = 0; k < NK; ++k) kout[k] = (TR * FLk[k] - TL * FRk[k] + a * (kr[k] - kl[k])) / b - wv * Kw[k];
+    } else if (n_state == 2) {  // HLLC
         if (fl.left_ydar) wv = SL;
-        R out[8];
-        if (SL >= wv || fl.left_ydar) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) out[k] = FL[k] - wv * UL[k];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) kout[k] = FLk[k] - wv * kl[k];
-        } else if (SL <= wv && SM >= wv) {
-            out[0] = FL[0] + SL * (rzL - r1) - wv * UZL[0];
-            out[4] = FL[4] + SL * (ezL - e1) - wv * UZL[4];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) kout[k] = FLk[k] + SL * (kl[k] * suLm - kl[k]) - wv * (kl[k] * suLm);
-#pragma unroll
-            for (int k = 1; k < 4; ++k) out[k] = FL[k] + SL * (UZL[k] - UL[k]) - wv * UZL[k];
-#pragma unroll
-            for (int k = 5; k < 8; ++k) out[k] = FL[k] + SL * (UZL[k] - UL[k]) - wv * UZL[k];
-        } else if (SM <= wv && SR > wv) {
-            out[0] = FR[0] + SR * (rzR - r2) - wv * UZR[0];
-            out[4] = FR[4] + SR * (ezR - e2) - wv * UZR[4];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) kout[k] = FRk[k] + SR * (kr[k] * suRm - kr[k]) - wv * (kr[k] * suRm);
-#pragma unroll
-            for (int k = 1; k < 4; ++k) out[k] = FR[k] + SR * (UZR[k] - UR[k]) - wv * UZR[k];
-#pragma unroll
-            for (int k = 5; k < 8; ++k) out[k] = FR[k] + SR * (UZR[k] - UR[k]) - wv * UZR[k];
-        } else if (SR <= wv) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) out[k] = FR[k] - wv * UR[k];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) kout[k] = FRk[k] - wv * kr[k];
-        } else {
-            return 2;
-        }
-        qout[0] = out[0];
-        qout[4] = out[4];
-        qv[0] = out[1];
-        qv[1] = out[2];
-        qv[2] = out[3];
-        qb[0] = out[5];
-        qb[1] = out[6];
-        qb[2] = out[7];
-        SN = rmax(fabs(SL), fabs(SR));
-        if (wv > SR)
-            wbn = wv * bR[0];
-        else if (wv < SL)
-            wbn = wv * bL[0];
+        int zone;
+        if (SL >= wv || fl.left_ydar)
+            zone = 1;
+        else if (SL <= wv && SM >= wv)
+            zone = 2;
+        else if (SM <= wv && SR > wv)
+            zone = 3;
+        else if (SR <= wv)
+            zone = 4;
         else
-            wbn = wv * (bL[0] + bR[0]) / R(2);
-    } else if (n_state == 3) {
-        const R ptz = (suR * r2 * ptL - suL * r1 * ptR + r1 * r2 * suR * suL * (vR[0] - vL[0])) /
-                      (suR * r2 - suL * r1);
+            return 2;
+        const bool left = zone <= 2;
+        const R e1 = energy1(), e2 = energy2();
+        R FX[8], UX[8];
+        if (left)
+            side_flux(r1, vL, bL, ptL, e1, sbv1, FX, UX);
+        else
+            side_flux(r2, vR, bR, ptR, e2, sbv2, FX, UX);
+        if (zone == 1 || zone == 4) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) out[k] = FX[k] - wv * UX[k];
+#pragma unroll
+            for (int k = 0; k < NK; ++k) kout[k] = (left ? FLk[k] : FRk[k]) - wv * (left ? kl[k] : kr[k]);
+        } else {
+            // HLL average state; component 4 is not used by HLLC
+            R UL[8], UR[8], FL[8], FR[8], UZ[8];
+            side_flux(r1, vL, bL, ptL, e1, sbv1, FL, UL);
+            side_flux(r2, vR, bR, ptR, e2, sbv2, FR, UR);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) UZ[k] = (SR * UR[k] - SL * UL[k] + FL[k] - FR[k]) / (SR - SL);
+            if (fl.null_bn) UZ[5] = R(0);
+            const R ptz = (suR * r2 * ptL - suL * r1 * ptR + r1 * r2 * suR * suL * (vR[0] - vL[0])) /
+                          (suR * r2 - suL * r1);
+            const R sbvz = (UZ[5] * UZ[1] + UZ[6] * UZ[2] + UZ[7] * UZ[3]) / UZ[0];
+            const R S = left ? SL : SR;
+            const R su = left ? suL : suR;
+            const R rX = left ? r1 : r2;
+            const R eX = left ? e1 : e2;
+            const R ptX = left ? ptL : ptR;
+            const R* vX = left ? vL : vR;
+            const R* bX = left ? bL : bR;
+            const R sbvX = left ? sbv1 : sbv2;
+            const R sum = su / (S - SM);
+            const R rz = rX * sum;
+            R vz1 = vX[1] + UZ[5] * (bX[1] - UZ[6]) / su / rX;
+            R vz2 = vX[2] + UZ[5] * (bX[2] - UZ[7]) / su / rX;
+            R bz1 = UZ[6], bz2 = UZ[7];
+            const R ez = eX * sum + (ptz * SM - ptX * vX[0] + UZ[5] * (sbvX - sbvz)) / (S - SM);
+            if (fabs(UZ[5]) <= RConst<R>::epsb()) {
+                vz1 = vX[1];
+                vz2 = vX[2];
+                bz1 = bX[1] * sum;
+                bz2 = bX[2] * sum;
+            }
+            R UZX[8];
+            UZX[0] = rz;
+            UZX[1] = SM * rz;
+            UZX[2] = vz1 * rz;
+            UZX[3] = vz2 * rz;
+            UZX[4] = ez;
+            UZX[5] = UZ[5];
+            UZX[6] = bz1;
+            UZX[7] = bz2;
+            out[0] = FX[0] + S * (rz - rX) - wv * UZX[0];
+            out[4] = FX[4] + S * (ez - eX) - wv * UZX[4];
+#pragma unroll
+            for (int k = 1; k < 4; ++k) out[k] = FX[k] + S * (UZX[k] - UX[k]) - wv * UZX[k];
+#pragma unroll
+            for (int k = 5; k < 8; ++k) out[k] = FX[k] + S * (UZX[k] - UX[k]) - wv * UZX[k];
+#pragma unroll
+            for (int k = 0; k < NK; ++k) {
+                const R K = left ? kl[k] : kr[k];
+                kout[k] = (left ? FLk[k] : FRk[k]) + S * (K * sum - K) - wv * (K * sum);
+            }
+        }
+    } else if (n_state == 3) {  // HLLD
+        // normal field of the HLL average state (the flux of B_n is 0 on both sides)
+        R bn = (SR * bR[0] - SL * bL[0] + R(0) - R(0)) / (SR - SL);
+        if (fl.null_bn) bn = R(0);
         const R suRm = suR / (SR - SM);
         const R suLm = suL / (SL - SM);
         const R rzR = r2 * suRm;
         const R rzL = r1 * suLm;
-        const R bn = UZ[5];
-        const R bn2 = bn * bn;
-        R tvR, tbR, tvL, tbL;
-        const R ttR = r2 * suR * (SR - SM) - bn2;
-        if (fabs(ttR) < RConst<R>::tt_eps()) {
-            tvR = R(0);
-            tbR = R(0);
-        } else {
-            tvR = (SM - vR[0]) / ttR;
-            tbR = (r2 * suR * suR - bn2) / ttR;
-        }
-        const R ttL = r1 * suL * (SL - SM) - bn2;
-        if (fabs(ttL) < RConst<R>::tt_eps()) {
-            tvL = R(0);
-            tbL = R(0);
-        } else {
-            tvL = (SM - vL[0]) / ttL;
-            tbL = (r1 * suL * suL - bn2) / ttL;
-        }
-        const R vzL1 = vL[1] - bn * bL[1] * tvL;
-        const R vzL2 = vL[2] - bn * bL[2] * tvL;
-        const R vzR1 = vR[1] - bn * bR[1] * tvR;
-        const R vzR2 = vR[2] - bn * bR[2] * tvR;
-        const R bzL1 = bL[1] * tbL;
-        const R bzL2 = bL[2] * tbL;
-        const R bzR1 = bR[1] * tbR;
-        const R bzR2 = bR[2] * tbR;
-        const R sbvL = bn * SM + bzL1 * vzL1 + bzL2 * vzL2;
-        const R sbvR = bn * SM + bzR1 * vzR1 + bzR2 * vzR2;
-        const R ezR = e2 * suRm + (ptz * SM - ptR * vR[0] + bn * (sbv2 - sbvR)) / (SR - SM);
-        const R ezL = e1 * suLm + (ptz * SM - ptL * vL[0] + bn * (sbv1 - sbvL)) / (SL - SM);
         const R rzRs = sqrt(rzR);
         const R rzLs = sqrt(rzL);
-        const R rzss = rzRs + rzLs;
-        const R rzps = rzRs * rzLs;
         R SZL = SM - fabs(bn) / rzLs;
         R SZR = SM + fabs(bn) / rzRs;
         R sbn;
@@ -408,52 +351,8 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
             SZL = SM;
             SZR = SM;
         }
-        const R vzz1 = (rzLs * vzL1 + rzRs * vzR1 + sbn * (bzR1 - bzL1)) / rzss;
-        const R vzz2 = (rzLs * vzL2 + rzRs * vzR2 + sbn * (bzR2 - bzL2)) / rzss;
-        const R bzz1 = (rzLs * bzR1 + rzRs * bzL1 + sbn * rzps * (vzR1 - vzL1)) / rzss;
-        const R bzz2 = (rzLs * bzR2 + rzRs * bzL2 + sbn * rzps * (vzR2 - vzL2)) / rzss;
-        const R sbzz = bn * SM + bzz1 * vzz1 + bzz2 * vzz2;
-        const R ezzR = ezR + rzRs * sbn * (sbvR - sbzz);
-        const R ezzL = ezL - rzLs * sbn * (sbvL - sbzz);
-
-        // Star (UZ*) and double-star (UZZ*) states; the reference keeps
-        // rho** = rho* and v**_n = SM.
-        R UZL[8], UZR[8], UZZL[8], UZZR[8];
-        UZL[0] = rzL;
-        UZL[1] = SM * rzL;
-        UZL[2] = vzL1 * rzL;
-        UZL[3] = vzL2 * rzL;
-        UZL[4] = ezL;
-        UZL[5] = bn;
-        UZL[6] = bzL1;
-        UZL[7] = bzL2;
-        UZR[0] = rzR;
-        UZR[1] = SM * rzR;
-        UZR[2] = vzR1 * rzR;
-        UZR[3] = vzR2 * rzR;
-        UZR[4] = ezR;
-        UZR[5] = bn;
-        UZR[6] = bzR1;
-        UZR[7] = bzR2;
-        UZZL[0] = rzL;
-        UZZL[1] = SM * rzL;
-        UZZL[2] = vzz1 * rzL;
-        UZZL[3] = vzz2 * rzL;
-        UZZL[4] = ezzL;
-        UZZL[5] = bn;
-        UZZL[6] = bzz1;
-        UZZL[7] = bzz2;
-        UZZR[0] = rzR;
-        UZZR[1] = SM * rzR;
-        UZZR[2] = vzz1 * rzR;
-        UZZR[3] = vzz2 * rzR;
-        UZZR[4] = ezzR;
-        UZZR[5] = bn;
-        UZZR[6] = bzz1;
-        UZZR[7] = bzz2;
-
         if (fl.left_ydar) wv = SL;
-        int zone = 0;  // the reference's j_ccs: 1..6, later tests overwrite earlier ones
+        int zone = 0;  // replay of the reference's tests; later ones overwrite
         if (SL >= wv || fl.left_ydar)
             zone = 1;
         else if (SL <= wv && SZL >= wv)
@@ -470,62 +369,138 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
             zone = 6;
         if (zone == 0) return 3;
 
-        R out[8];
-        const R* FX = (zone <= 3) ? FL : FR;
-        const R* UX = (zone <= 3) ? UL : UR;
-        const R* KX = (zone <= 3) ? kl : kr;
+        const bool left = zone <= 3;
+        const R eX = left ? energy1() : energy2();
+        R FX[8], UX[8];
+        if (left)
+            side_flux(r1, vL, bL, ptL, eX, sbv1, FX, UX);
+        else
+            side_flux(r2, vR, bR, ptR, eX, sbv2, FX, UX);
+        const R* KX = left ? kl : kr;
         if (zone == 1 || zone == 6) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) out[k] = FX[k] - wv * UX[k];
 #pragma unroll
-            for (int k = 0; k < NK; ++k) kout[k] = (zone == 1 ? FLk[k] : FRk[k]) - wv * KX[k];
-        } else if (zone == 2 || zone == 5) {
-            const R* UZX = (zone == 2) ? UZL : UZR;
-            const R S = (zone == 2) ? SL : SR;
-            const R sm = (zone == 2) ? suLm : suRm;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) out[k] = FX[k] + S * (UZX[k] - UX[k]) - wv * UZX[k];
-#pragma unroll
-            for (int k = 0; k < NK; ++k)
-                kout[k] = (zone == 2 ? FLk[k] : FRk[k]) + S * (KX[k] * sm - KX[k]) - wv * (KX[k] * sm);
+            for (int k = 0; k < NK; ++k) kout[k] = (left ? FLk[k] : FRk[k]) - wv * KX[k];
         } else {
-            const R* UZX = (zone == 3) ? UZL : UZR;
-            const R* UZZX = (zone == 3) ? UZZL : UZZR;
-            const R S = (zone == 3) ? SL : SR;
-            const R SZ = (zone == 3) ? SZL : SZR;
-            const R sm = (zone == 3) ? suLm : suRm;
+            const R ptz = (suR * r2 * ptL - suL * r1 * ptR + r1 * r2 * suR * suL * (vR[0] - vL[0])) /
+                          (suR * r2 - suL * r1);
+            const R bn2 = bn * bn;
+            // single-star velocity / field of the left (zones 2, 3, 4) and right (3, 4, 5) states
+            R vzL1 = R(0), vzL2 = R(0), bzL1 = R(0), bzL2 = R(0);
+            R vzR1 = R(0), vzR2 = R(0), bzR1 = R(0), bzR2 = R(0);
+            if (zone != 5) {
+                R tvL, tbL;
+                const R ttL = r1 * suL * (SL - SM) - bn2;
+                if (fabs(ttL) < RConst<R>::tt_eps()) {
+                    tvL = R(0);
+                    tbL = R(0);
+                } else {
+                    tvL = (SM - vL[0]) / ttL;
+                    tbL = (r1 * suL * suL - bn2) / ttL;
+                }
+                vzL1 = vL[1] - bn * bL[1] * tvL;
+                vzL2 = vL[2] - bn * bL[2] * tvL;
+                bzL1 = bL[1] * tbL;
+                bzL2 = bL[2] * tbL;
+            }
+            if (zone != 2) {
+                R tvR, tbR;
+                const R ttR = r2 * suR * (SR - SM) - bn2;
+                if (fabs(ttR) < RConst<R>::tt_eps()) {
+                    tvR = R(0);
+                    tbR = R(0);
+                } else {
+                    tvR = (SM - vR[0]) / ttR;
+                    tbR = (r2 * suR * suR - bn2) / ttR;
+                }
+                vzR1 = vR[1] - bn * bR[1] * tvR;
+                vzR2 = vR[2] - bn * bR[2] * tvR;
+                bzR1 = bR[1] * tbR;
+                bzR2 = bR[2] * tbR;
+            }
+            // single-star state of the side the zone belongs to
+            const R vz1 = left ? vzL1 : vzR1, vz2 = left ? vzL2 : vzR2;
+            const R bz1 = left ? bzL1 : bzR1, bz2 = left ? bzL2 : bzR2;
+            const R sbvX = bn * SM + bz1 * vz1 + bz2 * vz2;
+            const R rz = left ? rzL : rzR;
+            const R sum = left ? suLm : suRm;
+            const R S = left ? SL : SR;
+            const R ez = eX * sum + (ptz * SM - (left ? ptL : ptR) * (left ? vL[0] : vR[0]) +
+                                     bn * ((left ? sbv1 : sbv2) - sbvX)) /
+                                        (S - SM);
+            R UZX[8];
+            UZX[0] = rz;
+            UZX[1] = SM * rz;
+            UZX[2] = vz1 * rz;
+            UZX[3] = vz2 * rz;
+            UZX[4] = ez;
+            UZX[5] = bn;
+            UZX[6] = bz1;
+            UZX[7] = bz2;
+            if (zone == 2 || zone == 5) {
 #pragma unroll
-            for (int k = 0; k < 8; ++k) out[k] = FX[k] + SZ * (UZZX[k] - UZX[k]) + S * (UZX[k] - UX[k]) - wv * UZZX[k];
+                for (int k = 0; k < 8; ++k) out[k] = FX[k] + S * (UZX[k] - UX[k]) - wv * UZX[k];
 #pragma unroll
-            for (int k = 0; k < NK; ++k) {
-                const R qz = KX[k] * sm;
-                kout[k] = (zone == 3 ? FLk[k] : FRk[k]) + SZ * (qz - qz) + S * (qz - KX[k]) - wv * qz;
+                for (int k = 0; k < NK; ++k)
+                    kout[k] = (left ? FLk[k] : FRk[k]) + S * (KX[k] * sum - KX[k]) - wv * (KX[k] * sum);
+            } else {
+                // double-star state (rho** = rho*, v**_n = SM)
+                const R rzss = rzRs + rzLs;
+                const R rzps = rzRs * rzLs;
+                const R vzz1 = (rzLs * vzL1 + rzRs * vzR1 + sbn * (bzR1 - bzL1)) / rzss;
+                const R vzz2 = (rzLs * vzL2 + rzRs * vzR2 + sbn * (bzR2 - bzL2)) / rzss;
+                const R bzz1 = (rzLs * bzR1 + rzRs * bzL1 + sbn * rzps * (vzR1 - vzL1)) / rzss;
+                const R bzz2 = (rzLs * bzR2 + rzRs * bzL2 + sbn * rzps * (vzR2 - vzL2)) / rzss;
+                const R sbzz = bn * SM + bzz1 * vzz1 + bzz2 * vzz2;
+                const R ezz = left ? ez - rzLs * sbn * (sbvX - sbzz) : ez + rzRs * sbn * (sbvX - sbzz);
+                const R SZ = left ? SZL : SZR;
+                R UZZ[8];
+                UZZ[0] = rz;
+                UZZ[1] = SM * rz;
+                UZZ[2] = vzz1 * rz;
+                UZZ[3] = vzz2 * rz;
+                UZZ[4] = ezz;
+                UZZ[5] = bn;
+                UZZ[6] = bzz1;
+                UZZ[7] = bzz2;
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    out[k] = FX[k] + SZ * (UZZ[k] - UZX[k]) + S * (UZX[k] - UX[k]) - wv * UZZ[k];
+#pragma unroll
+                for (int k = 0; k < NK; ++k) {
+                    const R qz = KX[k] * sum;
+                    kout[k] = (left ? FLk[k] : FRk[k]) + SZ * (qz - qz) + S * (qz - KX[k]) - wv * qz;
+                }
             }
         }
-        qout[0] = out[0];
-        qout[4] = out[4];
-        qv[0] = out[1];
-        qv[1] = out[2];
-        qv[2] = out[3];
-        qb[0] = out[5];
-        qb[1] = out[6];
-        qb[2] = out[7];
-        SN = rmax(fabs(SL), fabs(SR));
+    } else {
+        return 4;
+    }
+    R SN, wbn;
+    SN = rmax(fabs(SL), fabs(SR));
+    if (n_state <= 1) {
+        if (wv >= SR)
+            wbn = wv * bR[0];
+        else if (wv <= SL)
+            wbn = wv * bL[0];
+        else
+            wbn = wv * (bL[0] + bR[0]) / R(2);
+    } else {
         if (wv > SR)
             wbn = wv * bR[0];
         else if (wv < SL)
             wbn = wv * bL[0];
         else
             wbn = wv * (bL[0] + bR[0]) / R(2);
-    } else {
-        return 4;
     }
-    qb[0] = -SN * (bR[0] - bL[0]) - wbn;
-    if (fl.null_bn) qb[0] = R(0);
+    const R qb0 = fl.null_bn ? R(0) : -SN * (bR[0] - bL[0]) - wbn;
+    qout[0] = out[0];
+    qout[4] = out[4];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        qout[i + 1] = n[i] * qv[0] + t[i] * qv[1] + m[i] * qv[2];
-        qout[i + 5] = spi4 * (n[i] * qb[0] + t[i] * qb[1] + m[i] * qb[2]);
+        qout[i + 1] = n[i] * out[1] + t[i] * out[2] + m[i] * out[3];
+        qout[i + 5] = spi4 * (n[i] * qb0 + t[i] * out[6] + m[i] * out[7]);
     }
     return 0;
 }

@@ -252,8 +252,8 @@ struct FluxLayout {
     static constexpr int stride = (sizeof(FT) == 8) ? ((n + 1) & ~1) : ((n + 3) & ~3);
 };
 
-template <typename R, typename FT, int NK, bool MOVE>
-__global__ void __launch_bounds__(128) face_flux_kernel(FaceArgs a) {
+template <typename R, typename FT, int NK, bool MOVE, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 100000000.0;  // identity of the min (Setka_physics.cpp:1607)
     if (f < a.M.nface && a.st->err_kind == 0) {
@@ -454,8 +454,8 @@ static __device__ __noinline__ void bera_sources(const Params& P, const double* 
     S[3] = Es * ddp;
 }
 
-template <typename FT, int NK, bool MOVE, int SRC>
-__global__ void __launch_bounds__(256) cell_update_kernel(CellArgs a) {
+template <typename FT, int NK, bool MOVE, int SRC, int BS>
+__global__ void __launch_bounds__(BS) cell_update_kernel(CellArgs a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const bool ok = a.st->err_kind == 0;
     if (c < a.M.ncell && ok) {

@@ -95,6 +95,9 @@ struct titan_ctx {
     cudaGraphExec_t graph = nullptr;
     int graph_cur = -1, graph_scur = -1;
 
+    int face_variant = 0;  // launch shapes (autotuned, see titan_autotune)
+    int cell_variant = 0;
+
     bool profiling = false;
     std::map<std::string, KernelClock> clocks;
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -169,9 +172,9 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     fa.st = ctx->d_status;
     const int nk = ctx->prm.npassive;
     if (ctx->fp32)
-        e = timed(ctx, "face_flux_fp32", [&] { return launch_face_flux_fp32(fa, nk, move, ctx->stream); });
+        e = timed(ctx, "face_flux_fp32", [&] { return launch_face_flux_fp32(fa, nk, move, ctx->face_variant, ctx->stream); });
     else
-        e = timed(ctx, "face_flux_fp64", [&] { return launch_face_flux_fp64(fa, nk, move, ctx->stream); });
+        e = timed(ctx, "face_flux_fp64", [&] { return launch_face_flux_fp64(fa, nk, move, ctx->face_variant, ctx->stream); });
     if (e) return e;
     CellArgs ca;
     ca.M = M;
@@ -185,7 +188,8 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     ca.src = ctx->d_src;
     ca.st = ctx->d_status;
     const int src = ctx->use_src ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
-    e = timed(ctx, "cell_update", [&] { return launch_cell_update(ca, ctx->fp32, nk, move, src, ctx->stream); });
+    e = timed(ctx, "cell_update",
+              [&] { return launch_cell_update(ca, ctx->fp32, nk, move, src, ctx->cell_variant, ctx->stream); });
     if (e) return e;
     ctx->scur ^= 1;
     if (move) ctx->cur = nxt;
@@ -763,6 +767,134 @@ int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, con
     for (void* p : ps)
         if (p) cudaFree(p);
     if (e) return fail(TITAN_ECUDA, std::string("riemann_batch: ") + cudaGetErrorString(e));
+    return TITAN_OK;
+}
+
+int titan_set_tuning(titan_ctx* ctx, int32_t face_variant, int32_t cell_variant) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    if (face_variant < 0 || face_variant >= kFaceVariants || cell_variant < 0 || cell_variant >= kCellVariants)
+        return fail(TITAN_EINVAL, "variant out of range");
+    ctx->face_variant = face_variant;
+    ctx->cell_variant = cell_variant;
+    drop_graph(ctx);
+    return TITAN_OK;
+}
+
+int titan_get_tuning(titan_ctx* ctx, int32_t* face_variant, int32_t* cell_variant, int32_t* face_block,
+                     int32_t* face_min_blocks, int32_t* cell_block) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    if (face_variant) *face_variant = ctx->face_variant;
+    if (cell_variant) *cell_variant = ctx->cell_variant;
+    if (face_block) *face_block = kFaceVariant[ctx->face_variant].block;
+    if (face_min_blocks) *face_min_blocks = kFaceVariant[ctx->face_variant].min_blocks;
+    if (cell_block) *cell_block = kCellBlock[ctx->cell_variant];
+    return TITAN_OK;
+}
+
+int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
+    if (!ctx || reps <= 0) return fail(TITAN_EINVAL, "bad argument");
+    const int src = ctx->use_src ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
+    char key[256];
+    snprintf(key, sizeof key, "sm_100a cells=%lld faces=%lld move=%d flux=%d npassive=%d src=%d",
+             (long long)ctx->ncell, (long long)ctx->nface, ctx->prm.move, ctx->prm.flux_precision,
+             ctx->prm.npassive, src);
+    if (cache_path) {
+        FILE* f = fopen(cache_path, "r");
+        if (f) {
+            char line[512];
+            while (fgets(line, sizeof line, f)) {
+                char* bar = strchr(line, '|');
+                if (!bar) continue;
+                *bar = 0;
+                int fv = -1, cv = -1;
+                if (strcmp(line, key) == 0 && sscanf(bar + 1, "%d %d", &fv, &cv) == 2 && fv >= 0 &&
+                    fv < kFaceVariants && cv >= 0 && cv < kCellVariants) {
+                    fclose(f);
+                    return titan_set_tuning(ctx, fv, cv);
+                }
+            }
+            fclose(f);
+        }
+    }
+    cudaStream_t s = ctx->stream;
+    const MeshView M = ctx->view();
+    const bool move = ctx->prm.move != 0;
+    const int nxt = ctx->cur ^ 1;
+    // the next layer = the current one, so every input the kernels read is valid
+    if (move) {
+        CK(cudaMemcpyAsync(ctx->layer[nxt].xyz, ctx->layer[ctx->cur].xyz, sizeof(double) * 3 * ctx->nnode,
+                           cudaMemcpyDeviceToDevice, s));
+        CK(launch_cell_geometry(M, ctx->layer[nxt], s));
+        CK(launch_face_geometry(M, ctx->layer[nxt], s));
+    }
+    DevStatus init{};
+    init.dt = 1e-5;
+    init.dt_next_bits = 0x4197D78400000000ull;
+    FaceArgs fa;
+    fa.M = M;
+    fa.P = ctx->P;
+    fa.L1 = ctx->layer[ctx->cur];
+    fa.xyz2 = ctx->layer[nxt].xyz;
+    fa.state = ctx->d_state[ctx->scur];
+    fa.flux = ctx->d_flux;
+    fa.st = ctx->d_status;
+    CellArgs ca;
+    ca.M = M;
+    ca.P = ctx->P;
+    ca.vol1 = ctx->layer[ctx->cur].vol;
+    ca.vol2 = ctx->layer[nxt].vol;
+    ca.state = ctx->d_state[ctx->scur];
+    ca.state2 = ctx->d_state[ctx->scur ^ 1];
+    ca.flux = ctx->d_flux;
+    ca.hfl = ctx->d_hfl;
+    ca.src = ctx->d_src;
+    ca.st = ctx->d_status;
+    const int nk = ctx->prm.npassive;
+    auto time_it = [&](auto launch, float* ms_out) -> cudaError_t {
+        std::memcpy(ctx->h_status, &init, sizeof(DevStatus));
+        cudaError_t e = cudaMemcpyAsync(ctx->d_status, ctx->h_status, sizeof(DevStatus), cudaMemcpyHostToDevice, s);
+        if (!e) e = launch();
+        if (!e) e = cudaEventRecord(ctx->ev[0], s);
+        for (int r = 0; r < reps && !e; ++r) e = launch();
+        if (!e) e = cudaEventRecord(ctx->ev[1], s);
+        if (!e) e = cudaEventSynchronize(ctx->ev[1]);
+        if (!e) e = cudaEventElapsedTime(ms_out, ctx->ev[0], ctx->ev[1]);
+        return e;
+    };
+    float best = 1e30f;
+    int best_fv = 0, best_cv = 0;
+    float fms[kFaceVariants], cms[kCellVariants];
+    for (int v = 0; v < kFaceVariants; ++v) {
+        CK(time_it([&] { return ctx->fp32 ? launch_face_flux_fp32(fa, nk, move, v, s)
+                                          : launch_face_flux_fp64(fa, nk, move, v, s); },
+                   &fms[v]));
+        if (fms[v] < best) {
+            best = fms[v];
+            best_fv = v;
+        }
+    }
+    best = 1e30f;
+    for (int v = 0; v < kCellVariants; ++v) {
+        CK(time_it([&] { return launch_cell_update(ca, ctx->fp32, nk, move, src, v, s); }, &cms[v]));
+        if (cms[v] < best) {
+            best = cms[v];
+            best_cv = v;
+        }
+    }
+    CK(cudaStreamSynchronize(s));
+    const int rc = titan_set_tuning(ctx, best_fv, best_cv);
+    if (rc) return rc;
+    if (cache_path) {
+        FILE* f = fopen(cache_path, "a");
+        if (f) {
+            fprintf(f, "%s|%d %d  # face ms/launch:", key, best_fv, best_cv);
+            for (int v = 0; v < kFaceVariants; ++v) fprintf(f, " %.4f", fms[v] / reps);
+            fprintf(f, "  cell:");
+            for (int v = 0; v < kCellVariants; ++v) fprintf(f, " %.4f", cms[v] / reps);
+            fprintf(f, "\n");
+            fclose(f);
+        }
+    }
     return TITAN_OK;
 }
 

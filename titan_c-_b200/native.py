@@ -82,6 +82,9 @@ SIGNATURES = {
                            ctypes.c_int),
     "titan_riemann_batch": ([ctypes.c_int64, I8, D, D, D, D, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, D, D,
                              I32], ctypes.c_int),
+    "titan_autotune": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p], ctypes.c_int),
+    "titan_set_tuning": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
+    "titan_get_tuning": ([ctypes.c_void_p, I32, I32, I32, I32, I32], ctypes.c_int),
     "titan_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "titan_set_profiling": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "titan_kernel_times": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p), D, I64, ctypes.c_int32],

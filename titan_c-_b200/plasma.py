@@ -152,6 +152,20 @@ class PlasmaStep:
         N.check(self._lib.titan_get_permutation(self._ctx, N.ptr(c, N.I32), N.ptr(f, N.I32), N.ptr(n, N.I32)))
         return c, f, n
 
+    def autotune(self, reps: int = 5, cache: str | None = None) -> dict:
+        """Times the launch-shape variants on this mesh and keeps the fastest."""
+        N.check(self._lib.titan_autotune(self._ctx, int(reps), cache.encode() if cache else None))
+        return self.tuning()
+
+    def set_tuning(self, face_variant: int, cell_variant: int):
+        N.check(self._lib.titan_set_tuning(self._ctx, int(face_variant), int(cell_variant)))
+
+    def tuning(self) -> dict:
+        v = [np.zeros(1, dtype=np.int32) for _ in range(5)]
+        N.check(self._lib.titan_get_tuning(self._ctx, *[N.ptr(a, N.I32) for a in v]))
+        keys = ["face_variant", "cell_variant", "face_block", "face_min_blocks", "cell_block"]
+        return {k: int(a[0]) for k, a in zip(keys, v)}
+
     def stream(self) -> int:
         return int(self._lib.titan_stream(self._ctx) or 0)
 

@@ -259,3 +259,18 @@ def test_autotune_picks_a_shape_and_caches_it(T, tmp_path):
     assert np.array_equal(g.download_state(), g3.download_state())
     for x in (g, g2, g3):
         x.close()
+
+
+def test_moving_mesh_geometry_matches_oracle(T, oracle_lib):
+    """After steps with node motion the geometry the GPU formed inside its
+    kernels equals the oracle's Calculating_measure of the moved nodes."""
+    m, p, st, _ = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True)
+    gpu, run = _pair(T, m, p)
+    gpu.upload_state(st)
+    gpu.go(3)
+    xyz = gpu.nodes()
+    a = gpu.geometry()
+    b = run.geometry(xyz)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    gpu.close()

@@ -4,7 +4,8 @@
 
 Translation units and their floating-point flags:
   kernels_fp64.cu  -fmad=false  geometry, FP64 flux, cell update (bit-exact FP64)
-  kernels_fp32.cu  -fmad=true   FP32 Riemann flux of the mixed-precision step
+  kernels_fp32.cu  -fmad=true -prec-div=false -prec-sqrt=false
+                                FP32 Riemann flux of the mixed-precision step
   titan_api.cu, renumber.cpp    host side of the C ABI
 """
 from __future__ import annotations
@@ -24,7 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
-    ("kernels_fp32.cu", ["-fmad=true"]),
+    ("kernels_fp32.cu", ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("titan_api.cu", []),
     ("renumber.cpp", []),
 ]

@@ -1,6 +1,8 @@
 // FP32-flux translation unit: the Riemann flux in single precision (the
 // mixed-precision step keeps reconstruction, accumulation, update and the CFL
-// reduction in FP64). Contraction to FMA is allowed here.
+// reduction in FP64). Contraction to FMA is allowed here, and single-precision
+// division and square root use the fast approximate forms (-prec-div=false,
+// -prec-sqrt=false): the flux error budget is 1e-4, far above their few ulp.
 #include "launch.h"
 #include "step_kernels.cuh"
 

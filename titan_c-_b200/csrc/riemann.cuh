@@ -229,28 +229,30 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
         for (int i = 0; i < NK; ++i) UZk[i] = (SR * kr[i] - SL * kl[i] + FLk[i] - FRk[i]) / (SR - SL);
         if (fl.left_ydar) wv = SL;
         R TL = SL, TR = SR;
-        const R* Uw;
-        const R* Kw;
+        int wsel;  // state the face moves through: 0 left, 1 HLL average, 2 right
         if (SL > wv || fl.left_ydar) {
             TL = R(0);
-            Uw = UL;
-            Kw = kl;
+            wsel = 0;
         } else if (SL <= wv && wv <= SR) {
-            Uw = UZ;
-            Kw = UZk;
+            wsel = 1;
         } else if (SR < wv) {
             TR = R(0);
-            Uw = UR;
-            Kw = kr;
+            wsel = 2;
         } else {
             return 1;
         }
         const R a = TR * TL;
         const R b = TR - TL;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) out[k] = (TR * FL[k] - TL * FR[k] + a * (UR[k] - UL[k])) / b - wv * Uw[k];
+        for (int k = 0; k < 8; ++k) {
+            const R Uw = wsel == 0 ? UL[k] : (wsel == 1 ? UZ[k] : UR[k]);
+            out[k] = (TR * FL[k] - TL * FR[k] + a * (UR[k] - UL[k])) / b - wv * Uw;
+        }
 #pragma unroll
-        for (int k = 0; k < NK; ++k) kout[k] = (TR * FLk[k] - TL * FRk[k] + a * (kr[k] - kl[k])) / b - wv * Kw[k];
+        for (int k = 0; k < NK; ++k) {
+            const R Kw = wsel == 0 ? kl[k] : (wsel == 1 ? UZk[k] : kr[k]);
+            kout[k] = (TR * FLk[k] - TL * FRk[k] + a * (kr[k] - kl[k])) / b - wv * Kw;
+        }
     } else if (n_state == 2) {  // HLLC
         if (fl.left_ydar) wv = SL;
         int zone;
@@ -292,20 +294,20 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
             const R rX = left ? r1 : r2;
             const R eX = left ? e1 : e2;
             const R ptX = left ? ptL : ptR;
-            const R* vX = left ? vL : vR;
-            const R* bX = left ? bL : bR;
+            const R vX0 = left ? vL[0] : vR[0], vX1 = left ? vL[1] : vR[1], vX2 = left ? vL[2] : vR[2];
+            const R bX1 = left ? bL[1] : bR[1], bX2 = left ? bL[2] : bR[2];
             const R sbvX = left ? sbv1 : sbv2;
             const R sum = su / (S - SM);
             const R rz = rX * sum;
-            R vz1 = vX[1] + UZ[5] * (bX[1] - UZ[6]) / su / rX;
-            R vz2 = vX[2] + UZ[5] * (bX[2] - UZ[7]) / su / rX;
+            R vz1 = vX1 + UZ[5] * (bX1 - UZ[6]) / su / rX;
+            R vz2 = vX2 + UZ[5] * (bX2 - UZ[7]) / su / rX;
             R bz1 = UZ[6], bz2 = UZ[7];
-            const R ez = eX * sum + (ptz * SM - ptX * vX[0] + UZ[5] * (sbvX - sbvz)) / (S - SM);
+            const R ez = eX * sum + (ptz * SM - ptX * vX0 + UZ[5] * (sbvX - sbvz)) / (S - SM);
             if (fabs(UZ[5]) <= RConst<R>::epsb()) {
-                vz1 = vX[1];
-                vz2 = vX[2];
-                bz1 = bX[1] * sum;
-                bz2 = bX[2] * sum;
+                vz1 = vX1;
+                vz2 = vX2;
+                bz1 = bX1 * sum;
+                bz2 = bX2 * sum;
             }
             R UZX[8];
             UZX[0] = rz;
@@ -376,12 +378,11 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
             side_flux(r1, vL, bL, ptL, eX, sbv1, FX, UX);
         else
             side_flux(r2, vR, bR, ptR, eX, sbv2, FX, UX);
-        const R* KX = left ? kl : kr;
         if (zone == 1 || zone == 6) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) out[k] = FX[k] - wv * UX[k];
 #pragma unroll
-            for (int k = 0; k < NK; ++k) kout[k] = (left ? FLk[k] : FRk[k]) - wv * KX[k];
+            for (int k = 0; k < NK; ++k) kout[k] = (left ? FLk[k] : FRk[k]) - wv * (left ? kl[k] : kr[k]);
         } else {
             const R ptz = (suR * r2 * ptL - suL * r1 * ptR + r1 * r2 * suR * suL * (vR[0] - vL[0])) /
                           (suR * r2 - suL * r1);
@@ -442,8 +443,10 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
 #pragma unroll
                 for (int k = 0; k < 8; ++k) out[k] = FX[k] + S * (UZX[k] - UX[k]) - wv * UZX[k];
 #pragma unroll
-                for (int k = 0; k < NK; ++k)
-                    kout[k] = (left ? FLk[k] : FRk[k]) + S * (KX[k] * sum - KX[k]) - wv * (KX[k] * sum);
+                for (int k = 0; k < NK; ++k) {
+                    const R K = left ? kl[k] : kr[k];
+                    kout[k] = (left ? FLk[k] : FRk[k]) + S * (K * sum - K) - wv * (K * sum);
+                }
             } else {
                 // double-star state (rho** = rho*, v**_n = SM)
                 const R rzss = rzRs + rzLs;
@@ -469,8 +472,9 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
                     out[k] = FX[k] + SZ * (UZZ[k] - UZX[k]) + S * (UZX[k] - UX[k]) - wv * UZZ[k];
 #pragma unroll
                 for (int k = 0; k < NK; ++k) {
-                    const R qz = KX[k] * sum;
-                    kout[k] = (left ? FLk[k] : FRk[k]) + SZ * (qz - qz) + S * (qz - KX[k]) - wv * qz;
+                    const R K = left ? kl[k] : kr[k];
+                    const R qz = K * sum;
+                    kout[k] = (left ? FLk[k] : FRk[k]) + SZ * (qz - qz) + S * (qz - K) - wv * qz;
                 }
             }
         }

@@ -82,47 +82,68 @@ __device__ __forceinline__ void load_node(const double* xyz, int nn, int i, doub
     p[2] = xyz[2 * nn + i];
 }
 
-// Cell centre (Cell.cpp:909-930) and volume by method 1 (Cell.cpp:958-1001).
-static __global__ void cell_geometry_kernel(MeshView M, Layer L) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= M.ncell) return;
-    const int nc = M.ncell, nn = M.nnode;
-    double x = 0.0, y = 0.0, z = 0.0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int i = M.cell_nodes[k * nc + c];
-        x += L.xyz[i];
-        y += L.xyz[nn + i];
-        z += L.xyz[2 * nn + i];
-    }
-    const double C[3] = {x / 8, y / 8, z / 8};
-    L.cc[c] = C[0];
-    L.cc[nc + c] = C[1];
-    L.cc[2 * nc + c] = C[2];
+// Cell centre (Cell.cpp:909-930) and volume by method 1 (Cell.cpp:958-1001):
+// two tetrahedra (C, P0, P1, P2) and (C, P0, P3, P2) per face, in face order.
+// P(s, k) returns node k of face slot s.
+template <typename NodeOf>
+__device__ __forceinline__ double cell_volume(const double C[3], NodeOf P) {
     double V = 0.0;
-    const int nf = M.nface;
+#pragma unroll
     for (int s = 0; s < 6; ++s) {
-        const int f = M.cell_faces[s * nc + c] & 0x7fffffff;
         double P0[3], P1[3], P2[3], P3[3];
-        load_node(L.xyz, nn, M.face_nodes[f], P0);
-        load_node(L.xyz, nn, M.face_nodes[nf + f], P1);
-        load_node(L.xyz, nn, M.face_nodes[2 * nf + f], P2);
-        load_node(L.xyz, nn, M.face_nodes[3 * nf + f], P3);
+        P(s, 0, P0);
+        P(s, 1, P1);
+        P(s, 2, P2);
+        P(s, 3, P3);
         V += tet_vol(C, P0, P1, P2);
         V += tet_vol(C, P0, P3, P2);
     }
-    L.vol[c] = V;
+    return V;
 }
 
-// Face centre, area, normal oriented from cells[0] to cells[1] (Gran.cpp:112-218)
-// and half the centre distance used by the CFL estimate (Setka_physics.cpp:2298-2307).
-static __global__ void face_geometry_kernel(MeshView M, Layer L) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= M.nface) return;
-    const int nf = M.nface, nn = M.nnode, nc = M.ncell;
-    double P[4][3];
+__device__ __forceinline__ void cell_centre(const double X[8][3], double C[3]) {
+    double x = 0.0, y = 0.0, z = 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) load_node(L.xyz, nn, M.face_nodes[k * nf + f], P[k]);
+    for (int k = 0; k < 8; ++k) {
+        x += X[k][0];
+        y += X[k][1];
+        z += X[k][2];
+    }
+    C[0] = x / 8;
+    C[1] = y / 8;
+    C[2] = z / 8;
+}
+
+static __global__ void cell_geometry_kernel(MeshView M, Layer L) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= M.ncell) return;
+    const int nc = M.ncell, nn = M.nnode, nf = M.nface;
+    double X[8][3];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) load_node(L.xyz, nn, M.cell_nodes[k * nc + c], X[k]);
+    double C[3];
+    cell_centre(X, C);
+    L.cc[c] = C[0];
+    L.cc[nc + c] = C[1];
+    L.cc[2 * nc + c] = C[2];
+    L.vol[c] = cell_volume(C, [&](int s, int k, double* p) {
+        const int f = M.cell_faces[s * nc + c] & 0x7fffffff;
+        load_node(L.xyz, nn, M.face_nodes[k * nf + f], p);
+    });
+}
+
+struct FaceGeom {
+    double c[3];  // centre
+    double n[3];  // unit normal from cells[0] to cells[1]
+    double area;
+    double half_dist;
+};
+
+// Face centre, area (2 triangles), normal from edge midpoints oriented from
+// cells[0] to cells[1] (Gran.cpp:112-218) and half the distance between the
+// two cell centres used by the CFL estimate (Setka_physics.cpp:2298-2307).
+__device__ __forceinline__ FaceGeom face_geometry(const double P[4][3], const double c0[3], const double* c1) {
+    FaceGeom g;
     double xc = 0.0, yc = 0.0, zc = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -133,13 +154,13 @@ static __global__ void face_geometry_kernel(MeshView M, Layer L) {
     xc /= 4;
     yc /= 4;
     zc /= 4;
-    L.fc[f] = xc;
-    L.fc[nf + f] = yc;
-    L.fc[2 * nf + f] = zc;
+    g.c[0] = xc;
+    g.c[1] = yc;
+    g.c[2] = zc;
     double S = 0.0;
     S += tri_area(P[0][0], P[0][1], P[0][2], P[1][0], P[1][1], P[1][2], P[2][0], P[2][1], P[2][2]);
     S += tri_area(P[0][0], P[0][1], P[0][2], P[3][0], P[3][1], P[3][2], P[2][0], P[2][1], P[2][2]);
-    L.fa[f] = S;
+    g.area = S;
     const double x1 = (P[0][0] + P[1][0]) / 2.0, y1 = (P[0][1] + P[1][1]) / 2.0, z1 = (P[0][2] + P[1][2]) / 2.0;
     const double x2 = (P[1][0] + P[2][0]) / 2.0, y2 = (P[1][1] + P[2][1]) / 2.0, z2 = (P[1][2] + P[2][2]) / 2.0;
     const double x3 = (P[2][0] + P[3][0]) / 2.0, y3 = (P[2][1] + P[3][1]) / 2.0, z3 = (P[2][2] + P[3][2]) / 2.0;
@@ -152,23 +173,48 @@ static __global__ void face_geometry_kernel(MeshView M, Layer L) {
     n1 /= nrm;
     n2 /= nrm;
     n3 /= nrm;
-    const int c0 = M.face_c0[f];
-    const double c0x = L.cc[c0], c0y = L.cc[nc + c0], c0z = L.cc[2 * nc + c0];
-    if (n1 * (c0x - xc) + n2 * (c0y - yc) + n3 * (c0z - zc) > 0.0) {
+    if (n1 * (c0[0] - xc) + n2 * (c0[1] - yc) + n3 * (c0[2] - zc) > 0.0) {
         n1 = -n1;
         n2 = -n2;
         n3 = -n3;
     }
-    L.fn[f] = n1;
-    L.fn[nf + f] = n2;
-    L.fn[2 * nf + f] = n3;
-    const int c1 = M.face_c1[f];
-    double d = 0.0;
-    if (c1 >= 0) {
-        const double dx = c0x - L.cc[c1], dy = c0y - L.cc[nc + c1], dz = c0z - L.cc[2 * nc + c1];
-        d = sqrt(dx * dx + dy * dy + dz * dz) / 2.0;
+    g.n[0] = n1;
+    g.n[1] = n2;
+    g.n[2] = n3;
+    g.half_dist = 0.0;
+    if (c1) {
+        const double dx = c0[0] - c1[0], dy = c0[1] - c1[1], dz = c0[2] - c1[2];
+        g.half_dist = sqrt(dx * dx + dy * dy + dz * dz) / 2.0;
     }
-    L.fd[f] = d;
+    return g;
+}
+
+__device__ __forceinline__ void load_cc(const double* cc, int nc, int c, double* p) {
+    p[0] = cc[c];
+    p[1] = cc[nc + c];
+    p[2] = cc[2 * nc + c];
+}
+
+static __global__ void face_geometry_kernel(MeshView M, Layer L) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= M.nface) return;
+    const int nf = M.nface, nn = M.nnode, nc = M.ncell;
+    double P[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) load_node(L.xyz, nn, M.face_nodes[k * nf + f], P[k]);
+    double c0[3], c1[3];
+    load_cc(L.cc, nc, M.face_c0[f], c0);
+    const int i1 = M.face_c1[f];
+    if (i1 >= 0) load_cc(L.cc, nc, i1, c1);
+    const FaceGeom g = face_geometry(P, c0, i1 >= 0 ? c1 : nullptr);
+    L.fc[f] = g.c[0];
+    L.fc[nf + f] = g.c[1];
+    L.fc[2 * nf + f] = g.c[2];
+    L.fa[f] = g.area;
+    L.fn[f] = g.n[0];
+    L.fn[nf + f] = g.n[1];
+    L.fn[2 * nf + f] = g.n[2];
+    L.fd[f] = g.half_dist;
 }
 
 // ---------------------------------------------------------------------------
@@ -211,7 +257,7 @@ __device__ __forceinline__ void to_cartesian(double z, double x, double y, doubl
 // Zone_1 cells are carried radially from the cell centre to the face centre:
 // rho, Q, rho_He ~ r^-2, p ~ r^-2gamma, B_r ~ r^-2, B_t ~ r^-1, velocity
 // direction rotated (Setka_gran_snos.cpp:744-873).
-static __device__ __noinline__ void zone1_scale(double* s, double ax, double ay, double az, double gx, double gy, double gz,
+static __device__ __forceinline__ void zone1_scale(double* s, double ax, double ay, double az, double gx, double gy, double gz,
                                          double gamma) {
     const double r1 = sqrt(ax * ax + ay * ay + az * az);
     const double rr = sqrt(gx * gx + gy * gy + gz * gz);
@@ -262,22 +308,46 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         const int nf = M.nface, nc = M.ncell;
         const int type = M.face_type[f];
         const int c0 = M.face_c0[f];
-        const double n[3] = {a.L1.fn[f], a.L1.fn[nf + f], a.L1.fn[2 * nf + f]};
-        const double area = a.L1.fa[f];
+        double n[3], area, dist = 0.0, gc[3];
         double w = 0.0;
         if (MOVE) {
-            const double time = a.st->dt;
+            // geometry of this layer from the face's nodes (as Gran::Culc_measure),
+            // then the face speed from the node displacement (Gran::culc_velosity)
             const int nn = M.nnode;
+            int nid[4];
+            double P[4][3];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                nid[k] = M.face_nodes[k * nf + f];
+                load_node(a.L1.xyz, nn, nid[k], P[k]);
+            }
+            double cA[3], cB[3];
+            load_cc(a.L1.cc, nc, c0, cA);
+            if (type == 0) load_cc(a.L1.cc, nc, M.face_c1[f], cB);
+            const FaceGeom g = face_geometry(P, cA, type == 0 ? cB : nullptr);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                n[k] = g.n[k];
+                gc[k] = g.c[k];
+            }
+            area = g.area;
+            dist = g.half_dist;
+            const double time = a.st->dt;
             double ddot = 0.0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const int i = M.face_nodes[k * nf + f];
-                const double dx = a.xyz2[i] - a.L1.xyz[i];
-                const double dy = a.xyz2[nn + i] - a.L1.xyz[nn + i];
-                const double dz = a.xyz2[2 * nn + i] - a.L1.xyz[2 * nn + i];
+                const int i = nid[k];
+                const double dx = a.xyz2[i] - P[k][0];
+                const double dy = a.xyz2[nn + i] - P[k][1];
+                const double dz = a.xyz2[2 * nn + i] - P[k][2];
                 ddot = ddot + (dx * n[0] + dy * n[1] + dz * n[2]);
             }
             w = ddot / 4.0 / time;
+        } else {
+            n[0] = a.L1.fn[f];
+            n[1] = a.L1.fn[nf + f];
+            n[2] = a.L1.fn[2 * nf + f];
+            area = a.L1.fa[f];
         }
         constexpr int NS = 8 + NK;
         double Ls[NV], Rs[NV];
@@ -291,11 +361,18 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
             for (int k = 0; k < NS; ++k) Rs[k] = a.state[k * nc + c1];
 #pragma unroll
             for (int k = NS; k < NV; ++k) Rs[k] = 0.0;
-            const double gx = a.L1.fc[f], gy = a.L1.fc[nf + f], gz = a.L1.fc[2 * nf + f];
-            if (M.cell_type[c0] == 1)
-                zone1_scale(Ls, a.L1.cc[c0], a.L1.cc[nc + c0], a.L1.cc[2 * nc + c0], gx, gy, gz, P.gamma);
-            if (M.cell_type[c1] == 1)
-                zone1_scale(Rs, a.L1.cc[c1], a.L1.cc[nc + c1], a.L1.cc[2 * nc + c1], gx, gy, gz, P.gamma);
+            const bool z0 = M.cell_type[c0] == 1, z1 = M.cell_type[c1] == 1;
+            if (z0 || z1) {
+                if (!MOVE) {
+                    gc[0] = a.L1.fc[f];
+                    gc[1] = a.L1.fc[nf + f];
+                    gc[2] = a.L1.fc[2 * nf + f];
+                }
+                if (z0)
+                    zone1_scale(Ls, a.L1.cc[c0], a.L1.cc[nc + c0], a.L1.cc[2 * nc + c0], gc[0], gc[1], gc[2], P.gamma);
+                if (z1)
+                    zone1_scale(Rs, a.L1.cc[c1], a.L1.cc[nc + c1], a.L1.cc[2 * nc + c1], gc[0], gc[1], gc[2], P.gamma);
+            }
         } else if (type == 3) {
             // Outer_Soft: copy the interior cell, with the reference's outflow fix-ups
             if (P.soft_fixups) {
@@ -348,7 +425,7 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         const int rc = riemann_flux<R, NK>(method, nr, R(w), qL, qR, kl, kr, q, kq, dsl, dsc, dsr, fl, R(P.gamma));
         if (rc) record_error(a.st, 10 + rc, f);
         if (type == 0) {
-            const double dist = a.L1.fd[f];
+            if (!MOVE) dist = a.L1.fd[f];
             const double dnt = P.KFL * dist / (rmax(fabs(double(dsl)), fabs(double(dsr))) + fabs(w));
             contrib = 10000000.0;
             if (dnt < contrib) contrib = dnt;
@@ -397,7 +474,7 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
 
 // Bera charge-exchange sources of the plasma (Setka_physics.cpp:766-1258,
 // no pickup ions), returning m_x, m_y, m_z, E times n_H_LISM / Kn.
-static __device__ __noinline__ void bera_sources(const Params& P, const double* prim, int ctype, const double* H, int nc,
+static __device__ __forceinline__ void bera_sources(const Params& P, const double* prim, int ctype, const double* H, int nc,
                                           int c, double* S) {
     const double rho = prim[0], p = prim[4], Q = prim[8], rho_He = prim[9];
     int zone;
@@ -463,7 +540,24 @@ __global__ void __launch_bounds__(BS) cell_update_kernel(CellArgs a) {
         const int nc = M.ncell;
         const double time = a.st->dt;
         const double Volume = a.vol1[c];
-        const double Volume2 = MOVE ? a.vol2[c] : Volume;
+        double Volume2 = Volume;
+        if (MOVE) {
+            // centre and volume of the next layer (Cell::Culc_center / Culc_volume)
+            const int nn = M.nnode;
+            double X[8][3];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) load_node(a.L2.xyz, nn, M.cell_nodes[k * nc + c], X[k]);
+            double C[3];
+            cell_centre(X, C);
+            a.L2.cc[c] = C[0];
+            a.L2.cc[nc + c] = C[1];
+            a.L2.cc[2 * nc + c] = C[2];
+            Volume2 = cell_volume(C, [&](int s, int k, double* p) {
+                const int li = (M.cell_fmap[s * nc + c] >> (3 * k)) & 7;
+                load_node(a.L2.xyz, nn, M.cell_nodes[li * nc + c], p);
+            });
+            a.L2.vol[c] = Volume2;
+        }
         using L = FluxLayout<FT, NK>;
         double PO[9 + NK];
 #pragma unroll

@@ -44,6 +44,8 @@ struct MeshView {
     const unsigned char* cell_tvd;
     const double* node_amp;       // [nnode] or null
     const double* node_phase;     // [nnode] or null
+    const unsigned short* cell_fmap;  // [6][ncell]: the 4 nodes of each face slot as
+                                      // 3-bit indices into the cell's 8 nodes (ALE)
 };
 
 struct Layer {  // geometry of one time layer (the reference's [2] arrays)
@@ -70,7 +72,9 @@ struct CellArgs {
     MeshView M;
     Params P;
     const double* vol1;
-    const double* vol2;
+    const double* vol2;    // stationary mesh: the same volumes
+    Layer L2;              // moving mesh: node coordinates of the next layer (read);
+                           // its cell centres and volumes are written here
     const double* state;   // [NV][ncell] current
     double* state2;        // [NV][ncell] next
     const void* flux;

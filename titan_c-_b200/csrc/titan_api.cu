@@ -76,6 +76,7 @@ struct titan_ctx {
     int8_t* d_cell_type = nullptr;
     uint8_t* d_cell_tvd = nullptr;
     double *d_node_amp = nullptr, *d_node_phase = nullptr;
+    uint16_t* d_cell_fmap = nullptr;
 
     Layer layer[2]{};
     int cur = 0;
@@ -122,6 +123,7 @@ struct titan_ctx {
         M.cell_tvd = d_cell_tvd;
         M.node_amp = d_node_amp;
         M.node_phase = d_node_phase;
+        M.cell_fmap = d_cell_fmap;
         return M;
     }
 };
@@ -152,14 +154,12 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     const int nxt = ctx->cur ^ 1;
     cudaError_t e = cudaSuccess;
     if (move) {
+        // the geometry of the next layer is formed inside face_flux (faces of
+        // this layer) and cell_update (cells of the next layer)
         e = timed(ctx, "move_nodes", [&] {
             return launch_move_nodes(M, ctx->P, ctx->layer[ctx->cur].xyz, ctx->layer[nxt].xyz, ctx->d_status,
                                      ctx->stream);
         });
-        if (e) return e;
-        e = timed(ctx, "cell_geometry", [&] { return launch_cell_geometry(M, ctx->layer[nxt], ctx->stream); });
-        if (e) return e;
-        e = timed(ctx, "face_geometry", [&] { return launch_face_geometry(M, ctx->layer[nxt], ctx->stream); });
         if (e) return e;
     }
     FaceArgs fa;
@@ -180,7 +180,8 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     ca.M = M;
     ca.P = ctx->P;
     ca.vol1 = ctx->layer[ctx->cur].vol;
-    ca.vol2 = move ? ctx->layer[nxt].vol : ctx->layer[ctx->cur].vol;
+    ca.vol2 = ctx->layer[ctx->cur].vol;
+    ca.L2 = ctx->layer[nxt];
     ca.state = ctx->d_state[ctx->scur];
     ca.state2 = ctx->d_state[ctx->scur ^ 1];
     ca.flux = ctx->d_flux;
@@ -314,10 +315,12 @@ int titan_destroy(titan_ctx* ctx) {
                     ctx->d_face_nodes, ctx->d_face_type, ctx->d_face_surf, ctx->d_face_method, ctx->d_bc_vals,
                     ctx->d_cell_faces, ctx->d_cell_nodes, ctx->d_cell_type, ctx->d_cell_tvd, ctx->d_node_amp,
                     ctx->d_node_phase, ctx->d_state[0], ctx->d_state[1], ctx->d_flux, ctx->d_hfl, ctx->d_src,
-                    ctx->d_stage, ctx->d_status};
+                    ctx->d_stage, ctx->d_status, ctx->d_cell_fmap};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    for (int l = 0; l < 2; ++l) {
+    // without node motion layer[1] aliases layer[0]: free it once
+    const int nlayers = (ctx->layer[1].xyz != ctx->layer[0].xyz) ? 2 : 1;
+    for (int l = 0; l < nlayers; ++l) {
         Layer& L = ctx->layer[l];
         void* lp[] = {L.xyz, L.cc, L.vol, L.fc, L.fn, L.fa, L.fd};
         for (void* p : lp)
@@ -337,6 +340,7 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     const std::string v = validate(m, p);
     if (!v.empty()) return fail(TITAN_EMESH, v);
 
+    (void)cudaGetLastError();  // launch checks below must not see an earlier call's error
     titan_ctx* ctx = new titan_ctx();
     ctx->ncell = m->ncell;
     ctx->nface = m->nface;
@@ -404,6 +408,31 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
         cell_type[c] = m->cell_type[o];
         cell_tvd[c] = m->cell_tvd[o];
     }
+    // face slot -> the 4 face nodes as indices into the cell's 8 nodes (ALE geometry)
+    std::vector<uint16_t> fmap;
+    if (p->move) {
+        fmap.resize(6 * nc);
+        for (int64_t c = 0; c < nc; ++c) {
+            const int64_t o = R.cell_n2o[c];
+            for (int s = 0; s < 6; ++s) {
+                const int32_t fo = m->cell_faces[6 * o + s];
+                uint16_t code = 0;
+                for (int k = 0; k < 4; ++k) {
+                    int li = -1;
+                    for (int j = 0; j < 8; ++j)
+                        if (m->cell_nodes[8 * o + j] == m->face_nodes[4 * (int64_t)fo + k]) li = j;
+                    if (li < 0) {
+                        char buf[160];
+                        snprintf(buf, sizeof buf, "face %d of cell %lld has a node the cell does not list", fo,
+                                 (long long)o);
+                        return bail(fail(TITAN_EMESH, buf));
+                    }
+                    code |= (uint16_t)(li << (3 * k));
+                }
+                fmap[s * nc + c] = code;
+            }
+        }
+    }
     std::vector<double> xyz(3 * nn), amp, phase;
     for (int64_t i = 0; i < nn; ++i) {
         const int32_t o = R.node_n2o[i];
@@ -446,6 +475,7 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
         DA(ctx->d_node_amp, nn);
         DA(ctx->d_node_phase, nn);
     }
+    if (p->move) DA(ctx->d_cell_fmap, 6 * nc);
     const int nlayers = p->move ? 2 : 1;
     for (int l = 0; l < nlayers; ++l) {
         Layer& L = ctx->layer[l];
@@ -501,6 +531,7 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
         put(ctx->d_node_amp, amp);
         put(ctx->d_node_phase, phase);
     }
+    if (p->move) put(ctx->d_cell_fmap, fmap);
     if (rc) return bail(rc);
     e = cudaMemsetAsync(ctx->d_state[0], 0, sizeof(double) * ctx->ns * nc, s);
     if (!e) e = cudaMemsetAsync(ctx->d_state[1], 0, sizeof(double) * ctx->ns * nc, s);
@@ -661,6 +692,8 @@ int titan_download_geometry(titan_ctx* ctx, double* cc, double* vol, double* fc,
     if (!ctx) return fail(TITAN_EINVAL, "null argument");
     const int64_t nc = ctx->ncell, nf = ctx->nface;
     const Layer& L = ctx->layer[ctx->cur];
+    // a moving mesh keeps only node and cell geometry between steps
+    if (ctx->prm.move) CK(launch_face_geometry(ctx->view(), L, ctx->stream));
     std::vector<double> hcc(3 * nc), hvol(nc), hfc(3 * nf), hfn(3 * nf), hfa(nf);
     CK(cudaMemcpyAsync(hcc.data(), L.cc, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(hvol.data(), L.vol, sizeof(double) * nc, cudaMemcpyDeviceToHost, ctx->stream));
@@ -821,12 +854,9 @@ int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     const bool move = ctx->prm.move != 0;
     const int nxt = ctx->cur ^ 1;
     // the next layer = the current one, so every input the kernels read is valid
-    if (move) {
+    if (move)
         CK(cudaMemcpyAsync(ctx->layer[nxt].xyz, ctx->layer[ctx->cur].xyz, sizeof(double) * 3 * ctx->nnode,
                            cudaMemcpyDeviceToDevice, s));
-        CK(launch_cell_geometry(M, ctx->layer[nxt], s));
-        CK(launch_face_geometry(M, ctx->layer[nxt], s));
-    }
     DevStatus init{};
     init.dt = 1e-5;
     init.dt_next_bits = 0x4197D78400000000ull;
@@ -842,7 +872,8 @@ int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     ca.M = M;
     ca.P = ctx->P;
     ca.vol1 = ctx->layer[ctx->cur].vol;
-    ca.vol2 = ctx->layer[nxt].vol;
+    ca.vol2 = ctx->layer[ctx->cur].vol;
+    ca.L2 = ctx->layer[nxt];
     ca.state = ctx->d_state[ctx->scur];
     ca.state2 = ctx->d_state[ctx->scur ^ 1];
     ca.flux = ctx->d_flux;

@@ -169,7 +169,7 @@ int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, con
 
 /* Launch-shape autotuner (no reference counterpart: the reference's OpenMP
  * loops have no launch shapes). Times every face-flux variant (threads per
- * block x minimum resident blocks per SM) and every cell-update block size on
+ * block x minimum resident blocks per SM) and every cell-update shape on
  * this context's mesh and state, `reps` launches each, and keeps the fastest.
  * Call after titan_upload_state. With a cache file, a line for the same mesh
  * size and step options is reused instead of timing, and new results are

@@ -133,6 +133,11 @@ def test_brio_wu_face_fluxes_match_oracle(T, oracle_lib):
     dict(move=True, zones=True, npassive=2, nh=4),
 ])
 def test_heliosphere_shell_steps_match_oracle(T, oracle_lib, features):
+    """Five steps without re-synchronising. Zone_1 reconstruction and the Bera
+    sources call acos/atan/sin/cos/pow/log, where CUDA's math library and glibc
+    may round differently by an ulp; those differences compound over the run,
+    so the bar is REL per step times the steps times a growth margin of 10.
+    Without those features the match is exact."""
     m, p, st, hf = T.problems.heliosphere_shell(nq=8, nlayer=6, **features)
     gpu, run = _pair(T, m, p, hf=hf)
     gpu.upload_state(st)
@@ -143,16 +148,21 @@ def test_heliosphere_shell_steps_match_oracle(T, oracle_lib, features):
     s_gpu = gpu.download_state()
     ns = 8 + p["npassive"]
     e = rel_err(s_gpu[:ns], s_or[:ns])
-    assert e <= REL, e
+    transcendental = features["zones"] or features["nh"] > 0
+    assert e <= (REL * 5 * 10 if transcendental else REL), e
+    if not transcendental:
+        assert np.array_equal(s_gpu[:ns], s_or[:ns])
     np.testing.assert_array_equal(gpu.nodes(), run.xyz)
     assert abs(gpu.dt - run.clock[0]) <= REL * run.clock[0]
     gpu.close()
 
 
-def test_per_step_parity_over_a_run(T, oracle_lib):
-    """Re-synchronise the oracle to the GPU state every step: per-step error <= 1e-12."""
-    m, p, st, hf = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, zones=True, npassive=2)
-    gpu, run = _pair(T, m, p)
+@pytest.mark.parametrize("nh", [0, 4])
+def test_per_step_parity_over_a_run(T, oracle_lib, nh):
+    """Re-synchronise the oracle to the GPU state every step: per-step error <= 1e-12,
+    with every feature on (node motion, Zone_1/Zone_2 cells, passive scalars, Bera sources)."""
+    m, p, st, hf = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, zones=True, npassive=2, nh=nh)
+    gpu, run = _pair(T, m, p, hf=hf)
     gpu.upload_state(st)
     worst = 0.0
     for k in range(20):
@@ -225,7 +235,7 @@ def test_every_launch_shape_gives_identical_results(T):
     m, p, st, hf = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, zones=True, npassive=2)
     outs = []
     for fv in range(6):
-        for cv in range(3):
+        for cv in range(5):
             if cv and fv:
                 continue
             g = T.PlasmaStep(m, p)
@@ -245,7 +255,7 @@ def test_autotune_picks_a_shape_and_caches_it(T, tmp_path):
     g.set_face_method(meth)
     g.upload_state(st)
     t1 = g.autotune(reps=2, cache=cache)
-    assert 0 <= t1["face_variant"] < 6 and 0 <= t1["cell_variant"] < 3
+    assert 0 <= t1["face_variant"] < 6 and 0 <= t1["cell_variant"] < 5
     assert open(cache).read().count("|") == 1
     g2 = T.PlasmaStep(m, p)
     g2.upload_state(st)

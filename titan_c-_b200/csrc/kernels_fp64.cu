@@ -53,20 +53,30 @@ cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, int vari
     return cudaErrorInvalidValue;
 }
 
-template <typename FT, int NK, bool MOVE, int BS>
+template <typename FT, int NK, bool MOVE, int BS, int MINB>
 static void cell_update_src(const CellArgs& a, int src, cudaStream_t s) {
     const unsigned int g = blocks_for(a.M.ncell, BS);
-    if (src == 0) cell_update_kernel<FT, NK, MOVE, 0, BS><<<g, BS, 0, s>>>(a);
-    else if (src == 1) cell_update_kernel<FT, NK, MOVE, 1, BS><<<g, BS, 0, s>>>(a);
-    else cell_update_kernel<FT, NK, MOVE, 2, BS><<<g, BS, 0, s>>>(a);
+    if (src == 0) cell_update_kernel<FT, NK, MOVE, 0, BS, MINB><<<g, BS, 0, s>>>(a);
+    else if (src == 1) cell_update_kernel<FT, NK, MOVE, 1, BS, MINB><<<g, BS, 0, s>>>(a);
+    else cell_update_kernel<FT, NK, MOVE, 2, BS, MINB><<<g, BS, 0, s>>>(a);
 }
 
 template <typename FT, int NK, bool MOVE>
 static cudaError_t cell_update_variant(const CellArgs& a, int src, int v, cudaStream_t s) {
-    if (v == 0) cell_update_src<FT, NK, MOVE, kCellBlock[0]>(a, src, s);
-    else if (v == 1) cell_update_src<FT, NK, MOVE, kCellBlock[1]>(a, src, s);
-    else if (v == 2) cell_update_src<FT, NK, MOVE, kCellBlock[2]>(a, src, s);
-    else return cudaErrorInvalidValue;
+    switch (v) {
+#define TITAN_CELL_CASE(i)                                                                   \
+    case i:                                                                                \
+        cell_update_src<FT, NK, MOVE, kCellVariant[i].block, kCellVariant[i].min_blocks>(a, src, s); \
+        break;
+        TITAN_CELL_CASE(0)
+        TITAN_CELL_CASE(1)
+        TITAN_CELL_CASE(2)
+        TITAN_CELL_CASE(3)
+        TITAN_CELL_CASE(4)
+#undef TITAN_CELL_CASE
+        default:
+            return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -531,8 +531,8 @@ static __device__ __forceinline__ void bera_sources(const Params& P, const doubl
     S[3] = Es * ddp;
 }
 
-template <typename FT, int NK, bool MOVE, int SRC, int BS>
-__global__ void __launch_bounds__(BS) cell_update_kernel(CellArgs a) {
+template <typename FT, int NK, bool MOVE, int SRC, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) cell_update_kernel(CellArgs a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const bool ok = a.st->err_kind == 0;
     if (c < a.M.ncell && ok) {

@@ -820,7 +820,7 @@ int titan_get_tuning(titan_ctx* ctx, int32_t* face_variant, int32_t* cell_varian
     if (cell_variant) *cell_variant = ctx->cell_variant;
     if (face_block) *face_block = kFaceVariant[ctx->face_variant].block;
     if (face_min_blocks) *face_min_blocks = kFaceVariant[ctx->face_variant].min_blocks;
-    if (cell_block) *cell_block = kCellBlock[ctx->cell_variant];
+    if (cell_block) *cell_block = kCellVariant[ctx->cell_variant].block;
     return TITAN_OK;
 }
 

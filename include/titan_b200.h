@@ -191,6 +191,60 @@ int titan_kernel_times(titan_ctx* ctx, const char** names, double* total_ms, int
 /* Bytes of device memory the context holds. */
 int64_t titan_device_bytes(titan_ctx* ctx);
 
+/* ---------------------------------------------------------------------------
+ * titan_step_noalloc — one plasma step that allocates nothing.
+ *
+ * No counterpart in the reference. It exists for callers that cannot call
+ * cudaMalloc when they step: a code whose allocator owns all device memory (a
+ * framework's caching allocator or a pool sized at start-up), a real-time
+ * loop that forbids allocation after initialisation, or an embedding that
+ * must not touch the CUDA allocator. They pass device arrays they already own
+ * (titan_dev_mesh, the states) and get one step of titan_step's kernels.
+ *
+ * The step's scratch — the per-face flux buffer and its status word — is a
+ * fixed array compiled into the library (about 12.6 MB, present on every GPU
+ * that loads the library until the process exits), so at most
+ * TITAN_NOALLOC_MAX_FACES faces; larger meshes get TITAN_EINVAL. Stationary
+ * meshes only (params->move = 0). The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress) and caches it: make that first
+ * call before any stream capture. All calls share the array, which keeps the
+ * previous call's contents (each call resets the status word itself), so calls
+ * that overlap on the GPU race; run them one at a time.
+ *
+ * All pointers in titan_dev_mesh and state_in/state_out are DEVICE memory,
+ * in the library's kernel layout, in any consistent cell/face numbering:
+ * states SoA [8 + npassive][ncell]; per-face arrays [nface]; [3][n] SoA for
+ * vectors; bc_vals SoA [TITAN_NV][nbc]; cell_faces [6][ncell] face ids with
+ * bit 31 set where the cell is the face's cells[1]. dt: this step's dt.
+ * dt_next (host): the CFL dt of the next step. err_kind (host, may be NULL):
+ * the step's failure kind as in titan_step_info. `stream` is a cudaStream_t
+ * (NULL: the legacy default stream); the call returns after it synchronises. */
+#define TITAN_NOALLOC_MAX_FACES 131072
+
+typedef struct titan_dev_mesh {
+    int64_t ncell, nface, nbc;
+    const int32_t* face_c0;        /* [nface] cells[0] */
+    const int32_t* face_c1;        /* [nface] cells[1], -1 on boundary faces */
+    const int8_t*  face_type;      /* [nface] Type_Gran */
+    const int8_t*  face_surf;      /* [nface] Type_Gran_surf */
+    const int8_t*  face_method;    /* [nface] n_state, read when method_policy = 0 */
+    const int32_t* face_bc;        /* [nface] column of bc_vals for hard faces, else -1 */
+    const double*  bc_vals;        /* [TITAN_NV][nbc] */
+    const int32_t* cell_faces;     /* [6][ncell] */
+    const int8_t*  cell_type;      /* [ncell] */
+    const uint8_t* cell_tvd;       /* [ncell] */
+    const double*  cell_center;    /* [3][ncell] */
+    const double*  cell_volume;    /* [ncell] */
+    const double*  face_center;    /* [3][nface] */
+    const double*  face_normal;    /* [3][nface] unit, from cells[0] to cells[1] */
+    const double*  face_area;      /* [nface] */
+    const double*  face_half_dist; /* [nface] half the distance between the two cell centres */
+    const double*  hfluids;        /* [5*nh][ncell] or NULL when nh = 0 */
+} titan_dev_mesh;
+
+int titan_step_noalloc(const titan_dev_mesh* mesh, const titan_params* params, double dt, const double* state_in,
+                       double* state_out, double* dt_next, int32_t* err_kind, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

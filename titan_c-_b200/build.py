@@ -7,6 +7,7 @@ Translation units and their floating-point flags:
   kernels_fp32.cu  -fmad=true -prec-div=false -prec-sqrt=false
                                 FP32 Riemann flux of the mixed-precision step
   titan_api.cu, renumber.cpp    host side of the C ABI
+  noalloc.cu       -fmad=false  titan_step_noalloc (fixed scratch array, no allocation)
 """
 from __future__ import annotations
 
@@ -27,6 +28,7 @@ UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
     ("kernels_fp32.cu", ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("titan_api.cu", []),
+    ("noalloc.cu", ["-fmad=false"]),
     ("renumber.cpp", []),
 ]
 

@@ -50,6 +50,11 @@ cudaError_t dput(T* d, const std::vector<T>& h, cudaStream_t s) {
 
 }  // namespace
 
+namespace titan {
+// Lets other translation units report through titan_last_error().
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace titan
+
 struct KernelClock {
     double ms = 0.0;
     int64_t launches = 0;

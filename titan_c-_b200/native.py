@@ -53,6 +53,15 @@ class TitanParams(ctypes.Structure):
     ]
 
 
+class TitanDevMesh(ctypes.Structure):
+    """titan_dev_mesh: device pointers (as integers) for titan_step_noalloc."""
+    _fields_ = [("ncell", ctypes.c_int64), ("nface", ctypes.c_int64), ("nbc", ctypes.c_int64)] + [
+        (name, ctypes.c_void_p) for name in (
+            "face_c0", "face_c1", "face_type", "face_surf", "face_method", "face_bc", "bc_vals", "cell_faces",
+            "cell_type", "cell_tvd", "cell_center", "cell_volume", "face_center", "face_normal", "face_area",
+            "face_half_dist", "hfluids")]
+
+
 class TitanStepInfo(ctypes.Structure):
     _fields_ = [
         ("steps_done", ctypes.c_int64), ("err_index", ctypes.c_int64), ("n_rho_floor", ctypes.c_int64),
@@ -90,6 +99,9 @@ SIGNATURES = {
     "titan_kernel_times": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p), D, I64, ctypes.c_int32],
                            ctypes.c_int),
     "titan_device_bytes": ([ctypes.c_void_p], ctypes.c_int64),
+    "titan_step_noalloc": ([ctypes.POINTER(TitanDevMesh), ctypes.POINTER(TitanParams), ctypes.c_double,
+                            ctypes.c_void_p, ctypes.c_void_p, D, ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p],
+                           ctypes.c_int),
 }
 
 _lib = None

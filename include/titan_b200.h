@@ -167,6 +167,35 @@ int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, con
                         const double* q2, int32_t flags, int32_t precision, double gamma, double* flux,
                         double* ds, int32_t* rc);
 
+/* Monte-Carlo neutral hydrogen through the current plasma state: the source
+ * generator the closure is trained on. Physics of the reference's
+ * Setka::MK_fly_immit (TITAN/source/Setka_MK.cpp:1752-2314: charge-exchange
+ * rate from Velosity_1 :40-50, new velocity by M_K_Change_Velosity :2788-2852),
+ * with momentum and energy exchange tallies the reference does not keep
+ * (it tallies densities only, Cell.cpp:1042-1085). Neutrals enter through the
+ * boundary faces whose Type_Gran bit is set in `face_types`, from a drifting
+ * Maxwellian exp(-|v - u_H|^2 / cp_H^2) of density n_H, in proportion to each
+ * face's inflow flux. out [5][ncell], original numbering: n_H, then the plasma
+ * momentum (3) and energy sources per unit time and volume (the plasma mass
+ * source of charge exchange is identically zero). */
+typedef struct titan_mc_params {
+    double n_H;
+    double u_H[3];
+    double cp_H;
+    int64_t n_particles;
+    uint64_t seed;
+    int32_t max_cells;   /* cell visits before a particle counts as lost (0: 1000000) */
+    int32_t face_types;  /* e.g. (1 << TITAN_FACE_OUTER_HARD) | (1 << TITAN_FACE_OUTER_SOFT) */
+} titan_mc_params;
+
+typedef struct titan_mc_info {
+    int64_t particles, lost;
+    double inflow_rate;  /* neutrals entering per unit time */
+    double gpu_ms;
+} titan_mc_info;
+
+int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* params, double* out, titan_mc_info* info);
+
 /* Launch-shape autotuner (no reference counterpart: the reference's OpenMP
  * loops have no launch shapes). Times every face-flux variant (threads per
  * block x minimum resident blocks per SM) and every cell-update shape on

@@ -2,7 +2,9 @@
 
 FP64: bit-exact where the arithmetic is the reference's (Riemann solver,
 geometry, update); the bar written into every comparison is 1e-12 relative per
-cell per step, and the tests also report whether the match is exact.
+cell per step on the conserved fields, and tests assert exact equality where no
+transcendental function is involved. Zone_1 reconstruction calls acos / atan /
+sin / cos / pow, where CUDA's math library and glibc can differ by an ulp.
 FP32 flux: relative L1 error against the FP64 oracle below 1e-4.
 """
 import numpy as np
@@ -15,11 +17,34 @@ pytestmark = pytest.mark.gpu
 REL = 1e-12
 
 
+def conserved(x, gamma=5.0 / 3.0):
+    """Primitive state rows (rho, V, p, B Gaussian, Q, rho_He) -> conserved
+    (rho, rho V, E = p/(gamma-1) + rho V^2/2 + B^2/(8 pi), B, Q, rho_He)."""
+    x = np.asarray(x, dtype=np.float64)
+    u = x.copy()
+    u[1:4] = x[0] * x[1:4]
+    u[4] = x[4] / (gamma - 1.0) + 0.5 * x[0] * np.sum(x[1:4] ** 2, axis=0) + np.sum(x[5:8] ** 2, axis=0) / (8 * np.pi)
+    return u
+
+
 def rel_err(a, b):
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
-    scale = np.maximum(np.abs(b), 1e-300)
-    return float(np.max(np.abs(a - b) / np.maximum(scale, 1e-12 * np.max(np.abs(b)))))
+    """Largest relative error per cell over the conserved fields: rho, E, Q and
+    rho_He against their value, the vectors rho V and B as |d| / |vector|, each
+    floored at 1e-12 of the field's largest magnitude in the mesh. (Pressure is
+    recovered from E by cancellation; in hypersonic cells an ulp of E is many
+    ulps of p, so p itself is not the per-cell measure.)"""
+    a, b = conserved(a), conserved(b)
+    out = 0.0
+    groups = [[0], [1, 2, 3], [4], [5, 6, 7], [8], [9]]
+    for g in groups:
+        g = [k for k in g if k < b.shape[0]]
+        if not g:
+            continue
+        d = np.sqrt(np.sum((a[g] - b[g]) ** 2, axis=0))
+        mag = np.sqrt(np.sum(b[g] ** 2, axis=0))
+        floor = max(1e-12 * float(mag.max()), 1e-300)
+        out = max(out, float(np.max(d / np.maximum(mag, floor))))
+    return out
 
 
 @pytest.fixture(scope="module")

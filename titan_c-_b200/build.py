@@ -6,6 +6,7 @@ Translation units and their floating-point flags:
   kernels_fp64.cu  -fmad=false  geometry, FP64 flux, cell update (bit-exact FP64)
   kernels_fp32.cu  -fmad=true -prec-div=false -prec-sqrt=false
                                 FP32 Riemann flux of the mixed-precision step
+  mc_neutral.cu                 Monte-Carlo neutral hydrogen (source generator)
   titan_api.cu, renumber.cpp    host side of the C ABI
   noalloc.cu       -fmad=false  titan_step_noalloc (fixed scratch array, no allocation)
 """
@@ -27,6 +28,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
     ("kernels_fp32.cu", ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
+    ("mc_neutral.cu", []),
     ("titan_api.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("renumber.cpp", []),

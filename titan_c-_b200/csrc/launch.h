@@ -40,6 +40,9 @@ cudaError_t launch_riemann_batch_fp32(long long n, const signed char* ns, const 
                                       const double* q1, const double* q2, double* flux, double* ds, int* rc,
                                       int flags, double gamma, cudaStream_t s);
 
+cudaError_t launch_mc_trace(const McArgs& a, cudaStream_t s);
+cudaError_t launch_mc_normalise(double* tally, const double* vol, int ncell, cudaStream_t s);
+
 inline unsigned int blocks_for(long long n, int bs) { return (unsigned int)((n + bs - 1) / bs); }
 
 }  // namespace titan

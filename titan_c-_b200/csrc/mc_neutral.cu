@@ -1,0 +1,258 @@
+// Monte-Carlo neutral hydrogen on the plasma mesh: the source generator the
+// closure is trained on and falls back to.
+//
+// Physics restated from TITAN's MK_fly_immit (TITAN/source/Setka_MK.cpp:1752-2314):
+//  * a neutral flies straight through the cells; in a cell its charge-exchange
+//    frequency is nu = rho_Th * uz * sigma(uz) / Kn, uz = Velosity_1(|v - V_p|, cp)
+//    (the Maxwell-averaged relative speed, Setka_MK.cpp:40-50), cp = sqrt(2 p_Th / rho_Th),
+//    sigma(u) = (1 - a2 ln u)^2 (Phys_param.h:177-180) (Setka_MK.cpp:1976-1988);
+//  * the optical depth accumulates nu * dt until it reaches -ln(1 - xi);
+//  * at a charge exchange the new neutral velocity is drawn from the local proton
+//    Maxwellian weighted by u sigma(u), by the rejection scheme of
+//    Setka::M_K_Change_Velosity (Setka_MK.cpp:2788-2852);
+//  * rho_Th, p_Th from Phys_param::Plasma_components_1 (Phys_param.cpp:628-665) with the
+//    cell type as zone (Setka_MK.cpp:1956), floored as at Setka_MK.cpp:1966-1967.
+// Added here (the reference tallies only densities, Cell.cpp:1042-1085): the
+// momentum and energy the plasma gains at each exchange, mu (v_old - v_new) and
+// mu (|v_old|^2 - |v_new|^2) / 2, per unit time and volume.
+//
+// Launch: neutrals enter through the hard outer boundary faces from a drifting
+// Maxwellian (density n_H, bulk velocity u_H, thermal speed cp_H), the number per
+// face proportional to its inflow flux; each carries weight mu = total inflow
+// per unit time / N, so sum(mu * time in cell) / V is the density.
+// Random numbers: a counter-based generator (SplitMix64 finaliser over seed,
+// particle id and draw counter), so a run is reproducible for any launch shape.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/titan_b200.h"
+#include "launch.h"
+#include "step_kernels.cuh"
+
+namespace titan {
+namespace mc {
+
+constexpr double kSqrtPi = 1.77245385;  // sqrtpi_ of TITAN/source/Header.h:94
+
+struct Rng {
+    unsigned long long key;
+    unsigned long long ctr;
+    __device__ double uniform() {
+        // SplitMix64 finaliser (Steele, Lea, Flood 2014) of a counter: a value in (0, 1)
+        unsigned long long z = key + 0x9E3779B97F4A7C15ull * (++ctr);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z = z ^ (z >> 31);
+        return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    }
+};
+
+// Velosity_1 (Setka_MK.cpp:40-50): mean relative speed of a neutral moving at u
+// through protons of thermal speed cp.
+__device__ __forceinline__ double velosity_1(double u, double cp) {
+    if (u < 0.00001)
+        return 2.0 * cp / kSqrtPi + 2.0 * u * u / (3.0 * cp * kSqrtPi) - u * u * u * u / (15.0 * cp * cp * cp * kSqrtPi);
+    return exp(-u * u / (cp * cp)) * cp / kSqrtPi + (u + (cp * cp) / (2.0 * u)) * erf(u / cp);
+}
+
+__device__ __forceinline__ double sigma(double a2, double x) {
+    const double s = 1.0 - a2 * log(x);
+    return s * s;
+}
+
+using Args = McArgs;
+
+__device__ void plasma_in_cell(const Args& a, int c, double& rho_th, double& cp, double V[3]) {
+    const int nc = a.M.ncell;
+    const double rho = a.state[c], p = a.state[4 * nc + c];
+    const double Q = a.P.npassive ? a.state[8 * nc + c] : 0.0;
+    const double rho_He = a.P.npassive ? a.state[9 * nc + c] : 0.0;
+    V[0] = a.state[nc + c];
+    V[1] = a.state[2 * nc + c];
+    V[2] = a.state[3 * nc + c];
+    (void)Q;
+    // the Monte-Carlo passes the cell type as the zone (Setka_MK.cpp:1956)
+    const int al = (a.M.cell_type[c] <= 2) ? 2 : 1;
+    double r = -(kMeDmp * al * rho_He + 4.0 * (-rho + rho_He)) / (4.0 * (1.0 + kMeDmp));
+    double pt = p * (4.0 * rho - (4.0 + al * kMeDmp) * rho_He) / (8.0 * rho + (-7.0 + al + (1.0 - al) * kMeDmp) * rho_He);
+    if (r <= 1e-8) r = 1e-8;
+    if (pt <= 1e-8 / 2.0) pt = 1e-8 / 2.0;
+    rho_th = r;
+    cp = sqrt(2.0 * pt / r);
+}
+
+// New neutral velocity after an exchange (Setka::M_K_Change_Velosity): Ur/U are
+// the proton bulk and V the old neutral velocity, all in units of cp.
+__device__ void change_velocity(Rng& rng, double a2, double cp, const double U[3], const double Vn[3], double W[3]) {
+    const double X = sqrt((Vn[0] - U[0]) * (Vn[0] - U[0]) + (Vn[1] - U[1]) * (Vn[1] - U[1]) +
+                          (Vn[2] - U[2]) * (Vn[2] - U[2]));
+    const double p4 = 0.5 * kSqrtPi * X / (1.0 + 0.5 * kSqrtPi * X);
+    double v1 = U[0], v2 = U[1], v3 = U[2];
+    for (int it = 0; it < 1000; ++it) {
+        const double k1 = rng.uniform(), k2 = rng.uniform(), k3 = rng.uniform();
+        const double k4 = rng.uniform(), k5 = rng.uniform(), k6 = rng.uniform();
+        double y1, y2, y3;
+        if (p4 < k1) {
+            const double om1 = 1.0 - 2.0 * k4;
+            const double so = sqrt(1.0 - om1 * om1);
+            const double om2 = so * cos(2.0 * kPi * k5), om3 = so * sin(2.0 * kPi * k5);
+            const double lo = sqrt(-log(k2 * k3));
+            y1 = lo * om1;
+            y2 = lo * om2;
+            y3 = lo * om3;
+        } else {
+            y1 = sqrt(-log(k2)) * cos(kPi * k3);
+            y2 = sqrt(-log(k4)) * cos(2.0 * kPi * k5);
+            y3 = sqrt(-log(k4)) * sin(2.0 * kPi * k5);
+        }
+        v1 = y1 + U[0];
+        v2 = y2 + U[1];
+        v3 = y3 + U[2];
+        const double u1 = Vn[0] - v1, u2 = Vn[1] - v2, u3 = Vn[2] - v3;
+        const double uuu = sqrt(u1 * u1 + u2 * u2 + u3 * u3);
+        const double yy = sqrt(y1 * y1 + y2 * y2 + y3 * y3);
+        const double h = (uuu * sigma(a2, uuu * cp)) / (sigma(a2, X * cp) * (X + yy));
+        if (!(h < k6)) break;
+    }
+    W[0] = v1;
+    W[1] = v2;
+    W[2] = v3;
+}
+
+__global__ void __launch_bounds__(128) trace_kernel(Args a) {
+    const long long pid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (pid >= a.nparticles) return;
+    const MeshView& M = a.M;
+    const int nc = M.ncell, nf = M.nface;
+    Rng rng{a.seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(pid + 1)), 0ull};
+    // stratified choice of the inflow face by its share of the flux
+    const double s = ((double)pid + rng.uniform()) / (double)a.nparticles;
+    int lo = 0, hi = a.ninflow - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a.inflow_cdf[mid] < s)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    const int f0 = a.inflow_face[lo];
+    // position: uniform on the quad (two triangles by area)
+    double P[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) load_node(a.L.xyz, M.nnode, M.face_nodes[k * nf + f0], P[k]);
+    const double A1 = tri_area(P[0][0], P[0][1], P[0][2], P[1][0], P[1][1], P[1][2], P[2][0], P[2][1], P[2][2]);
+    const double A2 = tri_area(P[0][0], P[0][1], P[0][2], P[3][0], P[3][1], P[3][2], P[2][0], P[2][1], P[2][2]);
+    const int tb = (rng.uniform() * (A1 + A2) < A1) ? 1 : 3;
+    double b1 = rng.uniform(), b2 = rng.uniform();
+    if (b1 + b2 > 1.0) {
+        b1 = 1.0 - b1;
+        b2 = 1.0 - b2;
+    }
+    double x[3];
+    for (int k = 0; k < 3; ++k) x[k] = P[0][k] + b1 * (P[tb][k] - P[0][k]) + b2 * (P[2][k] - P[0][k]);
+    // velocity: flux-weighted drifting Maxwellian through the inward normal
+    const double nin[3] = {-a.L.fn[f0], -a.L.fn[nf + f0], -a.L.fn[2 * nf + f0]};
+    const double un = a.uH0 * nin[0] + a.uH1 * nin[1] + a.uH2 * nin[2];
+    const double vmax = fmax(un, 0.0) + 6.0 * a.cpH;
+    double v[3] = {a.uH0, a.uH1, a.uH2};
+    for (int it = 0; it < 4096; ++it) {
+        // Box-Muller pairs for exp(-y^2) per component
+        const double r1 = sqrt(-log(rng.uniform())), t1 = 2.0 * kPi * rng.uniform();
+        const double r2 = sqrt(-log(rng.uniform())), t2 = 2.0 * kPi * rng.uniform();
+        v[0] = a.uH0 + a.cpH * r1 * cos(t1);
+        v[1] = a.uH1 + a.cpH * r1 * sin(t1);
+        v[2] = a.uH2 + a.cpH * r2 * cos(t2);
+        const double vn = v[0] * nin[0] + v[1] * nin[1] + v[2] * nin[2];
+        if (vn > 0.0 && rng.uniform() * vmax < vn) break;
+    }
+    int cell = M.face_c0[f0];
+    double ksi = -log(1.0 - rng.uniform());
+    double I = 0.0;
+    double* T = a.tally;
+    for (int visit = 0; visit < a.max_cells; ++visit) {
+        // exit through the face of this cell that the ray reaches first
+        double t_exit = 1e300;
+        int fexit = -1;
+        bool ext = false;
+#pragma unroll
+        for (int sl = 0; sl < 6; ++sl) {
+            const int fs = M.cell_faces[sl * nc + cell];
+            const int f = fs & 0x7fffffff;
+            const double sg = (fs < 0) ? -1.0 : 1.0;  // outward normal of this cell
+            const double n0 = sg * a.L.fn[f], n1 = sg * a.L.fn[nf + f], n2 = sg * a.L.fn[2 * nf + f];
+            const double vn = v[0] * n0 + v[1] * n1 + v[2] * n2;
+            if (vn <= 0.0) continue;
+            const double d = (a.L.fc[f] - x[0]) * n0 + (a.L.fc[nf + f] - x[1]) * n1 + (a.L.fc[2 * nf + f] - x[2]) * n2;
+            const double t = fmax(d, 0.0) / vn;
+            if (t < t_exit) {
+                t_exit = t;
+                fexit = f;
+                ext = (fs < 0);
+            }
+        }
+        if (fexit < 0) break;  // no outgoing face (degenerate): give up on this particle
+        double rho_th, cp, Vp[3];
+        plasma_in_cell(a, cell, rho_th, cp, Vp);
+        const double du0 = v[0] - Vp[0], du1 = v[1] - Vp[1], du2 = v[2] - Vp[2];
+        const double u = sqrt(du0 * du0 + du1 * du1 + du2 * du2);
+        const double uz = velosity_1(u, cp);
+        const double nu = rho_th * uz * sigma(a.P.par_a_2, uz) / a.P.par_Kn;
+        const double dI = nu * t_exit;
+        if (I + dI < ksi) {
+            atomicAdd(&T[cell], a.mu * t_exit);
+            I += dI;
+            for (int k = 0; k < 3; ++k) x[k] += t_exit * v[k];
+            const int other = ext ? M.face_c0[fexit] : M.face_c1[fexit];
+            if (other < 0) return;  // left through the boundary
+            cell = other;
+            continue;
+        }
+        // charge exchange inside this cell
+        const double t_ex = (ksi - I) / nu;
+        atomicAdd(&T[cell], a.mu * t_ex);
+        for (int k = 0; k < 3; ++k) x[k] += t_ex * v[k];
+        const double U[3] = {Vp[0] / cp, Vp[1] / cp, Vp[2] / cp};
+        const double Vn[3] = {v[0] / cp, v[1] / cp, v[2] / cp};
+        double W[3];
+        change_velocity(rng, a.P.par_a_2, cp, U, Vn, W);
+        const double w0 = W[0] * cp, w1 = W[1] * cp, w2 = W[2] * cp;
+        atomicAdd(&T[nc + cell], a.mu * (v[0] - w0));
+        atomicAdd(&T[2 * nc + cell], a.mu * (v[1] - w1));
+        atomicAdd(&T[3 * nc + cell], a.mu * (v[2] - w2));
+        atomicAdd(&T[4 * nc + cell],
+                  a.mu * 0.5 * ((v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) - (w0 * w0 + w1 * w1 + w2 * w2)));
+        v[0] = w0;
+        v[1] = w1;
+        v[2] = w2;
+        I = 0.0;
+        ksi = -log(1.0 - rng.uniform());
+    }
+    atomicAdd(a.lost, 1ull);
+}
+
+// Divides the tallies by the cell volumes: n_H and the source densities.
+__global__ void normalise_kernel(double* T, const double* vol, int nc) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const double V = vol[c];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) T[k * nc + c] /= V;
+}
+
+}  // namespace mc
+
+cudaError_t launch_mc_trace(const McArgs& a, cudaStream_t s) {
+    mc::trace_kernel<<<blocks_for(a.nparticles, 128), 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mc_normalise(double* tally, const double* vol, int ncell, cudaStream_t s) {
+    mc::normalise_kernel<<<blocks_for(ncell, 256), 256, 0, s>>>(tally, vol, ncell);
+    return cudaGetLastError();
+}
+
+}  // namespace titan

@@ -808,6 +808,100 @@ int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, con
     return TITAN_OK;
 }
 
+int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, titan_mc_info* info) {
+    if (!ctx || !mp || !out) return fail(TITAN_EINVAL, "null argument");
+    if (mp->n_particles <= 0 || !(mp->n_H > 0.0) || !(mp->cp_H > 0.0)) return fail(TITAN_EINVAL, "bad MC parameters");
+    const int64_t nc = ctx->ncell, nf = ctx->nface;
+    cudaStream_t s = ctx->stream;
+    const MeshView M = ctx->view();
+    const Layer& L = ctx->layer[ctx->cur];
+    if (ctx->prm.move) CK(launch_face_geometry(M, L, s));  // faces of the current layer
+    // inflow faces and their share of the flux of a drifting Maxwellian through
+    // the inward normal: n [cp e^{-s^2} / (2 sqrt(pi)) + u_n (1 + erf s) / 2], s = u_n / cp
+    std::vector<double> fn(3 * nf), fa(nf);
+    std::vector<int8_t> ft(nf);
+    CK(cudaMemcpyAsync(fn.data(), L.fn, sizeof(double) * 3 * nf, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(fa.data(), L.fa, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(ft.data(), ctx->d_face_type, nf, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<int32_t> faces;
+    std::vector<double> cdf;
+    double total = 0.0;
+    const double sqpi = std::sqrt(3.14159265358979323846);
+    for (int64_t f = 0; f < nf; ++f) {
+        if (ft[f] == 0 || !((mp->face_types >> ft[f]) & 1)) continue;
+        const double un = -(mp->u_H[0] * fn[f] + mp->u_H[1] * fn[nf + f] + mp->u_H[2] * fn[2 * nf + f]);
+        const double sr = un / mp->cp_H;
+        const double flux = mp->n_H * (mp->cp_H * std::exp(-sr * sr) / (2.0 * sqpi) + 0.5 * un * (1.0 + std::erf(sr)));
+        total += flux * fa[f];
+        faces.push_back((int32_t)f);
+        cdf.push_back(total);
+    }
+    if (faces.empty() || !(total > 0.0)) return fail(TITAN_EINVAL, "no inflow faces of the requested types");
+    for (double& c : cdf) c /= total;
+    cdf.back() = 1.0;
+    int32_t* d_faces = nullptr;
+    double *d_cdf = nullptr, *d_tally = nullptr;
+    unsigned long long* d_lost = nullptr;
+    int64_t tmp = 0;
+    cudaError_t e = dalloc(&d_faces, faces.size(), &tmp);
+    if (!e) e = dalloc(&d_cdf, cdf.size(), &tmp);
+    if (!e) e = dalloc(&d_tally, (size_t)5 * nc, &tmp);
+    if (!e) e = dalloc(&d_lost, 1, &tmp);
+    if (!e) e = cudaMemcpyAsync(d_faces, faces.data(), sizeof(int32_t) * faces.size(), cudaMemcpyHostToDevice, s);
+    if (!e) e = cudaMemcpyAsync(d_cdf, cdf.data(), sizeof(double) * cdf.size(), cudaMemcpyHostToDevice, s);
+    if (!e) e = cudaMemsetAsync(d_tally, 0, sizeof(double) * 5 * nc, s);
+    if (!e) e = cudaMemsetAsync(d_lost, 0, sizeof(unsigned long long), s);
+    McArgs a{};
+    a.M = M;
+    a.P = ctx->P;
+    a.L = L;
+    a.state = ctx->d_state[ctx->scur];
+    a.inflow_face = d_faces;
+    a.inflow_cdf = d_cdf;
+    a.ninflow = (int)faces.size();
+    a.nparticles = mp->n_particles;
+    a.mu = total / (double)mp->n_particles;
+    a.nH = mp->n_H;
+    a.uH0 = mp->u_H[0];
+    a.uH1 = mp->u_H[1];
+    a.uH2 = mp->u_H[2];
+    a.cpH = mp->cp_H;
+    a.seed = mp->seed;
+    a.max_cells = mp->max_cells > 0 ? mp->max_cells : 1000000;
+    a.tally = d_tally;
+    a.lost = d_lost;
+    float ms = 0.f;
+    if (!e) e = cudaEventRecord(ctx->ev[0], s);
+    if (!e) e = launch_mc_trace(a, s);
+    if (!e) e = launch_mc_normalise(d_tally, L.vol, (int)nc, s);
+    if (!e) e = cudaEventRecord(ctx->ev[1], s);
+    std::vector<double> h;
+    unsigned long long lost = 0;
+    if (!e) {
+        h.resize((size_t)5 * nc);
+        e = cudaMemcpyAsync(h.data(), d_tally, sizeof(double) * 5 * nc, cudaMemcpyDeviceToHost, s);
+    }
+    if (!e) e = cudaMemcpyAsync(&lost, d_lost, sizeof(lost), cudaMemcpyDeviceToHost, s);
+    if (!e) e = cudaStreamSynchronize(s);
+    if (!e) cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    void* ps[] = {d_faces, d_cdf, d_tally, d_lost};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (e) return fail(TITAN_ECUDA, std::string("mc: ") + cudaGetErrorString(e));
+    for (int64_t c = 0; c < nc; ++c) {
+        const int64_t o = ctx->R.cell_n2o[c];
+        for (int k = 0; k < 5; ++k) out[k * nc + o] = h[k * nc + c];
+    }
+    if (info) {
+        info->particles = mp->n_particles;
+        info->lost = (int64_t)lost;
+        info->inflow_rate = total;
+        info->gpu_ms = ms;
+    }
+    return TITAN_OK;
+}
+
 int titan_set_tuning(titan_ctx* ctx, int32_t face_variant, int32_t cell_variant) {
     if (!ctx) return fail(TITAN_EINVAL, "null argument");
     if (face_variant < 0 || face_variant >= kFaceVariants || cell_variant < 0 || cell_variant >= kCellVariants)

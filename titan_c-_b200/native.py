@@ -62,6 +62,17 @@ class TitanDevMesh(ctypes.Structure):
             "face_half_dist", "hfluids")]
 
 
+class TitanMcParams(ctypes.Structure):
+    _fields_ = [("n_H", ctypes.c_double), ("u_H", ctypes.c_double * 3), ("cp_H", ctypes.c_double),
+                ("n_particles", ctypes.c_int64), ("seed", ctypes.c_uint64), ("max_cells", ctypes.c_int32),
+                ("face_types", ctypes.c_int32)]
+
+
+class TitanMcInfo(ctypes.Structure):
+    _fields_ = [("particles", ctypes.c_int64), ("lost", ctypes.c_int64), ("inflow_rate", ctypes.c_double),
+                ("gpu_ms", ctypes.c_double)]
+
+
 class TitanStepInfo(ctypes.Structure):
     _fields_ = [
         ("steps_done", ctypes.c_int64), ("err_index", ctypes.c_int64), ("n_rho_floor", ctypes.c_int64),
@@ -91,6 +102,8 @@ SIGNATURES = {
                            ctypes.c_int),
     "titan_riemann_batch": ([ctypes.c_int64, I8, D, D, D, D, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, D, D,
                              I32], ctypes.c_int),
+    "titan_mc_sources": ([ctypes.c_void_p, ctypes.POINTER(TitanMcParams), D, ctypes.POINTER(TitanMcInfo)],
+                         ctypes.c_int),
     "titan_autotune": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p], ctypes.c_int),
     "titan_set_tuning": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
     "titan_get_tuning": ([ctypes.c_void_p, I32, I32, I32, I32, I32], ctypes.c_int),

@@ -152,6 +152,19 @@ class PlasmaStep:
         N.check(self._lib.titan_get_permutation(self._ctx, N.ptr(c, N.I32), N.ptr(f, N.I32), N.ptr(n, N.I32)))
         return c, f, n
 
+    def mc_sources(self, n_H: float, u_H, cp_H: float, n_particles: int, seed: int = 1,
+                   face_types: int = (1 << 2) | (1 << 3), max_cells: int = 0):
+        """Monte-Carlo neutrals through the current state: ([5, ncell] = n_H, S_m (3), S_E; info)."""
+        mp = N.TitanMcParams()
+        mp.n_H, mp.cp_H = n_H, cp_H
+        for k in range(3):
+            mp.u_H[k] = u_H[k]
+        mp.n_particles, mp.seed, mp.max_cells, mp.face_types = int(n_particles), int(seed), int(max_cells), face_types
+        out = np.empty((5, self.ncell))
+        info = N.TitanMcInfo()
+        N.check(self._lib.titan_mc_sources(self._ctx, ctypes.byref(mp), N.ptr(out), ctypes.byref(info)))
+        return out, {k: getattr(info, k) for k, _ in N.TitanMcInfo._fields_}
+
     def autotune(self, reps: int = 5, cache: str | None = None) -> dict:
         """Times the launch-shape variants on this mesh and keeps the fastest."""
         N.check(self._lib.titan_autotune(self._ctx, int(reps), cache.encode() if cache else None))

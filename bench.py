@@ -1,13 +1,20 @@
 """Benchmark of the B200 plasma step: MHD cell-updates/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--nq 96] [--nlayer 40] [--flux 64|32]
+                    [--mode mixed-mlp|fp64|fp32] [--nq 96] [--nlayer 40]
 
 Workload (N=1): the heliosphere-like shell — cubed sphere 6x96x96 x 40
 geometric layers = 2,211,840 hexahedra, r in [1, 100], supersonic Parker-spiral
 wind inside, interstellar inflow outside, seeded lognormal perturbation,
-HLLD where B^2/(8 pi p) > 0.01 else HLLC, prescribed radial node motion (ALE),
-all-FP64. One step = one pass of the plasma loop over every face and cell.
+HLLD where B^2/(8 pi p) > 0.01 else HLLC, prescribed radial node motion (ALE).
+One step = one pass of the plasma loop over every face and cell.
+
+Modes: mixed-mlp (default) — FP32 Riemann flux with FP64 accumulation, dt and
+pressure recovery, and charge-exchange sources from the MLP closure on the
+tensor cores every step; the same run also times the plain all-FP64 step on
+the same mesh and measures the mixed step's error against it after 100 and
+1000 steps (the FP64 GPU step equals the FP64 oracle per step). fp64 / fp32:
+the plain step alone at that flux precision.
 
 value: cell-updates/s with the state resident in HBM (device events around K
 steps on the library's stream). e2e: the same metric through the C ABI with
@@ -47,6 +54,21 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def peak_tflops():
+    """Dense BF16 tensor peak measured with cuBLAS, TFLOP/s: the sustained
+    figure, since the closure kernel runs inside a long step loop."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops_sustained"]), "measured (sustained)"
+    except Exception:
+        return 1400.0, "fallback (sustained)"
+
+
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel on
+# this workload: profiles/face_flux_shell.md has the command and the figures.
+TRAFFIC = {}
 
 
 class ClockSampler:
@@ -107,8 +129,61 @@ class ClockSampler:
 def build_problem(args):
     pkg = importlib.import_module("titan_c-_b200")
     m, p, st, _ = pkg.problems.heliosphere_shell(nq=args.nq, nlayer=args.nlayer, move=True,
-                                                 flux_precision=args.flux)
+                                                 flux_precision=64 if args.mode == "fp64" else 32)
     return pkg, m, p, st
+
+
+NET_PATH = os.path.join(ROOT, "titan_c-_b200", "data", "closure_shell.npz")
+
+
+def load_closure(pkg, m, st):
+    """The closure network of the shell problem: the trained one when it is
+    present, else the architecture with seeded random weights (the step's cost
+    does not depend on the weights) and output scales of a plausible size."""
+    cl = pkg.closure
+    if os.path.exists(NET_PATH):
+        d = np.load(NET_PATH)
+        return cl.Closure(float(d["n_inf"]), float(d["lam"]), d["params"], d["norm"]), "trained"
+    cc = m["node_xyz"][m["cell_nodes"]].mean(axis=1).T
+    X = cl.features(st, cc, 0.18, 0.0)
+    norm = cl.make_norm(X, np.ones((1, 5)))
+    norm[16:] = 1e-3
+    return cl.Closure(0.18, 0.0, norm=norm, seed=0), "random-init"
+
+
+def rel_errors(a, b):
+    """Relative L1 and Linf of rho, p and |B| of state a against state b."""
+    out = {}
+    fields = {"rho": (a[0], b[0]), "p": (a[4], b[4]),
+              "B": (np.linalg.norm(a[5:8], axis=0), np.linalg.norm(b[5:8], axis=0))}
+    for k, (x, y) in fields.items():
+        d = np.abs(x - y)
+        out[k] = {"l1": float(d.sum() / np.abs(y).sum()), "linf": float(d.max() / np.abs(y).max())}
+    return out
+
+
+def error_study(pkg, m, p, st, tuning, closure, checkpoints=(100, 1000)):
+    """Mixed step (FP32 flux) against the all-FP64 step from the same state:
+    the states at each checkpoint, with the closure installed in both or in neither."""
+    res = {}
+    for tag, net in (("with_mlp_sources", closure), ("no_sources", None)):
+        states = {}
+        for flux in (64, 32):
+            prm = dict(p)
+            prm["flux_precision"] = flux
+            g = pkg.PlasmaStep(m, prm)
+            g.upload_state(st)
+            g.set_tuning(tuning["face_variant"], tuning["cell_variant"])
+            if net is not None:
+                net.install(g)
+            done, states[flux] = 0, {}
+            for c in checkpoints:
+                g.go(c - done)
+                done = c
+                states[flux][c] = g.download_state()
+            g.close()
+        res[tag] = {str(c): rel_errors(states[32][c], states[64][c]) for c in checkpoints}
+    return res
 
 
 def face_flux_bytes(m, move: bool, fp32: bool) -> float:
@@ -126,6 +201,37 @@ def face_flux_bytes(m, move: bool, fp32: bool) -> float:
     return float(per_face * F + state + out + ale)
 
 
+def timed_steps(step, steps, barrier, stream, dev):
+    """Device time of `steps` steps (ms) with the clocks sampled meanwhile."""
+    import torch
+
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(dev) as clk:
+        ev0.record(stream)
+        step.go(steps)
+        ev1.record(stream)
+        barrier()
+    return ev0.elapsed_time(ev1), clk.summary()
+
+
+def make_step(pkg, m, p, st, flux, tuning_arg, closure=None):
+    prm = dict(p)
+    prm["flux_precision"] = flux
+    step = pkg.PlasmaStep(m, prm)
+    step.upload_state(st)
+    if closure is not None:
+        closure.install(step)
+    if tuning_arg == "auto":
+        tuning = step.autotune(reps=3)
+    else:
+        fv, cv = (int(x) for x in tuning_arg.split(","))
+        step.set_tuning(fv, cv)
+        tuning = step.tuning()
+    return step, tuning
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -134,36 +240,21 @@ def run_ours(args, rank, world):
     pkg, m, p, st = build_problem(args)
     C = m["cell_nodes"].shape[0]
     F = m["face_nodes"].shape[0]
-    step = pkg.PlasmaStep(m, p)
-    step.upload_state(st)
-    if args.tuning == "auto":
-        tuning = step.autotune(reps=3)
-    else:
-        fv, cv = (int(x) for x in args.tuning.split(","))
-        step.set_tuning(fv, cv)
-        tuning = step.tuning()
-    kernels_per_step = 3 if p["move"] else 2
-    flux_name = "face_flux_fp32" if args.flux == 32 else "face_flux_fp64"
-
-    # warm-up (also captures the CUDA graph)
-    step.go(max(args.warmup, 3))
-    stream = torch.cuda.ExternalStream(step.stream())
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    flux = 64 if args.mode == "fp64" else 32
+    closure, net_kind = (load_closure(pkg, m, st) if args.mode == "mixed-mlp" else (None, None))
+    step, tuning = make_step(pkg, m, p, st, flux, args.tuning, closure)
+    kernels_per_step = (3 if p["move"] else 2) + (1 if closure is not None else 0)
+    flux_name = f"face_flux_fp{flux}"
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    barrier()
-    with ClockSampler(dev) as clk:
-        ev0.record(stream)
-        step.go(args.steps)
-        ev1.record(stream)
-        barrier()
-    ms = ev0.elapsed_time(ev1)
-    clocks = clk.summary()
+    # warm-up (also captures the CUDA graph)
+    step.go(max(args.warmup, 3))
+    stream = torch.cuda.ExternalStream(step.stream())
+    ms, clocks = timed_steps(step, args.steps, barrier, stream, dev)
 
     # dominant kernel: per-launch device time with events on the library stream
     step.set_profiling(True)
@@ -180,34 +271,50 @@ def run_ours(args, rank, world):
     e2e_steps = max(3, min(args.steps, 20))
     barrier()
     t0 = time.perf_counter()
-    ev0.record(stream)
     for _ in range(e2e_steps):
         step.upload_state(host)
         step.go(1)
         step.download_state(host)
-    ev1.record(stream)
     barrier()
     e2e_wall = time.perf_counter() - t0
     ns = 8 + p["npassive"]
     step.close()
 
-    t = torch.tensor([ms, e2e_wall], dtype=torch.float64, device="cuda")
+    # the plain all-FP64 step on the same mesh, and the mixed step's error against it
+    plain = None
+    if args.mode == "mixed-mlp":
+        s64, tun64 = make_step(pkg, m, p, st, 64, args.tuning)
+        s64.go(max(args.warmup, 3))
+        ms64, clk64 = timed_steps(s64, args.steps, barrier, torch.cuda.ExternalStream(s64.stream()), dev)
+        s64.close()
+        plain = {"value": world * C * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+                 "tuning": tun64, "clocks": clk64}
+
+    t = torch.tensor([ms, e2e_wall] + ([plain["ms_per_step"]] if plain else []), dtype=torch.float64,
+                     device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     ms, e2e_wall = float(t[0]), float(t[1])
+    if plain:
+        plain["ms_per_step"] = float(t[2])
+        plain["value"] = world * C / (plain["ms_per_step"] / 1e3)
     if rank != 0:
         return None
     value = world * C * args.steps / (ms / 1e3)
     hbm, src = peaks()
-    bytes_launch = face_flux_bytes(m, bool(p["move"]), args.flux == 32)
+    bytes_launch = face_flux_bytes(m, bool(p["move"]), flux == 32)
     achieved = bytes_launch / (k_avg / 1e3) / 1e9
+    dtype = {"fp64": "f64", "fp32": "f32-flux/f64-update", "mixed-mlp": "f32-flux/f64-update, bf16 MLP"}[args.mode]
+    what = {"fp64": "FP64 flux", "fp32": "FP32 flux, FP64 accumulation",
+            "mixed-mlp": "FP32 flux, FP64 accumulation, MLP charge-exchange sources every step"}[args.mode]
+    traffic = TRAFFIC.get((flux_name, C))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.flux == 64 else "f32-flux/f64-update",
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype,
         "data": "synthetic (seeded heliosphere-like shell; no external data)",
         "config": {"workload": f"heliosphere shell 6x{args.nq}x{args.nq}x{args.nlayer} = {C} cells, {F} faces, "
-                               f"ALE, HLLD/HLLC, FP{args.flux} flux", "cells": C, "faces": F,
+                               f"ALE, HLLD/HLLC, {what}", "cells": C, "faces": F, "mode": args.mode,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "tuning": tuning,
                    "l2": "inputs larger than L2 (state 141 MB + face data 0.5 GB), no flush"},
         "face_fluxes_per_s": world * F * args.steps / (ms / 1e3),
@@ -215,12 +322,25 @@ def run_ours(args, rank, world):
                 "h2d_bytes_per_step": 8 * ns * C, "d2h_bytes_per_step": 8 * ns * C},
         "gpu_launches": args.steps * kernels_per_step,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": flux_name, "peak_source": src,
+                     "traffic": traffic, "kernel": flux_name, "peak_source": src,
                      "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": k_avg,
                      "kernel_share": k_ms / total_k},
         "kernel_ms_per_step": {k: v[0] / v[1] for k, v in kt.items()},
         "clocks": clocks,
     }
+    if closure is not None:
+        mlp_ms = kt["closure_mlp"][0] / kt["closure_mlp"][1]
+        flops = 2.0 * C * (16 * 128 + 3 * 128 * 128 + 128 * 16)
+        tf_peak, tf_src = peak_tflops()
+        line["closure"] = {"network": net_kind, "kernel": "closure_mlp (tcgen05, TMEM accumulators)",
+                           "avg_launch_ms": mlp_ms, "flops_per_launch": flops,
+                           "tflops": flops / (mlp_ms / 1e3) / 1e12, "tensor_peak_tflops": tf_peak,
+                           "peak_source": tf_src, "tensor_frac": flops / (mlp_ms / 1e3) / 1e12 / tf_peak}
+    if plain:
+        line["plain_fp64"] = plain
+        line["speedup_vs_plain_fp64"] = plain["ms_per_step"] / (ms / args.steps)
+        if world == 1 and args.error_study:
+            line["error_vs_fp64"] = error_study(pkg, m, p, st, tuning, closure)
     if args.cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args, m, p, st)
     return line
@@ -278,7 +398,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nq", type=int, default=96)
     ap.add_argument("--nlayer", type=int, default=40)
-    ap.add_argument("--flux", type=int, default=64, choices=[64, 32])
+    ap.add_argument("--mode", default="mixed-mlp", choices=["mixed-mlp", "fp64", "fp32"])
+    ap.add_argument("--no-error-study", dest="error_study", action="store_false")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--tuning", default="auto", help="auto, or 'face_variant,cell_variant'")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")

@@ -196,6 +196,42 @@ typedef struct titan_mc_info {
 
 int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* params, double* out, titan_mc_info* info);
 
+/* ---------------------------------------------------------------------------
+ * Learned charge-exchange closure (no reference counterpart: it stands in for
+ * re-running the Monte-Carlo neutral solver between plasma steps).
+ * An MLP 8 -> 128 -> 128 -> 128 -> 128 -> 5 with SiLU, BF16 weights and
+ * activations, FP32 accumulation. Parameters: FP32 masters, TITAN_MLP_NPARAM
+ * floats [W1 16x128 | b1 128 | W2 128x128 | b2 | W3 | b3 | W4 | b4 |
+ * W5 128x16 | b5 16], W stored [in][out]; inputs 8..15 and outputs 5..15 are
+ * padding kept at zero. norm: feature mean[8], 1/std[8], output scale[5].
+ * Features and outputs are defined in titan_c-_b200/csrc/closure.h. */
+#define TITAN_MLP_NPARAM 53776
+
+typedef struct titan_mlp_train_opts {
+    int32_t epochs;
+    int32_t batch;     /* rows per Adam step (rows are used in the caller's order) */
+    float lr, beta1, beta2;
+    float lr_decay;    /* per-epoch factor, 0 = none */
+} titan_mlp_train_opts;
+
+/* Inference of X [n][8] (unstandardised features) -> Y [n][5] on the tensor
+ * cores (tcgen05, the kernel the step uses). Host buffers. */
+int titan_mlp_forward(const float* params, const float* norm, const float* X, int64_t n, float* Y);
+/* Loss and gradient of the weighted MSE sum_r rw_r sum_k w_k (Y_rk - T_rk)^2 / n
+ * over one batch (BF16 tensor-core GEMMs). w [5] per output; row_w [n] per row
+ * (NULL: all 1); Y (may be NULL) receives the outputs. */
+int titan_mlp_grad(const float* params, const float* norm, const float* X, const float* T, const float* w,
+                   const float* row_w, int64_t n, float* grad, float* loss, float* Y);
+/* Adam on the GPU over the same loss; params in/out; loss_per_epoch [epochs]
+ * (may be NULL). */
+int titan_mlp_train(float* params, const float* norm, const float* X, const float* T, const float* w,
+                    const float* row_w, int64_t n, const titan_mlp_train_opts* opts, float* loss_per_epoch);
+/* Installs the closure in a context: every step then computes the plasma
+ * sources with the network (before the cell update) instead of the Bera
+ * formulas or titan_set_sources. params NULL removes it. n_inf / lambda: the
+ * cold-model neutral density proxy of the features. */
+int titan_set_closure(titan_ctx* ctx, const float* params, const float* norm, double n_inf, double lambda);
+
 /* Launch-shape autotuner (no reference counterpart: the reference's OpenMP
  * loops have no launch shapes). Times every face-flux variant (threads per
  * block x minimum resident blocks per SM) and every cell-update shape on

@@ -1,0 +1,154 @@
+"""The learned charge-exchange closure on the GPU: the BF16 tensor-core
+training gradient against the CPU network oracle, the tcgen05 inference kernel
+against the oracle's forward pass, training that lowers the loss, the closure
+inside the plasma step, and a trained closure judged against Monte-Carlo noise
+(what the network gains over holding the last Monte-Carlo sources fixed)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import mlp_oracle as mo  # noqa: E402
+
+
+def _rand_problem(titan, n, seed=0):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, 8)).astype(np.float32) * 2.0 + 1.0
+    norm = np.concatenate([np.full(8, 1.0), np.full(8, 0.5), np.ones(5)]).astype(np.float32)
+    c = titan.closure.Closure(0.18, 4.0, norm=norm, seed=seed)
+    c.params += (0.02 * rng.standard_normal(c.params.size) * (c.params != 0)).astype(np.float32)
+    for w, b, i, j in mo.offsets():     # non-zero biases (padding stays zero)
+        live = j if j == 128 else 5
+        c.params[b:b + live] = 0.05 * rng.standard_normal(live)
+    T = rng.standard_normal((n, 5)).astype(np.float32)
+    return c, X, T
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("n", [1, 200, 1001, 8192])
+def test_training_gradient_matches_the_cpu_oracle(titan, n):
+    c, X, T = _rand_problem(titan, n, seed=n)
+    w = np.array([1.0, 0.5, 2.0, 1.0, 0.25], np.float32)
+    rw = None if n % 2 == 0 else np.random.default_rng(n).uniform(0.1, 3.0, n).astype(np.float32)
+    loss, g, Y = c.grad(X, T, w, row_weights=rw)
+    lo, go = mo.loss_grad(c.params, c.norm, X, T, w, emulate_bf16=True, row_w=rw)
+    Yo, _ = mo.forward(c.params, c.norm, X, emulate_bf16=True)
+    assert _rel(Y, Yo) < 2e-3
+    assert abs(loss - lo) <= 2e-3 * lo
+    for li, (wo, bo, i, j) in enumerate(mo.offsets()):
+        assert _rel(g[wo:bo], go[wo:bo]) < 1e-2, ("W", li, _rel(g[wo:bo], go[wo:bo]))
+        assert _rel(g[bo:bo + j], go[bo:bo + j]) < 1e-2, ("b", li)
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 5000, 300_000])
+def test_tensor_core_inference_matches_the_oracle(titan, n):
+    """tcgen05 forward (SiLU through tanh.approx.bf16x2) against the oracle's
+    BF16-rounded forward: agreement to the BF16 rounding of the activations."""
+    c, X, _ = _rand_problem(titan, n, seed=7)
+    Y = c.forward(X)
+    m = min(n, 20000)
+    Yo, _ = mo.forward(c.params, c.norm, X[:m], emulate_bf16=True)
+    assert np.isfinite(Y).all()
+    assert _rel(Y[:m], Yo) < 3e-2, _rel(Y[:m], Yo)
+    # the GEMM path (training forward) agrees with the same accuracy
+    _, _, Yg = c.grad(X[:m], np.zeros((m, 5), np.float32))
+    assert _rel(Y[:m], Yg) < 3e-2
+
+
+def test_training_lowers_the_loss(titan):
+    rng = np.random.default_rng(2)
+    n = 32768
+    X = rng.standard_normal((n, 8)).astype(np.float32)
+    T = np.stack([np.sin(X[:, 0]) + X[:, 1] * X[:, 2], np.tanh(X[:, 3]), X[:, 4] ** 2 - 1.0,
+                  np.cos(X[:, 5] + X[:, 6]), X[:, 7] * X[:, 0]], axis=1).astype(np.float32)
+    c = titan.closure.Closure(0.18, 4.0, seed=1)
+    losses = c.fit(X, T, epochs=12, batch=1024, lr=2e-3, lr_decay=0.85)
+    assert losses[-1] < 0.1 * losses[0], losses
+    assert np.isfinite(c.params).all()
+    # padding stays zero
+    w1 = c.params[:16 * 128].reshape(16, 128)
+    assert not w1[8:].any()
+
+
+def _shell_run(titan, steps, nq=10, nlayer=14):
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=nq, nlayer=nlayer, move=False)
+    g = titan.PlasmaStep(m, p)
+    g.upload_state(st)
+    return m, p, g
+
+
+def test_closure_inside_the_step_equals_its_sources(titan):
+    """A step with the network installed equals a step given the same
+    network's sources through titan_set_sources (features on the device vs
+    numpy: equal up to float rounding of the features)."""
+    m, p, g = _shell_run(titan, 0)
+    g.go(5)
+    st0 = g.download_state()
+    dt0, t0 = g.dt, g.t
+    cc = g.geometry()["cell_center"].T
+    c, _, _ = _rand_problem(titan, 10, seed=3)
+    c.norm[:16] = np.concatenate([np.zeros(8), np.ones(8)])
+    c.norm[16:] = 1e-3
+    S = c.predict(st0, cc)
+    c.install(g)
+    g.go(1)
+    a = g.download_state()
+    c.uninstall(g)
+    g.upload_state(st0)
+    g.dt, g.t = dt0, t0
+    g.set_sources(np.ascontiguousarray(S[1:]))
+    g.go(1)
+    b = g.download_state()
+    g.close()
+    assert not np.array_equal(a, st0)
+    for k in range(8):
+        d = np.abs(a[k] - b[k]).max() / max(np.abs(b[k]).max(), 1e-30)
+        assert d < 1e-8, (k, d)
+
+
+def test_trained_closure_is_within_monte_carlo_noise(titan):
+    """Train on Monte-Carlo sources of three plasma snapshots, judge on a
+    fourth. Errors are volume-weighted L1 over cells (the sources enter the
+    conserved variables as S V): the closure's error against the mean of 4
+    Monte-Carlo seeds is below one seed's statistical scatter about that mean.
+    Rows are weighted by cell volume in training too, since the Monte-Carlo
+    samples a cell in proportion to the neutral path length inside it."""
+    m, p, g = _shell_run(titan, 0, nq=10, nlayer=14)
+    kw = dict(n_H=0.18, u_H=(-2.6, 0.0, 0.0), cp_H=1.424, n_particles=1_000_000)
+    geo = g.geometry()
+    cc, vol = geo["cell_center"].T, geo["cell_volume"]
+    snaps = []
+    for s in range(4):
+        g.go(60)
+        st = g.download_state()
+        seeds = [g.mc_sources(seed=100 * s + k, **kw)[0] for k in range(4)]
+        snaps.append((st, np.mean(seeds, axis=0), seeds))
+    g.close()
+    # the generator has charge exchange only, which conserves the neutrals:
+    # the cold-model proxy is flat (lambda = 0)
+    n_inf, lam = 0.18, 0.0
+    X = np.concatenate([titan.closure.features(st, cc, n_inf, lam) for st, _, _ in snaps[:3]])
+    # train on single seeds (noisy labels, as the generator gives them)
+    T = np.concatenate([titan.closure.targets(st, cc, sd[0], n_inf, lam) for st, _, sd in snaps[:3]])
+    c = titan.closure.Closure(n_inf, lam, seed=0)
+    losses = c.fit(X, T, epochs=60, batch=2048, lr=2e-3, lr_decay=0.95, row_weights=np.tile(vol, 3))
+    assert losses[-1] < losses[0]
+    st, mean, seeds = snaps[3]
+    pred = c.predict(st, cc)
+
+    def l1(a, b):
+        return float((np.abs(a[1:5] - b[1:5]) * vol).sum() / (np.abs(b[1:5]) * vol).sum())
+
+    err = l1(pred, mean)
+    noise = np.mean([l1(sd, mean) for sd in seeds]) * np.sqrt(4.0 / 3.0)
+    stale = l1(snaps[2][1], mean)
+    print(f"closure {err:.3e}  one-seed noise {noise:.3e}  previous snapshot's sources {stale:.3e}")
+    assert err < noise

@@ -7,12 +7,15 @@ Translation units and their floating-point flags:
   kernels_fp32.cu  -fmad=true -prec-div=false -prec-sqrt=false
                                 FP32 Riemann flux of the mixed-precision step
   mc_neutral.cu                 Monte-Carlo neutral hydrogen (source generator)
+  closure_mlp.cu                closure inference on tcgen05 / TMEM (per step)
+  closure_train.cu, closure_api.cu   closure training (BF16 tensor-core GEMMs), C ABI
   titan_api.cu, renumber.cpp    host side of the C ABI
   noalloc.cu       -fmad=false  titan_step_noalloc (fixed scratch array, no allocation)
 """
 from __future__ import annotations
 
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -29,6 +32,9 @@ UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
     ("kernels_fp32.cu", ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("mc_neutral.cu", []),
+    ("closure_mlp.cu", []),
+    ("closure_train.cu", []),
+    ("closure_api.cu", []),
     ("titan_api.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("renumber.cpp", []),
@@ -49,19 +55,29 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _includes(path: str, seen: set[str]) -> set[str]:
+    """Local headers `path` includes (#include "..."), transitively."""
+    for line in open(path, errors="replace"):
+        m = re.match(r'\s*#\s*include\s+"([^"]+)"', line)
+        if m:
+            h = os.path.normpath(os.path.join(os.path.dirname(path), m.group(1)))
+            if os.path.exists(h) and h not in seen:
+                seen.add(h)
+                _includes(h, seen)
+    return seen
+
+
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    headers.append(os.path.join(os.path.dirname(HERE), "include", "titan_b200.h"))
     objs = []
     for src, flags in UNITS:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
-        if force or _stale(o, [s, __file__] + headers):
+        if force or _stale(o, [s, __file__] + sorted(_includes(s, set()))):
             cmd = [nvcc(), *ARCH, *COMMON, *flags, *(extra or []), "-c", s, "-o", o]
             if src.endswith(".cpp"):
-                cmd = [nvcc(), *COMMON, "-x", "c++", "-c", s, "-o", o]
+                cmd = [nvcc(), *COMMON, "-Wno-deprecated-gpu-targets", "-x", "c++", "-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

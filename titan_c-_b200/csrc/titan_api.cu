@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/titan_b200.h"
+#include "closure.h"
 #include "launch.h"
 #include "renumber.h"
 
@@ -101,6 +102,11 @@ struct titan_ctx {
     cudaGraphExec_t graph = nullptr;
     int graph_cur = -1, graph_scur = -1;
 
+    ClosureDev closure;        // learned sources (titan_set_closure)
+    bool use_closure = false;
+    double closure_ninf = 0.0, closure_lambda = 0.0;
+    int sm_count = 148;
+
     int face_variant = 0;  // launch shapes (autotuned, see titan_autotune)
     int cell_variant = 0;
 
@@ -167,6 +173,24 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
         });
         if (e) return e;
     }
+    if (ctx->use_closure) {
+        // sources of this step from the network, on the current state
+        MlpArgs ma{};
+        ma.net = ctx->closure.view();
+        ma.n = (int)ctx->ncell;
+        ma.ncell = (int)ctx->ncell;
+        ma.state = ctx->d_state[ctx->scur];
+        ma.cc = ctx->layer[ctx->cur].cc;
+        ma.src = ctx->d_src;
+        ma.nH_inf = ctx->closure_ninf;
+        ma.lambda = ctx->closure_lambda;
+        ma.error = ctx->closure.error;
+        const int ntiles = (int)((ctx->ncell + kTile - 1) / kTile);
+        e = timed(ctx, "closure_mlp", [&] {
+            return launch_mlp_forward(ma, kModeSources, ntiles < ctx->sm_count ? ntiles : ctx->sm_count, ctx->stream);
+        });
+        if (e) return e;
+    }
     FaceArgs fa;
     fa.M = M;
     fa.P = ctx->P;
@@ -193,7 +217,7 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     ca.hfl = ctx->d_hfl;
     ca.src = ctx->d_src;
     ca.st = ctx->d_status;
-    const int src = ctx->use_src ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
+    const int src = (ctx->use_src || ctx->use_closure) ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
     e = timed(ctx, "cell_update",
               [&] { return launch_cell_update(ca, ctx->fp32, nk, move, src, ctx->cell_variant, ctx->stream); });
     if (e) return e;
@@ -316,6 +340,7 @@ const char* titan_last_error(void) { return g_err.c_str(); }
 int titan_destroy(titan_ctx* ctx) {
     if (!ctx) return TITAN_OK;
     drop_graph(ctx);
+    closure_destroy(&ctx->closure);
     void* ptrs[] = {ctx->d_cell_n2o, ctx->d_node_n2o, ctx->d_face_c0, ctx->d_face_c1, ctx->d_face_bc,
                     ctx->d_face_nodes, ctx->d_face_type, ctx->d_face_surf, ctx->d_face_method, ctx->d_bc_vals,
                     ctx->d_cell_faces, ctx->d_cell_nodes, ctx->d_cell_type, ctx->d_cell_tvd, ctx->d_node_amp,
@@ -654,6 +679,11 @@ int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout
     if (t_inout) *t_inout = st.t;
     int status = TITAN_OK;
     if (st.err_kind != 0) status = st.err_kind >= 20 ? TITAN_ENONFINITE : TITAN_ESOLVER;
+    if (ctx->use_closure) {
+        int cerr = 0;
+        CK(cudaMemcpy(&cerr, ctx->closure.error, sizeof(int), cudaMemcpyDeviceToHost));
+        if (cerr) return fail(TITAN_ETIMEOUT, "closure: a tensor-core wait ran out");
+    }
     if (info) {
         info->steps_done = (int64_t)st.steps_done;
         info->n_rho_floor = (int64_t)st.n_rho_floor;
@@ -808,6 +838,32 @@ int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, con
     return TITAN_OK;
 }
 
+int titan_set_closure(titan_ctx* ctx, const float* params, const float* norm, double n_inf, double lambda) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    drop_graph(ctx);
+    closure_destroy(&ctx->closure);
+    ctx->use_closure = false;
+    if (!params) return TITAN_OK;
+    if (!norm || !(n_inf > 0.0)) return fail(TITAN_EINVAL, "closure needs norm and n_inf > 0");
+    if (!ctx->d_src) {
+        int64_t dummy = 0;
+        CK(dalloc(&ctx->d_src, (size_t)4 * ctx->ncell, &dummy));
+        ctx->dev_bytes += dummy;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, dev));
+    cudaError_t e = closure_create(params, norm, &ctx->closure, ctx->stream);
+    if (e) {
+        closure_destroy(&ctx->closure);
+        return fail(TITAN_ECUDA, std::string("closure: ") + cudaGetErrorString(e));
+    }
+    ctx->closure_ninf = n_inf;
+    ctx->closure_lambda = lambda;
+    ctx->use_closure = true;
+    return TITAN_OK;
+}
+
 int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, titan_mc_info* info) {
     if (!ctx || !mp || !out) return fail(TITAN_EINVAL, "null argument");
     if (mp->n_particles <= 0 || !(mp->n_H > 0.0) || !(mp->cp_H > 0.0)) return fail(TITAN_EINVAL, "bad MC parameters");
@@ -925,7 +981,7 @@ int titan_get_tuning(titan_ctx* ctx, int32_t* face_variant, int32_t* cell_varian
 
 int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     if (!ctx || reps <= 0) return fail(TITAN_EINVAL, "bad argument");
-    const int src = ctx->use_src ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
+    const int src = (ctx->use_src || ctx->use_closure) ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
     char key[256];
     snprintf(key, sizeof key, "sm_100a cells=%lld faces=%lld move=%d flux=%d npassive=%d src=%d",
              (long long)ctx->ncell, (long long)ctx->nface, ctx->prm.move, ctx->prm.flux_precision,

@@ -73,6 +73,15 @@ class TitanMcInfo(ctypes.Structure):
                 ("gpu_ms", ctypes.c_double)]
 
 
+class TitanMlpTrainOpts(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("lr_decay", ctypes.c_float)]
+
+
+MLP_NPARAM = 53776
+F32 = ctypes.POINTER(ctypes.c_float)
+
+
 class TitanStepInfo(ctypes.Structure):
     _fields_ = [
         ("steps_done", ctypes.c_int64), ("err_index", ctypes.c_int64), ("n_rho_floor", ctypes.c_int64),
@@ -104,6 +113,11 @@ SIGNATURES = {
                              I32], ctypes.c_int),
     "titan_mc_sources": ([ctypes.c_void_p, ctypes.POINTER(TitanMcParams), D, ctypes.POINTER(TitanMcInfo)],
                          ctypes.c_int),
+    "titan_mlp_forward": ([F32, F32, F32, ctypes.c_int64, F32], ctypes.c_int),
+    "titan_mlp_grad": ([F32, F32, F32, F32, F32, F32, ctypes.c_int64, F32, F32, F32], ctypes.c_int),
+    "titan_mlp_train": ([F32, F32, F32, F32, F32, F32, ctypes.c_int64, ctypes.POINTER(TitanMlpTrainOpts), F32],
+                        ctypes.c_int),
+    "titan_set_closure": ([ctypes.c_void_p, F32, F32, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "titan_autotune": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p], ctypes.c_int),
     "titan_set_tuning": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
     "titan_get_tuning": ([ctypes.c_void_p, I32, I32, I32, I32, I32], ctypes.c_int),

@@ -92,6 +92,9 @@ typedef struct titan_params {
     int32_t TS_hard;       /* left_ydar on TS faces */
     int32_t contact_hard;  /* face speed = contact speed on HP faces */
     int32_t flux_precision;/* 64: all-FP64; 32: FP32 Riemann flux, FP64 accumulation/update/dt */
+    int32_t tvd;           /* Phys_param::TVD: second-order reconstruction on interior faces
+                              (Setka_gran_snos.cpp:188-735; neighbours from Setka::Init_TVD) */
+    int32_t snos_on_hp;    /* Phys_param::Snos_on_HP: second order on HP faces too */
 } titan_params;
 
 typedef struct titan_step_info {
@@ -155,6 +158,12 @@ int titan_download_face_fluxes(titan_ctx* ctx, double* flux);
 int titan_sfc_renumber(int64_t nnode, int64_t ncell, int64_t nface, const double* node_xyz,
                        const int32_t* cell_nodes, const int32_t* face_cells, int32_t* cell_new2old,
                        int32_t* face_new2old, int32_t* node_new2old);
+
+/* Second-order neighbours of every face (tvd contexts): out [nface*2] =
+ * (AA, BB) in original numbering, -1 when absent — Gran::cells_TVD as
+ * Setka::Init_TVD (TITAN/source/Setka_physics.cpp:646-738) chooses them on
+ * the geometry at titan_create. */
+int titan_get_tvd_neighbours(titan_ctx* ctx, int32_t* out);
 
 /* Permutations chosen at upload: new index -> original index. */
 int titan_get_permutation(titan_ctx* ctx, int32_t* cell_new2old, int32_t* face_new2old, int32_t* node_new2old);

@@ -72,6 +72,8 @@ struct OMesh {
     const double* bc_vals;       // nbc*10, fixed face values (Init_physics)
     const double* node_amp;      // nnode, radial velocity amplitude (ALE), may be null
     const double* node_phase;    // nnode, phase (ALE), may be null
+    const int32_t* face_tvd;     // nface*2, Gran::cells_TVD (AA beyond cells[0], BB beyond cells[1]),
+                                 // -1 when absent; may be null (no second-order faces)
 };
 
 struct OParams {
@@ -87,7 +89,9 @@ struct OParams {
     int32_t npassive;     // 0 or 2 (Q, rho_He carried as passive scalars)
     int32_t nh;           // number of frozen H fluids feeding the Bera sources (0 = none)
     int32_t TS_hard, contact_hard;
-    int32_t pad;
+    int32_t tvd;          // Phys_param::TVD: second-order reconstruction on interior faces
+    int32_t snos_on_hp;   // Phys_param::Snos_on_HP: second order on HP faces too
+    int32_t pad[2];
 };
 
 struct OStepInfo {
@@ -737,6 +741,182 @@ static void o_snos_side(const double* st, int64_t nc, int64_t c, int ctype, cons
     out[4] = st[4 * nc + c] * std::pow(r1, 2.0 * gamma) / std::pow(rr, 2.0 * gamma);
 }
 
+// ---------------------------------------------------------------------------
+// Second-order (TVD) reconstruction, Setka_gran_snos.cpp:188-735.
+// Cells on the line AA - A -|- B - BB (AA beyond cells[0], BB beyond
+// cells[1], Init_TVD) at coordinates -dd1-d1, -d1, 0 (face centre), d2,
+// d2+dd2. linear (Help_funk.cpp:55-63): minmod of the two slopes through
+// the middle point; linear2 (:65-70): the line through two points; both
+// evaluated at the face (y = 0).
+// ---------------------------------------------------------------------------
+static int o_signum(double x) { return x > 0.00000001 ? 1 : (x < -0.00000001 ? -1 : 0); }
+
+static double o_minmod(double x, double y) {
+    if (o_signum(x) + o_signum(y) == 0) return 0.0;
+    return ((o_signum(x) + o_signum(y)) / 2.0) * mn(std::fabs(x), std::fabs(y));
+}
+
+static double o_lin3(double x1, double t1, double x2, double t2, double x3, double t3) {
+    const double y = 0.0;
+    const double d = o_minmod((t1 - t2) / (x1 - x2), (t2 - t3) / (x2 - x3));
+    return (d * (y - x2) + t2);
+}
+
+static double o_lin2(double x1, double t1, double x2, double t2) {
+    const double y = 0.0;
+    const double d = (t1 - t2) / (x1 - x2);
+    return (d * (y - x2) + t2);
+}
+
+static inline double o_norm3(const double* a) { return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+
+// Face states L, R of an interior face on the second-order branch.
+// c[0..3] = AA, A, B, BB; ctype their Type_cell.
+static void o_snos_tvd(const double* st, int64_t nc, const int64_t c[4], const int ct[4], const double* cc,
+                       const double* G, double gamma, int npassive, double* L, double* R) {
+    const double *AAc = cc + 3 * c[0], *Ac = cc + 3 * c[1], *Bc = cc + 3 * c[2], *BBc = cc + 3 * c[3];
+    double v[3];
+    for (int j = 0; j < 3; ++j) v[j] = Ac[j] - G[j];
+    const double d1 = o_norm3(v);
+    for (int j = 0; j < 3; ++j) v[j] = Bc[j] - G[j];
+    const double d2 = o_norm3(v);
+    for (int j = 0; j < 3; ++j) v[j] = Ac[j] - AAc[j];
+    const double dd1 = o_norm3(v);
+    for (int j = 0; j < 3; ++j) v[j] = Bc[j] - BBc[j];
+    const double dd2 = o_norm3(v);
+    const double xAA = -dd1 - d1, xA = -d1, xB = d2, xBB = d2 + dd2;
+    auto S = [&](int k, int i) { return st[(int64_t)k * nc + c[i]]; };
+    const int a0 = ct[0], a1 = ct[1], b1 = ct[2], b0 = ct[3];
+    const bool z1111 = a0 == 1 && a1 == 1 && b1 == 1 && b0 == 1;
+    const bool z1112 = a0 == 1 && a1 == 1 && b1 == 1 && b0 == 2;
+    const bool z1122 = a0 == 1 && a1 == 1 && b1 == 2 && b0 == 2;
+    const bool z1222 = a0 == 1 && a1 == 2 && b1 == 2 && b0 == 2;
+    if (z1111 || z1112 || z1122) {
+        const double r3 = o_norm3(AAc), r1 = o_norm3(Ac), rr = o_norm3(G), r2 = o_norm3(Bc), r4 = o_norm3(BBc);
+        const double the1 = std::acos(G[2] / rr);
+        const bool band = the1 > kPi / 9 && the1 < 8 * kPi / 9;
+        // spherical components (Vr, Vphi, Vtheta) of a vector field of cell i,
+        // in the frame the band test selects (Setka_gran_snos.cpp:241-254 / :301-315)
+        auto sph = [&](int i, int k0, double* out) {
+            const double* X = cc + 3 * c[i];
+            const double vx = S(k0, i), vy = S(k0 + 1, i), vz = S(k0 + 2, i);
+            if (band)
+                o_spherical(X[2], X[0], X[1], vz, vx, vy, out[0], out[1], out[2]);
+            else
+                o_spherical(X[0], X[1], X[2], vx, vy, vz, out[0], out[1], out[2]);
+        };
+        auto cart = [&](const double* Vs, double* side, int k0) {
+            if (band)
+                o_cartesian(G[2], G[0], G[1], Vs[0], Vs[1], Vs[2], side[k0 + 2], side[k0], side[k0 + 1]);
+            else
+                o_cartesian(G[0], G[1], G[2], Vs[0], Vs[1], Vs[2], side[k0], side[k0 + 1], side[k0 + 2]);
+        };
+        for (int ik = 0; ik < 2; ++ik) {
+            const int k0 = ik == 0 ? 1 : 5;
+            double VAA[3], VA[3], VB[3], VBB[3], Vl[3], Vr[3];
+            sph(0, k0, VAA);
+            sph(1, k0, VA);
+            if (z1111) {
+                sph(2, k0, VB);
+                sph(3, k0, VBB);
+                for (int i = 0; i < 3; ++i) {
+                    if (ik == 1) {
+                        if (i == 0) {
+                            Vl[i] = o_lin3(xAA, VAA[i] * sq(r3), xA, VA[i] * sq(r1), xB, VB[i] * sq(r2)) / sq(rr);
+                            Vr[i] = o_lin3(xA, VA[i] * sq(r1), xB, VB[i] * sq(r2), xBB, VBB[i] * sq(r4)) / sq(rr);
+                        } else {
+                            Vl[i] = o_lin3(xAA, VAA[i] * (r3), xA, VA[i] * (r1), xB, VB[i] * (r2)) / (rr);
+                            Vr[i] = o_lin3(xA, VA[i] * (r1), xB, VB[i] * (r2), xBB, VBB[i] * (r4)) / (rr);
+                        }
+                    } else {
+                        Vl[i] = o_lin3(xAA, VAA[i], xA, VA[i], xB, VB[i]);
+                        Vr[i] = o_lin3(xA, VA[i], xB, VB[i], xBB, VBB[i]);
+                    }
+                }
+                cart(Vl, L, k0);
+                cart(Vr, R, k0);
+            } else if (z1112) {
+                sph(2, k0, VB);
+                for (int i = 0; i < 3; ++i) {
+                    Vl[i] = o_lin3(xAA, VAA[i], xA, VA[i], xB, VB[i]);
+                    Vr[i] = o_lin2(xA, VA[i], xB, VB[i]);
+                }
+                cart(Vl, L, k0);
+                cart(Vr, R, k0);
+            } else {  // z1122: left side only; the right side is set per name below
+                for (int i = 0; i < 3; ++i) Vl[i] = o_lin2(xAA, VAA[i], xA, VA[i]);
+                cart(Vl, L, k0);
+            }
+        }
+        const double g2 = 2.0 * gamma;
+        // rho, Q, rho_He scale as r^2 and p as r^(2 gamma) on the all-Zone_1
+        // branch; on the Zone_1/Zone_2 branches the r^2 scaling is overwritten
+        // by the plain line (the reference's `if` / `if ... else` sequence,
+        // Setka_gran_snos.cpp:502-532 and :617-644), so only p is scaled there.
+        const int scal[4] = {0, 8, 9, 4};
+        for (int q = 0; q < 4; ++q) {
+            const int k = scal[q];
+            const bool r2g = k == 4;
+            if (z1111) {
+                if (r2g) {
+                    L[k] = o_lin3(xAA, S(k, 0) * std::pow(r3, g2), xA, S(k, 1) * std::pow(r1, g2), xB,
+                                  S(k, 2) * std::pow(r2, g2)) / std::pow(rr, g2);
+                    R[k] = o_lin3(xA, S(k, 1) * std::pow(r1, g2), xB, S(k, 2) * std::pow(r2, g2), xBB,
+                                  S(k, 3) * std::pow(r4, g2)) / std::pow(rr, g2);
+                } else {
+                    L[k] = o_lin3(xAA, S(k, 0) * sq(r3), xA, S(k, 1) * sq(r1), xB, S(k, 2) * sq(r2)) / sq(rr);
+                    R[k] = o_lin3(xA, S(k, 1) * sq(r1), xB, S(k, 2) * sq(r2), xBB, S(k, 3) * sq(r4)) / sq(rr);
+                }
+            } else if (z1112) {
+                if (r2g) {
+                    L[k] = o_lin3(xAA, S(k, 0) * std::pow(r3, g2), xA, S(k, 1) * std::pow(r1, g2), xB,
+                                  S(k, 2) * std::pow(r2, g2)) / std::pow(rr, g2);
+                    R[k] = o_lin2(xA, S(k, 1) * std::pow(r1, g2), xB, S(k, 2) * std::pow(r2, g2)) / std::pow(rr, g2);
+                } else {
+                    L[k] = o_lin3(xAA, S(k, 0), xA, S(k, 1), xB, S(k, 2));
+                    R[k] = o_lin2(xA, S(k, 1), xB, S(k, 2));
+                }
+            } else {  // z1122
+                if (r2g)
+                    L[k] = o_lin2(xAA, S(k, 0) * std::pow(r3, g2), xA, S(k, 1) * std::pow(r1, g2)) / std::pow(rr, g2);
+                else
+                    L[k] = o_lin2(xAA, S(k, 0), xA, S(k, 1));
+                R[k] = o_lin2(xB, S(k, 2), xBB, S(k, 3));
+            }
+        }
+        if (z1122)
+            for (int k = 1; k < 8; ++k)
+                if (k != 4) R[k] = o_lin2(xB, S(k, 2), xBB, S(k, 3));
+    } else {
+        const bool l2 = (a0 == 2 && a1 == 2 && b1 == 3 && b0 == 3) || (a0 == 3 && a1 == 3 && b1 == 4 && b0 == 4);
+        const bool l3 = (a0 == 2 && a1 == 2 && b1 == 2 && b0 == 3) || (a0 == 3 && a1 == 3 && b1 == 3 && b0 == 4);
+        const bool l4 = z1222 || (a0 == 2 && a1 == 3 && b1 == 3 && b0 == 3) || (a0 == 3 && a1 == 4 && b1 == 4 && b0 == 4);
+        for (int k = 0; k < NV; ++k) {
+            if (l2) {
+                L[k] = o_lin2(xAA, S(k, 0), xA, S(k, 1));
+                R[k] = o_lin2(xB, S(k, 2), xBB, S(k, 3));
+            } else if (l3) {
+                L[k] = o_lin3(xAA, S(k, 0), xA, S(k, 1), xB, S(k, 2));
+                R[k] = o_lin2(xA, S(k, 1), xB, S(k, 2));
+            } else if (l4) {
+                L[k] = o_lin2(xA, S(k, 1), xB, S(k, 2));
+                R[k] = o_lin3(xA, S(k, 1), xB, S(k, 2), xBB, S(k, 3));
+            } else {
+                L[k] = o_lin3(xAA, S(k, 0), xA, S(k, 1), xB, S(k, 2));
+                R[k] = o_lin3(xA, S(k, 1), xB, S(k, 2), xBB, S(k, 3));
+            }
+        }
+    }
+    // positivity fall-back to the cell value (:710-720)
+    const int fl[4] = {0, 8, 9, 4};
+    for (int q = 0; q < 4; ++q) {
+        const int k = fl[q];
+        if (k >= 8 && k - 8 >= npassive) continue;
+        if (L[k] < 0.0000001) L[k] = S(k, 1);
+        if (R[k] < 0.0000001) R[k] = S(k, 2);
+    }
+}
+
 // Per-face flux, restating Setka::Culc_Gran_Potok (Setka_physics.cpp:2280-2571)
 // for the plasma: reconstruction, solver choice, chlld, local dt, flux*area,
 // Powell PdivB. Writes 11 values per face: rho, Vx, Vy, Vz, p(energy), Bx,
@@ -767,8 +947,16 @@ static double o_face(const OMesh* M, const OParams* P, const double* st, const d
     if (type == 0) {
         const double dx = cc[3 * A] - cc[3 * B], dy = cc[3 * A + 1] - cc[3 * B + 1], dz = cc[3 * A + 2] - cc[3 * B + 2];
         dist = std::sqrt(dx * dx + dy * dy + dz * dz) / 2.0;
-        o_snos_side(st, nc, A, M->cell_type[A], cc, fc + 3 * f, P->gamma, L);
-        o_snos_side(st, nc, B, M->cell_type[B], cc, fc + 3 * f, P->gamma, R);
+        const int64_t AA = M->face_tvd ? M->face_tvd[2 * f] : -1, BB = M->face_tvd ? M->face_tvd[2 * f + 1] : -1;
+        if (P->tvd && M->cell_tvd[A] && M->cell_tvd[B] && (M->face_surf[f] != 2 || P->snos_on_hp) && AA >= 0 &&
+            BB >= 0) {
+            const int64_t c4[4] = {AA, A, B, BB};
+            const int t4[4] = {M->cell_type[AA], M->cell_type[A], M->cell_type[B], M->cell_type[BB]};
+            o_snos_tvd(st, nc, c4, t4, cc, fc + 3 * f, P->gamma, P->npassive, L, R);
+        } else {
+            o_snos_side(st, nc, A, M->cell_type[A], cc, fc + 3 * f, P->gamma, L);
+            o_snos_side(st, nc, B, M->cell_type[B], cc, fc + 3 * f, P->gamma, R);
+        }
     } else {
         // boundary faces, Setka_gran_snos.cpp:7-65; plasma_condition (Phys_param.cpp:203-206):
         // Inner_Hard 2, Outer_Hard 2, Outer_Soft 1
@@ -1011,6 +1199,98 @@ void oracle_move_nodes(const OMesh* M, const OParams* P, const double* xyz1, dou
         xyz2[3 * i] = x + s * x;
         xyz2[3 * i + 1] = y + s * y;
         xyz2[3 * i + 2] = z + s * z;
+    }
+}
+
+// Second-order neighbours of every face, restating Setka::Init_TVD
+// (Setka_physics.cpp:646-738) on the geometry of `xyz`: beyond each side,
+// the neighbour through another face of that cell whose centre direction
+// from the face centre is most opposite to the side's outward normal (the
+// first minimum in the cell's face order), dropped when that direction is
+// within acos(0.1) of the face plane. out: nface*2 (AA, BB), -1 when absent.
+void oracle_tvd_neighbours(const OMesh* M, const double* xyz, int32_t* out) {
+    const int64_t nc = M->ncell, nf = M->nface;
+    std::vector<double> cc(3 * nc), vol(nc), fc(3 * nf), fn(3 * nf), fa(nf);
+    oracle_geometry(M, xyz, cc.data(), vol.data(), fc.data(), fn.data(), fa.data());
+    auto normalized = [](double* v) {
+        const double z = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
+        if (z > 0.0) {
+            const double s = std::sqrt(z);
+            v[0] = v[0] / s;
+            v[1] = v[1] / s;
+            v[2] = v[2] / s;
+        }
+    };
+    auto dot = [](const double* a, const double* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; };
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < nf; ++f) {
+        const double* G = fc.data() + 3 * f;
+        double nrm[3] = {fn[3 * f], fn[3 * f + 1], fn[3 * f + 2]};
+        out[2 * f] = out[2 * f + 1] = -1;
+        for (int side = 0; side < 2; ++side) {
+            const int64_t A = M->face_cells[2 * f + side];
+            if (A < 0) break;
+            double vec[3] = {nrm[0], nrm[1], nrm[2]};
+            if (side == 1)
+                for (int j = 0; j < 3; ++j) vec[j] = vec[j] * -1.0;
+            double best = 2.0;
+            int64_t pick = -1;
+            for (int k = 0; k < 6; ++k) {
+                const int64_t g = M->cell_faces[6 * A + k];
+                if (g == f) continue;
+                const int64_t g0 = M->face_cells[2 * g], g1 = M->face_cells[2 * g + 1];
+                if (g1 < 0) continue;  // boundary face: no neighbour (Get_Sosed)
+                const int64_t cel = g0 == A ? g1 : g0;
+                double u[3] = {cc[3 * cel] - G[0], cc[3 * cel + 1] - G[1], cc[3 * cel + 2] - G[2]};
+                normalized(u);
+                const double cosine = dot(vec, u);
+                if (cosine < best) {
+                    best = cosine;
+                    pick = cel;
+                }
+            }
+            out[2 * f + side] = (int32_t)pick;
+        }
+        if (M->face_cells[2 * f + 1] < 0) continue;
+        // direction checks against the face normal (:724-736)
+        for (int side = 0; side < 2; ++side) {
+            const int64_t cel = out[2 * f + side];
+            if (cel < 0) continue;
+            double k3[3] = {cc[3 * cel] - G[0], cc[3 * cel + 1] - G[1], cc[3 * cel + 2] - G[2]};
+            normalized(k3);
+            const double d = dot(nrm, k3);
+            if ((side == 0 ? -d : d) < 0.1) out[2 * f + side] = -1;
+        }
+    }
+}
+
+// Reconstructed face states of every interior face at layer `xyz` (the
+// states Culc_Gran_Potok hands to the Riemann solver): LR [nface][2][NV];
+// boundary faces are left untouched. used [nface]: 1 where the second-order
+// branch ran.
+void oracle_face_states(const OMesh* M, const OParams* P, const double* st, const double* xyz, double* LR,
+                        int8_t* used) {
+    const int64_t nc = M->ncell, nf = M->nface;
+    std::vector<double> cc(3 * nc), vol(nc), fc(3 * nf), fn(3 * nf), fa(nf);
+    oracle_geometry(M, xyz, cc.data(), vol.data(), fc.data(), fn.data(), fa.data());
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < nf; ++f) {
+        used[f] = 0;
+        if (M->face_type[f] != 0) continue;
+        const int64_t A = M->face_cells[2 * f], B = M->face_cells[2 * f + 1];
+        double* L = LR + 2 * NV * f;
+        double* R = L + NV;
+        const int64_t AA = M->face_tvd ? M->face_tvd[2 * f] : -1, BB = M->face_tvd ? M->face_tvd[2 * f + 1] : -1;
+        if (P->tvd && M->cell_tvd[A] && M->cell_tvd[B] && (M->face_surf[f] != 2 || P->snos_on_hp) && AA >= 0 &&
+            BB >= 0) {
+            const int64_t c4[4] = {AA, A, B, BB};
+            const int t4[4] = {M->cell_type[AA], M->cell_type[A], M->cell_type[B], M->cell_type[BB]};
+            o_snos_tvd(st, nc, c4, t4, cc.data(), fc.data() + 3 * f, P->gamma, P->npassive, L, R);
+            used[f] = 1;
+        } else {
+            o_snos_side(st, nc, A, M->cell_type[A], cc.data(), fc.data() + 3 * f, P->gamma, L);
+            o_snos_side(st, nc, B, M->cell_type[B], cc.data(), fc.data() + 3 * f, P->gamma, R);
+        }
     }
 }
 

@@ -41,6 +41,7 @@ class OMesh(ctypes.Structure):
         ("cell_nodes", I32), ("cell_faces", I32), ("cell_type", I8), ("cell_tvd", U8),
         ("face_nodes", I32), ("face_cells", I32), ("face_type", I8), ("face_surf", I8),
         ("face_method", I8), ("face_bc", I32), ("bc_vals", D), ("node_amp", D), ("node_phase", D),
+        ("face_tvd", I32),
     ]
 
 
@@ -51,7 +52,8 @@ class OParams(ctypes.Structure):
         ("par_Kn", ctypes.c_double), ("beta_switch", ctypes.c_double),
         ("move", ctypes.c_int32), ("soft_fixups", ctypes.c_int32), ("method_policy", ctypes.c_int32),
         ("npassive", ctypes.c_int32), ("nh", ctypes.c_int32), ("TS_hard", ctypes.c_int32),
-        ("contact_hard", ctypes.c_int32), ("pad", ctypes.c_int32),
+        ("contact_hard", ctypes.c_int32), ("tvd", ctypes.c_int32), ("snos_on_hp", ctypes.c_int32),
+        ("pad", ctypes.c_int32 * 2),
     ]
 
 
@@ -92,6 +94,8 @@ def oracle():
         lib.oracle_move_nodes.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D,
                                           ctypes.c_double, ctypes.c_double]
         lib.oracle_num_threads.restype = ctypes.c_int
+        lib.oracle_tvd_neighbours.argtypes = [ctypes.POINTER(OMesh), D, I32]
+        lib.oracle_face_states.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D, D, I8]
         _oracle = lib
     return _oracle
 
@@ -206,6 +210,11 @@ class OracleRun:
             if k != "pad":
                 setattr(p, k, params[k])
         self.params = p
+        self.face_tvd = None
+        if p.tvd:
+            self.face_tvd = keep("tvd", np.empty((m.nface, 2), dtype=np.int32), np.int32)
+            oracle().oracle_tvd_neighbours(ctypes.byref(m), _p(self.xyz), _p(self.face_tvd, I32))
+            m.face_tvd = _p(self.face_tvd, I32)
         self.ncell = m.ncell
         self.clock = np.array([1e-5, 0.0])
         self.hf = None
@@ -229,6 +238,15 @@ class OracleRun:
         fc, fn, fa = np.empty((nf, 3)), np.empty((nf, 3)), np.empty(nf)
         oracle().oracle_geometry(ctypes.byref(self.mesh), _p(xyz), _p(cc), _p(vol), _p(fc), _p(fn), _p(fa))
         return dict(cell_center=cc, cell_volume=vol, face_center=fc, face_normal=fn, face_area=fa)
+
+    def face_states(self, state: np.ndarray):
+        """(LR [nface, 2, 10] reconstructed face states of interior faces, used [nface] second order)."""
+        nf = self.mesh.nface
+        LR = np.zeros((nf, 2, NV))
+        used = np.zeros(nf, dtype=np.int8)
+        oracle().oracle_face_states(ctypes.byref(self.mesh), ctypes.byref(self.params),
+                                    _p(np.ascontiguousarray(state)), _p(self.xyz), _p(LR), _p(used, I8))
+        return LR, used
 
     def face_fluxes(self, state: np.ndarray, time: float = 1e-5):
         """Face fluxes (11 per face) of `state` at the current nodes (stationary w)."""

@@ -1,0 +1,119 @@
+"""Second-order (TVD) faces on the GPU against the oracle.
+
+The neighbours (Setka::Init_TVD) are integers and must match exactly. Steps:
+on the cube (no Zone_1 cells, no transcendental functions on the path) the
+GPU equals the oracle bit for bit; on the shell with zones, node motion and
+passive scalars every branch of Setka_gran_snos.cpp:188-735 runs, and the
+Zone_1 spherical transforms call acos / atan / sin / cos / pow, so the bar is
+1e-12 relative per cell per step on the conserved fields.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from test_gpu_parity import REL, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def T(titan, built_lib):
+    return titan
+
+
+def _pair(T, m, p, meth=None):
+    gpu = T.PlasmaStep(m, p)
+    run = ol.OracleRun(m, p)
+    if meth is not None:
+        gpu.set_face_method(meth)
+        run.set_face_method(meth)
+    return gpu, run
+
+
+@pytest.mark.parametrize("kind", ["cube", "shell", "shell_moving"])
+def test_neighbours_match_oracle(T, oracle_lib, kind):
+    if kind == "cube":
+        m, p, _, _ = T.problems.brio_wu_cube(10)
+    else:
+        m, p, _, _ = T.problems.heliosphere_shell(nq=8, nlayer=6, move=kind == "shell_moving", zones=True)
+    p = dict(p, tvd=1)
+    gpu, run = _pair(T, m, p)
+    got = gpu.tvd_neighbours()
+    np.testing.assert_array_equal(got, run.face_tvd)
+    assert (got[:, 0] >= 0).sum() > 0.5 * len(got)
+    gpu.close()
+
+
+@pytest.mark.parametrize("steps", [1, 6])
+def test_brio_wu_second_order_matches_oracle_exactly(T, oracle_lib, steps):
+    m, p, st, meth = T.problems.brio_wu_cube(14)
+    p = dict(p, tvd=1)
+    gpu, run = _pair(T, m, p, meth)
+    gpu.upload_state(st)
+    s_or = np.ascontiguousarray(st.copy())
+    gpu.go(steps)
+    assert run.go(s_or, steps).err_code == 0
+    s_gpu = gpu.download_state()
+    assert np.array_equal(s_gpu[:8], s_or[:8]), rel_err(s_gpu[:8], s_or[:8])
+    assert gpu.dt == run.clock[0]
+    gpu.close()
+
+
+@pytest.mark.parametrize("features", [
+    dict(move=False, zones=True, npassive=0),
+    dict(move=True, zones=True, npassive=2),
+    dict(move=True, zones=False, npassive=2),
+])
+def test_shell_second_order_per_step_parity(T, oracle_lib, features):
+    """Re-synchronise the oracle to the GPU state every step (15 steps)."""
+    m, p, st, _ = T.problems.heliosphere_shell(nq=8, nlayer=8, **features)
+    p = dict(p, tvd=1)
+    gpu, run = _pair(T, m, p)
+    gpu.upload_state(st)
+    ns = 8 + p["npassive"]
+    worst = 0.0
+    for _ in range(15):
+        before = np.ascontiguousarray(gpu.download_state())
+        run.xyz[:] = gpu.nodes()
+        run.clock[:] = (gpu.dt, gpu.t)
+        gpu.go(1)
+        assert run.go(before, 1).err_code == 0
+        worst = max(worst, rel_err(gpu.download_state()[:ns], before[:ns]))
+    assert worst <= REL, worst
+    gpu.close()
+
+
+def test_every_launch_shape_gives_identical_second_order_results(T):
+    m, p, st, _ = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, zones=True, npassive=2)
+    p = dict(p, tvd=1)
+    ref = None
+    for fv in range(6):
+        g = T.PlasmaStep(m, p)
+        g.upload_state(st)
+        g.set_tuning(fv, fv % 5)
+        g.go(4)
+        out = g.download_state()
+        g.close()
+        if ref is None:
+            ref = out
+        else:
+            assert np.array_equal(out, ref), fv
+
+
+def test_fp32_second_order_error_against_fp64(T):
+    """FP32 Riemann flux with second-order faces against the FP64 step: the
+    minmod limiter switches on the sign of slopes (with the reference's 1e-8
+    dead band), so rounding differences flip it in a few cells and the
+    difference is larger than with first-order faces (measured 3.3e-4 in
+    rho after 30 steps on this coarse mesh)."""
+    m, p, st, _ = T.problems.heliosphere_shell(nq=10, nlayer=8, move=True, zones=True)
+    out = {}
+    for prec in (64, 32):
+        g = T.PlasmaStep(m, dict(p, tvd=1, flux_precision=prec))
+        g.upload_state(st)
+        g.go(30)
+        out[prec] = g.download_state()
+        g.close()
+    for k in (0, 4):
+        l1 = np.abs(out[32][k] - out[64][k]).sum() / np.abs(out[64][k]).sum()
+        assert l1 < 1e-3, (k, l1)

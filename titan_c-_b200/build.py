@@ -6,6 +6,7 @@ Translation units and their floating-point flags:
   kernels_fp64.cu  -fmad=false  geometry, FP64 flux, cell update (bit-exact FP64)
   kernels_fp32.cu  -fmad=true -prec-div=false -prec-sqrt=false
                                 FP32 Riemann flux of the mixed-precision step
+  kernels_tvd_fp64.cu, kernels_tvd_fp32.cu   the same with second-order faces
   mc_neutral.cu                 Monte-Carlo neutral hydrogen (source generator)
   closure_mlp.cu                closure inference on tcgen05 / TMEM (per step)
   closure_train.cu, closure_api.cu   closure training (BF16 tensor-core GEMMs), C ABI
@@ -31,6 +32,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
     ("kernels_fp32.cu", ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
+    ("kernels_tvd_fp64.cu", ["-fmad=false"]),
+    ("kernels_tvd_fp32.cu", ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("mc_neutral.cu", []),
     ("closure_mlp.cu", []),
     ("closure_train.cu", []),
@@ -68,8 +71,11 @@ def _includes(path: str, seen: set[str]) -> set[str]:
 
 
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+    """Compiles the stale translation units in parallel and links the library."""
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src, flags in UNITS:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
@@ -78,9 +84,16 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
             cmd = [nvcc(), *ARCH, *COMMON, *flags, *(extra or []), "-c", s, "-o", o]
             if src.endswith(".cpp"):
                 cmd = [nvcc(), *COMMON, "-Wno-deprecated-gpu-targets", "-x", "c++", "-c", s, "-o", o]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    for cmd in cmds:
+        if verbose:
+            print(" ".join(cmd), flush=True)
+    workers = max(1, min(len(cmds), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        for r in list(pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            if r.stdout or r.stderr:
+                print(r.stdout + r.stderr, end="", flush=True)
+            r.check_returncode()
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         if verbose:

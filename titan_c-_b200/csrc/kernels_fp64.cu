@@ -1,8 +1,7 @@
 // FP64 translation unit: geometry, FP64 face flux, cell update, permutations.
 // Built with -fmad=false so that double-precision expressions round exactly as
 // the reference's x86-64 build (no fused multiply-add contraction).
-#include "launch.h"
-#include "step_kernels.cuh"
+#include "face_dispatch.cuh"
 
 namespace titan {
 
@@ -22,35 +21,8 @@ cudaError_t launch_face_geometry(const MeshView& M, const Layer& L, cudaStream_t
     return cudaGetLastError();
 }
 
-template <typename R, int NK, bool MOVE>
-static cudaError_t face_flux_variant(const FaceArgs& a, int v, cudaStream_t s) {
-    switch (v) {
-#define TITAN_FACE_CASE(i)                                                                              \
-    case i: {                                                                                         \
-        constexpr FaceVariant fv = kFaceVariant[i];                                                   \
-        face_flux_kernel<R, R, NK, MOVE, fv.block, fv.min_blocks>                                     \
-            <<<blocks_for(a.M.nface, fv.block), fv.block, 0, s>>>(a);                                 \
-        break;                                                                                        \
-    }
-        TITAN_FACE_CASE(0)
-        TITAN_FACE_CASE(1)
-        TITAN_FACE_CASE(2)
-        TITAN_FACE_CASE(3)
-        TITAN_FACE_CASE(4)
-        TITAN_FACE_CASE(5)
-#undef TITAN_FACE_CASE
-        default:
-            return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
-}
-
 cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s) {
-    if (nk == 0 && !move) return face_flux_variant<double, 0, false>(a, variant, s);
-    if (nk == 0 && move) return face_flux_variant<double, 0, true>(a, variant, s);
-    if (nk == 2 && !move) return face_flux_variant<double, 2, false>(a, variant, s);
-    if (nk == 2 && move) return face_flux_variant<double, 2, true>(a, variant, s);
-    return cudaErrorInvalidValue;
+    return face_flux_dispatch<double, false>(a, nk, move, variant, s);
 }
 
 template <typename FT, int NK, bool MOVE, int BS, int MINB>

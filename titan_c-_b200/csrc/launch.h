@@ -1,5 +1,6 @@
-// Host-callable launchers of the step kernels (implemented in kernels_fp64.cu,
-// built with -fmad=false, and kernels_fp32.cu, built with contraction on).
+// Host-callable launchers of the step kernels (implemented in kernels_fp64.cu
+// and kernels_tvd_fp64.cu, built with -fmad=false, and kernels_fp32.cu and
+// kernels_tvd_fp32.cu, built with contraction on).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -28,6 +29,10 @@ cudaError_t launch_cell_geometry(const MeshView& M, const Layer& L, cudaStream_t
 cudaError_t launch_face_geometry(const MeshView& M, const Layer& L, cudaStream_t s);
 cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s);
 cudaError_t launch_face_flux_fp32(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s);
+// second-order faces (kernels_tvd_fp64.cu, kernels_tvd_fp32.cu)
+cudaError_t launch_face_flux_tvd_fp64(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s);
+cudaError_t launch_face_flux_tvd_fp32(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s);
+cudaError_t launch_tvd_neighbours(const MeshView& M, const Layer& L, int* aa, int* bb, cudaStream_t s);
 // flux_fp32: the flux buffer holds floats
 cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, int variant,
                                cudaStream_t s);

@@ -298,7 +298,72 @@ struct FluxLayout {
     static constexpr int stride = (sizeof(FT) == 8) ? ((n + 1) & ~1) : ((n + 3) & ~3);
 };
 
-template <typename R, typename FT, int NK, bool MOVE, int BS, int MINB>
+}  // namespace titan
+#include "tvd.cuh"
+namespace titan {
+
+// Second-order neighbours of every face (Setka::Init_TVD,
+// Setka_physics.cpp:646-738) on the geometry of layer L: beyond each side, the
+// neighbour through another face of that cell whose centre direction from the
+// face centre is most opposite to the side's outward normal (the first
+// minimum in the cell's face order), dropped when that direction lies within
+// acos(0.1) of the face plane. Eigen's dot and normalized() orders.
+static __global__ void tvd_neighbours_kernel(MeshView M, Layer L, int* __restrict__ aa, int* __restrict__ bb) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= M.nface) return;
+    const int nf = M.nface, nc = M.ncell;
+    const double G[3] = {L.fc[f], L.fc[nf + f], L.fc[2 * nf + f]};
+    const double nrm[3] = {L.fn[f], L.fn[nf + f], L.fn[2 * nf + f]};
+    int pick[2] = {-1, -1};
+    for (int side = 0; side < 2; ++side) {
+        const int A = side == 0 ? M.face_c0[f] : M.face_c1[f];
+        if (A < 0) break;
+        double vec[3] = {nrm[0], nrm[1], nrm[2]};
+        if (side == 1)
+            for (int j = 0; j < 3; ++j) vec[j] = vec[j] * -1.0;
+        double best = 2.0;
+        for (int k = 0; k < 6; ++k) {
+            const int g = M.cell_faces[k * nc + A] & 0x7fffffff;
+            if (g == f) continue;
+            const int g0 = M.face_c0[g], g1 = M.face_c1[g];
+            if (g1 < 0) continue;
+            const int cel = g0 == A ? g1 : g0;
+            double u[3] = {L.cc[cel] - G[0], L.cc[nc + cel] - G[1], L.cc[2 * nc + cel] - G[2]};
+            const double z = (u[0] * u[0] + u[1] * u[1]) + u[2] * u[2];
+            if (z > 0.0) {
+                const double sz = sqrt(z);
+                u[0] = u[0] / sz;
+                u[1] = u[1] / sz;
+                u[2] = u[2] / sz;
+            }
+            const double cosine = (vec[0] * u[0] + vec[1] * u[1]) + vec[2] * u[2];
+            if (cosine < best) {
+                best = cosine;
+                pick[side] = cel;
+            }
+        }
+    }
+    if (M.face_c1[f] >= 0) {
+        for (int side = 0; side < 2; ++side) {
+            const int cel = pick[side];
+            if (cel < 0) continue;
+            double k3[3] = {L.cc[cel] - G[0], L.cc[nc + cel] - G[1], L.cc[2 * nc + cel] - G[2]};
+            const double z = (k3[0] * k3[0] + k3[1] * k3[1]) + k3[2] * k3[2];
+            if (z > 0.0) {
+                const double sz = sqrt(z);
+                k3[0] = k3[0] / sz;
+                k3[1] = k3[1] / sz;
+                k3[2] = k3[2] / sz;
+            }
+            const double d = (nrm[0] * k3[0] + nrm[1] * k3[1]) + nrm[2] * k3[2];
+            if ((side == 0 ? -d : d) < 0.1) pick[side] = -1;
+        }
+    }
+    aa[f] = pick[0];
+    bb[f] = pick[1];
+}
+
+template <typename R, typename FT, int NK, bool MOVE, int BS, int MINB, bool TVD = false>
 __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 100000000.0;  // identity of the min (Setka_physics.cpp:1607)
@@ -361,7 +426,34 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
             for (int k = 0; k < NS; ++k) Rs[k] = a.state[k * nc + c1];
 #pragma unroll
             for (int k = NS; k < NV; ++k) Rs[k] = 0.0;
-            const bool z0 = M.cell_type[c0] == 1, z1 = M.cell_type[c1] == 1;
+            bool second = false;
+            if (TVD) {
+                const int aa = M.face_aa[f], bb = M.face_bb[f];
+                if (aa >= 0 && bb >= 0 && M.cell_tvd[c0] && M.cell_tvd[c1] &&
+                    (M.face_surf[f] != 2 || P.snos_on_hp)) {
+                    // second-order branch (Setka_gran_snos.cpp:188-735)
+                    if (!MOVE) {
+                        gc[0] = a.L1.fc[f];
+                        gc[1] = a.L1.fc[nf + f];
+                        gc[2] = a.L1.fc[2 * nf + f];
+                    }
+                    const int c4[4] = {aa, c0, c1, bb};
+                    double S4[4][NV], X4[4][3];
+                    int t4[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                        for (int k = 0; k < NS; ++k) S4[i][k] = a.state[k * nc + c4[i]];
+#pragma unroll
+                        for (int k = NS; k < NV; ++k) S4[i][k] = 0.0;
+                        load_cc(a.L1.cc, nc, c4[i], X4[i]);
+                        t4[i] = M.cell_type[c4[i]];
+                    }
+                    snos_tvd<NK>(S4, X4, t4, gc, P.gamma, Ls, Rs);
+                    second = true;
+                }
+            }
+            const bool z0 = !second && M.cell_type[c0] == 1, z1 = !second && M.cell_type[c1] == 1;
             if (z0 || z1) {
                 if (!MOVE) {
                     gc[0] = a.L1.fc[f];

@@ -26,6 +26,7 @@ struct DevStatus {
 struct Params {
     double gamma, KFL, velosity_inf, omega, par_a_2, par_n_H_LISM, par_Kn, beta_switch;
     int move, soft_fixups, method_policy, npassive, nh, TS_hard, contact_hard, src_mode;
+    int tvd, snos_on_hp;   // second-order faces (Phys_param::TVD, Snos_on_HP)
 };
 
 struct MeshView {
@@ -46,6 +47,8 @@ struct MeshView {
     const double* node_phase;     // [nnode] or null
     const unsigned short* cell_fmap;  // [6][ncell]: the 4 nodes of each face slot as
                                       // 3-bit indices into the cell's 8 nodes (ALE)
+    const int* face_aa;           // [nface] second-order neighbour beyond cells[0] or -1
+    const int* face_bb;           // [nface] second-order neighbour beyond cells[1] or -1
 };
 
 struct Layer {  // geometry of one time layer (the reference's [2] arrays)

@@ -83,6 +83,7 @@ struct titan_ctx {
     uint8_t* d_cell_tvd = nullptr;
     double *d_node_amp = nullptr, *d_node_phase = nullptr;
     uint16_t* d_cell_fmap = nullptr;
+    int32_t *d_face_aa = nullptr, *d_face_bb = nullptr;  // second-order neighbours (tvd)
 
     Layer layer[2]{};
     int cur = 0;
@@ -135,6 +136,8 @@ struct titan_ctx {
         M.node_amp = d_node_amp;
         M.node_phase = d_node_phase;
         M.cell_fmap = d_cell_fmap;
+        M.face_aa = d_face_aa;
+        M.face_bb = d_face_bb;
         return M;
     }
 };
@@ -200,10 +203,17 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     fa.flux = ctx->d_flux;
     fa.st = ctx->d_status;
     const int nk = ctx->prm.npassive;
-    if (ctx->fp32)
-        e = timed(ctx, "face_flux_fp32", [&] { return launch_face_flux_fp32(fa, nk, move, ctx->face_variant, ctx->stream); });
-    else
-        e = timed(ctx, "face_flux_fp64", [&] { return launch_face_flux_fp64(fa, nk, move, ctx->face_variant, ctx->stream); });
+    const int fv = ctx->face_variant;
+    if (ctx->P.tvd) {
+        if (ctx->fp32)
+            e = timed(ctx, "face_flux_tvd_fp32", [&] { return launch_face_flux_tvd_fp32(fa, nk, move, fv, ctx->stream); });
+        else
+            e = timed(ctx, "face_flux_tvd_fp64", [&] { return launch_face_flux_tvd_fp64(fa, nk, move, fv, ctx->stream); });
+    } else if (ctx->fp32) {
+        e = timed(ctx, "face_flux_fp32", [&] { return launch_face_flux_fp32(fa, nk, move, fv, ctx->stream); });
+    } else {
+        e = timed(ctx, "face_flux_fp64", [&] { return launch_face_flux_fp64(fa, nk, move, fv, ctx->stream); });
+    }
     if (e) return e;
     CellArgs ca;
     ca.M = M;
@@ -270,6 +280,7 @@ std::string validate(const titan_mesh* m, const titan_params* p) {
     if (p->npassive != 0 && p->npassive != 2) return "npassive must be 0 or 2";
     if (p->nh < 0 || p->nh > 4) return "nh must be 0..4";
     if (p->flux_precision != 64 && p->flux_precision != 32) return "flux_precision must be 64 or 32";
+    if (p->tvd != 0 && p->tvd != 1) return "tvd must be 0 or 1";
     if (!(p->gamma > 1.0)) return "gamma must exceed 1";
     for (int64_t i = 0; i < 3 * m->nnode; ++i)
         if (!std::isfinite(m->node_xyz[i])) return "non-finite node coordinate";
@@ -345,7 +356,7 @@ int titan_destroy(titan_ctx* ctx) {
                     ctx->d_face_nodes, ctx->d_face_type, ctx->d_face_surf, ctx->d_face_method, ctx->d_bc_vals,
                     ctx->d_cell_faces, ctx->d_cell_nodes, ctx->d_cell_type, ctx->d_cell_tvd, ctx->d_node_amp,
                     ctx->d_node_phase, ctx->d_state[0], ctx->d_state[1], ctx->d_flux, ctx->d_hfl, ctx->d_src,
-                    ctx->d_stage, ctx->d_status, ctx->d_cell_fmap};
+                    ctx->d_stage, ctx->d_status, ctx->d_cell_fmap, ctx->d_face_aa, ctx->d_face_bb};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     // without node motion layer[1] aliases layer[0]: free it once
@@ -396,6 +407,8 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     P.TS_hard = p->TS_hard;
     P.contact_hard = p->contact_hard;
     P.src_mode = 0;
+    P.tvd = p->tvd;
+    P.snos_on_hp = p->snos_on_hp;
 
     auto bail = [&](int code) {
         titan_destroy(ctx);
@@ -506,6 +519,10 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
         DA(ctx->d_node_phase, nn);
     }
     if (p->move) DA(ctx->d_cell_fmap, 6 * nc);
+    if (p->tvd) {
+        DA(ctx->d_face_aa, nf);
+        DA(ctx->d_face_bb, nf);
+    }
     const int nlayers = p->move ? 2 : 1;
     for (int l = 0; l < nlayers; ++l) {
         Layer& L = ctx->layer[l];
@@ -569,9 +586,27 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     const MeshView M = ctx->view();
     if (!e) e = launch_cell_geometry(M, ctx->layer[0], s);
     if (!e) e = launch_face_geometry(M, ctx->layer[0], s);
+    // second-order neighbours from the initial geometry (Setka::Init_TVD runs once, before Go)
+    if (!e && p->tvd) e = launch_tvd_neighbours(M, ctx->layer[0], ctx->d_face_aa, ctx->d_face_bb, s);
     if (!e) e = cudaStreamSynchronize(s);
     if (e) return bail(fail(TITAN_ECUDA, std::string("create: ") + cudaGetErrorString(e)));
     *out = ctx;
+    return TITAN_OK;
+}
+
+int titan_get_tvd_neighbours(titan_ctx* ctx, int32_t* out) {
+    if (!ctx || !out) return fail(TITAN_EINVAL, "null argument");
+    if (!ctx->P.tvd) return fail(TITAN_EINVAL, "context was created with tvd = 0");
+    const int64_t nf = ctx->nface;
+    std::vector<int32_t> aa(nf), bb(nf);
+    CK(cudaMemcpyAsync(aa.data(), ctx->d_face_aa, sizeof(int32_t) * nf, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(bb.data(), ctx->d_face_bb, sizeof(int32_t) * nf, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int64_t f = 0; f < nf; ++f) {
+        const int64_t o = ctx->R.face_n2o[f];
+        out[2 * o] = aa[f] >= 0 ? ctx->R.cell_n2o[aa[f]] : -1;
+        out[2 * o + 1] = bb[f] >= 0 ? ctx->R.cell_n2o[bb[f]] : -1;
+    }
     return TITAN_OK;
 }
 

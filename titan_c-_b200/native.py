@@ -50,6 +50,7 @@ class TitanParams(ctypes.Structure):
         ("move", ctypes.c_int32), ("soft_fixups", ctypes.c_int32), ("method_policy", ctypes.c_int32),
         ("npassive", ctypes.c_int32), ("nh", ctypes.c_int32), ("TS_hard", ctypes.c_int32),
         ("contact_hard", ctypes.c_int32), ("flux_precision", ctypes.c_int32),
+        ("tvd", ctypes.c_int32), ("snos_on_hp", ctypes.c_int32),
     ]
 
 
@@ -117,6 +118,7 @@ SIGNATURES = {
     "titan_mlp_grad": ([F32, F32, F32, F32, F32, F32, ctypes.c_int64, F32, F32, F32], ctypes.c_int),
     "titan_mlp_train": ([F32, F32, F32, F32, F32, F32, ctypes.c_int64, ctypes.POINTER(TitanMlpTrainOpts), F32],
                         ctypes.c_int),
+    "titan_get_tvd_neighbours": ([ctypes.c_void_p, I32], ctypes.c_int),
     "titan_set_closure": ([ctypes.c_void_p, F32, F32, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "titan_autotune": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p], ctypes.c_int),
     "titan_set_tuning": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),

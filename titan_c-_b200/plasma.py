@@ -145,6 +145,12 @@ class PlasmaStep:
         N.check(self._lib.titan_download_face_fluxes(self._ctx, N.ptr(out)))
         return out
 
+    def tvd_neighbours(self) -> np.ndarray:
+        """[nface, 2] second-order neighbours (AA, BB), original numbering, -1 when absent."""
+        out = np.empty((self.nface, 2), dtype=np.int32)
+        N.check(self._lib.titan_get_tvd_neighbours(self._ctx, N.ptr(out, N.I32)))
+        return out
+
     def permutation(self):
         c = np.empty(self.ncell, dtype=np.int32)
         f = np.empty(self.nface, dtype=np.int32)

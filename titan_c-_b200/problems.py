@@ -24,7 +24,7 @@ GAMMA = 5.0 / 3.0
 DEFAULT_PARAMS = dict(
     gamma=GAMMA, KFL=0.4, velosity_inf=-2.54327, omega=2.0 * np.pi, par_a_2=0.102046, par_n_H_LISM=3.0,
     par_Kn=40.0906, beta_switch=0.01, move=0, soft_fixups=1, method_policy=0, npassive=0, nh=0, TS_hard=0,
-    contact_hard=0, flux_precision=64,
+    contact_hard=0, flux_precision=64, tvd=0, snos_on_hp=0,
 )
 
 
@@ -84,7 +84,7 @@ def _lism(n: int, rho=0.06, u=2.6, mach=2.0, b=0.3, angle_deg=60.0, gamma=GAMMA)
 
 def heliosphere_shell(nq: int = 96, nlayer: int = 40, seed: int = 20261203, move: bool = True,
                       zones: bool = False, npassive: int = 0, nh: int = 0, flux_precision: int = 64,
-                      r_mid: float = 25.0, width: float = 3.0, amp: float = 1e-3):
+                      r_mid: float = 25.0, width: float = 3.0, amp: float = 1e-3, tvd: bool = False):
     """(mesh, params, state [10, C], hfluids [5 nh, C] or None)."""
     m = _mesh.shell_mesh(nq, nlayer)
     rng = np.random.default_rng(seed)
@@ -142,7 +142,7 @@ def heliosphere_shell(nq: int = 96, nlayer: int = 40, seed: int = 20261203, move
         m["node_phase"] = np.ascontiguousarray(phase_ray[m["node_ray"]])
 
     prm = params(KFL=0.4, soft_fixups=1, method_policy=1, beta_switch=0.01, move=int(move),
-                 npassive=npassive, nh=nh, flux_precision=flux_precision)
+                 npassive=npassive, nh=nh, flux_precision=flux_precision, tvd=int(tvd))
     hf = None
     if nh:
         hf = np.zeros((5 * nh, C))

@@ -86,9 +86,11 @@ def _shell_run(titan, steps, nq=10, nlayer=14):
 
 
 def test_closure_inside_the_step_equals_its_sources(titan):
-    """A step with the network installed equals a step given the same
-    network's sources through titan_set_sources (features on the device vs
-    numpy: equal up to float rounding of the features)."""
+    """A step with the network installed changes the state as a step given
+    the same network's sources through titan_set_sources does. The kernel
+    forms the features in FP32 and numpy in FP64; a feature that lands on the
+    other side of a BF16 rounding boundary moves that cell's output by a BF16
+    step, so the source-driven changes are compared to 2e-2 (L2, relative)."""
     m, p, g = _shell_run(titan, 0)
     g.go(5)
     st0 = g.download_state()
@@ -98,20 +100,24 @@ def test_closure_inside_the_step_equals_its_sources(titan):
     c.norm[:16] = np.concatenate([np.zeros(8), np.ones(8)])
     c.norm[16:] = 1e-3
     S = c.predict(st0, cc)
-    c.install(g)
-    g.go(1)
-    a = g.download_state()
+
+    def one_step(setup):
+        g.upload_state(st0)
+        g.dt, g.t = dt0, t0
+        setup()
+        g.go(1)
+        return g.download_state()
+
+    plain = one_step(lambda: None)
+    a = one_step(lambda: c.install(g))
     c.uninstall(g)
-    g.upload_state(st0)
-    g.dt, g.t = dt0, t0
-    g.set_sources(np.ascontiguousarray(S[1:]))
-    g.go(1)
-    b = g.download_state()
+    b = one_step(lambda: g.set_sources(np.ascontiguousarray(S[1:])))
     g.close()
-    assert not np.array_equal(a, st0)
-    for k in range(8):
-        d = np.abs(a[k] - b[k]).max() / max(np.abs(b[k]).max(), 1e-30)
-        assert d < 1e-8, (k, d)
+    for k in (1, 2, 3, 4):
+        da, db = a[k] - plain[k], b[k] - plain[k]
+        assert np.linalg.norm(db) > 0.0
+        rel = np.linalg.norm(da - db) / np.linalg.norm(db)
+        assert rel < 2e-2, (k, rel)
 
 
 def test_trained_closure_is_within_monte_carlo_noise(titan):

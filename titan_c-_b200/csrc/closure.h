@@ -21,13 +21,19 @@ namespace titan {
 
 constexpr int kIn = 8, kInPad = 16, kHid = 128, kOut = 5, kOutPad = 16, kTile = 128;
 constexpr int kModeRaw = 0, kModeSources = 1;
-// packed bf16 weights: W1 (128 x 16), W2..W4 (128 x 128), W5 (16 x 128)
-constexpr int kWPack = kHid * kInPad + 3 * kHid * kHid + kOutPad * kHid;
-constexpr int kBias = 4 * kHid + kOutPad;
+// Packed bf16 operands of the inference kernel, each an N x K block in the
+// canonical K-major layout, in this order:
+//   W1'  128 x 16: 0.5 W1 for k < 8, 0.5 b1 at k = 8 (the input tile carries 1 there)
+//   W2'..W4'  128 x 128: 0.5 W
+//   W5   16 x 128
+//   B2'..B4'  128 x 16: 0.5 b at k = 0 (multiplied by a constant tile with 1 at k = 0)
+//   B5   16 x 16: b5 at k = 0
+// The 0.5 makes the hidden-layer accumulator h = (z + b) / 2, so the epilogue
+// forms SiLU(z + b) = h (1 + tanh h) without a bias add or a scaling.
+constexpr int kWPack = kHid * kInPad + 3 * kHid * kHid + kOutPad * kHid + 3 * kHid * kInPad + kOutPad * kInPad;
 
 struct MlpNet {
-    const void* wpack;   // kWPack bf16, canonical K-major blocks (see closure_mlp.cu)
-    const float* bias;   // kBias
+    const void* wpack;   // kWPack bf16 (above)
     const float* fmean;  // kIn
     const float* fistd;  // kIn
     const float* oscale; // kOut
@@ -48,76 +54,78 @@ struct MlpArgs {
     int* error;
 };
 
-__host__ __device__ inline double log_nh_proxy(double n_inf, double lambda, double x, double r) {
-    double c = x / r;
-    c = c > 1.0 ? 1.0 : (c < -1.0 ? -1.0 : c);
-    const double th = acos(c);
-    double s = sin(th);
-    s = s < 1e-3 ? 1e-3 : s;
-    double e = -lambda * th / (r * s);
-    e = e < -30.0 ? -30.0 : e;
-    return log(n_inf) + e;
+// log of the cold-model neutral density n_inf exp(-lambda theta / (r sin theta)),
+// theta the angle from +x, in FP32 (features inside the inference kernel).
+__device__ __forceinline__ float log_nh_proxy_f(float n_inf, float lambda, float x, float r) {
+    const float c = fminf(fmaxf(x / r, -1.0f), 1.0f);
+    const float th = acosf(c);
+    const float s = fmaxf(sinf(th), 1e-3f);
+    return __logf(n_inf) + fmaxf(-lambda * th / (r * s), -30.0f);
 }
 
-// Sources from the network outputs of one cell (sources mode).
+// Sources from the network outputs of one cell (sources mode), formed in FP32
+// and stored as FP64: m_x, m_y, m_z in the frame e1 = V/|V| (radial when V =
+// 0), e2 = the inflow direction -x made orthogonal to e1, e3 = e1 x e2; E.
 __device__ inline void write_sources(const MlpArgs& a, int c, const float* y) {
     const int nc = a.ncell;
-    const double rho = a.state[c], vx = a.state[nc + c], vy = a.state[2 * nc + c], vz = a.state[3 * nc + c];
-    const double x = a.cc[c], yy = a.cc[nc + c], z = a.cc[2 * nc + c];
-    const double r = sqrt(x * x + yy * yy + z * z);
-    const double norm = rho * exp(log_nh_proxy(a.nH_inf, a.lambda, x, r));
-    const double vm = sqrt(vx * vx + vy * vy + vz * vz);
-    double e1[3], e2[3], e3[3];
-    if (vm > 0.0) {
-        e1[0] = vx / vm;
-        e1[1] = vy / vm;
-        e1[2] = vz / vm;
+    const float rho = (float)a.state[c], vx = (float)a.state[nc + c], vy = (float)a.state[2 * nc + c];
+    const float vz = (float)a.state[3 * nc + c];
+    const float x = (float)a.cc[c], yy = (float)a.cc[nc + c], z = (float)a.cc[2 * nc + c];
+    const float r = sqrtf(x * x + yy * yy + z * z);
+    const float norm = rho * __expf(log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, x, r));
+    const float vm = sqrtf(vx * vx + vy * vy + vz * vz);
+    float e1[3], e2[3], e3[3];
+    if (vm > 0.0f) {
+        const float iv = 1.0f / vm;
+        e1[0] = vx * iv;
+        e1[1] = vy * iv;
+        e1[2] = vz * iv;
     } else {
-        e1[0] = x / r;
-        e1[1] = yy / r;
-        e1[2] = z / r;
+        const float ir = 1.0f / r;
+        e1[0] = x * ir;
+        e1[1] = yy * ir;
+        e1[2] = z * ir;
     }
-    // inflow direction (-x) made orthogonal to e1
-    const double d = -e1[0];
-    e2[0] = -1.0 - d * e1[0];
+    const float d = -e1[0];
+    e2[0] = -1.0f - d * e1[0];
     e2[1] = -d * e1[1];
     e2[2] = -d * e1[2];
-    double n2 = sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
-    if (n2 < 1e-12) {  // flow along x: any perpendicular
-        e2[0] = 0.0;
-        e2[1] = 1.0;
-        e2[2] = 0.0;
-        n2 = 1.0;
+    float n2 = sqrtf(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+    if (n2 < 1e-6f) {  // flow along x: any perpendicular
+        e2[0] = 0.0f;
+        e2[1] = 1.0f;
+        e2[2] = 0.0f;
+        n2 = 1.0f;
     }
-    e2[0] /= n2;
-    e2[1] /= n2;
-    e2[2] /= n2;
+    const float in2 = 1.0f / n2;
+    e2[0] *= in2;
+    e2[1] *= in2;
+    e2[2] *= in2;
     e3[0] = e1[1] * e2[2] - e1[2] * e2[1];
     e3[1] = e1[2] * e2[0] - e1[0] * e2[2];
     e3[2] = e1[0] * e2[1] - e1[1] * e2[0];
-    const double s1 = norm * y[1] * a.net.oscale[1], s2 = norm * y[2] * a.net.oscale[2];
-    const double s3 = norm * y[3] * a.net.oscale[3];
-    a.src[c] = s1 * e1[0] + s2 * e2[0] + s3 * e3[0];
-    a.src[nc + c] = s1 * e1[1] + s2 * e2[1] + s3 * e3[1];
-    a.src[2 * nc + c] = s1 * e1[2] + s2 * e2[2] + s3 * e3[2];
-    a.src[3 * nc + c] = norm * y[4] * a.net.oscale[4];
+    const float s1 = norm * y[1] * a.net.oscale[1], s2 = norm * y[2] * a.net.oscale[2];
+    const float s3 = norm * y[3] * a.net.oscale[3];
+    a.src[c] = (double)(s1 * e1[0] + s2 * e2[0] + s3 * e3[0]);
+    a.src[nc + c] = (double)(s1 * e1[1] + s2 * e2[1] + s3 * e3[1]);
+    a.src[2 * nc + c] = (double)(s1 * e1[2] + s2 * e2[2] + s3 * e3[2]);
+    a.src[3 * nc + c] = (double)(norm * y[4] * a.net.oscale[4]);
 }
 
 cudaError_t mlp_prepare();  // once per process, before any launch (sets the shared-memory size)
-cudaError_t launch_mlp_forward(const MlpArgs& a, int mode, int grid, cudaStream_t s);
+// grid: one CTA per SM at most (sm_count), three tiles of 128 rows in flight per CTA
+cudaError_t launch_mlp_forward(const MlpArgs& a, int mode, int sm_count, cudaStream_t s);
 size_t mlp_forward_smem_bytes();
 
-// A network resident on the device (packed bf16 weights, biases, normalisation).
+// A network resident on the device (packed bf16 operands, normalisation).
 struct ClosureDev {
     float* params = nullptr;
     void* wpack = nullptr;
-    float* bias = nullptr;
     float* norm = nullptr;  // fmean[8], fistd[8], oscale[5]
     int* error = nullptr;
     MlpNet view() const {
         MlpNet n;
         n.wpack = wpack;
-        n.bias = bias;
         n.fmean = norm;
         n.fistd = norm + kIn;
         n.oscale = norm + 2 * kIn;

@@ -58,16 +58,14 @@ struct Buf {
     }
 };
 
-// Device copies of a network: packed bf16 weights, biases, normalisation.
+// Device copies of a network: FP32 masters, packed bf16 operands, normalisation.
 struct DevNet {
     float* params;
     void* wpack;
-    float* bias;
     float* norm;  // fmean[8], fistd[8], oscale[5]
     MlpNet view() const {
         MlpNet n;
         n.wpack = wpack;
-        n.bias = bias;
         n.fmean = norm;
         n.fistd = norm + kIn;
         n.oscale = norm + 2 * kIn;
@@ -78,17 +76,11 @@ struct DevNet {
 cudaError_t upload_net(Buf& b, const float* params, const float* norm, DevNet& d, cudaStream_t s) {
     d.params = b.get<float>(kNParam);
     d.wpack = b.get<uint16_t>(kWPack);
-    d.bias = b.get<float>(kBias);
     d.norm = b.get<float>(2 * kIn + kOut);
     if (b.err) return b.err;
     cudaError_t e = cudaMemcpyAsync(d.params, params, sizeof(float) * kNParam, cudaMemcpyHostToDevice, s);
     if (!e) e = cudaMemcpyAsync(d.norm, norm, sizeof(float) * (2 * kIn + kOut), cudaMemcpyHostToDevice, s);
     if (!e) e = launch_pack(d.params, d.wpack, s);
-    // biases in the kernel's order: b1..b4 (128 each) then b5 (16)
-    const int boff[5] = {ob1, ob2, ob3, ob4, ob5};
-    for (int l = 0; l < 5 && !e; ++l)
-        e = cudaMemcpyAsync(d.bias + l * kHid, d.params + boff[l], sizeof(float) * (l < 4 ? kHid : kOutPad),
-                            cudaMemcpyDeviceToDevice, s);
     return e;
 }
 
@@ -178,23 +170,18 @@ cudaError_t closure_create(const float* params, const float* norm, ClosureDev* d
     cudaError_t e = mlp_prepare();
     if (!e) e = cudaMalloc((void**)&d->params, sizeof(float) * kNParam);
     if (!e) e = cudaMalloc(&d->wpack, sizeof(uint16_t) * kWPack);
-    if (!e) e = cudaMalloc((void**)&d->bias, sizeof(float) * kBias);
     if (!e) e = cudaMalloc((void**)&d->norm, sizeof(float) * (2 * kIn + kOut));
     if (!e) e = cudaMalloc((void**)&d->error, sizeof(int));
     if (!e) e = cudaMemcpyAsync(d->params, params, sizeof(float) * kNParam, cudaMemcpyHostToDevice, s);
     if (!e) e = cudaMemcpyAsync(d->norm, norm, sizeof(float) * (2 * kIn + kOut), cudaMemcpyHostToDevice, s);
     if (!e) e = cudaMemsetAsync(d->error, 0, sizeof(int), s);
     if (!e) e = launch_pack(d->params, d->wpack, s);
-    const int boff[5] = {ob1, ob2, ob3, ob4, ob5};
-    for (int l = 0; l < 5 && !e; ++l)
-        e = cudaMemcpyAsync(d->bias + l * kHid, d->params + boff[l], sizeof(float) * (l < 4 ? kHid : kOutPad),
-                            cudaMemcpyDeviceToDevice, s);
     if (!e) e = cudaStreamSynchronize(s);
     return e;
 }
 
 void closure_destroy(ClosureDev* d) {
-    void* ps[] = {d->params, d->wpack, d->bias, d->norm, d->error};
+    void* ps[] = {d->params, d->wpack, d->norm, d->error};
     for (void* p : ps)
         if (p) cudaFree(p);
     *d = ClosureDev{};
@@ -225,11 +212,10 @@ int titan_mlp_forward(const float* params, const float* norm, const float* X, in
     a.x = dX;
     a.y = dY;
     a.error = derr;
-    const int ntiles = (int)((n + kTile - 1) / kTile);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (!e) e = launch_mlp_forward(a, kModeRaw, ntiles < sms ? ntiles : sms, s);
+    if (!e) e = launch_mlp_forward(a, kModeRaw, sms, s);
     int herr = 0;
     if (!e) e = cudaMemcpyAsync(Y, dY, sizeof(float) * n * kOut, cudaMemcpyDeviceToHost, s);
     if (!e) e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);

@@ -3,15 +3,24 @@
 // neutral solver would produce (titan_mc_sources), so the step can run without
 // re-tracing neutrals. BF16 weights and activations, FP32 accumulation.
 //
-// Inference (every step) runs on the 5th-generation tensor cores: one CTA owns
-// a tile of 128 cells; the layer weights stay in shared memory for the whole
-// kernel in the canonical K-major "interleave" layout (8x16-byte core
-// matrices); each layer is M=128 x N x K=16 tcgen05.mma instructions issued by
-// one thread with the accumulator in TMEM (128 fp32 columns); the four warps
-// read their 32 rows back with tcgen05.ld, apply bias and SiLU, and write the
-// next layer's BF16 activations into shared memory. Completion goes through an
-// mbarrier whose waits are bounded: a wait that runs out records an error and
-// the kernel stops issuing work, releases TMEM and returns.
+// Inference (every step) runs on the 5th-generation tensor cores. A CTA holds
+// the layer operands in shared memory for the whole kernel, in the canonical
+// K-major "interleave" layout (8x16-byte core matrices), and runs three
+// warpgroups, each with its own tile of 128 cells in flight and its own
+// 128-column TMEM accumulator: while one warpgroup turns its accumulator into
+// the next layer's BF16 activations (tcgen05.ld, SiLU), the tensor core works
+// on the other warpgroups' layers. Each layer is M=128 x N x K=16
+// tcgen05.mma instructions issued by one thread of the warpgroup; completion
+// goes through the warpgroup's mbarrier; waiting threads sleep (try_wait with
+// a suspend hint) and the waits are bounded: a wait that runs out records an
+// error and the warpgroup stops issuing work; the CTA releases TMEM and
+// returns.
+//
+// The hidden-layer operands carry a factor 0.5 and the biases (closure.h), so
+// the accumulator holds h = (z + b) / 2 and the epilogue turns a pair of
+// columns into SiLU(z + b) = h (1 + tanh h) with one conversion to bf16x2,
+// one tanh.approx.bf16x2 and one bf16x2 FMA. Features and sources are formed
+// in FP32 (the network itself is BF16).
 //
 // Training uses the same networks through mma.sync tiles (closure_train.cu).
 #include <cuda_bf16.h>
@@ -64,28 +73,6 @@ __device__ __forceinline__ void commit(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
 }
 
-// Bounded wait on an mbarrier phase (non-blocking test_wait polled against the
-// global timer: at most ~1 s and 2^26 polls); false when it ran out.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-    uint64_t t0;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    for (int it = 0; it < (1 << 26); ++it) {
-        uint32_t done = 0;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(mbar), "r"(phase)
-            : "memory");
-        if (done) return true;
-        if ((it & 255) == 255) {
-            uint64_t t;
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-            if (t - t0 > 1000000000ull) return false;
-        }
-    }
-    return false;
-}
-
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
     uint32_t r[32];
     asm volatile(
@@ -116,112 +103,155 @@ __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::be
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// SiLU of two values in bf16: z * (1 + tanh(z / 2)) / 2, one packed MUFU op.
-__device__ __forceinline__ uint32_t silu_bf16x2(float a, float b) {
-    __nv_bfloat162 z = __floats2bfloat162_rn(a, b);
-    const __nv_bfloat162 half = __floats2bfloat162_rn(0.5f, 0.5f);
-    __nv_bfloat162 h = __hmul2(z, half);
-    uint32_t hu = *reinterpret_cast<uint32_t*>(&h), tu;
-    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(tu) : "r"(hu));
-    __nv_bfloat162 t = *reinterpret_cast<__nv_bfloat162*>(&tu);
-    __nv_bfloat162 s = __hfma2(t, half, half);
-    __nv_bfloat162 y = __hmul2(z, s);
-    return *reinterpret_cast<uint32_t*>(&y);
+// SiLU of a pair of columns from the accumulator h = (z + b) / 2 (FP32):
+// h (1 + tanh h) in bf16x2 — one conversion, one tanh, one FMA.
+__device__ __forceinline__ uint32_t silu_pair(float h0, float h1) {
+    uint32_t hb, t, y;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hb) : "f"(h1), "f"(h0));
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(hb));
+    asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(hb), "r"(t));
+    return y;
 }
 
-// Shared memory of one CTA (bytes).
+constexpr int kGroups = 3;  // warpgroups per CTA, one tile in flight each
+
+// Shared memory of one CTA. The operand blocks (w1 .. bw5) are contiguous in
+// the order of the packed array (closure.h).
 struct alignas(128) Smem {
-    __nv_bfloat16 w1[kHid * kInPad];    // layer 1, N=128 x K=16
-    __nv_bfloat16 w[3][kHid * kHid];    // layers 2..4, N=128 x K=128
-    __nv_bfloat16 w5[kOutPad * kHid];   // layer 5, N=16 x K=128
-    __nv_bfloat16 x[kTile * kInPad];    // input tile, M=128 x K=16
-    __nv_bfloat16 a[kTile * kHid];      // activations, M=128 x K=128
-    float bias[4 * kHid + kOutPad];
+    __nv_bfloat16 w1[kHid * kInPad];           // W1'  N=128 x K=16
+    __nv_bfloat16 w[3][kHid * kHid];           // W2'..W4'  N=128 x K=128
+    __nv_bfloat16 w5[kOutPad * kHid];          // W5   N=16 x K=128
+    __nv_bfloat16 bw[3][kHid * kInPad];        // B2'..B4'  N=128 x K=16
+    __nv_bfloat16 bw5[kOutPad * kInPad];       // B5   N=16 x K=16
+    __nv_bfloat16 ones[kTile * kInPad];        // M=128 x K=16, 1 at k = 0
+    __nv_bfloat16 a[kGroups][kTile * kHid];    // activations M=128 x K=128; the input
+                                               // tile (K=16) aliases its first 4 KB
     float fmean[kIn], fistd[kIn];
-    uint64_t mbar;
+    uint64_t mbar[kGroups];
     uint32_t tmem;
-    int abort;
+    int abort[kGroups];  // written by the group's own threads before its barrier, read after it
 };
 
-// Input features of one cell from its state and centre (see closure.h).
+// Input features of one cell from its state and centre (closure.h), in FP32.
 __device__ __forceinline__ void cell_features(const MlpArgs& a, int c, float* f) {
     const int nc = a.ncell;
-    const double rho = a.state[c], vx = a.state[nc + c], vy = a.state[2 * nc + c], vz = a.state[3 * nc + c];
-    const double p = a.state[4 * nc + c];
-    const double x = a.cc[c], y = a.cc[nc + c], z = a.cc[2 * nc + c];
-    const double r = sqrt(x * x + y * y + z * z);
-    const double ur = (vx * x + vy * y + vz * z) / r;
-    const double ut2 = fmax(vx * vx + vy * vy + vz * vz - ur * ur, 0.0);
-    const double vmag = sqrt(vx * vx + vy * vy + vz * vz);
-    f[0] = (float)log(fmax(rho, 1e-30));
-    f[1] = (float)ur;
-    f[2] = (float)sqrt(ut2);
-    f[3] = (float)log(fmax(p / rho, 1e-30));
-    f[4] = (float)log(r);
-    f[5] = (float)acos(fmin(fmax(x / r, -1.0), 1.0));
-    f[6] = (float)(vmag > 0.0 ? -vx / vmag : 0.0);
-    f[7] = (float)log_nh_proxy(a.nH_inf, a.lambda, x, r);
+    const float rho = (float)a.state[c], vx = (float)a.state[nc + c], vy = (float)a.state[2 * nc + c];
+    const float vz = (float)a.state[3 * nc + c], p = (float)a.state[4 * nc + c];
+    const float x = (float)a.cc[c], y = (float)a.cc[nc + c], z = (float)a.cc[2 * nc + c];
+    const float r = sqrtf(x * x + y * y + z * z);
+    const float ir = 1.0f / r;
+    const float ur = (vx * x + vy * y + vz * z) * ir;
+    const float v2 = vx * vx + vy * vy + vz * vz;
+    const float vmag = sqrtf(v2);
+    f[0] = __logf(fmaxf(rho, 1e-30f));
+    f[1] = ur;
+    f[2] = sqrtf(fmaxf(v2 - ur * ur, 0.0f));
+    f[3] = __logf(fmaxf(p / rho, 1e-30f));
+    f[4] = __logf(r);
+    f[5] = acosf(fminf(fmaxf(x * ir, -1.0f), 1.0f));
+    f[6] = vmag > 0.0f ? -vx / vmag : 0.0f;
+    f[7] = log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, x, r);
+}
+
+// Named barrier of one warpgroup (ids 1..kGroups; 0 is __syncthreads).
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory");
+}
+
+// Sleeping wait on an mbarrier phase: try_wait with a suspend-time hint of
+// 100 us per call, at most ~1 s in total (globaltimer) and 2^14 calls; false
+// when it ran out. Waiting threads do not take issue slots from the others.
+__device__ __forceinline__ bool mbar_sleep_wait(uint32_t mbar, uint32_t phase) {
+    uint64_t t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (int it = 0; it < (1 << 14); ++it) {
+        uint32_t done = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase), "r"(100000u)
+            : "memory");
+        if (done) return true;
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > 1000000000ull) return false;
+    }
+    return false;
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(128, 1) mlp_forward_tc(MlpArgs args) {
+__global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = tid >> 7;          // warpgroup
+    const int row = tid & 127;       // this thread's row of the group's tile
+    const bool leader = row == 0;    // issues the group's MMAs
 
-    // weights (pre-packed in the canonical layout), biases, normalisation
+    // operands (pre-packed in the canonical layout), the constant tile, normalisation
     {
         const uint4* src = reinterpret_cast<const uint4*>(args.net.wpack);
         uint4* dst = reinterpret_cast<uint4*>(S.w1);
-        constexpr int n16 = (kHid * kInPad + 3 * kHid * kHid + kOutPad * kHid) * 2 / 16;
+        constexpr int n16 = kWPack * 2 / 16;
         for (int i = tid; i < n16; i += blockDim.x) dst[i] = src[i];
-        for (int i = tid; i < 4 * kHid + kOutPad; i += blockDim.x) S.bias[i] = args.net.bias[i];
+        uint4* on = reinterpret_cast<uint4*>(S.ones);
+        const uint32_t one_lo = 0x3F80u;  // bf16 1.0 in the low half (k = 0)
+        for (int r = tid; r < kTile; r += blockDim.x) {
+            on[canon_index(r, 0, kTile) / 8] = make_uint4(one_lo, 0u, 0u, 0u);
+            on[canon_index(r, 8, kTile) / 8] = make_uint4(0u, 0u, 0u, 0u);
+        }
         if (tid < kIn) {
             S.fmean[tid] = args.net.fmean[tid];
             S.fistd[tid] = args.net.fistd[tid];
         }
     }
-    const uint32_t mbar = smem_u32(&S.mbar);
     if (tid == 0) {
-        S.abort = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1));
+        for (int i = 0; i < kGroups; ++i) S.abort[i] = 0;
+        for (int i = 0; i < kGroups; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.mbar[i])), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    constexpr uint32_t kCols = kGroups <= 2 ? 256u : 512u;  // power of two >= 128 x groups
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
-                     "r"(kHid));
+                     "r"(kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
+    fence_async_smem();
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = S.tmem;
-    const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
+    // this group's accumulator: columns [128 g, 128 g + 128); this warp's 32 lanes
+    const uint32_t tmem = S.tmem + (uint32_t)(g * kHid);
+    const uint32_t tmem_row = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t mbar = smem_u32(&S.mbar[g]);
     uint32_t phase = 0;
 
     const uint32_t idesc_h = instr_desc(kTile, kHid);
     const uint32_t idesc_o = instr_desc(kTile, kOutPad);
-    const uint32_t x_base = smem_u32(S.x), a_base = smem_u32(S.a);
-    const uint32_t w1_base = smem_u32(S.w1), w5_base = smem_u32(S.w5);
+    const uint32_t a_base = smem_u32(S.a[g]), ones_base = smem_u32(S.ones);
+    const uint32_t w1_base = smem_u32(S.w1), w5_base = smem_u32(S.w5), bw5_base = smem_u32(S.bw5);
     const int ntiles = (args.n + kTile - 1) / kTile;
+    uint4* ar = reinterpret_cast<uint4*>(S.a[g]);
 
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int row = tile * kTile + tid;
-        const bool valid = row < args.n;
-        // ---- input features -> x tile (bf16, K padded to 16 with zeros)
+    for (int tile = blockIdx.x + g * gridDim.x; tile < ntiles; tile += kGroups * gridDim.x) {
+        const int cell = tile * kTile + row;
+        const bool valid = cell < args.n;
+        // ---- input features -> input tile (bf16; k = 8 carries 1 for the bias, 9..15 zero)
         float f[kIn];
         if (MODE == kModeRaw) {
 #pragma unroll
-            for (int k = 0; k < kIn; ++k) f[k] = valid ? args.x[(size_t)row * kIn + k] : 0.0f;
+            for (int k = 0; k < kIn; ++k) f[k] = valid ? args.x[(size_t)cell * kIn + k] : 0.0f;
         } else {
             if (valid)
-                cell_features(args, row, f);
+                cell_features(args, cell, f);
             else
 #pragma unroll
                 for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
         }
         {
-            uint32_t packed[kInPad / 2];
+            uint32_t packed[kIn / 2];
 #pragma unroll
             for (int k = 0; k < kIn; k += 2) {
                 const float f0 = valid ? (f[k] - S.fmean[k]) * S.fistd[k] : 0.0f;
@@ -229,29 +259,24 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_tc(MlpArgs args) {
                 __nv_bfloat162 v = __floats2bfloat162_rn(f0, f1);
                 packed[k / 2] = *reinterpret_cast<uint32_t*>(&v);
             }
-#pragma unroll
-            for (int k = kIn; k < kInPad; k += 2) packed[k / 2] = 0u;
-            uint4* xr = reinterpret_cast<uint4*>(S.x);
-            xr[canon_index(tid, 0, kTile) / 8] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-            xr[canon_index(tid, 8, kTile) / 8] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+            ar[canon_index(row, 0, kTile) / 8] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            ar[canon_index(row, 8, kTile) / 8] = make_uint4(0x3F80u, 0u, 0u, 0u);
         }
         fence_async_smem();
         fence_before();
-        __syncthreads();
+        group_sync(g);
         fence_after();
-        if (S.abort) break;
-        // ---- layer 1: D = X (128x16) . W1^T
-        if (tid == 0) {
-            mma_bf16(tmem, smem_desc(x_base, kTile * 16, 128), smem_desc(w1_base, kHid * 16, 128), idesc_h, 0);
+        if (S.abort[g]) break;
+        // ---- layer 1: H = X' (128x16) . W1'^T  (bias through the 1 at k = 8)
+        if (leader) {
+            mma_bf16(tmem, smem_desc(a_base, kTile * 16, 128), smem_desc(w1_base, kHid * 16, 128), idesc_h, 0);
             commit(mbar);
         }
         for (int layer = 0; layer < 4; ++layer) {
-            if (!mbar_wait(mbar, phase)) S.abort = 1;
+            if (!mbar_sleep_wait(mbar, phase)) S.abort[g] = 1;
             phase ^= 1;
             fence_after();
-            // bias + SiLU -> next activations (this thread's row)
-            const float* b = S.bias + layer * kHid;
-            uint4* ar = reinterpret_cast<uint4*>(S.a);
+            // h -> SiLU -> next activations (this thread's row)
 #pragma unroll
             for (int c0 = 0; c0 < kHid; c0 += 32) {
                 float v[32];
@@ -261,59 +286,60 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_tc(MlpArgs args) {
                 for (int j = 0; j < 32; j += 8) {
                     uint32_t q[4];
 #pragma unroll
-                    for (int e = 0; e < 4; ++e)
-                        q[e] = silu_bf16x2(v[j + 2 * e] + b[c0 + j + 2 * e], v[j + 2 * e + 1] + b[c0 + j + 2 * e + 1]);
-                    ar[canon_index(tid, c0 + j, kTile) / 8] = make_uint4(q[0], q[1], q[2], q[3]);
+                    for (int e = 0; e < 4; ++e) q[e] = silu_pair(v[j + 2 * e], v[j + 2 * e + 1]);
+                    ar[canon_index(row, c0 + j, kTile) / 8] = make_uint4(q[0], q[1], q[2], q[3]);
                 }
             }
             fence_async_smem();
             fence_before();
-            __syncthreads();
+            group_sync(g);
             fence_after();
-            if (S.abort) break;
-            if (tid == 0) {
+            if (S.abort[g]) break;
+            if (leader) {
                 if (layer < 3) {
                     const uint32_t wb = smem_u32(S.w[layer]);
 #pragma unroll
                     for (int s = 0; s < kHid / 16; ++s)
                         mma_bf16(tmem, smem_desc(a_base + s * 2 * kTile * 16, kTile * 16, 128),
                                  smem_desc(wb + s * 2 * kHid * 16, kHid * 16, 128), idesc_h, s > 0);
+                    mma_bf16(tmem, smem_desc(ones_base, kTile * 16, 128),
+                             smem_desc(smem_u32(S.bw[layer]), kHid * 16, 128), idesc_h, 1);
                 } else {
 #pragma unroll
                     for (int s = 0; s < kHid / 16; ++s)
                         mma_bf16(tmem, smem_desc(a_base + s * 2 * kTile * 16, kTile * 16, 128),
                                  smem_desc(w5_base + s * 2 * kOutPad * 16, kOutPad * 16, 128), idesc_o, s > 0);
+                    mma_bf16(tmem, smem_desc(ones_base, kTile * 16, 128), smem_desc(bw5_base, kOutPad * 16, 128),
+                             idesc_o, 1);
                 }
                 commit(mbar);
             }
         }
-        if (S.abort) break;
-        // ---- output layer
-        if (!mbar_wait(mbar, phase)) S.abort = 1;
+        if (S.abort[g]) break;
+        // ---- output layer (bias included)
+        if (!mbar_sleep_wait(mbar, phase)) S.abort[g] = 1;
         phase ^= 1;
         fence_after();
         float y[16];
         tmem_ld16(tmem_row, y);
         tmem_wait_ld();
-#pragma unroll
-        for (int k = 0; k < kOutPad; ++k) y[k] += S.bias[4 * kHid + k];
         if (valid) {
             if (MODE == kModeRaw) {
 #pragma unroll
-                for (int k = 0; k < kOut; ++k) args.y[(size_t)row * kOut + k] = y[k];
+                for (int k = 0; k < kOut; ++k) args.y[(size_t)cell * kOut + k] = y[k];
             } else {
-                write_sources(args, row, y);
+                write_sources(args, cell, y);
             }
         }
         fence_before();
-        __syncthreads();
+        group_sync(g);
         fence_after();
     }
-    if (S.abort && tid == 0) atomicExch(args.error, 1);
+    if (S.abort[g] && row == 0) atomicExch(args.error, 1);
     fence_before();
     __syncthreads();
     fence_after();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kHid));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S.tmem), "r"(kCols));
 }
 
 }  // namespace mlp
@@ -327,12 +353,16 @@ cudaError_t mlp_prepare() {
     return e;
 }
 
-cudaError_t launch_mlp_forward(const MlpArgs& a, int mode, int grid, cudaStream_t s) {
+cudaError_t launch_mlp_forward(const MlpArgs& a, int mode, int sm_count, cudaStream_t s) {
     const size_t smem = sizeof(mlp::Smem) + 1024;
+    const int ntiles = (a.n + kTile - 1) / kTile;
+    const int want = (ntiles + mlp::kGroups - 1) / mlp::kGroups;
+    const int grid = want < sm_count ? want : sm_count;
+    if (grid <= 0) return cudaSuccess;
     if (mode == kModeRaw)
-        mlp::mlp_forward_tc<kModeRaw><<<grid, 128, smem, s>>>(a);
+        mlp::mlp_forward_tc<kModeRaw><<<grid, 128 * mlp::kGroups, smem, s>>>(a);
     else
-        mlp::mlp_forward_tc<kModeSources><<<grid, 128, smem, s>>>(a);
+        mlp::mlp_forward_tc<kModeSources><<<grid, 128 * mlp::kGroups, smem, s>>>(a);
     return cudaGetLastError();
 }
 

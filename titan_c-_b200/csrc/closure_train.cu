@@ -198,34 +198,62 @@ __global__ void input_kernel(const float* X, const float* mean, const float* ist
     X0[i] = __float2bfloat16(k < kIn ? (X[(size_t)r * kIn + k] - mean[k]) * istd[k] : 0.0f);
 }
 
-// Canonical K-major bf16 pack of the FP32 masters for the tcgen05 kernel.
+// Canonical K-major bf16 pack of the FP32 masters for the tcgen05 kernel
+// (the operand list of closure.h): element j of an R x K block is row
+// n = (j / 64 % (R / 8)) * 8 + j % 64 / 8, column k = (j / 64 / (R / 8)) * 8 + j % 8.
 __global__ void pack_kernel(const float* P, __nv_bfloat16* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kWPack) return;
-    // offsets of the layers in the master vector
-    const int oW1 = 0, oW2 = kInPad * kHid + kHid, oW3 = oW2 + kHid * kHid + kHid, oW4 = oW3 + kHid * kHid + kHid;
-    const int oW5 = oW4 + kHid * kHid + kHid;
-    int base, out_dim, j;
-    if (i < kHid * kInPad) {
-        j = i;
-        base = oW1;
-        out_dim = kHid;
-    } else if (i < kHid * kInPad + 3 * kHid * kHid) {
-        const int t = (i - kHid * kInPad) / (kHid * kHid);
-        j = (i - kHid * kInPad) % (kHid * kHid);
-        base = t == 0 ? oW2 : (t == 1 ? oW3 : oW4);
-        out_dim = kHid;
+    // offsets of the layers in the master vector [W1 | b1 | W2 | b2 | ... | W5 | b5]
+    const int oW1 = 0, ob1 = kInPad * kHid;
+    const int oW2 = ob1 + kHid, ob2 = oW2 + kHid * kHid;
+    const int oW3 = ob2 + kHid, ob3 = oW3 + kHid * kHid;
+    const int oW4 = ob3 + kHid, ob4 = oW4 + kHid * kHid;
+    const int oW5 = ob4 + kHid, ob5 = oW5 + kHid * kOutPad;
+    constexpr int sW1 = kHid * kInPad, sW = kHid * kHid, sW5 = kOutPad * kHid, sB = kHid * kInPad;
+    int j = i, R, region;
+    if (j < sW1) {
+        region = 0, R = kHid;
+    } else if ((j -= sW1) < 3 * sW) {
+        region = 1 + j / sW, R = kHid, j %= sW;
+    } else if ((j -= 3 * sW) < sW5) {
+        region = 4, R = kOutPad;
+    } else if ((j -= sW5) < 3 * sB) {
+        region = 5 + j / sB, R = kHid, j %= sB;
     } else {
-        j = i - (kHid * kInPad + 3 * kHid * kHid);
-        base = oW5;
-        out_dim = kOutPad;
+        j -= 3 * sB;
+        region = 8, R = kOutPad;
     }
-    // j is the canonical index of (n = out, k = in) in an out_dim x in_dim block
     const int core = j / 64, within = j % 64;
-    const int rgroups = out_dim / 8;
-    const int kc = core / rgroups, rg = core % rgroups;
-    const int n = rg * 8 + within / 8, k = kc * 8 + within % 8;
-    out[i] = __float2bfloat16(P[base + (size_t)k * out_dim + n]);
+    const int rgroups = R / 8;
+    const int n = (core % rgroups) * 8 + within / 8, k = (core / rgroups) * 8 + within % 8;
+    float v = 0.0f;
+    switch (region) {
+        case 0:  // W1' (K = 16): 0.5 W1 for k < 8, 0.5 b1 at k = 8
+            v = k < kIn ? 0.5f * P[oW1 + k * kHid + n] : (k == kIn ? 0.5f * P[ob1 + n] : 0.0f);
+            break;
+        case 1:
+        case 2:
+        case 3: {  // W2'..W4'
+            const int oW = region == 1 ? oW2 : (region == 2 ? oW3 : oW4);
+            v = 0.5f * P[oW + k * kHid + n];
+            break;
+        }
+        case 4:  // W5 (N = 16)
+            v = P[oW5 + k * kOutPad + n];
+            break;
+        case 5:
+        case 6:
+        case 7: {  // B2'..B4'
+            const int ob = region == 5 ? ob2 : (region == 6 ? ob3 : ob4);
+            v = k == 0 ? 0.5f * P[ob + n] : 0.0f;
+            break;
+        }
+        default:  // B5
+            v = k == 0 ? P[ob5 + n] : 0.0f;
+            break;
+    }
+    out[i] = __float2bfloat16(v);
 }
 
 }  // namespace train

@@ -188,10 +188,7 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
         ma.nH_inf = ctx->closure_ninf;
         ma.lambda = ctx->closure_lambda;
         ma.error = ctx->closure.error;
-        const int ntiles = (int)((ctx->ncell + kTile - 1) / kTile);
-        e = timed(ctx, "closure_mlp", [&] {
-            return launch_mlp_forward(ma, kModeSources, ntiles < ctx->sm_count ? ntiles : ctx->sm_count, ctx->stream);
-        });
+        e = timed(ctx, "closure_mlp", [&] { return launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->stream); });
         if (e) return e;
     }
     FaceArgs fa;

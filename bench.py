@@ -66,9 +66,10 @@ def peak_tflops():
         return 1400.0, "fallback (sustained)"
 
 
-# DRAM bytes (read + write) per launch from one ncu capture of the kernel on
-# this workload: profiles/face_flux_shell.md has the command and the figures.
-TRAFFIC = {}
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel on the
+# 6x64x64x40 shell, scaled by faces (x2.25) to the 6x96x96x40 workload:
+# profiles/face_flux_shell.md has the command and the figures.
+TRAFFIC = {("face_flux_fp64", 2211840): 1264.7e6, ("face_flux_fp32", 2211840): 777.1e6}
 
 
 class ClockSampler:
@@ -322,7 +323,8 @@ def run_ours(args, rank, world):
                 "h2d_bytes_per_step": 8 * ns * C, "d2h_bytes_per_step": 8 * ns * C},
         "gpu_launches": args.steps * kernels_per_step,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "kernel": flux_name, "peak_source": src,
+                     "traffic": traffic, "traffic_source": "ncu capture at 6x64x64x40 scaled by faces" if traffic else None,
+                     "kernel": flux_name, "peak_source": src,
                      "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": k_avg,
                      "kernel_share": k_ms / total_k},
         "kernel_ms_per_step": {k: v[0] / v[1] for k, v in kt.items()},

@@ -69,7 +69,7 @@ def peak_tflops():
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel on the
 # 6x64x64x40 shell, scaled by faces (x2.25) to the 6x96x96x40 workload:
 # profiles/face_flux_shell.md has the command and the figures.
-TRAFFIC = {("face_flux_fp64", 2211840): 1264.7e6, ("face_flux_fp32", 2211840): 777.1e6}
+TRAFFIC = {("face_flux_fp64", 2211840): 1264.7e6}
 
 
 class ClockSampler:
@@ -164,26 +164,67 @@ def rel_errors(a, b):
 
 
 def error_study(pkg, m, p, st, tuning, closure, checkpoints=(100, 1000)):
-    """Mixed step (FP32 flux) against the all-FP64 step from the same state:
-    the states at each checkpoint, with the closure installed in both or in neither."""
-    res = {}
-    for tag, net in (("with_mlp_sources", closure), ("no_sources", None)):
-        states = {}
-        for flux in (64, 32):
-            prm = dict(p)
-            prm["flux_precision"] = flux
-            g = pkg.PlasmaStep(m, prm)
-            g.upload_state(st)
-            g.set_tuning(tuning["face_variant"], tuning["cell_variant"])
-            if net is not None:
-                net.install(g)
-            done, states[flux] = 0, {}
-            for c in checkpoints:
-                g.go(c - done)
-                done = c
-                states[flux][c] = g.download_state()
-            g.close()
-        res[tag] = {str(c): rel_errors(states[32][c], states[64][c]) for c in checkpoints}
+    """Error of the mixed step (FP32 Riemann arithmetic) against the all-FP64 step.
+
+    * over_run: both from the same initial state, states compared at each
+      checkpoint, with the closure installed in both or in neither;
+    * fp64_sensitivity: the FP64 step against itself from an initial state
+      perturbed by 1e-7 relative (seeded) — how far an FP32-sized difference
+      carries in this flow by the same checkpoints (shocks and floors make the
+      run-to-run spread itself of order 1e-4 .. 1e-3 after ~150 steps);
+    * one_step: one step of each from identical states taken along the FP64
+      run, |mixed - FP64| relative to |FP64 step change| (the precision the
+      flux arithmetic itself delivers per step)."""
+    res = {"over_run": {}}
+
+    def make(flux, net=None):
+        prm = dict(p)
+        prm["flux_precision"] = flux
+        g = pkg.PlasmaStep(m, prm)
+        g.set_tuning(tuning["face_variant"], tuning["cell_variant"])
+        if net is not None:
+            net.install(g)
+        return g
+
+    def trajectory(flux, s0, net=None):
+        g = make(flux, net)
+        g.upload_state(s0)
+        done, out = 0, {}
+        for c in checkpoints:
+            g.go(c - done)
+            done = c
+            out[c] = (g.download_state(), g.dt, g.t)
+        g.close()
+        return out
+
+    ref = trajectory(64, st)
+    for tag, net in (("no_sources", None), ("with_mlp_sources", closure)):
+        r64 = ref if net is None else trajectory(64, st, net)
+        r32 = trajectory(32, st, net)
+        res["over_run"][tag] = {str(c): rel_errors(r32[c][0], r64[c][0]) for c in checkpoints}
+    rng = np.random.default_rng(1)
+    pert = trajectory(64, st * (1.0 + 1e-7 * rng.standard_normal(st.shape)))
+    res["fp64_sensitivity"] = {"perturbation": 1e-7,
+                               **{str(c): rel_errors(pert[c][0], ref[c][0]) for c in checkpoints}}
+    g64, g32 = make(64), make(32)
+    res["one_step"] = {}
+    for c in (0,) + tuple(checkpoints):
+        s0, dt, t = (st, 1e-5, 0.0) if c == 0 else ref[c]
+        outs = []
+        for g in (g64, g32):
+            g.upload_state(s0)
+            g.dt, g.t = dt, t
+            g.go(1)
+            outs.append(g.download_state())
+        d64 = outs[0] - s0
+        e = {}
+        for k, i in (("rho", 0), ("p", 4)):
+            e[k] = float(np.abs(outs[1][i] - outs[0][i]).sum() / max(np.abs(d64[i]).sum(), 1e-300))
+        db = np.linalg.norm(outs[1][5:8] - outs[0][5:8], axis=0).sum()
+        e["B"] = float(db / max(np.linalg.norm(d64[5:8], axis=0).sum(), 1e-300))
+        res["one_step"][f"from_step_{c}"] = e
+    g64.close()
+    g32.close()
     return res
 
 
@@ -195,7 +236,7 @@ def face_flux_bytes(m, move: bool, fp32: bool) -> float:
     N = m["node_xyz"].shape[0]
     per_face = 8 + 2 + 3 * 8 + 8 + 8      # c0,c1 | type,method | normal | area | half distance
     state = 8 * 8 * C                       # 8 FP64 primitives per cell, read once
-    out = (9 * (4 if fp32 else 8)) * F      # 9 fluxes (x area) per face
+    out = (9 * 8) * F                       # 9 fluxes (x area) per face, FP64 records in every mode
     # moving mesh: face node ids + node coordinates of both layers replace the
     # stored normal / area / half distance, and cell centres are read instead
     ale = (16 * F + 2 * 24 * N + 24 * C - 40 * F) if move else 0

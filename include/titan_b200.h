@@ -91,7 +91,9 @@ typedef struct titan_params {
     int32_t nh;            /* frozen neutral fluids for the Bera sources (0..4) */
     int32_t TS_hard;       /* left_ydar on TS faces */
     int32_t contact_hard;  /* face speed = contact speed on HP faces */
-    int32_t flux_precision;/* 64: all-FP64; 32: FP32 Riemann flux, FP64 accumulation/update/dt */
+    int32_t flux_precision;/* 64: all-FP64; 32: FP32 Riemann-solver arithmetic (faces wholly in one
+                              side's wave region take that side's FP64 flux), FP64 flux records,
+                              accumulation, update, pressure recovery and dt */
     int32_t tvd;           /* Phys_param::TVD: second-order reconstruction on interior faces
                               (Setka_gran_snos.cpp:188-735; neighbours from Setka::Init_TVD) */
     int32_t snos_on_hp;    /* Phys_param::Snos_on_HP: second order on HP faces too */

@@ -1,5 +1,7 @@
 // Launch-shape dispatch of the face-flux kernel, shared by the translation
-// units that instantiate it (FP64 / FP32 flux, first / second order).
+// units that instantiate it (FP64 / FP32 Riemann arithmetic, first / second
+// order). The flux records are FP64 in every mode: the flux times area is
+// part of the conservative accumulation.
 #pragma once
 #include "launch.h"
 #include "step_kernels.cuh"
@@ -12,7 +14,7 @@ static cudaError_t face_flux_variant(const FaceArgs& a, int v, cudaStream_t s) {
 #define TITAN_FACE_CASE(i)                                                                              \
     case i: {                                                                                         \
         constexpr FaceVariant fv = kFaceVariant[i];                                                   \
-        face_flux_kernel<R, R, NK, MOVE, fv.block, fv.min_blocks, TVD>                                \
+        face_flux_kernel<R, double, NK, MOVE, fv.block, fv.min_blocks, TVD>                           \
             <<<blocks_for(a.M.nface, fv.block), fv.block, 0, s>>>(a);                                 \
         break;                                                                                        \
     }

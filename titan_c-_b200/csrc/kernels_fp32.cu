@@ -1,8 +1,10 @@
-// FP32-flux translation unit: the Riemann flux in single precision (the
-// mixed-precision step keeps reconstruction, accumulation, update and the CFL
-// reduction in FP64). Contraction to FMA is allowed here, and single-precision
-// division and square root use the fast approximate forms (-prec-div=false,
-// -prec-sqrt=false): the flux error budget is 1e-4, far above their few ulp.
+// FP32-flux translation unit: the Riemann solver's arithmetic in single
+// precision. Reconstruction, the flux records (flux x area, FP64), the
+// accumulation, update and CFL reduction stay in FP64, and faces that lie
+// wholly in one side's wave region (supersonic faces) take their flux from the
+// FP64 physical flux of that side (upwind_flux_fp64). Contraction to FMA is
+// allowed here, and single-precision division and square root use the fast
+// approximate forms (-prec-div=false, -prec-sqrt=false).
 #include "face_dispatch.cuh"
 
 namespace titan {

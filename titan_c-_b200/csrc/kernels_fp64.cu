@@ -52,19 +52,12 @@ static cudaError_t cell_update_variant(const CellArgs& a, int src, int v, cudaSt
     return cudaGetLastError();
 }
 
-template <typename FT>
-static cudaError_t cell_update_ft(const CellArgs& a, int nk, bool move, int src, int v, cudaStream_t s) {
-    if (nk == 0 && !move) return cell_update_variant<FT, 0, false>(a, src, v, s);
-    if (nk == 0 && move) return cell_update_variant<FT, 0, true>(a, src, v, s);
-    if (nk == 2 && !move) return cell_update_variant<FT, 2, false>(a, src, v, s);
-    if (nk == 2 && move) return cell_update_variant<FT, 2, true>(a, src, v, s);
+cudaError_t launch_cell_update(const CellArgs& a, int nk, bool move, int src, int variant, cudaStream_t s) {
+    if (nk == 0 && !move) return cell_update_variant<double, 0, false>(a, src, variant, s);
+    if (nk == 0 && move) return cell_update_variant<double, 0, true>(a, src, variant, s);
+    if (nk == 2 && !move) return cell_update_variant<double, 2, false>(a, src, variant, s);
+    if (nk == 2 && move) return cell_update_variant<double, 2, true>(a, src, variant, s);
     return cudaErrorInvalidValue;
-}
-
-cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, int variant,
-                               cudaStream_t s) {
-    return flux_fp32 ? cell_update_ft<float>(a, nk, move, src, variant, s)
-                     : cell_update_ft<double>(a, nk, move, src, variant, s);
 }
 
 cudaError_t launch_gather(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s) {

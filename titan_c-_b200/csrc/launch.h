@@ -33,9 +33,8 @@ cudaError_t launch_face_flux_fp32(const FaceArgs& a, int nk, bool move, int vari
 cudaError_t launch_face_flux_tvd_fp64(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s);
 cudaError_t launch_face_flux_tvd_fp32(const FaceArgs& a, int nk, bool move, int variant, cudaStream_t s);
 cudaError_t launch_tvd_neighbours(const MeshView& M, const Layer& L, int* aa, int* bb, cudaStream_t s);
-// flux_fp32: the flux buffer holds floats
-cudaError_t launch_cell_update(const CellArgs& a, bool flux_fp32, int nk, bool move, int src, int variant,
-                               cudaStream_t s);
+// the flux buffer holds FP64 records in every mode
+cudaError_t launch_cell_update(const CellArgs& a, int nk, bool move, int src, int variant, cudaStream_t s);
 cudaError_t launch_gather(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s);
 cudaError_t launch_scatter(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s);
 cudaError_t launch_riemann_batch_fp64(long long n, const signed char* ns, const double* nrm, const double* w,

@@ -171,7 +171,7 @@ extern "C" int titan_step_noalloc(const titan_dev_mesh* m, const titan_params* p
     ca.hfl = m->hfluids;
     ca.src = nullptr;
     ca.st = st;
-    if (!e) e = launch_cell_update(ca, fp32, p->npassive, false, p->nh > 0 ? 1 : 0, 0, s);
+    if (!e) e = launch_cell_update(ca, p->npassive, false, p->nh > 0 ? 1 : 0, 0, s);
     DevStatus h{};
     if (!e) e = cudaMemcpyAsync(&h, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, s);
     if (!e) e = cudaStreamSynchronize(s);

@@ -104,10 +104,15 @@ __device__ __forceinline__ void side_flux(R r, const R v[3], const R b[3], R pt,
 // wave region, i.e. NaN speeds) for the HLL/HLLC/HLLD branches, 4 for a bad
 // n_state. q1/q2: rho, u, v, w, p, Bx, By, Bz (Gaussian B). qout: 8 fluxes.
 // kl/kr/kout: NK passive scalars carried by the contact.
-template <typename R, int NK>
+// TRACK: when the face lies wholly in one side's region (HLLC zones 1/4, HLLD
+// zones 1/6), *upw is set to 1 (left) or 2 (right) and *wv_out to the frame
+// speed used, so that a caller can form that flux again in higher precision
+// (upwind_flux_fp64); qout is filled as usual either way.
+template <typename R, int NK, bool TRACK = false>
 __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, const R* q1, const R* q2,
                                             const R* kl, const R* kr, R* qout, R* kout, R& dsl, R& dsc,
-                                            R& dsr, RiemannFlags fl, R gamma) {
+                                            R& dsr, RiemannFlags fl, R gamma, int* upw = nullptr,
+                                            R* wv_out = nullptr) {
     const R spi4 = RConst<R>::spi4();
     const R g1 = gamma - R(1);
     R wv = w;
@@ -274,6 +279,10 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
         else
             side_flux(r2, vR, bR, ptR, e2, sbv2, FX, UX);
         if (zone == 1 || zone == 4) {
+            if (TRACK) {
+                *upw = left ? 1 : 2;
+                *wv_out = wv;
+            }
 #pragma unroll
             for (int k = 0; k < 8; ++k) out[k] = FX[k] - wv * UX[k];
 #pragma unroll
@@ -379,6 +388,10 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
         else
             side_flux(r2, vR, bR, ptR, eX, sbv2, FX, UX);
         if (zone == 1 || zone == 6) {
+            if (TRACK) {
+                *upw = left ? 1 : 2;
+                *wv_out = wv;
+            }
 #pragma unroll
             for (int k = 0; k < 8; ++k) out[k] = FX[k] - wv * UX[k];
 #pragma unroll
@@ -507,6 +520,60 @@ __device__ __forceinline__ int riemann_flux(int n_state, const R nrm[3], R w, co
         qout[i + 5] = spi4 * (n[i] * qb0 + t[i] * out[6] + m[i] * out[7]);
     }
     return 0;
+}
+
+// Flux through a face that lies wholly in one side's wave region (HLLC zones
+// 1/4, HLLD zones 1/6): the physical flux of that side minus wv U, with the
+// normal-B term -SN (bR - bL) - wv bn of riemann_flux, evaluated in FP64 from
+// the FP64 face states. The FP32 solver supplies the region (left), the frame
+// speed wv and the wave speeds SL, SR. Supersonic faces, where the upwind
+// state's flux is the whole answer, thus keep FP64 accuracy in the
+// mixed-precision step. The flux is formed directly in Cartesian components
+// (the face basis cancels out of an upwind flux), so this path is an ulp or
+// so from the FP64 solver's rotated result, not bit-matched to it.
+template <int NK>
+__device__ __forceinline__ void upwind_flux_fp64(const double nrm[3], double wv, const double* q1, const double* q2,
+                                                 const double* kl, const double* kr, bool left, double SL, double SR,
+                                                 bool null_bn, double gamma, double* qout, double* kout) {
+    const double spi4 = RConst<double>::spi4();
+    const double ispi4 = 1.0 / 3.5449077018110318;
+    const double ig1 = 1.0 / (gamma - 1.0);
+    const double* q = left ? q1 : q2;
+    const double r = q[0], v0 = q[1], v1 = q[2], v2 = q[3], p = q[4];
+    const double B0 = q[5] * ispi4, B1 = q[6] * ispi4, B2 = q[7] * ispi4;
+    const double vn = nrm[0] * v0 + nrm[1] * v1 + nrm[2] * v2;
+    const double bn = nrm[0] * B0 + nrm[1] * B1 + nrm[2] * B2;
+    const double b2 = B0 * B0 + B1 * B1 + B2 * B2;
+    const double pt = p + b2 * 0.5;
+    const double vb = v0 * B0 + v1 * B1 + v2 * B2;
+    const double e = p * ig1 + r * ((v0 * v0 + v1 * v1 + v2 * v2) * 0.5) + b2 * 0.5;
+    const double rvw = r * (vn - wv);
+    qout[0] = rvw;
+    qout[1] = rvw * v0 + pt * nrm[0] - bn * B0;
+    qout[2] = rvw * v1 + pt * nrm[1] - bn * B1;
+    qout[3] = rvw * v2 + pt * nrm[2] - bn * B2;
+    qout[4] = (e + pt) * vn - bn * vb - wv * e;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        const double K = left ? kl[k] : kr[k];
+        kout[k] = K * vn - wv * K;
+    }
+    const double bL0 = (nrm[0] * q1[5] + nrm[1] * q1[6] + nrm[2] * q1[7]) * ispi4;
+    const double bR0 = (nrm[0] * q2[5] + nrm[1] * q2[6] + nrm[2] * q2[7]) * ispi4;
+    const double SN = rmax(fabs(SL), fabs(SR));
+    double wbn;
+    if (wv > SR)
+        wbn = wv * bR0;
+    else if (wv < SL)
+        wbn = wv * bL0;
+    else
+        wbn = wv * (bL0 + bR0) * 0.5;
+    const double qb0 = null_bn ? 0.0 : -SN * (bR0 - bL0) - wbn;
+    // tangential part of (vn B - bn v - wv B) plus qb0 along the normal
+    const double tb = -wv * bn;  // normal component of (vn B - bn v - wv B)
+    const double Bv[3] = {B0, B1, B2}, vv[3] = {v0, v1, v2};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) qout[5 + i] = spi4 * (nrm[i] * qb0 + (vn * Bv[i] - bn * vv[i] - wv * Bv[i] - tb * nrm[i]));
 }
 
 }  // namespace titan

@@ -363,6 +363,100 @@ static __global__ void tvd_neighbours_kernel(MeshView M, Layer L, int* __restric
     bb[f] = pick[1];
 }
 
+// Loads through the L2 that the compiler may neither merge with earlier loads
+// of the same address nor move: the mixed-precision face kernel reads a face's
+// states again after the Riemann solve instead of keeping them live across it.
+__device__ __forceinline__ double ld_fresh(const double* p) {
+    double v;
+    asm volatile("ld.global.cg.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
+// Face states of one face (Setka::Snos_on_Gran): the two cells' states,
+// with the second-order branch (TVD), the Zone_1 radial scaling, the
+// Outer_Soft copy with its outflow fix-ups, or the fixed boundary values.
+// gc: face centre (set by the caller when MOVE; loaded here otherwise).
+// FRESH: every load through ld_fresh (a second evaluation after the solve).
+template <int NK, bool MOVE, bool TVD, bool FRESH>
+__device__ __forceinline__ void face_states(const FaceArgs& a, int f, int type, int c0, const double* n, double* gc,
+                                            double* Ls, double* Rs) {
+    const MeshView& M = a.M;
+    const Params& P = a.P;
+    const int nf = M.nface, nc = M.ncell;
+    auto ld = [](const double* p) { return FRESH ? ld_fresh(p) : *p; };
+    constexpr int NS = 8 + NK;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) Ls[k] = ld(a.state + k * nc + c0);
+#pragma unroll
+    for (int k = NS; k < NV; ++k) Ls[k] = 0.0;
+    if (type == 0) {
+        const int c1 = M.face_c1[f];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) Rs[k] = ld(a.state + k * nc + c1);
+#pragma unroll
+        for (int k = NS; k < NV; ++k) Rs[k] = 0.0;
+        bool second = false;
+        if (TVD) {
+            const int aa = M.face_aa[f], bb = M.face_bb[f];
+            if (aa >= 0 && bb >= 0 && M.cell_tvd[c0] && M.cell_tvd[c1] && (M.face_surf[f] != 2 || P.snos_on_hp)) {
+                // second-order branch (Setka_gran_snos.cpp:188-735)
+                if (!MOVE) {
+                    gc[0] = ld(a.L1.fc + f);
+                    gc[1] = ld(a.L1.fc + nf + f);
+                    gc[2] = ld(a.L1.fc + 2 * nf + f);
+                }
+                const int c4[4] = {aa, c0, c1, bb};
+                double S4[4][NV], X4[4][3];
+                int t4[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) S4[i][k] = ld(a.state + k * nc + c4[i]);
+#pragma unroll
+                    for (int k = NS; k < NV; ++k) S4[i][k] = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) X4[i][k] = ld(a.L1.cc + k * nc + c4[i]);
+                    t4[i] = M.cell_type[c4[i]];
+                }
+                snos_tvd<NK>(S4, X4, t4, gc, P.gamma, Ls, Rs);
+                second = true;
+            }
+        }
+        const bool z0 = !second && M.cell_type[c0] == 1, z1 = !second && M.cell_type[c1] == 1;
+        if (z0 || z1) {
+            if (!MOVE) {
+                gc[0] = ld(a.L1.fc + f);
+                gc[1] = ld(a.L1.fc + nf + f);
+                gc[2] = ld(a.L1.fc + 2 * nf + f);
+            }
+            if (z0)
+                zone1_scale(Ls, ld(a.L1.cc + c0), ld(a.L1.cc + nc + c0), ld(a.L1.cc + 2 * nc + c0), gc[0], gc[1],
+                            gc[2], P.gamma);
+            if (z1)
+                zone1_scale(Rs, ld(a.L1.cc + c1), ld(a.L1.cc + nc + c1), ld(a.L1.cc + 2 * nc + c1), gc[0], gc[1],
+                            gc[2], P.gamma);
+        }
+    } else if (type == 3) {
+        // Outer_Soft: copy the interior cell, with the reference's outflow fix-ups
+        if (P.soft_fixups) {
+            if (n[0] < -0.95) {
+                if (Ls[1] > P.velosity_inf / 7.0) Ls[1] = P.velosity_inf / 5.0;
+            } else if (Ls[1] * n[0] + Ls[2] * n[1] + Ls[3] * n[2] < 0.0) {
+                Ls[1] = 0.1 * n[0];
+                Ls[2] = 0.1 * n[1];
+                Ls[3] = 0.1 * n[2];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) Rs[k] = Ls[k];
+    } else {
+        // Inner_Hard / Outer_Hard: fixed face values
+        const int row = M.face_bc[f];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) Rs[k] = ld(M.bc_vals + k * M.nbc + row);
+    }
+}
+
 template <typename R, typename FT, int NK, bool MOVE, int BS, int MINB, bool TVD = false>
 __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -414,76 +508,8 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
             n[2] = a.L1.fn[2 * nf + f];
             area = a.L1.fa[f];
         }
-        constexpr int NS = 8 + NK;
         double Ls[NV], Rs[NV];
-#pragma unroll
-        for (int k = 0; k < NS; ++k) Ls[k] = a.state[k * nc + c0];
-#pragma unroll
-        for (int k = NS; k < NV; ++k) Ls[k] = 0.0;
-        if (type == 0) {
-            const int c1 = M.face_c1[f];
-#pragma unroll
-            for (int k = 0; k < NS; ++k) Rs[k] = a.state[k * nc + c1];
-#pragma unroll
-            for (int k = NS; k < NV; ++k) Rs[k] = 0.0;
-            bool second = false;
-            if (TVD) {
-                const int aa = M.face_aa[f], bb = M.face_bb[f];
-                if (aa >= 0 && bb >= 0 && M.cell_tvd[c0] && M.cell_tvd[c1] &&
-                    (M.face_surf[f] != 2 || P.snos_on_hp)) {
-                    // second-order branch (Setka_gran_snos.cpp:188-735)
-                    if (!MOVE) {
-                        gc[0] = a.L1.fc[f];
-                        gc[1] = a.L1.fc[nf + f];
-                        gc[2] = a.L1.fc[2 * nf + f];
-                    }
-                    const int c4[4] = {aa, c0, c1, bb};
-                    double S4[4][NV], X4[4][3];
-                    int t4[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-#pragma unroll
-                        for (int k = 0; k < NS; ++k) S4[i][k] = a.state[k * nc + c4[i]];
-#pragma unroll
-                        for (int k = NS; k < NV; ++k) S4[i][k] = 0.0;
-                        load_cc(a.L1.cc, nc, c4[i], X4[i]);
-                        t4[i] = M.cell_type[c4[i]];
-                    }
-                    snos_tvd<NK>(S4, X4, t4, gc, P.gamma, Ls, Rs);
-                    second = true;
-                }
-            }
-            const bool z0 = !second && M.cell_type[c0] == 1, z1 = !second && M.cell_type[c1] == 1;
-            if (z0 || z1) {
-                if (!MOVE) {
-                    gc[0] = a.L1.fc[f];
-                    gc[1] = a.L1.fc[nf + f];
-                    gc[2] = a.L1.fc[2 * nf + f];
-                }
-                if (z0)
-                    zone1_scale(Ls, a.L1.cc[c0], a.L1.cc[nc + c0], a.L1.cc[2 * nc + c0], gc[0], gc[1], gc[2], P.gamma);
-                if (z1)
-                    zone1_scale(Rs, a.L1.cc[c1], a.L1.cc[nc + c1], a.L1.cc[2 * nc + c1], gc[0], gc[1], gc[2], P.gamma);
-            }
-        } else if (type == 3) {
-            // Outer_Soft: copy the interior cell, with the reference's outflow fix-ups
-            if (P.soft_fixups) {
-                if (n[0] < -0.95) {
-                    if (Ls[1] > P.velosity_inf / 7.0) Ls[1] = P.velosity_inf / 5.0;
-                } else if (Ls[1] * n[0] + Ls[2] * n[1] + Ls[3] * n[2] < 0.0) {
-                    Ls[1] = 0.1 * n[0];
-                    Ls[2] = 0.1 * n[1];
-                    Ls[3] = 0.1 * n[2];
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < NV; ++k) Rs[k] = Ls[k];
-        } else {
-            // Inner_Hard / Outer_Hard: fixed face values
-            const int row = M.face_bc[f];
-#pragma unroll
-            for (int k = 0; k < NV; ++k) Rs[k] = M.bc_vals[k * M.nbc + row];
-        }
+        face_states<NK, MOVE, TVD, false>(a, f, type, c0, n, gc, Ls, Rs);
         int method;
         if (P.method_policy == 1) {
             const double bb = ((Ls[5] * Ls[5] + Ls[6] * Ls[6] + Ls[7] * Ls[7]) +
@@ -493,6 +519,8 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         } else {
             method = M.face_method[f];
         }
+        // Powell term: the face-normal B of the two states, averaged (divB * area)
+        const double bsum = 0.5 * (n[0] * (Ls[5] + Rs[5]) + n[1] * (Ls[6] + Rs[6]) + n[2] * (Ls[7] + Rs[7]));
         const int surf = M.face_surf[f];
         RiemannFlags fl;
         fl.null_bn = false;
@@ -514,8 +542,26 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         nr[1] = R(n[1]);
         nr[2] = R(n[2]);
         R dsl, dsc, dsr;
-        const int rc = riemann_flux<R, NK>(method, nr, R(w), qL, qR, kl, kr, q, kq, dsl, dsc, dsr, fl, R(P.gamma));
+        // mixed precision: the FP32 solver reports faces that lie wholly in one
+        // side's region, whose flux is then formed again in FP64
+        constexpr bool kMixed = sizeof(R) < sizeof(double);
+        int upw = 0;
+        R wvo = R(0);
+        const int rc = riemann_flux<R, NK, kMixed>(method, nr, R(w), qL, qR, kl, kr, q, kq, dsl, dsc, dsr, fl,
+                                                    R(P.gamma), &upw, &wvo);
         if (rc) record_error(a.st, 10 + rc, f);
+        double qd[8], kqd[NK > 0 ? NK : 1];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) qd[k] = double(q[k]);
+#pragma unroll
+        for (int k = 0; k < NK; ++k) kqd[k] = double(kq[k]);
+        if (kMixed && upw) {
+            // the face's states again, loaded anew rather than kept live across the solve
+            double L2[NV], R2[NV];
+            face_states<NK, MOVE, TVD, true>(a, f, type, c0, n, gc, L2, R2);
+            upwind_flux_fp64<NK>(n, double(wvo), L2, R2, L2 + 8, R2 + 8, upw == 1, double(dsl), double(dsr),
+                                 fl.null_bn, P.gamma, qd, kqd);
+        }
         if (type == 0) {
             if (!MOVE) dist = a.L1.fd[f];
             const double dnt = P.KFL * dist / (rmax(fabs(double(dsl)), fabs(double(dsr))) + fabs(w));
@@ -527,10 +573,10 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         using L = FluxLayout<FT, NK>;
         FT out[L::stride];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) out[k] = FT(double(q[k]) * area);
-        out[8] = FT(0.5 * (n[0] * (Ls[5] + Rs[5]) + n[1] * (Ls[6] + Rs[6]) + n[2] * (Ls[7] + Rs[7])) * area);
+        for (int k = 0; k < 8; ++k) out[k] = FT(qd[k] * area);
+        out[8] = FT(bsum * area);
 #pragma unroll
-        for (int k = 0; k < NK; ++k) out[9 + k] = FT(double(kq[k]) * area);
+        for (int k = 0; k < NK; ++k) out[9 + k] = FT(kqd[k] * area);
 #pragma unroll
         for (int k = L::n; k < L::stride; ++k) out[k] = FT(0);
         FT* dst = reinterpret_cast<FT*>(a.flux) + size_t(f) * L::stride;

@@ -161,6 +161,20 @@ cudaError_t timed(titan_ctx* ctx, const char* name, F fn) {
     return e;
 }
 
+// The face-flux kernel of this context: FP64 or FP32 Riemann arithmetic,
+// first- or second-order faces.
+cudaError_t face_launch(const titan_ctx* ctx, const FaceArgs& fa, int nk, bool move, int variant, cudaStream_t s) {
+    if (ctx->P.tvd)
+        return ctx->fp32 ? launch_face_flux_tvd_fp32(fa, nk, move, variant, s)
+                         : launch_face_flux_tvd_fp64(fa, nk, move, variant, s);
+    return ctx->fp32 ? launch_face_flux_fp32(fa, nk, move, variant, s) : launch_face_flux_fp64(fa, nk, move, variant, s);
+}
+
+const char* face_kernel_name(const titan_ctx* ctx) {
+    if (ctx->P.tvd) return ctx->fp32 ? "face_flux_tvd_fp32" : "face_flux_tvd_fp64";
+    return ctx->fp32 ? "face_flux_fp32" : "face_flux_fp64";
+}
+
 // Enqueue one step; flips the layer and state buffers.
 cudaError_t enqueue_step(titan_ctx* ctx) {
     const MeshView M = ctx->view();
@@ -200,17 +214,7 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     fa.flux = ctx->d_flux;
     fa.st = ctx->d_status;
     const int nk = ctx->prm.npassive;
-    const int fv = ctx->face_variant;
-    if (ctx->P.tvd) {
-        if (ctx->fp32)
-            e = timed(ctx, "face_flux_tvd_fp32", [&] { return launch_face_flux_tvd_fp32(fa, nk, move, fv, ctx->stream); });
-        else
-            e = timed(ctx, "face_flux_tvd_fp64", [&] { return launch_face_flux_tvd_fp64(fa, nk, move, fv, ctx->stream); });
-    } else if (ctx->fp32) {
-        e = timed(ctx, "face_flux_fp32", [&] { return launch_face_flux_fp32(fa, nk, move, fv, ctx->stream); });
-    } else {
-        e = timed(ctx, "face_flux_fp64", [&] { return launch_face_flux_fp64(fa, nk, move, fv, ctx->stream); });
-    }
+    e = timed(ctx, face_kernel_name(ctx), [&] { return face_launch(ctx, fa, nk, move, ctx->face_variant, ctx->stream); });
     if (e) return e;
     CellArgs ca;
     ca.M = M;
@@ -226,7 +230,7 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     ca.st = ctx->d_status;
     const int src = (ctx->use_src || ctx->use_closure) ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
     e = timed(ctx, "cell_update",
-              [&] { return launch_cell_update(ca, ctx->fp32, nk, move, src, ctx->cell_variant, ctx->stream); });
+              [&] { return launch_cell_update(ca, nk, move, src, ctx->cell_variant, ctx->stream); });
     if (e) return e;
     ctx->scur ^= 1;
     if (move) ctx->cur = nxt;
@@ -536,8 +540,8 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     DA(ctx->d_state[1], (size_t)ctx->ns * nc);
     {
         const int n = 9 + p->npassive;
-        ctx->flux_elem = ctx->fp32 ? 4 : 8;
-        ctx->flux_stride = ctx->fp32 ? ((n + 3) & ~3) : ((n + 1) & ~1);
+        ctx->flux_elem = 8;  // FP64 records in every mode
+        ctx->flux_stride = (n + 1) & ~1;
         char* fp = nullptr;
         DA(fp, (size_t)nf * ctx->flux_stride * ctx->flux_elem);
         ctx->d_flux = fp;
@@ -797,12 +801,7 @@ int titan_download_face_fluxes(titan_ctx* ctx, double* flux) {
         double* dst = flux + 11 * (int64_t)ctx->R.face_n2o[f];
         for (int k = 0; k < 11; ++k) {
             double v = 0.0;
-            if (k < n) {
-                if (ctx->fp32)
-                    v = reinterpret_cast<const float*>(raw.data())[(size_t)f * stride + k];
-                else
-                    v = reinterpret_cast<const double*>(raw.data())[(size_t)f * stride + k];
-            }
+            if (k < n) v = reinterpret_cast<const double*>(raw.data())[(size_t)f * stride + k];
             dst[k] = v;
         }
     }
@@ -1015,9 +1014,9 @@ int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     if (!ctx || reps <= 0) return fail(TITAN_EINVAL, "bad argument");
     const int src = (ctx->use_src || ctx->use_closure) ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
     char key[256];
-    snprintf(key, sizeof key, "sm_100a cells=%lld faces=%lld move=%d flux=%d npassive=%d src=%d",
+    snprintf(key, sizeof key, "sm_100a cells=%lld faces=%lld move=%d flux=%d npassive=%d src=%d tvd=%d",
              (long long)ctx->ncell, (long long)ctx->nface, ctx->prm.move, ctx->prm.flux_precision,
-             ctx->prm.npassive, src);
+             ctx->prm.npassive, src, ctx->P.tvd);
     if (cache_path) {
         FILE* f = fopen(cache_path, "r");
         if (f) {
@@ -1083,9 +1082,7 @@ int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     int best_fv = 0, best_cv = 0;
     float fms[kFaceVariants], cms[kCellVariants];
     for (int v = 0; v < kFaceVariants; ++v) {
-        CK(time_it([&] { return ctx->fp32 ? launch_face_flux_fp32(fa, nk, move, v, s)
-                                          : launch_face_flux_fp64(fa, nk, move, v, s); },
-                   &fms[v]));
+        CK(time_it([&] { return face_launch(ctx, fa, nk, move, v, s); }, &fms[v]));
         if (fms[v] < best) {
             best = fms[v];
             best_fv = v;
@@ -1093,7 +1090,7 @@ int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     }
     best = 1e30f;
     for (int v = 0; v < kCellVariants; ++v) {
-        CK(time_it([&] { return launch_cell_update(ca, ctx->fp32, nk, move, src, v, s); }, &cms[v]));
+        CK(time_it([&] { return launch_cell_update(ca, nk, move, src, v, s); }, &cms[v]));
         if (cms[v] < best) {
             best = cms[v];
             best_cv = v;

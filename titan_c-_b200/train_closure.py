@@ -14,8 +14,10 @@ sources and judges it against the Monte-Carlo noise.
 3. The network trains on the GPU (BF16 tensor-core forward/backward, Adam).
 4. On the held-out snapshot: the closure's error against the mean of the
    seeds, one seed's statistical scatter about that mean, the error of holding
-   the previous snapshot's Monte-Carlo sources fixed, and the time of one
-   Monte-Carlo pass against one closure evaluation.
+   the previous snapshot's Monte-Carlo sources fixed (all volume-weighted L1,
+   relative), and the time of one Monte-Carlo pass against one closure launch.
+Training rows are weighted by cell volume: the Monte-Carlo samples a cell in
+proportion to the neutral path length inside it.
 """
 from __future__ import annotations
 
@@ -38,9 +40,10 @@ def _pkg():
     return importlib.import_module("titan_c-_b200")
 
 
-def l1(a, b):
-    """Mean absolute difference over cells of the momentum and energy sources."""
-    return float(np.abs(a[1:5] - b[1:5]).mean())
+def l1(a, b, vol):
+    """Volume-weighted L1 difference of the momentum and energy sources,
+    relative to b (the sources enter the conserved variables as S V)."""
+    return float((np.abs(a[1:5] - b[1:5]) * vol).sum() / (np.abs(b[1:5]) * vol).sum())
 
 
 def main(argv=None):
@@ -77,7 +80,8 @@ def main(argv=None):
         g.go(every * (k + 1) - done)
         done = every * (k + 1)
         state = g.download_state()
-        cc = g.geometry()["cell_center"].T.copy()
+        geo = g.geometry()
+        cc, vol = geo["cell_center"].T.copy(), geo["cell_volume"].copy()
         nseed = a.seeds if k == a.snapshots - 1 else 1
         runs = []
         for s in range(nseed):
@@ -85,26 +89,28 @@ def main(argv=None):
             out, info = g.mc_sources(seed=1000 * k + s + 1, **kw)
             mc_ms.append(1e3 * (time.perf_counter() - t0))
             runs.append(out)
-        snaps.append({"step": done, "state": state, "cc": cc, "runs": runs})
+        snaps.append({"step": done, "state": state, "cc": cc, "vol": vol, "runs": runs})
         print(f"snapshot step {done}: MC {nseed} seed(s), last {mc_ms[-1]:.0f} ms, lost {info['lost']}",
               flush=True)
 
     train, test = snaps[:-1], snaps[-1]
     X = np.concatenate([cl.features(s["state"], s["cc"], a.n_inf, a.lam) for s in train])
     T = np.concatenate([cl.targets(s["state"], s["cc"], s["runs"][0], a.n_inf, a.lam) for s in train])
+    rw = np.concatenate([s["vol"] for s in train])  # the Monte-Carlo samples a cell in proportion to its volume
     net = cl.Closure(a.n_inf, a.lam, seed=0)
     t0 = time.perf_counter()
-    losses = net.fit(X, T, epochs=a.epochs, batch=a.batch, lr=a.lr, lr_decay=0.8)
+    losses = net.fit(X, T, epochs=a.epochs, batch=a.batch, lr=a.lr, lr_decay=0.8, row_weights=rw)
     train_s = time.perf_counter() - t0
     print(f"trained on {X.shape[0]} rows in {train_s:.1f} s; loss {losses[0]:.4f} -> {losses[-1]:.4f}", flush=True)
 
     mean = np.mean(test["runs"], axis=0)
     t0 = time.perf_counter()
     pred = net.predict(test["state"], test["cc"])
-    err = l1(pred, mean)
+    vol = test["vol"]
+    err = l1(pred, mean, vol)
     ns = len(test["runs"])
-    noise = float(np.mean([l1(r, mean) for r in test["runs"]]) * np.sqrt(ns / max(ns - 1, 1)))
-    stale = l1(train[-1]["runs"][0], mean)
+    noise = float(np.mean([l1(r, mean, vol) for r in test["runs"]]) * np.sqrt(ns / max(ns - 1, 1)))
+    stale = l1(train[-1]["runs"][0], mean, vol)
     # closure cost inside the step: one launch of the tensor-core kernel per step
     net.install(g)
     g.set_profiling(True)
@@ -113,10 +119,13 @@ def main(argv=None):
     g.close()
     mlp_ms = kt["closure_mlp"][0] / kt["closure_mlp"][1]
     comp = {}
+    def l1c(x, y):
+        return float((np.abs(x - y) * vol).sum() / (np.abs(y) * vol).sum())
+
     for i, name in enumerate(["S_mx", "S_my", "S_mz", "S_E"]):
-        comp[name] = {"closure": float(np.abs(pred[1 + i] - mean[1 + i]).mean()),
-                      "one_seed_noise": float(np.mean([np.abs(r[1 + i] - mean[1 + i]).mean()
-                                                       for r in test["runs"]]) * np.sqrt(ns / max(ns - 1, 1)))}
+        comp[name] = {"closure": l1c(pred[1 + i], mean[1 + i]),
+                      "one_seed_noise": float(np.mean([l1c(r[1 + i], mean[1 + i]) for r in test["runs"]])
+                                              * np.sqrt(ns / max(ns - 1, 1)))}
     report = {
         "mesh": f"shell 6x{a.nq}x{a.nq}x{a.nlayer} = {m['cell_nodes'].shape[0]} cells (moving)",
         "snapshots": [s["step"] for s in snaps], "train_snapshots": [s["step"] for s in train],

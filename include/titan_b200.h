@@ -143,6 +143,27 @@ int titan_set_sources(titan_ctx* ctx, const double* src);
  * step. t_inout: accumulated physical time (drives the node motion). */
 int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout, titan_step_info* info);
 
+/* Node coordinates [nnode*3] (original numbering) for the current layer; the
+ * layer's geometry (and the second-order neighbours of a tvd context) is formed
+ * again from them, as Setka::Download_cell_parameters followed by
+ * Calculating_measure and Init_TVD does (TITAN/source/TITAN.cpp:36-55). */
+int titan_upload_nodes(titan_ctx* ctx, const double* xyz);
+
+/* Cell-parameter checkpoints in the reference's binary layout
+ * (Setka::Save_cell_parameters / Download_cell_parameters,
+ * TITAN/source/Setka_physics.cpp:4108-4231): per cell a count and key/value
+ * pairs, then an optional node block. Host-only, no context needed.
+ * read: fills state [TITAN_NV][ncell] for the keys rho, Vx, Vy, Vz, p, Bx, By,
+ * Bz, Q, rho_He that the file holds (others are skipped; absent ones leave the
+ * caller's values); fields_found: bit k set when field k occurred; xyz
+ * [nnode*3] (may be NULL) receives the node block when the file has one
+ * (has_nodes = 1). write: the first nfields fields per cell, and the node
+ * block when xyz is not NULL. */
+int titan_read_cell_parameters(const char* path, int64_t ncell, int64_t nnode, double* state, double* xyz,
+                               int32_t* fields_found, int32_t* has_nodes);
+int titan_write_cell_parameters(const char* path, int64_t ncell, int32_t nfields, const double* state, int64_t nnode,
+                                const double* xyz);
+
 /* Node coordinates [nnode*3] and geometry of the current layer (original numbering). */
 int titan_download_nodes(titan_ctx* ctx, double* xyz);
 int titan_download_geometry(titan_ctx* ctx, double* cell_center, double* cell_volume, double* face_center,

@@ -309,3 +309,25 @@ def test_moving_mesh_geometry_matches_oracle(T, oracle_lib):
     for k in a:
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
     gpu.close()
+
+
+def test_checkpoint_round_trip_through_contexts(T, tmp_path):
+    """Save a moved, stepped state as a reference cell-parameter file; a fresh
+    context loading it has the same state bit for bit and, after the node
+    block replaces its nodes, the same geometry as the saving context."""
+    m, p, st, _ = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, npassive=2)
+    a = T.PlasmaStep(m, p)
+    a.upload_state(st)
+    a.go(7)
+    path = str(tmp_path / "parameters_0007.bin")
+    a.save_checkpoint(path)
+    b = T.PlasmaStep(m, p)
+    info = b.load_checkpoint(path)
+    assert info["nodes"] and info["fields"] == list(T.FIELDS)
+    assert np.array_equal(b.download_state(), a.download_state())
+    assert np.array_equal(b.nodes(), a.nodes())
+    ga, gb = a.geometry(), b.geometry()
+    for k in ga:
+        assert np.array_equal(ga[k], gb[k]), k
+    a.close()
+    b.close()

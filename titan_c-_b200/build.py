@@ -11,6 +11,7 @@ Translation units and their floating-point flags:
   closure_mlp.cu                closure inference on tcgen05 / TMEM (per step)
   closure_train.cu, closure_api.cu   closure training (BF16 tensor-core GEMMs), C ABI
   titan_api.cu, renumber.cpp    host side of the C ABI
+  checkpoint.cpp                cell-parameter files in the reference's layout
   noalloc.cu       -fmad=false  titan_step_noalloc (fixed scratch array, no allocation)
 """
 from __future__ import annotations
@@ -41,6 +42,7 @@ UNITS = [
     ("titan_api.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("renumber.cpp", []),
+    ("checkpoint.cpp", []),
 ]
 
 

@@ -747,6 +747,26 @@ int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout
     return TITAN_OK;
 }
 
+int titan_upload_nodes(titan_ctx* ctx, const double* xyz) {
+    if (!ctx || !xyz) return fail(TITAN_EINVAL, "null argument");
+    const int64_t nn = ctx->nnode;
+    for (int64_t i = 0; i < 3 * nn; ++i)
+        if (!std::isfinite(xyz[i])) return fail(TITAN_EINVAL, "non-finite node coordinate");
+    std::vector<double> h(3 * nn);
+    for (int64_t i = 0; i < nn; ++i)
+        for (int k = 0; k < 3; ++k) h[k * nn + i] = xyz[3 * (int64_t)ctx->R.node_n2o[i] + k];
+    drop_graph(ctx);
+    const Layer& L = ctx->layer[ctx->cur];
+    CK(cudaMemcpyAsync(L.xyz, h.data(), sizeof(double) * 3 * nn, cudaMemcpyHostToDevice, ctx->stream));
+    const MeshView M = ctx->view();
+    CK(launch_cell_geometry(M, L, ctx->stream));
+    CK(launch_face_geometry(M, L, ctx->stream));
+    // as in the reference, where Init_TVD runs after Download_cell_parameters
+    if (ctx->P.tvd) CK(launch_tvd_neighbours(M, L, ctx->d_face_aa, ctx->d_face_bb, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TITAN_OK;
+}
+
 int titan_download_nodes(titan_ctx* ctx, double* xyz) {
     if (!ctx || !xyz) return fail(TITAN_EINVAL, "null argument");
     const int64_t nn = ctx->nnode;

@@ -119,6 +119,10 @@ SIGNATURES = {
     "titan_mlp_train": ([F32, F32, F32, F32, F32, F32, ctypes.c_int64, ctypes.POINTER(TitanMlpTrainOpts), F32],
                         ctypes.c_int),
     "titan_get_tvd_neighbours": ([ctypes.c_void_p, I32], ctypes.c_int),
+    "titan_upload_nodes": ([ctypes.c_void_p, D], ctypes.c_int),
+    "titan_read_cell_parameters": ([ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64, D, D, I32, I32], ctypes.c_int),
+    "titan_write_cell_parameters": ([ctypes.c_char_p, ctypes.c_int64, ctypes.c_int32, D, ctypes.c_int64, D],
+                                    ctypes.c_int),
     "titan_set_closure": ([ctypes.c_void_p, F32, F32, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "titan_autotune": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p], ctypes.c_int),
     "titan_set_tuning": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),

@@ -145,6 +145,34 @@ class PlasmaStep:
         N.check(self._lib.titan_download_face_fluxes(self._ctx, N.ptr(out)))
         return out
 
+    def upload_nodes(self, xyz: np.ndarray):
+        """Node coordinates [nnode, 3]; the geometry is formed again from them."""
+        a = np.ascontiguousarray(xyz, dtype=np.float64)
+        assert a.shape == (self.nnode, 3)
+        N.check(self._lib.titan_upload_nodes(self._ctx, N.ptr(a)))
+
+    def save_checkpoint(self, path: str, nodes: bool = True):
+        """The state (and nodes) as a reference cell-parameter file (Setka::Save_cell_parameters)."""
+        st = np.ascontiguousarray(self.download_state())
+        xyz = np.ascontiguousarray(self.nodes()) if nodes else None
+        N.check(self._lib.titan_write_cell_parameters(path.encode(), self.ncell, 8 + int(self.params["npassive"]), N.ptr(st),
+                                                      self.nnode, N.ptr(xyz)))
+
+    def load_checkpoint(self, path: str) -> dict:
+        """A reference cell-parameter file (Setka::Download_cell_parameters): the
+        plasma fields it holds replace the state; its node block, if any, the nodes."""
+        st = np.ascontiguousarray(self.download_state())
+        xyz = np.empty((self.nnode, 3))
+        found = ctypes.c_int32(0)
+        has_nodes = ctypes.c_int32(0)
+        N.check(self._lib.titan_read_cell_parameters(path.encode(), self.ncell, self.nnode, N.ptr(st), N.ptr(xyz),
+                                                     ctypes.byref(found), ctypes.byref(has_nodes)))
+        self.upload_state(st)
+        if has_nodes.value:
+            self.upload_nodes(xyz)
+        return {"fields": [n for k, n in enumerate(N.FIELDS) if found.value >> k & 1],
+                "nodes": bool(has_nodes.value)}
+
     def tvd_neighbours(self) -> np.ndarray:
         """[nface, 2] second-order neighbours (AA, BB), original numbering, -1 when absent."""
         out = np.empty((self.nface, 2), dtype=np.int32)

@@ -97,6 +97,9 @@ typedef struct titan_params {
     int32_t tvd;           /* Phys_param::TVD: second-order reconstruction on interior faces
                               (Setka_gran_snos.cpp:188-735; neighbours from Setka::Init_TVD) */
     int32_t snos_on_hp;    /* Phys_param::Snos_on_HP: second order on HP faces too */
+    int32_t bn_in_p_on_hp; /* Phys_param::bn_in_p_on_HP: on HP faces the magnetic pressure goes into p
+                              and the exact gas-dynamic solver Godunov_Solver_Alexashov runs
+                              (Setka_physics.cpp:2378-2409, Phys_param.cpp:1938-2385) */
 } titan_params;
 
 typedef struct titan_step_info {
@@ -105,7 +108,9 @@ typedef struct titan_step_info {
     int64_t n_rho_floor;     /* cells where rho < 1e-7 was reset (Setka_physics.cpp:1784-1794) */
     int64_t n_p_floor;       /* cells where p < 1e-8 was reset (Setka_physics.cpp:1981-2001) */
     int32_t status;          /* titan_status of the step loop */
-    int32_t err_kind;        /* 0, 11-14 solver region/branch, 20 non-finite density */
+    int32_t err_kind;        /* 0, 11-14 solver region/branch, 15-18 exact HP solver (negative pressure,
+                                Newton / bisection without convergence, no wave pattern), 20 non-finite
+                                density */
     double  dt_next;         /* CFL dt that the next step will use */
     double  t;               /* accumulated physical time */
     double  gpu_ms;          /* device time of this call's step loop (CUDA events) */
@@ -198,6 +203,15 @@ int titan_get_permutation(titan_ctx* ctx, int32_t* cell_new2old, int32_t* face_n
 int titan_riemann_batch(int64_t n, const int8_t* n_state, const double* nrm, const double* w, const double* q1,
                         const double* q2, int32_t flags, int32_t precision, double gamma, double* flux,
                         double* ds, int32_t* rc);
+
+/* Stateless batch of Phys_param::Godunov_Solver_Alexashov calls (the exact
+ * gas-dynamic solver of HP faces, Phys_param.cpp:1938-2385) on the device,
+ * host buffers. nrm [n*3], w [n], q1/q2 [n*5] (rho, u, v, w, p), contact [n]
+ * (0/1). Outputs flux [n*5] (mass, momentum, energy), ds [n*3] = (dsl, dsc,
+ * dsr), rc [n]: 0, or 1-4 where the reference would exit (negative pressure
+ * in Newton, Newton / bisection without convergence, no wave pattern). */
+int titan_godunov_batch(int64_t n, const double* nrm, const double* w, const double* q1, const double* q2,
+                        const int8_t* contact, double gamma, double* flux, double* ds, int32_t* rc);
 
 /* Monte-Carlo neutral hydrogen through the current plasma state: the source
  * generator the closure is trained on. Physics of the reference's

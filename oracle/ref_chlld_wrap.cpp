@@ -66,6 +66,22 @@ void titan_ref_chlld(int n_state, const double* nrm, double w, const double* q1,
     ds[2] = dsr;
 }
 
+// One call of the reference's exact gas-dynamic Godunov solver used on HP
+// faces with bn_in_p_on_HP (Phys_param::Godunov_Solver_Alexashov,
+// Phys_param.cpp:1938-2385). q1/q2: (rho,u,v,w,p,...); qout: 5 fluxes
+// (mass, momentum, energy); ds: dsl, dsc, dsr. The reference exits on
+// inputs its Newton iterations cannot handle; callers pass valid states.
+void titan_ref_godunov(const double* nrm, double w, const double* q1, const double* q2, int contact,
+                       double* qout, double* ds) {
+    std::vector<double> qqq1(q1, q1 + 8), qqq2(q2, q2 + 8), qqq(8, 0.0), n(nrm, nrm + 3);
+    double dsl = 0, dsp = 0, dsc = 0;
+    g_param->Godunov_Solver_Alexashov(qqq1, qqq2, n, qqq, dsl, dsp, dsc, w, contact != 0);
+    for (int i = 0; i < 5; ++i) qout[i] = qqq[i];
+    ds[0] = dsl;
+    ds[1] = dsc;
+    ds[2] = dsp;
+}
+
 // Batched form: n faces, arrays of stride 8 (states/fluxes) and 3 (normals, ds).
 void titan_ref_chlld_batch(long n, const int* n_state, const double* nrm, const double* w,
                            const double* q1, const double* q2, double* qout, double* ds) {

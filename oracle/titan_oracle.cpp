@@ -37,6 +37,7 @@ const double kPi = 3.14159265358979323846;
 const double kCpi4 = 4.0 * kPi;
 const double kSpi4 = std::sqrt(kCpi4);
 const double kEpsB = 1E-4;
+const double kEps = 1E-12;
 const double kMeDmp = (1.0 / 1836.15);
 // Literal 8*pi used by the energy update, Setka_physics.cpp:1927-1929.
 const double kC8Pi = 25.13274122871834590768;
@@ -91,7 +92,8 @@ struct OParams {
     int32_t TS_hard, contact_hard;
     int32_t tvd;          // Phys_param::TVD: second-order reconstruction on interior faces
     int32_t snos_on_hp;   // Phys_param::Snos_on_HP: second order on HP faces too
-    int32_t pad[2];
+    int32_t bn_in_p_on_hp;  // Phys_param::bn_in_p_on_HP: exact gas-dynamic solver on HP faces
+    int32_t pad;
 };
 
 struct OStepInfo {
@@ -742,6 +744,305 @@ static void o_snos_side(const double* st, int64_t nc, int64_t c, int ctype, cons
 }
 
 // ---------------------------------------------------------------------------
+// Exact gas-dynamic Godunov solver of HP faces with bn_in_p_on_HP,
+// Phys_param::Godunov_Solver_Alexashov (Phys_param.cpp:1938-2385) with its
+// Newton (:2387-2442), bisection (:2444-2519) and pressure-function (:2521-2536)
+// helpers. The reference's macros (Phys_param.cpp:3-11: ga = gamma, g1 =
+// ga - 1, g2 = ga + 1, gp = (g2/ga)/2, gm = (g1/ga)/2, gga = ga) are
+// parenthesised, so their values are formed once here. Where the reference
+// exits (negative pressure in Newton, 1100 iterations without convergence)
+// this returns 1 / 2 / 3; 4 where no wave pattern applies (NaN input).
+// q1, q2: rho, u, v, w, p; out: 5 fluxes; ds: dsl, dsc, dsr.
+// ---------------------------------------------------------------------------
+namespace {
+struct GodunovK {
+    double ga, g1, g2, gp, gm;
+    explicit GodunovK(double gamma)
+        : ga(gamma), g1(gamma - 1.0), g2(gamma + 1.0), gp(((gamma + 1.0) / gamma) / 2.0),
+          gm(((gamma - 1.0) / gamma) / 2.0) {}
+};
+
+double o_lev(const GodunovK& K, double enI, double pI, double rI, double enII, double pII, double rII, double uuu) {
+    const double cI = std::sqrt(K.ga * pI / rI);
+    const double cII = std::sqrt(K.ga * pII / rII);
+    const double fI = (uuu - pI) / (rI * cI * std::sqrt(K.gp * uuu / pI + K.gm));
+    const double fII = 2.0 / K.g1 * cII * (std::pow((uuu / pII), K.gm) - 1.0);
+    const double f1 = fI + fII;
+    const double f2 = enI - enII;
+    return f1 - f2;
+}
+
+int o_newton(const GodunovK& K, double enI, double pI, double rI, double enII, double pII, double rII, double& p) {
+    const double cI = std::sqrt(K.ga * pI / rI);
+    const double cII = std::sqrt(K.ga * pII / rII);
+    double pn = pI * rII * cII + pII * rI * cI + (enI - enII) * rI * cI * rII * cII;
+    pn = pn / (rI * cI + rII * cII);
+    const double pee = pn;
+    int kiter = 0;
+    while (true) {
+        p = pn;
+        if (p <= 0.0) return 1;
+        kiter = kiter + 1;
+        const double fI = (p - pI) / (rI * cI * std::sqrt(K.gp * p / pI + K.gm));
+        double fIs = (K.ga + 1.0) * p / pI + (3.0 * K.ga - 1.0);
+        fIs = fIs / (4.0 * K.ga * rI * cI * std::pow((K.gp * p / pI + K.gm), (3.0 / 2.0)));
+        const double fII = (p - pII) / (rII * cII * std::sqrt(K.gp * p / pII + K.gm));
+        double fIIs = (K.ga + 1.0) * p / pII + (3.0 * K.ga - 1.0);
+        fIIs = fIIs / (4.0 * K.ga * rII * cII * std::pow((K.gp * p / pII + K.gm), (3.0 / 2.0)));
+        if (kiter == 1100) return 2;
+        pn = p - (fI + fII - (enI - enII)) / (fIs + fIIs);
+        if (!(std::fabs(pn / pee - p / pee) >= kEps)) break;
+    }
+    p = pn;
+    return 0;
+}
+
+int o_devtwo(const GodunovK& K, double enI, double pI, double rI, double enII, double pII, double rII, double& p) {
+    const double epsil = 10e-10;
+    double kl = pI, kp = pII;
+    double ksi = o_lev(K, enI, pI, rI, enII, pII, rII, kl);
+    double ksir = o_lev(K, enI, pI, rI, enII, pII, rII, kp);
+    if (std::fabs(ksi) <= epsil) {
+        p = kl;
+        return 0;
+    }
+    if (std::fabs(ksir) <= epsil) {
+        p = kp;
+        return 0;
+    }
+    int kpizd = 0;
+    while (true) {
+        kpizd = kpizd + 1;
+        if (kpizd == 1100) return 3;
+        const double kc = (kl + kp) / 2.0;
+        const double ksit = o_lev(K, enI, pI, rI, enII, pII, rII, kc);
+        if (std::fabs(ksit) <= epsil) {
+            p = kc;
+            return 0;
+        }
+        if ((ksi * ksit) <= 0.0) {
+            kp = kc;
+            ksir = ksit;
+        } else {
+            kl = kc;
+            ksi = ksit;
+        }
+    }
+}
+}  // namespace
+
+int o_godunov(const double* nrm, double w, const double* q1, const double* q2, int contact, double gamma,
+              double* out, double* ds) {
+    const GodunovK K(gamma);
+    const double al = nrm[0], be = nrm[1], ge = nrm[2];
+    double t[3], m[3];
+    o_bazis(nrm, t, m);
+    const double al2 = t[0], be2 = t[1], ge2 = t[2], al3 = m[0], be3 = m[1], ge3 = m[2];
+    double enI = al * q1[1] + be * q1[2] + ge * q1[3];
+    double teI2 = al2 * q1[1] + be2 * q1[2] + ge2 * q1[3];
+    double teI3 = al3 * q1[1] + be3 * q1[2] + ge3 * q1[3];
+    double enII = al * q2[1] + be * q2[2] + ge * q2[3];
+    double teII2 = al2 * q2[1] + be2 * q2[2] + ge2 * q2[3];
+    double teII3 = al3 * q2[1] + be3 * q2[2] + ge3 * q2[3];
+    double pI = q1[4], pII = q2[4], rI = q1[0], rII = q2[0];
+    int ipiz = 0;
+    if (pI > pII) {  // the higher pressure on the right
+        const double eno2 = enII, teo22 = teII2, teo23 = teII3, p2 = pII, r2 = rII;
+        const double eno1 = enI, teo12 = teI2, teo13 = teI3, p1 = pI, r1 = rI;
+        enI = -eno2;
+        teI2 = teo22;
+        teI3 = teo23;
+        pI = p2;
+        rI = r2;
+        enII = -eno1;
+        teII2 = teo12;
+        teII3 = teo13;
+        pII = p1;
+        rII = r1;
+        w = -w;
+        ipiz = 1;
+    }
+    double cI = 0.0, cII = 0.0;
+    if (pI != 0.0) cI = std::sqrt(gamma * pI / rI);
+    if (pII != 0.0) cII = std::sqrt(gamma * pII / rII);
+    const double a = std::sqrt(rI * (K.g2 * pII + K.g1 * pI) / 2.0);
+    const double Uud = (pII - pI) / a;
+    const double Urz = -2.0 * cII / K.g1 * (1.0 - std::pow((pI / pII), K.gm));
+    const double Uvk = -2.0 * (cII + cI) / K.g1;
+    const double Udf = enI - enII;
+    int il = 9, ip = 9, rc = 0;
+    double p = 0.0, r = 0.0, te2 = 0.0, te3 = 0.0, en = 0.0, dsl = 0.0, dsp = 0.0, dsc = 0.0;
+    if (Udf < Uvk) {
+        il = -1;
+        ip = -1;
+    } else if ((Udf >= Uvk) && (Udf <= Urz)) {
+        p = pI * std::pow(((Udf - Uvk) / (Urz - Uvk)), (1.0 / K.gm));
+        il = 0;
+        ip = 0;
+    } else if ((Udf > Urz) && (Udf <= Uud)) {
+        rc = o_devtwo(K, enI, pI, rI, enII, pII, rII, p);
+        il = 1;
+        ip = 0;
+    } else if (Udf > Uud) {
+        rc = o_newton(K, enI, pI, rI, enII, pII, rII, p);
+        il = 1;
+        ip = 1;
+    }
+    if (rc) return rc;
+    if (il == 9) return 4;
+    if ((il == 1) && (ip == 1)) {  // two shocks
+        const double aI = std::sqrt(rI * (K.g2 / 2.0 * p + K.g1 / 2.0 * pI));
+        const double aII = std::sqrt(rII * (K.g2 / 2.0 * p + K.g1 / 2.0 * pII));
+        const double u = (aI * enI + aII * enII + pI - pII) / (aI + aII);
+        const double dI = enI - aI / rI;
+        const double dII = enII + aII / rII;
+        dsl = dI;
+        dsp = dII;
+        dsc = u;
+        if (contact) w = u;
+        if (w <= dI) {
+            en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
+        } else if ((w > dI) && (w <= u)) {
+            en = u; r = rI * aI / (aI - rI * (enI - u)); te2 = teI2; te3 = teI3;
+        } else if ((w > u) && (w < dII)) {
+            en = u; r = rII * aII / (aII + rII * (enII - u)); te2 = teII2; te3 = teII3;
+        } else if (w >= dII) {
+            en = enII; p = pII; r = rII; te2 = teII2; te3 = teII3;
+        }
+    }
+    if ((il == 1) && (ip == 0)) {  // left shock, right rarefaction
+        const double aI = std::sqrt(rI * (K.g2 / 2.0 * p + K.g1 / 2.0 * pI));
+        double aII;
+        if (std::fabs(p - pII) < kEps)
+            aII = rII * cII;
+        else
+            aII = K.gm * rII * cII * (1.0 - p / pII) / (1.0 - std::pow((p / pII), K.gm));
+        const double u = (aI * enI + aII * enII + pI - pII) / (aI + aII);
+        const double dI = enI - aI / rI;
+        const double dII = enII + cII;
+        const double ddII = u + cII - K.g1 * (enII - u) / 2.0;
+        dsl = dI;
+        dsp = dII;
+        dsc = u;
+        if (contact) w = u;
+        if (w <= dI) {
+            en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
+        }
+        if ((w > dI) && (w <= u)) {
+            en = u; r = rI * aI / (aI - rI * (enI - u)); te2 = teI2; te3 = teI3;
+        }
+        if ((w > u) && (w <= ddII)) {
+            const double ce = cII - K.g1 / 2.0 * (enII - u);
+            en = u; r = K.ga * p / ce / ce; te2 = teII2; te3 = teII3;
+        }
+        if ((w > ddII) && (w < dII)) {
+            const double ce = -K.g1 / K.g2 * (enII - w) + 2.0 / K.g2 * cII;
+            en = w - ce; p = pII * std::pow((ce / cII), (1.0 / K.gm)); r = K.ga * p / ce / ce;
+            te2 = teII2; te3 = teII3;
+        }
+        if (w >= dII) {
+            en = enII; p = pII; r = rII; te2 = teII2; te3 = teII3;
+        }
+    }
+    if ((il == 0) && (ip == 0)) {  // two rarefactions
+        double aI, aII;
+        if (std::fabs(p - pI) < kEps)
+            aI = rI * cI;
+        else
+            aI = K.gm * rI * cI * (1.0 - p / pI) / (1.0 - std::pow((p / pI), K.gm));
+        if (std::fabs(p - pII) < kEps)
+            aII = rII * cII;
+        else
+            aII = K.gm * rII * cII * (1.0 - p / pII) / (1.0 - std::pow((p / pII), K.gm));
+        const double u = (aI * enI + aII * enII + pI - pII) / (aI + aII);
+        const double dI = enI - cI;
+        const double ddI = u - cI - K.g1 * (enI - u) / 2.0;
+        const double dII = enII + cII;
+        const double ddII = u + cII - K.g1 * (enII - u) / 2.0;
+        dsl = dI;
+        dsp = dII;
+        dsc = u;
+        if (contact) w = u;
+        if (w <= dI) {
+            en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
+        }
+        if ((w > dI) && (w < ddI)) {
+            const double ce = K.g1 / K.g2 * (enI - w) + 2.0 / K.g2 * cI;
+            en = w + ce; p = pI * std::pow((ce / cI), (1.0 / K.gm)); r = K.ga * p / ce / ce;
+            te2 = teI2; te3 = teI3;
+        }
+        if ((w >= ddI) && (w <= u)) {
+            const double ce = cI + K.g1 / 2.0 * (enI - u);
+            en = u; r = K.ga * p / ce / ce; te2 = teI2; te3 = teI3;
+        }
+        if ((w > u) && (w <= ddII)) {
+            const double ce = cII - K.g1 / 2.0 * (enII - u);
+            en = u; r = K.ga * p / ce / ce; te2 = teII2; te3 = teII3;
+        }
+        if ((w > ddII) && (w < dII)) {
+            const double ce = -K.g1 / K.g2 * (enII - w) + 2.0 / K.g2 * cII;
+            en = w - ce; p = pII * std::pow((ce / cII), (1.0 / K.gm)); r = K.ga * p / ce / ce;
+            te2 = teII2; te3 = teII3;
+        }
+        if (w >= dII) {
+            en = enII; p = pII; r = rII; te2 = teII2; te3 = teII3;
+        }
+    }
+    if ((il == -1) && (ip == -1)) {  // vacuum
+        const double dI = enI - cI;
+        const double ddI = enI + 2.0 / K.g1 * cI;
+        const double dII = enII + cII;
+        const double ddII = enII - 2.0 / K.g1 * cII;
+        dsl = dI;
+        dsp = dII;
+        dsc = (dI + dII) / 2.0;
+        if (contact) w = dsc;
+        if (w <= dI) {
+            en = enI; p = pI; r = rI; te2 = teI2; te3 = teI3;
+        }
+        if ((w > dI) && (w < ddI)) {
+            const double ce = K.g1 / K.g2 * (enI - w) + 2.0 / K.g2 * cI;
+            en = w + ce; p = pI * std::pow((ce / cI), (1.0 / K.gm)); r = K.ga * p / ce / ce;
+            te2 = teI2; te3 = teI3;
+        }
+        if ((w >= ddI) && (w <= ddII)) {
+            en = w; p = 0.0; r = 0.0; te2 = 0.0; te3 = 0.0;
+        }
+        if ((w > ddII) && (w < dII)) {
+            const double ce = -K.g1 / K.g2 * (enII - w) + 2.0 / K.g2 * cII;
+            en = w - ce; p = pII * std::pow((ce / cII), (1.0 / K.gm)); r = K.ga * p / ce / ce;
+            te2 = teII2; te3 = teII3;
+        }
+        if (w >= dII) {
+            en = enII; p = pII; r = rII; te2 = teII2; te3 = teII3;
+        }
+    }
+    if (ipiz == 1) {
+        en = -en;
+        const double dsl1 = dsl, dsp1 = dsp;
+        dsl = -dsp1;
+        dsp = -dsl1;
+        dsc = -dsc;
+        w = -w;
+    }
+    const double uo = al * en + al2 * te2 + al3 * te3;
+    const double vo = be * en + be2 * te2 + be3 * te3;
+    const double wo = ge * en + ge2 * te2 + ge3 * te3;
+    const double eo = p / K.g1 + 0.5 * r * (uo * uo + vo * vo + wo * wo);
+    en = al * uo + be * vo + ge * wo;
+    if (contact) w = en;
+    out[0] = (r * (en - w));
+    out[1] = (r * (en - w) * uo + al * p);
+    out[2] = (r * (en - w) * vo + be * p);
+    out[3] = (r * (en - w) * wo + ge * p);
+    out[4] = ((en - w) * eo + en * p);
+    ds[0] = dsl;
+    ds[1] = dsc;
+    ds[2] = dsp;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
 // Second-order (TVD) reconstruction, Setka_gran_snos.cpp:188-735.
 // Cells on the line AA - A -|- B - BB (AA beyond cells[0], BB beyond
 // cells[1], Init_TVD) at coordinates -dd1-d1, -d1, 0 (face centre), d2,
@@ -996,14 +1297,32 @@ static double o_face(const OMesh* M, const OParams* P, const double* st, const d
     const int contact = (surf == 2 && P->contact_hard) ? 1 : 0;
     const int nk = P->npassive;
     double q[8], kq[2] = {0.0, 0.0}, ds[3];
-    const int rc = o_chlld(method, n, w, L, R, 0, 0, nk, L + 8, R + 8, q, kq, ds, left_ydar, contact, P->gamma);
-    if (rc) *err = 10 + rc;
+    double bn_sum = 0.5 * (n[0] * (L[5] + R[5]) + n[1] * (L[6] + R[6]) + n[2] * (L[7] + R[7]));
+    if (surf == 2 && P->bn_in_p_on_hp) {
+        // Setka_physics.cpp:2378-2409: magnetic pressure into p, B = 0, the exact
+        // gas-dynamic solver; no B or passive flux, PdivB = 0 (:2467-2470)
+        double q1[5] = {L[0], L[1], L[2], L[3], L[4]}, q2[5] = {R[0], R[1], R[2], R[3], R[4]};
+        q1[4] += (L[5] * L[5] + L[6] * L[6] + L[7] * L[7]) / (8.0 * kPi);
+        q2[4] += (R[5] * R[5] + R[6] * R[6] + R[7] * R[7]) / (8.0 * kPi);
+        double gd[5], gds[3];
+        const int rcg = o_godunov(n, w, q1, q2, P->contact_hard, P->gamma, gd, gds);
+        if (rcg) *err = 14 + rcg;
+        for (int k = 0; k < 5; ++k) q[k] = gd[k];
+        q[5] = q[6] = q[7] = 0.0;
+        ds[0] = gds[0];
+        ds[1] = gds[1];
+        ds[2] = gds[2];
+        bn_sum = 0.0;
+    } else {
+        const int rc = o_chlld(method, n, w, L, R, 0, 0, nk, L + 8, R + 8, q, kq, ds, left_ydar, contact, P->gamma);
+        if (rc) *err = 10 + rc;
+    }
     if (type == 0) {
         const double dnt = P->KFL * dist / (mx(std::fabs(ds[0]), std::fabs(ds[2])) + std::fabs(w));
         if (dnt < loc_time) loc_time = mn(loc_time, dnt);
     }
     for (int k = 0; k < 8; ++k) out[k] = q[k] * area;
-    out[8] = 0.5 * (n[0] * (L[5] + R[5]) + n[1] * (L[6] + R[6]) + n[2] * (L[7] + R[7])) * area;
+    out[8] = bn_sum * area;
     out[9] = kq[0] * area;
     out[10] = kq[1] * area;
     return loc_time;
@@ -1426,6 +1745,11 @@ void oracle_chlld_batch(int64_t n, const int* n_state, const double* nrm, const 
         rc[i] = o_chlld(n_state[i], nrm + 3 * i, w[i], q1 + 8 * i, q2 + 8 * i, 0, 0, 0, &dummy, &dummy,
                         qout + 8 * i, &dummy, ds + 3 * i, 0, 0, gamma);
     }
+}
+
+int oracle_godunov(const double* nrm, double w, const double* q1, const double* q2, int contact, double gamma,
+                   double* out, double* ds) {
+    return o_godunov(nrm, w, q1, q2, contact, gamma, out, ds);
 }
 
 int oracle_num_threads(void) {

@@ -53,7 +53,7 @@ class OParams(ctypes.Structure):
         ("move", ctypes.c_int32), ("soft_fixups", ctypes.c_int32), ("method_policy", ctypes.c_int32),
         ("npassive", ctypes.c_int32), ("nh", ctypes.c_int32), ("TS_hard", ctypes.c_int32),
         ("contact_hard", ctypes.c_int32), ("tvd", ctypes.c_int32), ("snos_on_hp", ctypes.c_int32),
-        ("pad", ctypes.c_int32 * 2),
+        ("bn_in_p_on_hp", ctypes.c_int32), ("pad", ctypes.c_int32),
     ]
 
 
@@ -95,6 +95,8 @@ def oracle():
                                           ctypes.c_double, ctypes.c_double]
         lib.oracle_num_threads.restype = ctypes.c_int
         lib.oracle_tvd_neighbours.argtypes = [ctypes.POINTER(OMesh), D, I32]
+        lib.oracle_godunov.argtypes = [D, ctypes.c_double, D, D, ctypes.c_int, ctypes.c_double, D, D]
+        lib.oracle_godunov.restype = ctypes.c_int
         lib.oracle_face_states.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D, D, I8]
         _oracle = lib
     return _oracle
@@ -117,10 +119,50 @@ def ref():
         lib.titan_ref_chlld.argtypes = [ctypes.c_int, D, ctypes.c_double, D, D, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, D, D, D, D, D, ctypes.c_int, ctypes.c_int]
         lib.titan_ref_set_gamma.argtypes = [ctypes.c_double]
+        lib.titan_ref_godunov.argtypes = [D, ctypes.c_double, D, D, ctypes.c_int, D, D]
         lib.titan_ref_plasma_components_1.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                       ctypes.c_double, D]
         _ref = lib
     return _ref
+
+
+def godunov(lib_kind: str, nrm, w, q1, q2, contact=0, gamma=5.0 / 3.0):
+    """One exact Godunov solve (Phys_param::Godunov_Solver_Alexashov) through the
+    oracle ('oracle') or the reference ('ref'): (flux[5], ds[3] = dsl, dsc, dsr, rc)."""
+    nrm = np.ascontiguousarray(nrm, dtype=np.float64)
+    qa = np.zeros(8)
+    qb = np.zeros(8)
+    qa[:len(q1)] = q1
+    qb[:len(q2)] = q2
+    out, ds = np.zeros(5), np.zeros(3)
+    if lib_kind == "ref":
+        r = ref()
+        r.titan_ref_set_gamma(gamma)
+        r.titan_ref_godunov(_p(nrm), float(w), _p(qa), _p(qb), int(contact), _p(out), _p(ds))
+        rc = 0
+    else:
+        rc = oracle().oracle_godunov(_p(nrm), float(w), _p(qa), _p(qb), int(contact), float(gamma), _p(out), _p(ds))
+    return out, ds, rc
+
+
+def random_godunov_cases(n: int, seed: int = 0):
+    """Face problems spread over the exact solver's four wave patterns (two
+    shocks, shock + rarefaction, two rarefactions, vacuum), both pressure
+    orders, moving faces: (nrm [n,3], w [n], q1 [n,5], q2 [n,5])."""
+    rng = np.random.default_rng(seed)
+    nrm = rng.standard_normal((n, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    w = 0.2 * rng.standard_normal(n)
+    q1, q2 = np.zeros((n, 5)), np.zeros((n, 5))
+    for q in (q1, q2):
+        q[:, 0] = np.exp(rng.uniform(-3, 1, n))
+        q[:, 4] = np.exp(rng.uniform(-4, 1, n))
+        q[:, 1:4] = 0.5 * rng.standard_normal((n, 3))
+    # relative normal velocity from strongly colliding to strongly separating
+    du = rng.uniform(-12.0, 6.0, n)
+    q1[:, 1:4] += (0.5 * du)[:, None] * nrm
+    q2[:, 1:4] -= (0.5 * du)[:, None] * nrm
+    return nrm, w, q1, q2
 
 
 def chlld(lib_kind: str, n_state, nrm, w, q1, q2, *, null_bn=0, n_disc=0, kl=(), kr=(), left_ydar=0,

@@ -60,6 +60,25 @@ cudaError_t launch_cell_update(const CellArgs& a, int nk, bool move, int src, in
     return cudaErrorInvalidValue;
 }
 
+static __global__ void godunov_batch_kernel(long long n, const double* __restrict__ nrm, const double* __restrict__ w,
+                                            const double* __restrict__ q1, const double* __restrict__ q2,
+                                            const signed char* __restrict__ contact, double gamma,
+                                            double* __restrict__ flux, double* __restrict__ ds, int* __restrict__ rc) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double out[5] = {0, 0, 0, 0, 0}, d[3] = {0, 0, 0};
+    rc[i] = godunov_exact(nrm + 3 * i, w[i], q1 + 5 * i, q2 + 5 * i, contact[i], gamma, out, d);
+    for (int k = 0; k < 5; ++k) flux[5 * i + k] = out[k];
+    for (int k = 0; k < 3; ++k) ds[3 * i + k] = d[k];
+}
+
+cudaError_t launch_godunov_batch(long long n, const double* nrm, const double* w, const double* q1, const double* q2,
+                                 const signed char* contact, double gamma, double* flux, double* ds, int* rc,
+                                 cudaStream_t s) {
+    godunov_batch_kernel<<<blocks_for(n, 128), 128, 0, s>>>(n, nrm, w, q1, q2, contact, gamma, flux, ds, rc);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gather(const double* src, double* dst, const int* perm, int n, int nfields, cudaStream_t s) {
     gather_fields_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, perm, n, nfields);
     return cudaGetLastError();

@@ -44,6 +44,10 @@ cudaError_t launch_riemann_batch_fp32(long long n, const signed char* ns, const 
                                       const double* q1, const double* q2, double* flux, double* ds, int* rc,
                                       int flags, double gamma, cudaStream_t s);
 
+cudaError_t launch_godunov_batch(long long n, const double* nrm, const double* w, const double* q1, const double* q2,
+                                 const signed char* contact, double gamma, double* flux, double* ds, int* rc,
+                                 cudaStream_t s);
+
 cudaError_t launch_mc_trace(const McArgs& a, cudaStream_t s);
 cudaError_t launch_mc_normalise(double* tally, const double* vol, int ncell, cudaStream_t s);
 

@@ -95,6 +95,7 @@ extern "C" int titan_step_noalloc(const titan_dev_mesh* m, const titan_params* p
     }
     if (p->move) return nfail(TITAN_EINVAL, "titan_step_noalloc: stationary meshes only (move = 0)");
     if (p->tvd) return nfail(TITAN_EINVAL, "titan_step_noalloc: first-order faces only (tvd = 0)");
+    if (p->bn_in_p_on_hp) return nfail(TITAN_EINVAL, "titan_step_noalloc: no exact HP solver (bn_in_p_on_hp = 0)");
     if (p->npassive != 0 && p->npassive != 2) return nfail(TITAN_EINVAL, "titan_step_noalloc: npassive must be 0 or 2");
     if (p->flux_precision != 64 && p->flux_precision != 32)
         return nfail(TITAN_EINVAL, "titan_step_noalloc: flux_precision must be 64 or 32");

@@ -22,6 +22,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "godunov.cuh"
 #include "riemann.cuh"
 #include "step_types.h"
 
@@ -527,6 +528,23 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         fl.n_disc = 0;
         fl.left_ydar = (surf == 1 && P.TS_hard);
         fl.contact = (surf == 2 && P.contact_hard);
+        double qd[8], kqd[NK > 0 ? NK : 1], dsl_d, dsr_d, bsum_f = bsum;
+        if (P.bn_in_p_on_hp && surf == 2) {
+            // HP face with the magnetic pressure in p: the exact gas-dynamic
+            // solver (Setka_physics.cpp:2378-2409); no B or passive flux, no PdivB
+            const GodunovFlux gd =
+                godunov_hp_face(n[0], n[1], n[2], w, Ls[0], Ls[1], Ls[2], Ls[3], Ls[4], Ls[5], Ls[6], Ls[7], Rs[0],
+                                Rs[1], Rs[2], Rs[3], Rs[4], Rs[5], Rs[6], Rs[7], P.contact_hard, P.gamma);
+            if (gd.rc) record_error(a.st, 14 + gd.rc, f);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) qd[k] = gd.q[k];
+            qd[5] = qd[6] = qd[7] = 0.0;
+#pragma unroll
+            for (int k = 0; k < NK; ++k) kqd[k] = 0.0;
+            dsl_d = gd.dsl;
+            dsr_d = gd.dsr;
+            bsum_f = 0.0;
+        } else {
         R qL[8], qR[8], kl[NK > 0 ? NK : 1], kr[NK > 0 ? NK : 1], q[8], kq[NK > 0 ? NK : 1], nr[3];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -550,7 +568,6 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         const int rc = riemann_flux<R, NK, kMixed>(method, nr, R(w), qL, qR, kl, kr, q, kq, dsl, dsc, dsr, fl,
                                                     R(P.gamma), &upw, &wvo);
         if (rc) record_error(a.st, 10 + rc, f);
-        double qd[8], kqd[NK > 0 ? NK : 1];
 #pragma unroll
         for (int k = 0; k < 8; ++k) qd[k] = double(q[k]);
 #pragma unroll
@@ -562,9 +579,12 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
             upwind_flux_fp64<NK>(n, double(wvo), L2, R2, L2 + 8, R2 + 8, upw == 1, double(dsl), double(dsr),
                                  fl.null_bn, P.gamma, qd, kqd);
         }
+        dsl_d = double(dsl);
+        dsr_d = double(dsr);
+        }
         if (type == 0) {
             if (!MOVE) dist = a.L1.fd[f];
-            const double dnt = P.KFL * dist / (rmax(fabs(double(dsl)), fabs(double(dsr))) + fabs(w));
+            const double dnt = P.KFL * dist / (rmax(fabs(dsl_d), fabs(dsr_d)) + fabs(w));
             contrib = 10000000.0;
             if (dnt < contrib) contrib = dnt;
         } else {
@@ -574,7 +594,7 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         FT out[L::stride];
 #pragma unroll
         for (int k = 0; k < 8; ++k) out[k] = FT(qd[k] * area);
-        out[8] = FT(bsum * area);
+        out[8] = FT(bsum_f * area);
 #pragma unroll
         for (int k = 0; k < NK; ++k) out[9 + k] = FT(kqd[k] * area);
 #pragma unroll

@@ -27,6 +27,7 @@ struct Params {
     double gamma, KFL, velosity_inf, omega, par_a_2, par_n_H_LISM, par_Kn, beta_switch;
     int move, soft_fixups, method_policy, npassive, nh, TS_hard, contact_hard, src_mode;
     int tvd, snos_on_hp;   // second-order faces (Phys_param::TVD, Snos_on_HP)
+    int bn_in_p_on_hp;     // HP faces: magnetic pressure in p, exact gas-dynamic solver
 };
 
 struct MeshView {

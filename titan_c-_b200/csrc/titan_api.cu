@@ -410,6 +410,7 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     P.src_mode = 0;
     P.tvd = p->tvd;
     P.snos_on_hp = p->snos_on_hp;
+    P.bn_in_p_on_hp = p->bn_in_p_on_hp;
 
     auto bail = [&](int code) {
         titan_destroy(ctx);
@@ -912,6 +913,40 @@ int titan_set_closure(titan_ctx* ctx, const float* params, const float* norm, do
     ctx->closure_ninf = n_inf;
     ctx->closure_lambda = lambda;
     ctx->use_closure = true;
+    return TITAN_OK;
+}
+
+int titan_godunov_batch(int64_t n, const double* nrm, const double* w, const double* q1, const double* q2,
+                        const int8_t* contact, double gamma, double* flux, double* ds, int32_t* rc) {
+    if (n <= 0 || !nrm || !w || !q1 || !q2 || !contact || !flux || !ds || !rc)
+        return fail(TITAN_EINVAL, "titan_godunov_batch: bad argument");
+    double *dn = nullptr, *dw = nullptr, *d1 = nullptr, *d2 = nullptr, *df = nullptr, *dd = nullptr;
+    int8_t* dc = nullptr;
+    int* drc = nullptr;
+    auto release = [&] {
+        void* ps[] = {dn, dw, d1, d2, df, dd, dc, drc};
+        for (void* p : ps)
+            if (p) cudaFree(p);
+    };
+    cudaError_t e = cudaMalloc((void**)&dn, sizeof(double) * 3 * n);
+    if (!e) e = cudaMalloc((void**)&dw, sizeof(double) * n);
+    if (!e) e = cudaMalloc((void**)&d1, sizeof(double) * 5 * n);
+    if (!e) e = cudaMalloc((void**)&d2, sizeof(double) * 5 * n);
+    if (!e) e = cudaMalloc((void**)&df, sizeof(double) * 5 * n);
+    if (!e) e = cudaMalloc((void**)&dd, sizeof(double) * 3 * n);
+    if (!e) e = cudaMalloc((void**)&dc, n);
+    if (!e) e = cudaMalloc((void**)&drc, sizeof(int) * n);
+    if (!e) e = cudaMemcpy(dn, nrm, sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(dw, w, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d1, q1, sizeof(double) * 5 * n, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(d2, q2, sizeof(double) * 5 * n, cudaMemcpyHostToDevice);
+    if (!e) e = cudaMemcpy(dc, contact, n, cudaMemcpyHostToDevice);
+    if (!e) e = launch_godunov_batch(n, dn, dw, d1, d2, reinterpret_cast<const signed char*>(dc), gamma, df, dd, drc, 0);
+    if (!e) e = cudaMemcpy(flux, df, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost);
+    if (!e) e = cudaMemcpy(ds, dd, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost);
+    if (!e) e = cudaMemcpy(rc, drc, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    release();
+    if (e) return fail(TITAN_ECUDA, std::string("titan_godunov_batch: ") + cudaGetErrorString(e));
     return TITAN_OK;
 }
 

@@ -50,7 +50,7 @@ class TitanParams(ctypes.Structure):
         ("move", ctypes.c_int32), ("soft_fixups", ctypes.c_int32), ("method_policy", ctypes.c_int32),
         ("npassive", ctypes.c_int32), ("nh", ctypes.c_int32), ("TS_hard", ctypes.c_int32),
         ("contact_hard", ctypes.c_int32), ("flux_precision", ctypes.c_int32),
-        ("tvd", ctypes.c_int32), ("snos_on_hp", ctypes.c_int32),
+        ("tvd", ctypes.c_int32), ("snos_on_hp", ctypes.c_int32), ("bn_in_p_on_hp", ctypes.c_int32),
     ]
 
 
@@ -119,6 +119,7 @@ SIGNATURES = {
     "titan_mlp_train": ([F32, F32, F32, F32, F32, F32, ctypes.c_int64, ctypes.POINTER(TitanMlpTrainOpts), F32],
                         ctypes.c_int),
     "titan_get_tvd_neighbours": ([ctypes.c_void_p, I32], ctypes.c_int),
+    "titan_godunov_batch": ([ctypes.c_int64, D, D, D, D, I8, ctypes.c_double, D, D, I32], ctypes.c_int),
     "titan_upload_nodes": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_read_cell_parameters": ([ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64, D, D, I32, I32], ctypes.c_int),
     "titan_write_cell_parameters": ([ctypes.c_char_p, ctypes.c_int64, ctypes.c_int32, D, ctypes.c_int64, D],

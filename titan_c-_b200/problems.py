@@ -24,7 +24,7 @@ GAMMA = 5.0 / 3.0
 DEFAULT_PARAMS = dict(
     gamma=GAMMA, KFL=0.4, velosity_inf=-2.54327, omega=2.0 * np.pi, par_a_2=0.102046, par_n_H_LISM=3.0,
     par_Kn=40.0906, beta_switch=0.01, move=0, soft_fixups=1, method_policy=0, npassive=0, nh=0, TS_hard=0,
-    contact_hard=0, flux_precision=64, tvd=0, snos_on_hp=0,
+    contact_hard=0, flux_precision=64, tvd=0, snos_on_hp=0, bn_in_p_on_hp=0,
 )
 
 

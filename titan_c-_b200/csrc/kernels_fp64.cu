@@ -25,40 +25,6 @@ cudaError_t launch_face_flux_fp64(const FaceArgs& a, int nk, bool move, int vari
     return face_flux_dispatch<double, false>(a, nk, move, variant, s);
 }
 
-template <typename FT, int NK, bool MOVE, int BS, int MINB>
-static void cell_update_src(const CellArgs& a, int src, cudaStream_t s) {
-    const unsigned int g = blocks_for(a.M.ncell, BS);
-    if (src == 0) cell_update_kernel<FT, NK, MOVE, 0, BS, MINB><<<g, BS, 0, s>>>(a);
-    else if (src == 1) cell_update_kernel<FT, NK, MOVE, 1, BS, MINB><<<g, BS, 0, s>>>(a);
-    else cell_update_kernel<FT, NK, MOVE, 2, BS, MINB><<<g, BS, 0, s>>>(a);
-}
-
-template <typename FT, int NK, bool MOVE>
-static cudaError_t cell_update_variant(const CellArgs& a, int src, int v, cudaStream_t s) {
-    switch (v) {
-#define TITAN_CELL_CASE(i)                                                                   \
-    case i:                                                                                \
-        cell_update_src<FT, NK, MOVE, kCellVariant[i].block, kCellVariant[i].min_blocks>(a, src, s); \
-        break;
-        TITAN_CELL_CASE(0)
-        TITAN_CELL_CASE(1)
-        TITAN_CELL_CASE(2)
-        TITAN_CELL_CASE(3)
-        TITAN_CELL_CASE(4)
-#undef TITAN_CELL_CASE
-        default:
-            return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_cell_update(const CellArgs& a, int nk, bool move, int src, int variant, cudaStream_t s) {
-    if (nk == 0 && !move) return cell_update_variant<double, 0, false>(a, src, variant, s);
-    if (nk == 0 && move) return cell_update_variant<double, 0, true>(a, src, variant, s);
-    if (nk == 2 && !move) return cell_update_variant<double, 2, false>(a, src, variant, s);
-    if (nk == 2 && move) return cell_update_variant<double, 2, true>(a, src, variant, s);
-    return cudaErrorInvalidValue;
-}
 
 static __global__ void godunov_batch_kernel(long long n, const double* __restrict__ nrm, const double* __restrict__ w,
                                             const double* __restrict__ q1, const double* __restrict__ q2,

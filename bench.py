@@ -9,7 +9,10 @@ wind inside, interstellar inflow outside, seeded lognormal perturbation,
 HLLD where B^2/(8 pi p) > 0.01 else HLLC, prescribed radial node motion (ALE).
 One step = one pass of the plasma loop over every face and cell.
 
-Modes: mixed-mlp (default) — FP32 Riemann flux with FP64 accumulation, dt and
+Modes: coupled — the large configuration's loop: the mixed step with MLP
+sources every step and a Monte-Carlo pass (1e7 particles) every 100 steps
+whose sources the cells outside the closure's training envelope use.
+mixed-mlp (default) — FP32 Riemann flux with FP64 accumulation, dt and
 pressure recovery, and charge-exchange sources from the MLP closure on the
 tensor cores every step; the same run also times the plain all-FP64 step on
 the same mesh and measures the mixed step's error against it after 100 and
@@ -143,8 +146,7 @@ def load_closure(pkg, m, st):
     does not depend on the weights) and output scales of a plausible size."""
     cl = pkg.closure
     if os.path.exists(NET_PATH):
-        d = np.load(NET_PATH)
-        return cl.Closure(float(d["n_inf"]), float(d["lam"]), d["params"], d["norm"]), "trained"
+        return cl.Closure.load(NET_PATH), "trained"
     cc = m["node_xyz"][m["cell_nodes"]].mean(axis=1).T
     X = cl.features(st, cc, 0.18, 0.0)
     norm = cl.make_norm(X, np.ones((1, 5)))
@@ -283,7 +285,7 @@ def run_ours(args, rank, world):
     C = m["cell_nodes"].shape[0]
     F = m["face_nodes"].shape[0]
     flux = 64 if args.mode == "fp64" else 32
-    closure, net_kind = (load_closure(pkg, m, st) if args.mode == "mixed-mlp" else (None, None))
+    closure, net_kind = (load_closure(pkg, m, st) if args.mode in ("mixed-mlp", "coupled") else (None, None))
     step, tuning = make_step(pkg, m, p, st, flux, args.tuning, closure)
     kernels_per_step = (3 if p["move"] else 2) + (1 if closure is not None else 0)
     flux_name = f"face_flux_fp{flux}"
@@ -296,7 +298,23 @@ def run_ours(args, rank, world):
     # warm-up (also captures the CUDA graph)
     step.go(max(args.warmup, 3))
     stream = torch.cuda.ExternalStream(step.stream())
-    ms, clocks = timed_steps(step, args.steps, barrier, stream, dev)
+    coupled = None
+    if args.mode == "coupled":
+        # the large configuration's loop: MLP sources every step, a Monte-Carlo
+        # pass every 100 steps whose sources the out-of-envelope cells use
+        mc = dict(n_H=0.18, u_H=(-2.6, 0.0, 0.0), cp_H=float(np.sqrt(2.0 * (0.06 * 1.3 ** 2 / (5.0 / 3.0)) / 0.06)),
+                  n_particles=10_000_000)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        with ClockSampler(dev) as clk:
+            ev0.record(stream)
+            coupled = pkg.closure.run_coupled(step, closure, args.steps, mc_every=100, **mc)
+            ev1.record(stream)
+            barrier()
+        ms, clocks = ev0.elapsed_time(ev1), clk.summary()
+    else:
+        ms, clocks = timed_steps(step, args.steps, barrier, stream, dev)
 
     # dominant kernel: per-launch device time with events on the library stream
     step.set_profiling(True)
@@ -324,7 +342,7 @@ def run_ours(args, rank, world):
 
     # the plain all-FP64 step on the same mesh, and the mixed step's error against it
     plain = None
-    if args.mode == "mixed-mlp":
+    if args.mode in ("mixed-mlp", "coupled"):
         s64, tun64 = make_step(pkg, m, p, st, 64, args.tuning)
         s64.go(max(args.warmup, 3))
         ms64, clk64 = timed_steps(s64, args.steps, barrier, torch.cuda.ExternalStream(s64.stream()), dev)
@@ -346,9 +364,12 @@ def run_ours(args, rank, world):
     hbm, src = peaks()
     bytes_launch = face_flux_bytes(m, bool(p["move"]), flux == 32)
     achieved = bytes_launch / (k_avg / 1e3) / 1e9
-    dtype = {"fp64": "f64", "fp32": "f32-flux/f64-update", "mixed-mlp": "f32-flux/f64-update, bf16 MLP"}[args.mode]
+    dtype = {"fp64": "f64", "fp32": "f32-flux/f64-update", "mixed-mlp": "f32-flux/f64-update, bf16 MLP",
+             "coupled": "f32-flux/f64-update, bf16 MLP, f64 Monte-Carlo"}[args.mode]
     what = {"fp64": "FP64 flux", "fp32": "FP32 flux, FP64 accumulation",
-            "mixed-mlp": "FP32 flux, FP64 accumulation, MLP charge-exchange sources every step"}[args.mode]
+            "mixed-mlp": "FP32 flux, FP64 accumulation, MLP charge-exchange sources every step",
+            "coupled": "FP32 flux, FP64 accumulation, MLP sources every step, Monte-Carlo (1e7 particles) "
+                       "fallback for out-of-envelope cells every 100 steps"}[args.mode]
     traffic = TRAFFIC.get((flux_name, C))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -375,6 +396,10 @@ def run_ours(args, rank, world):
         mlp_ms = kt["closure_mlp"][0] / kt["closure_mlp"][1]
         flops = 2.0 * C * (16 * 128 + 3 * 128 * 128 + 128 * 16)
         tf_peak, tf_src = peak_tflops()
+        if coupled is not None:
+            line["coupled"] = {"mc_passes": coupled["mc_passes"], "mc_every": 100,
+                               "cells_outside_envelope": coupled["outside_last_step"]}
+            line["gpu_launches"] = args.steps * kernels_per_step + 2 * coupled["mc_passes"]
         line["closure"] = {"network": net_kind, "kernel": "closure_mlp (tcgen05, TMEM accumulators)",
                            "avg_launch_ms": mlp_ms, "flops_per_launch": flops,
                            "tflops": flops / (mlp_ms / 1e3) / 1e12, "tensor_peak_tflops": tf_peak,
@@ -441,7 +466,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nq", type=int, default=96)
     ap.add_argument("--nlayer", type=int, default=40)
-    ap.add_argument("--mode", default="mixed-mlp", choices=["mixed-mlp", "fp64", "fp32"])
+    ap.add_argument("--mode", default="mixed-mlp", choices=["mixed-mlp", "fp64", "fp32", "coupled"])
     ap.add_argument("--no-error-study", dest="error_study", action="store_false")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--tuning", default="auto", help="auto, or 'face_variant,cell_variant'")

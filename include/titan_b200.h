@@ -278,6 +278,16 @@ int titan_mlp_train(float* params, const float* norm, const float* X, const floa
  * cold-model neutral density proxy of the features. */
 int titan_set_closure(titan_ctx* ctx, const float* params, const float* norm, double n_inf, double lambda);
 
+/* Training envelope of an installed closure and the sources it falls back
+ * on: a cell whose features (closure.h) leave [lo, hi] (8 floats each) takes
+ * its sources from src [4][ncell] (original numbering; m_x, m_y, m_z, E; the
+ * last Monte-Carlo pass, titan_mc_sources rows 1-4) instead of the network.
+ * src NULL keeps the previous table (none: the network everywhere); lo NULL
+ * removes envelope and table. titan_closure_outside returns how many cells
+ * were outside the envelope in the last step. */
+int titan_set_closure_fallback(titan_ctx* ctx, const float* lo, const float* hi, const double* src);
+int titan_closure_outside(titan_ctx* ctx, int64_t* n_outside);
+
 /* Launch-shape autotuner (no reference counterpart: the reference's OpenMP
  * loops have no launch shapes). Times every face-flux variant (threads per
  * block x minimum resident blocks per SM) and every cell-update shape on

@@ -158,3 +158,59 @@ def test_trained_closure_is_within_monte_carlo_noise(titan):
     stale = l1(snaps[2][1], mean)
     print(f"closure {err:.3e}  one-seed noise {noise:.3e}  previous snapshot's sources {stale:.3e}")
     assert err < noise
+
+
+def test_cells_outside_the_training_envelope_take_the_fallback_sources(titan):
+    """With an envelope that cuts the shell between two layers, the outer
+    cells take the fallback table (a Monte-Carlo pass's sources) exactly, the
+    inner ones the network, and the library counts the outer ones."""
+    m, p, g = _shell_run(titan, 0)
+    g.go(3)
+    st0 = g.download_state()
+    dt0, t0 = g.dt, g.t
+    cc = g.geometry()["cell_center"].T
+    r = np.linalg.norm(cc, axis=0)
+    logs = np.sort(np.unique(np.round(np.log(r), 2)))   # one value per radial layer
+    k = len(logs) // 2
+    cut = 0.5 * (logs[k] + logs[k + 1])
+    out_mask = np.log(r) > cut
+    assert 0 < out_mask.sum() < len(r)
+    c, _, _ = _rand_problem(titan, 10, seed=4)
+    c.norm[:16] = np.concatenate([np.zeros(8), np.ones(8)])
+    c.norm[16:] = 1e-3
+    lo = np.full(8, -3e38, np.float32)
+    hi = np.full(8, 3e38, np.float32)
+    hi[4] = cut
+    c.envelope = (lo, hi)
+    c.margined_envelope = lambda rel=0.0: (lo, hi)   # the cut exactly between two layers
+    rng = np.random.default_rng(8)
+    F = np.zeros((5, len(r)))
+    F[1:5] = 1e-4 * rng.standard_normal((4, len(r))) * st0[0]
+    S = c.predict(st0, cc)
+    S[1:5, out_mask] = F[1:5, out_mask]
+
+    def one_step(setup):
+        g.upload_state(st0)
+        g.dt, g.t = dt0, t0
+        setup()
+        g.go(1)
+        return g.download_state()
+
+    plain = one_step(lambda: None)
+
+    def with_closure():
+        c.install(g)
+        c.set_fallback(g, F)
+
+    a = one_step(with_closure)
+    n_out = titan.closure.Closure.outside(g)
+    c.uninstall(g)
+    b = one_step(lambda: g.set_sources(np.ascontiguousarray(S[1:5])))
+    g.close()
+    assert n_out == int(out_mask.sum())
+    for k in (1, 2, 3, 4):
+        da, db = a[k] - plain[k], b[k] - plain[k]
+        # outer cells: the fallback sources exactly, so identical updates
+        np.testing.assert_allclose(da[out_mask], db[out_mask], rtol=1e-12, atol=1e-300)
+        rel = np.linalg.norm(da - db) / np.linalg.norm(db)
+        assert rel < 2e-2, (k, rel)

@@ -142,11 +142,45 @@ class Closure:
     """A trained (or initial) network with its normalisation and proxy constants."""
 
     def __init__(self, n_inf: float, lam: float, params: np.ndarray | None = None,
-                 norm: np.ndarray | None = None, seed: int = 0):
+                 norm: np.ndarray | None = None, seed: int = 0, envelope=None):
         self.n_inf, self.lam = float(n_inf), float(lam)
         self.params = _f32(init_params(seed) if params is None else params)
         self.norm = None if norm is None else _f32(norm)
+        self.envelope = None if envelope is None else (_f32(envelope[0]), _f32(envelope[1]))
         self._lib = N.lib()
+
+    @classmethod
+    def load(cls, path: str) -> "Closure":
+        """A network saved by train_closure.py (params, norm, proxy, training envelope)."""
+        d = np.load(path)
+        env = (d["envelope_lo"], d["envelope_hi"]) if "envelope_lo" in d else None
+        return cls(float(d["n_inf"]), float(d["lam"]), d["params"], d["norm"], envelope=env)
+
+    def set_fallback(self, step, mc_sources: np.ndarray | None) -> None:
+        """Cells outside the training envelope take mc_sources[1:5] (a titan_mc_sources
+        result, [5][ncell]) instead of the network; None keeps the previous table."""
+        if self.envelope is None:
+            raise ValueError("this closure has no training envelope")
+        lo, hi = self.margined_envelope()
+        src = None if mc_sources is None else np.ascontiguousarray(mc_sources[1:5], dtype=np.float64)
+        N.check(self._lib.titan_set_closure_fallback(step.ctx, N.ptr(lo, N.F32), N.ptr(hi, N.F32), N.ptr(src)))
+
+    def margined_envelope(self, rel: float = 0.01):
+        """The training envelope widened by `rel` of each feature's range plus
+        1e-3 (1 + |bound|): the kernel forms features in FP32 with fast
+        logarithms, and a feature that was constant in training (zero range,
+        e.g. a flat proxy) must not push every cell outside."""
+        lo = self.envelope[0].astype(np.float64)
+        hi = self.envelope[1].astype(np.float64)
+        w = hi - lo
+        return (_f32(lo - rel * w - 1e-3 * (1.0 + np.abs(lo))), _f32(hi + rel * w + 1e-3 * (1.0 + np.abs(hi))))
+
+    @staticmethod
+    def outside(step) -> int:
+        """Cells outside the training envelope in the last step."""
+        v = ctypes.c_int64(0)
+        N.check(N.lib().titan_closure_outside(step.ctx, ctypes.byref(v)))
+        return int(v.value)
 
     # -- training -------------------------------------------------------------
     def fit(self, X: np.ndarray, T: np.ndarray, epochs: int = 20, batch: int = 4096, lr: float = 2e-3,
@@ -208,3 +242,21 @@ class Closure:
     @staticmethod
     def uninstall(step) -> None:
         N.check(N.lib().titan_set_closure(step.ctx, None, None, 0.0, 0.0))
+
+
+def run_coupled(step, net: Closure, steps: int, mc_every: int = 100, **mc) -> dict:
+    """The coupled loop of the large configuration: MLP sources every step,
+    and every `mc_every` steps a Monte-Carlo pass through the current plasma
+    whose sources the cells outside the training envelope use until the next
+    pass. mc: the keyword arguments of PlasmaStep.mc_sources."""
+    net.install(step)
+    done, passes, outside = 0, 0, []
+    while done < steps:
+        out, _ = step.mc_sources(seed=passes + 1, **mc)
+        net.set_fallback(step, out)
+        passes += 1
+        k = min(mc_every, steps - done)
+        step.go(k)
+        done += k
+        outside.append(Closure.outside(step))
+    return {"steps": done, "mc_passes": passes, "outside_last_step": outside}

@@ -52,6 +52,13 @@ struct MlpArgs {
     double* src;           // [4][ncell] m_x, m_y, m_z, E
     double nH_inf, lambda; // cold-model proxy
     int* error;
+    // training envelope (sources mode; env_lo null: none): a cell whose
+    // features leave [env_lo, env_hi] takes fallback[4][ncell] as its sources
+    // (the last Monte-Carlo pass) and is counted in *n_outside
+    const float* env_lo;
+    const float* env_hi;
+    const double* fallback;
+    unsigned long long* n_outside;
 };
 
 // log of the cold-model neutral density n_inf exp(-lambda theta / (r sin theta)),

@@ -127,6 +127,7 @@ struct alignas(128) Smem {
     __nv_bfloat16 a[kGroups][kTile * kHid];    // activations M=128 x K=128; the input
                                                // tile (K=16) aliases its first 4 KB
     float fmean[kIn], fistd[kIn];
+    float env_lo[kIn], env_hi[kIn];
     uint64_t mbar[kGroups];
     uint32_t tmem;
     int abort[kGroups];  // written by the group's own threads before its barrier, read after it
@@ -204,6 +205,8 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
         if (tid < kIn) {
             S.fmean[tid] = args.net.fmean[tid];
             S.fistd[tid] = args.net.fistd[tid];
+            S.env_lo[tid] = args.env_lo ? args.env_lo[tid] : -3.0e38f;
+            S.env_hi[tid] = args.env_lo ? args.env_hi[tid] : 3.0e38f;
         }
     }
     if (tid == 0) {
@@ -240,15 +243,19 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
         const bool valid = cell < args.n;
         // ---- input features -> input tile (bf16; k = 8 carries 1 for the bias, 9..15 zero)
         float f[kIn];
+        bool outside = false;
         if (MODE == kModeRaw) {
 #pragma unroll
             for (int k = 0; k < kIn; ++k) f[k] = valid ? args.x[(size_t)cell * kIn + k] : 0.0f;
         } else {
-            if (valid)
+            if (valid) {
                 cell_features(args, cell, f);
-            else
+#pragma unroll
+                for (int k = 0; k < kIn; ++k) outside |= !(f[k] >= S.env_lo[k] && f[k] <= S.env_hi[k]);
+            } else {
 #pragma unroll
                 for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
+            }
         }
         {
             uint32_t packed[kIn / 2];
@@ -327,9 +334,17 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
             if (MODE == kModeRaw) {
 #pragma unroll
                 for (int k = 0; k < kOut; ++k) args.y[(size_t)cell * kOut + k] = y[k];
+            } else if (outside && args.fallback) {
+                // outside the training envelope: the last Monte-Carlo sources
+#pragma unroll
+                for (int k = 0; k < 4; ++k) args.src[k * args.ncell + cell] = args.fallback[k * args.ncell + cell];
             } else {
                 write_sources(args, cell, y);
             }
+        }
+        if (MODE == kModeSources && args.n_outside) {
+            const unsigned int bal = __ballot_sync(0xffffffffu, valid && outside);
+            if ((threadIdx.x & 31) == 0 && bal) atomicAdd(args.n_outside, (unsigned long long)__popc(bal));
         }
         fence_before();
         group_sync(g);

@@ -105,6 +105,9 @@ struct titan_ctx {
 
     ClosureDev closure;        // learned sources (titan_set_closure)
     bool use_closure = false;
+    float* d_env = nullptr;    // [2][8] training envelope (titan_set_closure_fallback)
+    double* d_fallback = nullptr;       // [4][ncell] fallback sources, renumbered
+    unsigned long long* d_n_outside = nullptr;
     double closure_ninf = 0.0, closure_lambda = 0.0;
     int sm_count = 148;
 
@@ -202,6 +205,14 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
         ma.nH_inf = ctx->closure_ninf;
         ma.lambda = ctx->closure_lambda;
         ma.error = ctx->closure.error;
+        ma.env_lo = ctx->d_env;
+        ma.env_hi = ctx->d_env ? ctx->d_env + kIn : nullptr;
+        ma.fallback = ctx->d_fallback;
+        ma.n_outside = ctx->d_n_outside;
+        if (ctx->d_n_outside) {
+            e = cudaMemsetAsync(ctx->d_n_outside, 0, sizeof(unsigned long long), ctx->stream);
+            if (e) return e;
+        }
         e = timed(ctx, "closure_mlp", [&] { return launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->stream); });
         if (e) return e;
     }
@@ -357,7 +368,8 @@ int titan_destroy(titan_ctx* ctx) {
                     ctx->d_face_nodes, ctx->d_face_type, ctx->d_face_surf, ctx->d_face_method, ctx->d_bc_vals,
                     ctx->d_cell_faces, ctx->d_cell_nodes, ctx->d_cell_type, ctx->d_cell_tvd, ctx->d_node_amp,
                     ctx->d_node_phase, ctx->d_state[0], ctx->d_state[1], ctx->d_flux, ctx->d_hfl, ctx->d_src,
-                    ctx->d_stage, ctx->d_status, ctx->d_cell_fmap, ctx->d_face_aa, ctx->d_face_bb};
+                    ctx->d_stage, ctx->d_status, ctx->d_cell_fmap, ctx->d_face_aa, ctx->d_face_bb,
+                    ctx->d_env, ctx->d_fallback, ctx->d_n_outside};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     // without node motion layer[1] aliases layer[0]: free it once
@@ -947,6 +959,50 @@ int titan_godunov_batch(int64_t n, const double* nrm, const double* w, const dou
     if (!e) e = cudaMemcpy(rc, drc, sizeof(int) * n, cudaMemcpyDeviceToHost);
     release();
     if (e) return fail(TITAN_ECUDA, std::string("titan_godunov_batch: ") + cudaGetErrorString(e));
+    return TITAN_OK;
+}
+
+int titan_set_closure_fallback(titan_ctx* ctx, const float* lo, const float* hi, const double* src) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    if ((lo == nullptr) != (hi == nullptr)) return fail(TITAN_EINVAL, "lo and hi go together");
+    drop_graph(ctx);
+    if (!lo) {
+        void* ps[] = {ctx->d_env, ctx->d_fallback, ctx->d_n_outside};
+        for (void* p : ps)
+            if (p) cudaFree(p);
+        ctx->d_env = nullptr;
+        ctx->d_fallback = nullptr;
+        ctx->d_n_outside = nullptr;
+        return TITAN_OK;
+    }
+    const int64_t nc = ctx->ncell;
+    int64_t dummy = 0;
+    if (!ctx->d_env) CK(dalloc(&ctx->d_env, 2 * kIn, &dummy));
+    if (!ctx->d_n_outside) {
+        CK(dalloc(&ctx->d_n_outside, 1, &dummy));
+        CK(cudaMemsetAsync(ctx->d_n_outside, 0, sizeof(unsigned long long), ctx->stream));
+    }
+    float env[2 * kIn];
+    for (int k = 0; k < kIn; ++k) {
+        env[k] = lo[k];
+        env[kIn + k] = hi[k];
+    }
+    CK(cudaMemcpyAsync(ctx->d_env, env, sizeof(env), cudaMemcpyHostToDevice, ctx->stream));
+    if (src) {
+        if (!ctx->d_fallback) CK(dalloc(&ctx->d_fallback, (size_t)4 * nc, &dummy));
+        CK(cudaMemcpyAsync(ctx->d_stage, src, sizeof(double) * 4 * nc, cudaMemcpyHostToDevice, ctx->stream));
+        CK(launch_gather(ctx->d_stage, ctx->d_fallback, ctx->d_cell_n2o, (int)nc, 4, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TITAN_OK;
+}
+
+int titan_closure_outside(titan_ctx* ctx, int64_t* n_outside) {
+    if (!ctx || !n_outside) return fail(TITAN_EINVAL, "null argument");
+    unsigned long long v = 0;
+    if (ctx->d_n_outside)
+        CK(cudaMemcpy(&v, ctx->d_n_outside, sizeof(v), cudaMemcpyDeviceToHost));
+    *n_outside = (int64_t)v;
     return TITAN_OK;
 }
 

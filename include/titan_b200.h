@@ -223,7 +223,10 @@ int titan_godunov_batch(int64_t n, const double* nrm, const double* w, const dou
  * Maxwellian exp(-|v - u_H|^2 / cp_H^2) of density n_H, in proportion to each
  * face's inflow flux. out [5][ncell], original numbering: n_H, then the plasma
  * momentum (3) and energy sources per unit time and volume (the plasma mass
- * source of charge exchange is identically zero). */
+ * source of charge exchange is identically zero). out NULL keeps the result on
+ * the device only (for titan_closure_fallback_from_mc). The inflow split, the
+ * tracing and the tallies all run on the device; a pass is reproducible for a
+ * seed up to the order of the floating-point tally additions. */
 typedef struct titan_mc_params {
     double n_H;
     double u_H[3];
@@ -286,6 +289,11 @@ int titan_set_closure(titan_ctx* ctx, const float* params, const float* norm, do
  * removes envelope and table. titan_closure_outside returns how many cells
  * were outside the envelope in the last step. */
 int titan_set_closure_fallback(titan_ctx* ctx, const float* lo, const float* hi, const double* src);
+
+/* The fallback table of titan_set_closure_fallback from the last
+ * titan_mc_sources pass of this context (its rows 1-4), copied on the device.
+ * Needs an envelope (titan_set_closure_fallback with lo, hi) and a pass. */
+int titan_closure_fallback_from_mc(titan_ctx* ctx);
 int titan_closure_outside(titan_ctx* ctx, int64_t* n_outside);
 
 /* Launch-shape autotuner (no reference counterpart: the reference's OpenMP

@@ -214,3 +214,51 @@ def test_cells_outside_the_training_envelope_take_the_fallback_sources(titan):
         np.testing.assert_allclose(da[out_mask], db[out_mask], rtol=1e-12, atol=1e-300)
         rel = np.linalg.norm(da - db) / np.linalg.norm(db)
         assert rel < 2e-2, (k, rel)
+
+
+def test_fallback_from_a_device_pass_equals_the_host_table(titan):
+    """titan_closure_fallback_from_mc (the pass's sources copied on the device)
+    gives the same step as the same pass downloaded and handed back through
+    titan_set_closure_fallback; with every cell outside the envelope, the
+    step's sources are the pass's exactly (up to the order of the tallies'
+    atomic additions)."""
+    m, p, g = _shell_run(titan, 0, nq=8, nlayer=10)
+    g.go(5)
+    st0 = g.download_state()
+    dt0, t0 = g.dt, g.t
+    kw = dict(n_H=0.18, u_H=(-2.6, 0.0, 0.0), cp_H=1.424, n_particles=300_000, seed=5)
+    c, _, _ = _rand_problem(titan, 10, seed=2)
+    lo = np.full(8, 1e30, np.float32)     # an empty envelope: every cell outside
+    hi = np.full(8, -1e30, np.float32)
+    c.envelope = (lo, hi)
+    c.margined_envelope = lambda rel=0.0: (lo, hi)
+
+    def one_step(setup):
+        g.upload_state(st0)
+        g.dt, g.t = dt0, t0
+        setup()
+        g.go(1)
+        return g.download_state()
+
+    host, info = g.mc_sources(**kw)
+    assert info["lost"] == 0 and np.abs(host[1:5]).max() > 0
+
+    def via_host():
+        c.install(g)
+        c.set_fallback(g, host)
+
+    a = one_step(via_host)
+    assert titan.closure.Closure.outside(g) == g.ncell
+    c.uninstall(g)
+
+    def via_device():
+        c.install(g)
+        c.set_fallback(g, None)
+        g.mc_pass(**kw)
+        c.fallback_from_mc(g)
+
+    b = one_step(via_device)
+    c.uninstall(g)
+    g.close()
+    for k in range(8):
+        np.testing.assert_allclose(b[k], a[k], rtol=1e-9, atol=1e-13 * np.abs(a[k]).max())

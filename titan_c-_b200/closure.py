@@ -165,6 +165,10 @@ class Closure:
         src = None if mc_sources is None else np.ascontiguousarray(mc_sources[1:5], dtype=np.float64)
         N.check(self._lib.titan_set_closure_fallback(step.ctx, N.ptr(lo, N.F32), N.ptr(hi, N.F32), N.ptr(src)))
 
+    def fallback_from_mc(self, step) -> None:
+        """The fallback table from the step's last Monte-Carlo pass, on the device."""
+        N.check(self._lib.titan_closure_fallback_from_mc(step.ctx))
+
     def margined_envelope(self, rel: float = 0.01):
         """The training envelope widened by `rel` of each feature's range plus
         1e-3 (1 + |bound|): the kernel forms features in FP32 with fast
@@ -250,10 +254,11 @@ def run_coupled(step, net: Closure, steps: int, mc_every: int = 100, **mc) -> di
     whose sources the cells outside the training envelope use until the next
     pass. mc: the keyword arguments of PlasmaStep.mc_sources."""
     net.install(step)
+    net.set_fallback(step, None)  # the envelope; the table comes from each pass
     done, passes, outside = 0, 0, []
     while done < steps:
-        out, _ = step.mc_sources(seed=passes + 1, **mc)
-        net.set_fallback(step, out)
+        step.mc_pass(seed=passes + 1, **mc)
+        net.fallback_from_mc(step)
         passes += 1
         k = min(mc_every, steps - done)
         step.go(k)

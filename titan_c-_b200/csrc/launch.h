@@ -48,9 +48,6 @@ cudaError_t launch_godunov_batch(long long n, const double* nrm, const double* w
                                  const signed char* contact, double gamma, double* flux, double* ds, int* rc,
                                  cudaStream_t s);
 
-cudaError_t launch_mc_trace(const McArgs& a, cudaStream_t s);
-cudaError_t launch_mc_normalise(double* tally, const double* vol, int ncell, cudaStream_t s);
-
 inline unsigned int blocks_for(long long n, int bs) { return (unsigned int)((n + bs - 1) / bs); }
 
 }  // namespace titan

@@ -1,0 +1,53 @@
+// Monte-Carlo neutral tracing (mc_neutral.cu): arguments, the per-cell record
+// the tracer reads, and the launchers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "step_types.h"
+
+namespace titan {
+
+struct McArgs {
+    MeshView M;
+    Params P;
+    Layer L;                  // current geometry (face centres / normals, cell volumes)
+    const double* state;      // [ns][ncell]
+    const double* inflow_cdf; // [nface] share of the inflow through faces 0..f, last = 1
+    long long nparticles;
+    double mu;                // weight: inflow rate per particle
+    double nH, uH0, uH1, uH2, cpH;
+    unsigned face_types;      // bit t set: faces of type t let neutrals in
+    unsigned long long seed;
+    int max_cells;
+    double* tally;            // [5][ncell]: sum mu*t, sum mu*dv (3), sum mu*d(v^2)/2
+    unsigned long long* lost;
+};
+
+// One cell's tracing record, built once per Monte-Carlo pass: the six face
+// planes (outward normal, normal . face centre), the neighbour across each
+// face (-1 on the boundary), and the proton fluid the neutrals exchange with.
+// One 256-byte record per crossing replaces three dependent lookups (cell ->
+// faces -> face geometry and neighbour).
+struct alignas(16) McCell {
+    double plane[6][4];  // n0, n1, n2, d
+    int nbr[6];
+    double rho_th, cp;
+    double V[3];
+};
+static_assert(sizeof(McCell) == 256, "McCell is one 256-byte record");
+
+// Faces per block of the inflow scan, and the block-sum buffer it needs.
+constexpr int kMcScanChunk = 4096;
+inline int mc_scan_blocks(long long nface) { return (int)((nface + kMcScanChunk - 1) / kMcScanChunk); }
+
+// cdf[f] = (inflow through faces 0..f) / total, total = *total_out: the flux of
+// the drifting Maxwellian (nH, uH, cpH) through the inward normal of every face
+// whose type is in a.face_types, times its area. The sums run in a fixed order,
+// so a pass is reproducible. block_sums holds mc_scan_blocks(nface) doubles.
+cudaError_t launch_mc_inflow_cdf(const McArgs& a, double* cdf, double* block_sums, double* total_out,
+                                 cudaStream_t s);
+cudaError_t launch_mc_pack(const McArgs& a, McCell* cells, cudaStream_t s);
+cudaError_t launch_mc_trace_cells(const McArgs& a, const McCell* cells, cudaStream_t s);
+cudaError_t launch_mc_normalise(double* tally, const double* vol, int ncell, cudaStream_t s);
+
+}  // namespace titan

@@ -22,6 +22,10 @@
 // per unit time / N, so sum(mu * time in cell) / V is the density.
 // Random numbers: a counter-based generator (SplitMix64 finaliser over seed,
 // particle id and draw counter), so a run is reproducible for any launch shape.
+//
+// A pass on the device: the inflow CDF over all faces (a deterministic scan),
+// one 256-byte tracing record per cell (McCell), one thread per neutral over
+// those records, and the division of the tallies by the cell volumes.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -31,6 +35,7 @@
 
 #include "../../include/titan_b200.h"
 #include "launch.h"
+#include "mc.h"
 #include "step_kernels.cuh"
 
 namespace titan {
@@ -123,15 +128,130 @@ __device__ void change_velocity(Rng& rng, double a2, double cp, const double U[3
     W[2] = v3;
 }
 
-__global__ void __launch_bounds__(128) trace_kernel(Args a) {
+// ---- inflow CDF over all faces, summed in a fixed order ----
+
+constexpr double kSqrtPiFull = 1.7724538509055160273;  // sqrt(pi)
+
+// Neutral inflow through face f per unit time: the flux of the drifting
+// Maxwellian through the inward normal, n [cp e^{-s^2} / (2 sqrt(pi)) + u_n (1 + erf s) / 2]
+// with s = u_n / cp, times the face area; 0 for faces that let no neutrals in.
+__device__ __forceinline__ double inflow_weight(const Args& a, int f) {
+    const int t = a.M.face_type[f];
+    if (t <= 0 || t > 31 || !((a.face_types >> t) & 1u)) return 0.0;
+    const int nf = a.M.nface;
+    const double un = -(a.uH0 * a.L.fn[f] + a.uH1 * a.L.fn[nf + f] + a.uH2 * a.L.fn[2 * nf + f]);
+    const double sr = un / a.cpH;
+    const double flux = a.nH * (a.cpH * exp(-sr * sr) / (2.0 * kSqrtPiFull) + 0.5 * un * (1.0 + erf(sr)));
+    return flux * a.L.fa[f];
+}
+
+// Inclusive scan of v over a block of NT threads in a fixed order (warp shuffles,
+// then the warp totals in ascending order); *all = the block total.
+template <int NT>
+__device__ __forceinline__ double block_scan(double v, double* warp_tot, double* all) {
+    constexpr int kW = NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) warp_tot[w] = v;
+    __syncthreads();
+    double before = 0.0, sum = 0.0;
+    for (int k = 0; k < kW; ++k) {
+        if (k < w) before += warp_tot[k];
+        sum += warp_tot[k];
+    }
+    __syncthreads();  // warp_tot is reused by the next call
+    *all = sum;
+    return before + v;
+}
+
+constexpr int kScanThreads = 256;
+static_assert(kMcScanChunk % kScanThreads == 0, "whole rounds per block");
+
+// Per block of kMcScanChunk faces: the inclusive prefix of the weights within
+// the block into cdf, the block's total into block_sums.
+__global__ void __launch_bounds__(kScanThreads) inflow_scan_kernel(Args a, double* cdf, double* block_sums) {
+    __shared__ double warp_tot[kScanThreads / 32];
+    const long long nf = a.M.nface;
+    const long long base = (long long)blockIdx.x * kMcScanChunk;
+    double carry = 0.0;
+    for (int r = 0; r < kMcScanChunk / kScanThreads; ++r) {
+        const long long f = base + r * kScanThreads + threadIdx.x;
+        const double w = (f < nf) ? inflow_weight(a, (int)f) : 0.0;
+        double all;
+        const double incl = block_scan<kScanThreads>(w, warp_tot, &all);
+        if (f < nf) cdf[f] = carry + incl;
+        carry += all;
+    }
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = carry;
+}
+
+// One block: block_sums[b] becomes the sum of the blocks before b, *total the sum
+// of all. Each thread runs over a contiguous segment of the blocks.
+constexpr int kBlockScanThreads = 1024;
+__global__ void __launch_bounds__(kBlockScanThreads) inflow_blocks_kernel(double* block_sums, int nb,
+                                                                         double* total) {
+    __shared__ double warp_tot[kBlockScanThreads / 32];
+    const int per = (nb + kBlockScanThreads - 1) / kBlockScanThreads;
+    const int b0 = min(nb, (int)threadIdx.x * per), b1 = min(nb, b0 + per);
+    double seg = 0.0;
+    for (int b = b0; b < b1; ++b) {
+        const double v = block_sums[b];
+        block_sums[b] = seg;  // exclusive within the segment
+        seg += v;
+    }
+    double all;
+    const double before = block_scan<kBlockScanThreads>(seg, warp_tot, &all) - seg;
+    for (int b = b0; b < b1; ++b) block_sums[b] += before;
+    if (threadIdx.x == 0) *total = all;
+}
+
+// cdf[f] = (prefix within the block + blocks before) / total; the last entry is 1.
+__global__ void inflow_finish_kernel(double* cdf, const double* block_sums, const double* total, int nf) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const double T = *total;
+    if (!(T > 0.0)) return;  // no inflow: the host reports it
+    cdf[f] = (f == nf - 1) ? 1.0 : (cdf[f] + block_sums[f / kMcScanChunk]) / T;
+}
+
+// The tracing records of all cells (McCell): outward face planes in the
+// cell's face order, neighbours, and the proton fluid of plasma_in_cell.
+__global__ void pack_kernel(Args a, McCell* __restrict__ cells) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const MeshView& M = a.M;
+    const int nc = M.ncell, nf = M.nface;
+    if (c >= nc) return;
+    McCell R;
+#pragma unroll
+    for (int sl = 0; sl < 6; ++sl) {
+        const int fs = M.cell_faces[sl * nc + c];
+        const int f = fs & 0x7fffffff;
+        const double sg = (fs < 0) ? -1.0 : 1.0;  // outward normal of this cell
+        const double n0 = sg * a.L.fn[f], n1 = sg * a.L.fn[nf + f], n2 = sg * a.L.fn[2 * nf + f];
+        R.plane[sl][0] = n0;
+        R.plane[sl][1] = n1;
+        R.plane[sl][2] = n2;
+        R.plane[sl][3] = a.L.fc[f] * n0 + a.L.fc[nf + f] * n1 + a.L.fc[2 * nf + f] * n2;
+        R.nbr[sl] = (fs < 0) ? M.face_c0[f] : M.face_c1[f];
+    }
+    plasma_in_cell(a, c, R.rho_th, R.cp, R.V);
+    cells[c] = R;
+}
+
+__global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* __restrict__ cells) {
     const long long pid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (pid >= a.nparticles) return;
     const MeshView& M = a.M;
     const int nc = M.ncell, nf = M.nface;
     Rng rng{a.seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(pid + 1)), 0ull};
-    // stratified choice of the inflow face by its share of the flux
+    // stratified choice of the inflow face by its share of the flux (faces that
+    // let no neutrals in add nothing to the CDF, so are never chosen)
     const double s = ((double)pid + rng.uniform()) / (double)a.nparticles;
-    int lo = 0, hi = a.ninflow - 1;
+    int lo = 0, hi = nf - 1;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (a.inflow_cdf[mid] < s)
@@ -139,7 +259,7 @@ __global__ void __launch_bounds__(128) trace_kernel(Args a) {
         else
             hi = mid;
     }
-    const int f0 = a.inflow_face[lo];
+    const int f0 = lo;
     // position: uniform on the quad (two triangles by area)
     double P[4][3];
 #pragma unroll
@@ -174,29 +294,27 @@ __global__ void __launch_bounds__(128) trace_kernel(Args a) {
     double I = 0.0;
     double* T = a.tally;
     for (int visit = 0; visit < a.max_cells; ++visit) {
-        // exit through the face of this cell that the ray reaches first
+        // the cell's record: its face planes, neighbours and proton fluid; the
+        // ray leaves through the face it reaches first
+        const McCell* R = cells + cell;
         double t_exit = 1e300;
-        int fexit = -1;
-        bool ext = false;
+        int next = -2;
 #pragma unroll
         for (int sl = 0; sl < 6; ++sl) {
-            const int fs = M.cell_faces[sl * nc + cell];
-            const int f = fs & 0x7fffffff;
-            const double sg = (fs < 0) ? -1.0 : 1.0;  // outward normal of this cell
-            const double n0 = sg * a.L.fn[f], n1 = sg * a.L.fn[nf + f], n2 = sg * a.L.fn[2 * nf + f];
-            const double vn = v[0] * n0 + v[1] * n1 + v[2] * n2;
+            const double2 nab = __ldg(reinterpret_cast<const double2*>(R->plane[sl]));
+            const double2 ncd = __ldg(reinterpret_cast<const double2*>(R->plane[sl]) + 1);
+            const double vn = v[0] * nab.x + v[1] * nab.y + v[2] * ncd.x;
             if (vn <= 0.0) continue;
-            const double d = (a.L.fc[f] - x[0]) * n0 + (a.L.fc[nf + f] - x[1]) * n1 + (a.L.fc[2 * nf + f] - x[2]) * n2;
+            const double d = ncd.y - (x[0] * nab.x + x[1] * nab.y + x[2] * ncd.x);
             const double t = fmax(d, 0.0) / vn;
             if (t < t_exit) {
                 t_exit = t;
-                fexit = f;
-                ext = (fs < 0);
+                next = __ldg(R->nbr + sl);
             }
         }
-        if (fexit < 0) break;  // no outgoing face (degenerate): give up on this particle
-        double rho_th, cp, Vp[3];
-        plasma_in_cell(a, cell, rho_th, cp, Vp);
+        if (next == -2) break;  // no outgoing face (degenerate): give up on this particle
+        const double rho_th = __ldg(&R->rho_th), cp = __ldg(&R->cp);
+        const double Vp[3] = {__ldg(R->V), __ldg(R->V + 1), __ldg(R->V + 2)};
         const double du0 = v[0] - Vp[0], du1 = v[1] - Vp[1], du2 = v[2] - Vp[2];
         const double u = sqrt(du0 * du0 + du1 * du1 + du2 * du2);
         const double uz = velosity_1(u, cp);
@@ -206,9 +324,8 @@ __global__ void __launch_bounds__(128) trace_kernel(Args a) {
             atomicAdd(&T[cell], a.mu * t_exit);
             I += dI;
             for (int k = 0; k < 3; ++k) x[k] += t_exit * v[k];
-            const int other = ext ? M.face_c0[fexit] : M.face_c1[fexit];
-            if (other < 0) return;  // left through the boundary
-            cell = other;
+            if (next < 0) return;  // left through the boundary
+            cell = next;
             continue;
         }
         // charge exchange inside this cell
@@ -245,8 +362,22 @@ __global__ void normalise_kernel(double* T, const double* vol, int nc) {
 
 }  // namespace mc
 
-cudaError_t launch_mc_trace(const McArgs& a, cudaStream_t s) {
-    mc::trace_kernel<<<blocks_for(a.nparticles, 128), 128, 0, s>>>(a);
+cudaError_t launch_mc_inflow_cdf(const McArgs& a, double* cdf, double* block_sums, double* total_out,
+                                 cudaStream_t s) {
+    const int nb = mc_scan_blocks(a.M.nface);
+    mc::inflow_scan_kernel<<<nb, mc::kScanThreads, 0, s>>>(a, cdf, block_sums);
+    mc::inflow_blocks_kernel<<<1, mc::kBlockScanThreads, 0, s>>>(block_sums, nb, total_out);
+    mc::inflow_finish_kernel<<<blocks_for(a.M.nface, 256), 256, 0, s>>>(cdf, block_sums, total_out, a.M.nface);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mc_pack(const McArgs& a, McCell* cells, cudaStream_t s) {
+    mc::pack_kernel<<<blocks_for(a.M.ncell, 256), 256, 0, s>>>(a, cells);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mc_trace_cells(const McArgs& a, const McCell* cells, cudaStream_t s) {
+    mc::trace_cells_kernel<<<blocks_for(a.nparticles, 128), 128, 0, s>>>(a, cells);
     return cudaGetLastError();
 }
 

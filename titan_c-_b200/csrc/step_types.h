@@ -87,22 +87,4 @@ struct CellArgs {
     DevStatus* st;
 };
 
-// Monte-Carlo neutral tracing (mc_neutral.cu)
-struct McArgs {
-    MeshView M;
-    Params P;
-    Layer L;                  // current geometry (face centres / normals, cell volumes)
-    const double* state;      // [ns][ncell]
-    const int* inflow_face;   // [ninflow] boundary faces the neutrals enter through
-    const double* inflow_cdf; // [ninflow] cumulative share of the inflow, last = 1
-    int ninflow;
-    long long nparticles;
-    double mu;                // weight: inflow rate per particle
-    double nH, uH0, uH1, uH2, cpH;
-    unsigned long long seed;
-    int max_cells;
-    double* tally;            // [5][ncell]: sum mu*t, sum mu*dv (3), sum mu*d(v^2)/2
-    unsigned long long* lost;
-};
-
 }  // namespace titan

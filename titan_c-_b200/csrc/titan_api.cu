@@ -14,6 +14,7 @@
 #include "../../include/titan_b200.h"
 #include "closure.h"
 #include "launch.h"
+#include "mc.h"
 #include "renumber.h"
 
 using namespace titan;
@@ -110,6 +111,14 @@ struct titan_ctx {
     unsigned long long* d_n_outside = nullptr;
     double closure_ninf = 0.0, closure_lambda = 0.0;
     int sm_count = 148;
+
+    // Monte-Carlo pass buffers (titan_mc_sources), allocated by the first pass
+    McCell* d_mc_cells = nullptr;       // [ncell] tracing records
+    double* d_mc_cdf = nullptr;         // [nface] inflow CDF
+    double* d_mc_blocks = nullptr;      // [mc_scan_blocks(nface)] + 1: block sums, total
+    double* d_mc_tally = nullptr;       // [5][ncell]
+    unsigned long long* d_mc_lost = nullptr;
+    bool mc_valid = false;              // d_mc_tally holds a finished pass
 
     int face_variant = 0;  // launch shapes (autotuned, see titan_autotune)
     int cell_variant = 0;
@@ -369,7 +378,8 @@ int titan_destroy(titan_ctx* ctx) {
                     ctx->d_cell_faces, ctx->d_cell_nodes, ctx->d_cell_type, ctx->d_cell_tvd, ctx->d_node_amp,
                     ctx->d_node_phase, ctx->d_state[0], ctx->d_state[1], ctx->d_flux, ctx->d_hfl, ctx->d_src,
                     ctx->d_stage, ctx->d_status, ctx->d_cell_fmap, ctx->d_face_aa, ctx->d_face_bb,
-                    ctx->d_env, ctx->d_fallback, ctx->d_n_outside};
+                    ctx->d_env, ctx->d_fallback, ctx->d_n_outside, ctx->d_mc_cells, ctx->d_mc_cdf,
+                    ctx->d_mc_blocks, ctx->d_mc_tally, ctx->d_mc_lost};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     // without node motion layer[1] aliases layer[0]: free it once
@@ -997,6 +1007,22 @@ int titan_set_closure_fallback(titan_ctx* ctx, const float* lo, const float* hi,
     return TITAN_OK;
 }
 
+int titan_closure_fallback_from_mc(titan_ctx* ctx) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    if (!ctx->d_env) return fail(TITAN_EINVAL, "no closure envelope: call titan_set_closure_fallback first");
+    if (!ctx->mc_valid) return fail(TITAN_EINVAL, "no Monte-Carlo pass on this context");
+    const int64_t nc = ctx->ncell;
+    if (!ctx->d_fallback) {
+        int64_t dummy = 0;
+        CK(dalloc(&ctx->d_fallback, (size_t)4 * nc, &dummy));
+        drop_graph(ctx);  // the captured step reads the table's address
+    }
+    // the tallies are in the device's cell numbering, as the table is
+    CK(cudaMemcpyAsync(ctx->d_fallback, ctx->d_mc_tally + nc, sizeof(double) * 4 * nc, cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    return TITAN_OK;
+}
+
 int titan_closure_outside(titan_ctx* ctx, int64_t* n_outside) {
     if (!ctx || !n_outside) return fail(TITAN_EINVAL, "null argument");
     unsigned long long v = 0;
@@ -1007,90 +1033,73 @@ int titan_closure_outside(titan_ctx* ctx, int64_t* n_outside) {
 }
 
 int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, titan_mc_info* info) {
-    if (!ctx || !mp || !out) return fail(TITAN_EINVAL, "null argument");
+    if (!ctx || !mp) return fail(TITAN_EINVAL, "null argument");
     if (mp->n_particles <= 0 || !(mp->n_H > 0.0) || !(mp->cp_H > 0.0)) return fail(TITAN_EINVAL, "bad MC parameters");
     const int64_t nc = ctx->ncell, nf = ctx->nface;
     cudaStream_t s = ctx->stream;
     const MeshView M = ctx->view();
     const Layer& L = ctx->layer[ctx->cur];
     if (ctx->prm.move) CK(launch_face_geometry(M, L, s));  // faces of the current layer
-    // inflow faces and their share of the flux of a drifting Maxwellian through
-    // the inward normal: n [cp e^{-s^2} / (2 sqrt(pi)) + u_n (1 + erf s) / 2], s = u_n / cp
-    std::vector<double> fn(3 * nf), fa(nf);
-    std::vector<int8_t> ft(nf);
-    CK(cudaMemcpyAsync(fn.data(), L.fn, sizeof(double) * 3 * nf, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(fa.data(), L.fa, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(ft.data(), ctx->d_face_type, nf, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    std::vector<int32_t> faces;
-    std::vector<double> cdf;
-    double total = 0.0;
-    const double sqpi = std::sqrt(3.14159265358979323846);
-    for (int64_t f = 0; f < nf; ++f) {
-        if (ft[f] == 0 || !((mp->face_types >> ft[f]) & 1)) continue;
-        const double un = -(mp->u_H[0] * fn[f] + mp->u_H[1] * fn[nf + f] + mp->u_H[2] * fn[2 * nf + f]);
-        const double sr = un / mp->cp_H;
-        const double flux = mp->n_H * (mp->cp_H * std::exp(-sr * sr) / (2.0 * sqpi) + 0.5 * un * (1.0 + std::erf(sr)));
-        total += flux * fa[f];
-        faces.push_back((int32_t)f);
-        cdf.push_back(total);
+    const int nb = mc_scan_blocks(nf);
+    if (!ctx->d_mc_cells) {
+        int64_t tmp = 0;
+        cudaError_t e = dalloc(&ctx->d_mc_cells, (size_t)nc, &tmp);
+        if (!e) e = dalloc(&ctx->d_mc_cdf, (size_t)nf, &tmp);
+        if (!e) e = dalloc(&ctx->d_mc_blocks, (size_t)nb + 1, &tmp);
+        if (!e) e = dalloc(&ctx->d_mc_tally, (size_t)5 * nc, &tmp);
+        if (!e) e = dalloc(&ctx->d_mc_lost, 1, &tmp);
+        if (e) {
+            void* ps[] = {ctx->d_mc_cells, ctx->d_mc_cdf, ctx->d_mc_blocks, ctx->d_mc_tally, ctx->d_mc_lost};
+            for (void* p : ps)
+                if (p) cudaFree(p);
+            ctx->d_mc_cells = nullptr;
+            ctx->d_mc_cdf = ctx->d_mc_blocks = ctx->d_mc_tally = nullptr;
+            ctx->d_mc_lost = nullptr;
+            return fail(TITAN_ECUDA, std::string("mc buffers: ") + cudaGetErrorString(e));
+        }
     }
-    if (faces.empty() || !(total > 0.0)) return fail(TITAN_EINVAL, "no inflow faces of the requested types");
-    for (double& c : cdf) c /= total;
-    cdf.back() = 1.0;
-    int32_t* d_faces = nullptr;
-    double *d_cdf = nullptr, *d_tally = nullptr;
-    unsigned long long* d_lost = nullptr;
-    int64_t tmp = 0;
-    cudaError_t e = dalloc(&d_faces, faces.size(), &tmp);
-    if (!e) e = dalloc(&d_cdf, cdf.size(), &tmp);
-    if (!e) e = dalloc(&d_tally, (size_t)5 * nc, &tmp);
-    if (!e) e = dalloc(&d_lost, 1, &tmp);
-    if (!e) e = cudaMemcpyAsync(d_faces, faces.data(), sizeof(int32_t) * faces.size(), cudaMemcpyHostToDevice, s);
-    if (!e) e = cudaMemcpyAsync(d_cdf, cdf.data(), sizeof(double) * cdf.size(), cudaMemcpyHostToDevice, s);
-    if (!e) e = cudaMemsetAsync(d_tally, 0, sizeof(double) * 5 * nc, s);
-    if (!e) e = cudaMemsetAsync(d_lost, 0, sizeof(unsigned long long), s);
+    ctx->mc_valid = false;
+    double* d_total = ctx->d_mc_blocks + nb;
     McArgs a{};
     a.M = M;
     a.P = ctx->P;
     a.L = L;
     a.state = ctx->d_state[ctx->scur];
-    a.inflow_face = d_faces;
-    a.inflow_cdf = d_cdf;
-    a.ninflow = (int)faces.size();
+    a.inflow_cdf = ctx->d_mc_cdf;
     a.nparticles = mp->n_particles;
-    a.mu = total / (double)mp->n_particles;
     a.nH = mp->n_H;
     a.uH0 = mp->u_H[0];
     a.uH1 = mp->u_H[1];
     a.uH2 = mp->u_H[2];
     a.cpH = mp->cp_H;
+    a.face_types = (unsigned)mp->face_types;
     a.seed = mp->seed;
     a.max_cells = mp->max_cells > 0 ? mp->max_cells : 1000000;
-    a.tally = d_tally;
-    a.lost = d_lost;
-    float ms = 0.f;
-    if (!e) e = cudaEventRecord(ctx->ev[0], s);
-    if (!e) e = launch_mc_trace(a, s);
-    if (!e) e = launch_mc_normalise(d_tally, L.vol, (int)nc, s);
-    if (!e) e = cudaEventRecord(ctx->ev[1], s);
-    std::vector<double> h;
+    a.tally = ctx->d_mc_tally;
+    a.lost = ctx->d_mc_lost;
+    // inflow CDF on the device; its total sets the particle weight
+    double total = 0.0;
+    CK(cudaEventRecord(ctx->ev[0], s));
+    CK(launch_mc_inflow_cdf(a, ctx->d_mc_cdf, ctx->d_mc_blocks, d_total, s));
+    CK(cudaMemcpyAsync(&total, d_total, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (!(total > 0.0)) return fail(TITAN_EINVAL, "no inflow faces of the requested types");
+    a.mu = total / (double)mp->n_particles;
+    CK(cudaMemsetAsync(ctx->d_mc_tally, 0, sizeof(double) * 5 * nc, s));
+    CK(cudaMemsetAsync(ctx->d_mc_lost, 0, sizeof(unsigned long long), s));
+    CK(launch_mc_pack(a, ctx->d_mc_cells, s));
+    CK(launch_mc_trace_cells(a, ctx->d_mc_cells, s));
+    CK(launch_mc_normalise(ctx->d_mc_tally, L.vol, (int)nc, s));
+    // back to the caller's cell numbering on the device, then one copy
+    if (out) CK(launch_scatter(ctx->d_mc_tally, ctx->d_stage, ctx->d_cell_n2o, (int)nc, 5, s));
+    CK(cudaEventRecord(ctx->ev[1], s));
     unsigned long long lost = 0;
-    if (!e) {
-        h.resize((size_t)5 * nc);
-        e = cudaMemcpyAsync(h.data(), d_tally, sizeof(double) * 5 * nc, cudaMemcpyDeviceToHost, s);
-    }
-    if (!e) e = cudaMemcpyAsync(&lost, d_lost, sizeof(lost), cudaMemcpyDeviceToHost, s);
-    if (!e) e = cudaStreamSynchronize(s);
-    if (!e) cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
-    void* ps[] = {d_faces, d_cdf, d_tally, d_lost};
-    for (void* p : ps)
-        if (p) cudaFree(p);
-    if (e) return fail(TITAN_ECUDA, std::string("mc: ") + cudaGetErrorString(e));
-    for (int64_t c = 0; c < nc; ++c) {
-        const int64_t o = ctx->R.cell_n2o[c];
-        for (int k = 0; k < 5; ++k) out[k * nc + o] = h[k * nc + c];
-    }
+    if (out) CK(cudaMemcpyAsync(out, ctx->d_stage, sizeof(double) * 5 * nc, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&lost, ctx->d_mc_lost, sizeof(lost), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    ctx->mc_valid = true;
     if (info) {
         info->particles = mp->n_particles;
         info->lost = (int64_t)lost;

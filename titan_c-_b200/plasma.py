@@ -186,18 +186,36 @@ class PlasmaStep:
         N.check(self._lib.titan_get_permutation(self._ctx, N.ptr(c, N.I32), N.ptr(f, N.I32), N.ptr(n, N.I32)))
         return c, f, n
 
-    def mc_sources(self, n_H: float, u_H, cp_H: float, n_particles: int, seed: int = 1,
-                   face_types: int = (1 << 2) | (1 << 3), max_cells: int = 0):
-        """Monte-Carlo neutrals through the current state: ([5, ncell] = n_H, S_m (3), S_E; info)."""
+    @staticmethod
+    def _mc_params(n_H, u_H, cp_H, n_particles, seed, face_types, max_cells):
         mp = N.TitanMcParams()
         mp.n_H, mp.cp_H = n_H, cp_H
         for k in range(3):
             mp.u_H[k] = u_H[k]
         mp.n_particles, mp.seed, mp.max_cells, mp.face_types = int(n_particles), int(seed), int(max_cells), face_types
-        out = np.empty((5, self.ncell))
+        return mp
+
+    def mc_sources(self, n_H: float, u_H, cp_H: float, n_particles: int, seed: int = 1,
+                   face_types: int = (1 << 2) | (1 << 3), max_cells: int = 0, out: np.ndarray | None = None):
+        """Monte-Carlo neutrals through the current state: ([5, ncell] = n_H, S_m (3), S_E; info).
+        `out`, a C-contiguous float64 [5, ncell] array, is filled in place when given."""
+        mp = self._mc_params(n_H, u_H, cp_H, n_particles, seed, face_types, max_cells)
+        if out is None:
+            out = np.empty((5, self.ncell))
+        elif out.shape != (5, self.ncell) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (5, ncell)")
         info = N.TitanMcInfo()
         N.check(self._lib.titan_mc_sources(self._ctx, ctypes.byref(mp), N.ptr(out), ctypes.byref(info)))
         return out, {k: getattr(info, k) for k, _ in N.TitanMcInfo._fields_}
+
+    def mc_pass(self, n_H: float, u_H, cp_H: float, n_particles: int, seed: int = 1,
+                face_types: int = (1 << 2) | (1 << 3), max_cells: int = 0) -> dict:
+        """A Monte-Carlo pass whose sources stay on the device (for
+        Closure.fallback_from_mc); returns the pass's info."""
+        mp = self._mc_params(n_H, u_H, cp_H, n_particles, seed, face_types, max_cells)
+        info = N.TitanMcInfo()
+        N.check(self._lib.titan_mc_sources(self._ctx, ctypes.byref(mp), None, ctypes.byref(info)))
+        return {k: getattr(info, k) for k, _ in N.TitanMcInfo._fields_}
 
     def autotune(self, reps: int = 5, cache: str | None = None) -> dict:
         """Times the launch-shape variants on this mesh and keeps the fastest."""

@@ -131,7 +131,10 @@ int titan_destroy(titan_ctx* ctx);
  * data: n_state per face in original numbering. */
 int titan_set_face_method(titan_ctx* ctx, const int8_t* n_state);
 
-/* Cell::parameters[now] for all cells, SoA [TITAN_NV][ncell], original order. */
+/* Cell::parameters[now] for all cells, SoA [TITAN_NV][ncell], original order.
+ * Only the rows the context carries (8 + npassive) travel: the download leaves
+ * the others as the caller has them, as the reference's step leaves the
+ * parameters it does not evolve. */
 int titan_upload_state(titan_ctx* ctx, const double* state);
 int titan_download_state(titan_ctx* ctx, double* state);
 

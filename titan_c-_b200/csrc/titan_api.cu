@@ -662,7 +662,6 @@ int titan_download_state(titan_ctx* ctx, double* state) {
     CK(launch_scatter(ctx->d_state[ctx->scur], ctx->d_stage, ctx->d_cell_n2o, (int)nc, ctx->ns, ctx->stream));
     CK(cudaMemcpyAsync(state, ctx->d_stage, sizeof(double) * ctx->ns * nc, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    for (int k = ctx->ns; k < TITAN_NV; ++k) std::memset(state + k * nc, 0, sizeof(double) * nc);
     return TITAN_OK;
 }
 

@@ -101,7 +101,8 @@ class PlasmaStep:
         N.check(self._lib.titan_upload_state(self._ctx, N.ptr(a)))
 
     def download_state(self, out: np.ndarray | None = None) -> np.ndarray:
-        out = np.empty((N.NV, self.ncell)) if out is None else out
+        # rows the context does not carry stay as given (zeros in a new array)
+        out = np.zeros((N.NV, self.ncell)) if out is None else out
         N.check(self._lib.titan_download_state(self._ctx, N.ptr(out)))
         return out
 

@@ -126,6 +126,10 @@ struct titan_ctx {
     bool profiling = false;
     std::map<std::string, KernelClock> clocks;
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    // state transfers: copies on their own stream, one event per field, so the
+    // copy of one field overlaps the renumbering of another
+    cudaStream_t xfer = nullptr;
+    cudaEvent_t xev[TITAN_NV + 1] = {};
 
     MeshView view() const {
         MeshView M;
@@ -393,6 +397,9 @@ int titan_destroy(titan_ctx* ctx) {
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->xev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->xfer) cudaStreamDestroy(ctx->xfer);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return TITAN_OK;
@@ -442,6 +449,12 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     if (e) return bail(fail(TITAN_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)));
     cudaEventCreate(&ctx->ev[0]);
     cudaEventCreate(&ctx->ev[1]);
+    e = cudaStreamCreateWithFlags(&ctx->xfer, cudaStreamNonBlocking);
+    if (e) return bail(fail(TITAN_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)));
+    for (auto& x : ctx->xev) {
+        e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+        if (e) return bail(fail(TITAN_ECUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(e)));
+    }
 
     // --- renumbering and remapped host arrays ---
     ctx->R = sfc_renumber(m->nnode, m->ncell, m->nface, m->node_xyz, m->cell_nodes, m->face_cells);
@@ -650,18 +663,34 @@ int titan_set_face_method(titan_ctx* ctx, const int8_t* ns) {
 int titan_upload_state(titan_ctx* ctx, const double* state) {
     if (!ctx || !state) return fail(TITAN_EINVAL, "null argument");
     const int64_t nc = ctx->ncell;
-    CK(cudaMemcpyAsync(ctx->d_stage, state, sizeof(double) * ctx->ns * nc, cudaMemcpyHostToDevice, ctx->stream));
-    CK(launch_gather(ctx->d_stage, ctx->d_state[ctx->scur], ctx->d_cell_n2o, (int)nc, ctx->ns, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    cudaStream_t s = ctx->stream, x = ctx->xfer;
+    // field by field: the copy of field k+1 overlaps the gather of field k
+    CK(cudaEventRecord(ctx->xev[TITAN_NV], s));  // earlier users of the staging buffer
+    CK(cudaStreamWaitEvent(x, ctx->xev[TITAN_NV], 0));
+    for (int k = 0; k < ctx->ns; ++k) {
+        CK(cudaMemcpyAsync(ctx->d_stage + k * nc, state + k * nc, sizeof(double) * nc, cudaMemcpyHostToDevice, x));
+        CK(cudaEventRecord(ctx->xev[k], x));
+        CK(cudaStreamWaitEvent(s, ctx->xev[k], 0));
+        CK(launch_gather(ctx->d_stage + k * nc, ctx->d_state[ctx->scur] + k * nc, ctx->d_cell_n2o, (int)nc, 1, s));
+    }
+    CK(cudaStreamSynchronize(s));
     return TITAN_OK;
 }
 
 int titan_download_state(titan_ctx* ctx, double* state) {
     if (!ctx || !state) return fail(TITAN_EINVAL, "null argument");
     const int64_t nc = ctx->ncell;
-    CK(launch_scatter(ctx->d_state[ctx->scur], ctx->d_stage, ctx->d_cell_n2o, (int)nc, ctx->ns, ctx->stream));
-    CK(cudaMemcpyAsync(state, ctx->d_stage, sizeof(double) * ctx->ns * nc, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    cudaStream_t s = ctx->stream, x = ctx->xfer;
+    // field by field: the copy of field k overlaps the scatter of field k+1
+    for (int k = 0; k < ctx->ns; ++k) {
+        CK(launch_scatter(ctx->d_state[ctx->scur] + k * nc, ctx->d_stage + k * nc, ctx->d_cell_n2o, (int)nc, 1, s));
+        CK(cudaEventRecord(ctx->xev[k], s));
+    }
+    for (int k = 0; k < ctx->ns; ++k) {
+        CK(cudaStreamWaitEvent(x, ctx->xev[k], 0));
+        CK(cudaMemcpyAsync(state + k * nc, ctx->d_stage + k * nc, sizeof(double) * nc, cudaMemcpyDeviceToHost, x));
+    }
+    CK(cudaStreamSynchronize(x));
     return TITAN_OK;
 }
 

@@ -72,7 +72,7 @@ def peak_tflops():
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel on the
 # 6x64x64x40 shell, scaled by faces (x2.25) to the 6x96x96x40 workload:
 # profiles/face_flux_shell.md has the command and the figures.
-TRAFFIC = {("face_flux_fp64", 2211840): 1264.7e6}
+TRAFFIC = {("face_flux_fp64", 2211840): 1264.7e6, ("face_flux_fp32", 2211840): 987.7e6}
 
 
 class ClockSampler:
@@ -379,7 +379,8 @@ def run_ours(args, rank, world):
         "config": {"workload": f"heliosphere shell 6x{args.nq}x{args.nq}x{args.nlayer} = {C} cells, {F} faces, "
                                f"ALE, HLLD/HLLC, {what}", "cells": C, "faces": F, "mode": args.mode,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "tuning": tuning,
-                   "l2": "inputs larger than L2 (state 141 MB + face data 0.5 GB), no flush"},
+                   "l2": f"inputs larger than L2 (state {8 * ns * C / 1e6:.0f} MB + face records "
+                         f"{80 * F / 1e6:.0f} MB per step), no flush"},
         "face_fluxes_per_s": world * F * args.steps / (ms / 1e3),
         "e2e": {"value": world * C * e2e_steps / e2e_wall, "unit": UNIT,
                 "h2d_bytes_per_step": 8 * ns * C, "d2h_bytes_per_step": 8 * ns * C},

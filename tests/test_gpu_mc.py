@@ -85,3 +85,31 @@ def test_seed_reproduces_and_seeds_agree_statistically(titan):
     # a different seed: the same density field within Monte-Carlo noise
     tot_a, tot_c = a[0].sum(), c[0].sum()
     assert abs(tot_a / tot_c - 1.0) < 0.02
+
+
+def test_inflow_rate_is_the_maxwellian_flux_through_the_open_faces(titan):
+    """The device's inflow split (a fixed-order scan over all faces) totals the
+    drifting Maxwellian's flux through the inward normal of every face whose
+    type is open, n [cp e^{-s^2} / (2 sqrt(pi)) + u_n (1 + erf s) / 2] times the
+    area (s = u_n / cp), as numpy sums it from the downloaded geometry; a second
+    pass gives the identical total."""
+    from scipy.special import erf
+
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=8, nlayer=8, move=False)
+    g = titan.PlasmaStep(m, p)
+    g.upload_state(st)
+    nH, uH, cpH, types = 0.18, np.array([-2.6, 0.3, 0.1]), 1.3, (1 << 2) | (1 << 3)
+    kw = dict(n_H=nH, u_H=tuple(uH), cp_H=cpH, n_particles=50_000, seed=1, face_types=types)
+    _, info = g.mc_sources(**kw)
+    _, info2 = g.mc_sources(**kw)
+    geo = g.geometry()
+    g.close()
+    ft = m["face_type"].astype(np.int64)
+    open_ = (ft > 0) & (((types >> np.clip(ft, 0, 31)) & 1) == 1)
+    assert open_.any() and not open_.all()
+    un = -(geo["face_normal"][open_] @ uH)
+    sr = un / cpH
+    flux = nH * (cpH * np.exp(-sr * sr) / (2.0 * np.sqrt(np.pi)) + 0.5 * un * (1.0 + erf(sr)))
+    expected = float((flux * geo["face_area"][open_]).sum())
+    assert info["inflow_rate"] == pytest.approx(expected, rel=1e-12)
+    assert info2["inflow_rate"] == info["inflow_rate"]

@@ -109,8 +109,9 @@ typedef struct titan_step_info {
     int64_t n_p_floor;       /* cells where p < 1e-8 was reset (Setka_physics.cpp:1981-2001) */
     int32_t status;          /* titan_status of the step loop */
     int32_t err_kind;        /* 0, 11-14 solver region/branch, 15-18 exact HP solver (negative pressure,
-                                Newton / bisection without convergence, no wave pattern), 20 non-finite
-                                density */
+                                Newton / bisection without convergence, no wave pattern), 19 non-finite
+                                or subnormal contact speed of an HP face (surface tracking), 20
+                                non-finite density */
     double  dt_next;         /* CFL dt that the next step will use */
     double  t;               /* accumulated physical time */
     double  gpu_ms;          /* device time of this call's step loop (CUDA events) */
@@ -130,6 +131,31 @@ int titan_destroy(titan_ctx* ctx);
 /* Per-face solver choice (Gran::Get_method, TITAN/source/Gran.cpp:3-14) as
  * data: n_state per face in original numbering. */
 int titan_set_face_method(titan_ctx* ctx, const int8_t* n_state);
+
+/* Surface-tracking node motion, in place of the prescribed radial law of a
+ * context created with move = 1: Setka::Culc_Velocity_surface
+ * (TITAN/source/Setka_move.cpp:111-1358) and Luch::dvigenie (Luch.cpp:6-739),
+ * called from Setka::Go at Setka_physics.cpp:1616-1627. Every step, before its
+ * face loop, the faces of each moving surface (face_surf 1 = TS, 2 = HP,
+ * 3 = BS; HP faces with fewer than four surface neighbours are skipped) solve
+ * their Riemann problem at w = 0 on the step's state; each surface node moves
+ * along its direction by dt times the mean of velocity_X * ds * n over its
+ * faces (ds = dsl on TS, dsc on HP, dsr on BS; with bn_in_p_on_hp the HP
+ * faces use the exact gas-dynamic solver). The other nodes of each ray keep
+ * their fraction of the segment between the surface nodes and the ray's
+ * ends, on the ray's direction. rays: nray x ray_len node ids (original
+ * numbering) from the inner end; no node on two rays; radii and directions are
+ * taken from the current nodes. The reference's smoothing terms (sglag_*)
+ * are not applied. params NULL returns to the prescribed motion. */
+typedef struct titan_surface_params {
+    double velocity_TS, velocity_HP, velocity_BS; /* Phys_param::velocity_TS / _HP / _BS */
+    int32_t move_TS, move_HP, move_BS;            /* Phys_param::move_TS / _HP / _BS */
+    int32_t null_bn_on_HP;                        /* Phys_param::null_bn_on_HP: the HP cells and face
+                                                     states lose their normal B first */
+} titan_surface_params;
+
+int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* params, int64_t nray, int32_t ray_len,
+                             const int32_t* ray_nodes);
 
 /* Cell::parameters[now] for all cells, SoA [TITAN_NV][ncell], original order.
  * Only the rows the context carries (8 + npassive) travel: the download leaves

@@ -75,6 +75,13 @@ struct OMesh {
     const double* node_phase;    // nnode, phase (ALE), may be null
     const int32_t* face_tvd;     // nface*2, Gran::cells_TVD (AA beyond cells[0], BB beyond cells[1]),
                                  // -1 when absent; may be null (no second-order faces)
+    // Rays of nodes for the surface-tracking motion (Luch, Luch.h:9-25): node ids
+    // from the inner to the outer end, with the radii and the unit direction
+    // the ray had when tracking started (oracle_ray_geometry). May be null.
+    const int32_t* ray_nodes;    // nray*ray_len
+    const double* ray_r0;        // nray*ray_len
+    const double* ray_dir;       // nray*3
+    int64_t nray, ray_len;
 };
 
 struct OParams {
@@ -93,7 +100,12 @@ struct OParams {
     int32_t tvd;          // Phys_param::TVD: second-order reconstruction on interior faces
     int32_t snos_on_hp;   // Phys_param::Snos_on_HP: second order on HP faces too
     int32_t bn_in_p_on_hp;  // Phys_param::bn_in_p_on_HP: exact gas-dynamic solver on HP faces
-    int32_t pad;
+    int32_t surface_motion; // node motion by surface tracking (Setka::Culc_Velocity_surface) instead of
+                            // the prescribed radial law; needs move and the mesh's rays
+    int32_t move_TS, move_HP, move_BS;  // Phys_param::move_TS / move_HP / move_BS
+    int32_t null_bn_on_HP;  // Phys_param::null_bn_on_HP
+    int32_t pad2;
+    double velocity_TS, velocity_HP, velocity_BS;  // Phys_param::velocity_TS / _HP / _BS
 };
 
 struct OStepInfo {
@@ -1521,6 +1533,224 @@ void oracle_move_nodes(const OMesh* M, const OParams* P, const double* xyz1, dou
     }
 }
 
+// ---------------------------------------------------------------------------
+// Surface-tracking node motion: Setka::Culc_Velocity_surface
+// (TITAN/source/Setka_move.cpp:111-1358) and Luch::dvigenie (Luch.cpp:6-739)
+// restated for meshes whose rays are straight lines of nodes.
+//  * Surface faces (face_surf 1 = TS, 2 = HP, 3 = BS) of a moving surface take
+//    the Riemann solver at w = 0 on their reconstructed states (:128-181 TS,
+//    :187-361 HP, :363-447 BS) and give each of their four nodes
+//    velocity_X * ds * n: ds = dsl on TS, dsc on HP, dsr on BS. HP faces with
+//    fewer than four neighbours on the surface are skipped (:192); with
+//    null_bn_on_HP the normal B of both cells and of both face states is
+//    removed first (:196-224, :279-295); with bn_in_p_on_HP the magnetic
+//    pressure goes into p and Godunov_Solver_Alexashov gives dsc (:298-327).
+//    A non-finite or subnormal dsc is an error (:329-342; error kind 19).
+//    The three surfaces run in the reference's order, so BS sees the HP
+//    cells' B as null_bn_on_HP left it. The smoothing terms (sglag_*) are not
+//    part of this restatement.
+//  * Each node sums its faces' contributions in ascending face order (the
+//    reference sums under a mutex in thread order), divides by their number
+//    and moves along its own direction: x' = x + (V . x/|x|) dt x/|x|
+//    (:1213-1265; the reference's heliotail rays are parallel to the x axis
+//    and move HP nodes with x < 0 along (0, y, z); these rays are all radial).
+//  * Along each ray the end nodes and the surface nodes are anchors; every
+//    other node keeps its initial fraction of the segment between the
+//    anchors around it, on the ray's direction (the reference's A_Luch
+//    spacing is a fixed function of that fraction, Luch.cpp:47-200).
+// ---------------------------------------------------------------------------
+
+// Radii and directions of the rays at `xyz` (the start of tracking).
+void oracle_ray_geometry(const OMesh* M, const double* xyz, double* r0, double* dir) {
+    const int64_t L = M->ray_len;
+    for (int64_t r = 0; r < M->nray; ++r) {
+        for (int64_t j = 0; j < L; ++j) {
+            const int64_t i = M->ray_nodes[r * L + j];
+            const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+            r0[r * L + j] = std::sqrt(x * x + y * y + z * z);
+        }
+        const int64_t i0 = M->ray_nodes[r * L];
+        const double x = xyz[3 * i0], y = xyz[3 * i0 + 1], z = xyz[3 * i0 + 2];
+        const double n0 = std::sqrt(x * x + y * y + z * z);
+        dir[3 * r] = x / n0;
+        dir[3 * r + 1] = y / n0;
+        dir[3 * r + 2] = z / n0;
+    }
+}
+
+// Number of faces of the same surface sharing an edge with each surface face
+// (Gran::grans_surf).
+static std::vector<int> o_surface_neighbours(const OMesh* M) {
+    const int64_t nf = M->nface;
+    std::unordered_map<uint64_t, int> edges;
+    auto key = [](int64_t a, int64_t b, int s) {
+        if (a > b) std::swap(a, b);
+        return ((uint64_t)a << 34) ^ ((uint64_t)b << 2) ^ (uint64_t)s;
+    };
+    for (int64_t f = 0; f < nf; ++f) {
+        const int s = M->face_surf[f];
+        if (s < 1 || s > 3) continue;
+        for (int k = 0; k < 4; ++k) edges[key(M->face_nodes[4 * f + k], M->face_nodes[4 * f + (k + 1) % 4], s)]++;
+    }
+    std::vector<int> nb(nf, 0);
+    for (int64_t f = 0; f < nf; ++f) {
+        const int s = M->face_surf[f];
+        if (s < 1 || s > 3) continue;
+        for (int k = 0; k < 4; ++k)
+            nb[f] += edges[key(M->face_nodes[4 * f + k], M->face_nodes[4 * f + (k + 1) % 4], s)] - 1;
+    }
+    return nb;
+}
+
+static bool o_surface_moves(const OParams* P, int s) {
+    return (s == 1 && P->move_TS) || (s == 2 && P->move_HP) || (s == 3 && P->move_BS);
+}
+
+// Face states of an interior face, as o_face forms them.
+static void o_interior_states(const OMesh* M, const OParams* P, const double* st, const double* cc, const double* fc,
+                              int64_t f, double* L, double* R) {
+    const int64_t nc = M->ncell;
+    const int64_t A = M->face_cells[2 * f], B = M->face_cells[2 * f + 1];
+    const int64_t AA = M->face_tvd ? M->face_tvd[2 * f] : -1, BB = M->face_tvd ? M->face_tvd[2 * f + 1] : -1;
+    if (P->tvd && M->cell_tvd[A] && M->cell_tvd[B] && (M->face_surf[f] != 2 || P->snos_on_hp) && AA >= 0 && BB >= 0) {
+        const int64_t c4[4] = {AA, A, B, BB};
+        const int t4[4] = {M->cell_type[AA], M->cell_type[A], M->cell_type[B], M->cell_type[BB]};
+        o_snos_tvd(st, nc, c4, t4, cc, fc + 3 * f, P->gamma, P->npassive, L, R);
+    } else {
+        o_snos_side(st, nc, A, M->cell_type[A], cc, fc + 3 * f, P->gamma, L);
+        o_snos_side(st, nc, B, M->cell_type[B], cc, fc + 3 * f, P->gamma, R);
+    }
+}
+
+// One surface-tracking node motion xyz -> xyz2 with the step's dt `time`;
+// `st` loses the HP cells' normal B when null_bn_on_HP. Returns an error kind
+// (0 ok) and the face in *bad.
+static int o_surface_motion(const OMesh* M, const OParams* P, double* st, const double* xyz, double* xyz2,
+                            const double* cc, const double* fc, const double* fn, double time, int64_t* bad) {
+    const int64_t nn = M->nnode, nf = M->nface, nc = M->ncell;
+    const std::vector<int> nb = o_surface_neighbours(M);
+    std::vector<int8_t> node_surf(nn, 0);
+    std::vector<uint8_t> on(nf, 0);
+    for (int64_t f = 0; f < nf; ++f) {
+        const int s = M->face_surf[f];
+        if (s < 1 || s > 3) continue;
+        for (int k = 0; k < 4; ++k) node_surf[M->face_nodes[4 * f + k]] = (int8_t)s;
+        if (!o_surface_moves(P, s) || M->face_type[f] != 0) continue;
+        if (s == 2 && nb[f] < 4) continue;
+        on[f] = 1;
+    }
+    std::vector<double> vf(3 * nf, 0.0);
+    int err = 0;
+    for (int s = 1; s <= 3; ++s) {
+        const double vel = s == 1 ? P->velocity_TS : (s == 2 ? P->velocity_HP : P->velocity_BS);
+#pragma omp parallel for schedule(static)
+        for (int64_t f = 0; f < nf; ++f) {
+            if (!on[f] || M->face_surf[f] != s) continue;
+            const double* n = fn + 3 * f;
+            const bool nullbn = (s == 2 && P->null_bn_on_HP);
+            if (nullbn) {
+                const int64_t cs[2] = {M->face_cells[2 * f], M->face_cells[2 * f + 1]};
+                for (int64_t c : cs) {
+                    double* bx = st + 5 * nc + c;
+                    double* by = st + 6 * nc + c;
+                    double* bz = st + 7 * nc + c;
+                    const double dtpr = n[0] * *bx + n[1] * *by + n[2] * *bz;
+                    *bx -= dtpr * n[0];
+                    *by -= dtpr * n[1];
+                    *bz -= dtpr * n[2];
+                }
+            }
+            double L[NV], R[NV];
+            o_interior_states(M, P, st, cc, fc, f, L, R);
+            int method;
+            if (P->method_policy == 1) {
+                const double bb =
+                    ((L[5] * L[5] + L[6] * L[6] + L[7] * L[7]) + (R[5] * R[5] + R[6] * R[6] + R[7] * R[7])) / 2.0;
+                const double pp = (L[4] + R[4]) / 2.0;
+                method = (bb / kCpi4 / (2.0 * pp) > P->beta_switch) ? 3 : 2;
+            } else {
+                method = M->face_method[f];
+            }
+            if (nullbn) {
+                for (double* q : {L, R}) {
+                    const double dtpr = n[0] * q[5] + n[1] * q[6] + n[2] * q[7];
+                    q[5] -= dtpr * n[0];
+                    q[6] -= dtpr * n[1];
+                    q[7] -= dtpr * n[2];
+                }
+            }
+            double ds[3] = {0.0, 0.0, 0.0}, q[8], kq[2];
+            int e = 0;
+            if (s == 2 && P->bn_in_p_on_hp) {
+                double q1[5] = {L[0], L[1], L[2], L[3], L[4]}, q2[5] = {R[0], R[1], R[2], R[3], R[4]};
+                q1[4] += (L[5] * L[5] + L[6] * L[6] + L[7] * L[7]) / (8.0 * kPi);
+                q2[4] += (R[5] * R[5] + R[6] * R[6] + R[7] * R[7]) / (8.0 * kPi);
+                double gd[5];
+                const int rcg = o_godunov(n, 0.0, q1, q2, 0, P->gamma, gd, ds);
+                if (rcg) e = 14 + rcg;
+            } else {
+                const int rc = o_chlld(method, n, 0.0, L, R, 0, 0, 0, nullptr, nullptr, q, kq, ds, 0, 0, P->gamma);
+                if (rc) e = 10 + rc;
+            }
+            if (!e && s == 2 && (std::isnan(ds[1]) || std::fpclassify(ds[1]) == FP_SUBNORMAL)) e = 19;
+            const double d = s == 1 ? ds[0] : (s == 2 ? ds[1] : ds[2]);
+            for (int k = 0; k < 3; ++k) vf[3 * f + k] = vel * d * n[k];
+            if (e) {
+#pragma omp critical
+                if (!err) {
+                    err = e;
+                    *bad = f;
+                }
+            }
+        }
+    }
+    // node velocities: contributions in ascending face order, then the mean
+    std::vector<double> V(3 * nn, 0.0);
+    std::vector<int> num(nn, 0);
+    for (int64_t f = 0; f < nf; ++f) {
+        if (!on[f]) continue;
+        for (int k = 0; k < 4; ++k) {
+            const int64_t i = M->face_nodes[4 * f + k];
+            for (int j = 0; j < 3; ++j) V[3 * i + j] += vf[3 * f + j];
+            num[i]++;
+        }
+    }
+    std::memcpy(xyz2, xyz, sizeof(double) * 3 * nn);
+    for (int64_t i = 0; i < nn; ++i) {
+        if (!node_surf[i] || !o_surface_moves(P, node_surf[i])) continue;
+        double v[3] = {V[3 * i], V[3 * i + 1], V[3 * i + 2]};
+        if (num[i] > 0)
+            for (double& c : v) c /= num[i];
+        const double* A = xyz + 3 * i;
+        const double an = std::sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+        const double B[3] = {A[0] / an, A[1] / an, A[2] / an};
+        const double vb = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];
+        for (int k = 0; k < 3; ++k) xyz2[3 * i + k] = A[k] + vb * time * B[k];
+    }
+    // rays: the nodes between anchors keep their fraction of the segment
+    const int64_t RL = M->ray_len;
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < M->nray; ++r) {
+        const int32_t* rn = M->ray_nodes + r * RL;
+        const double* r0 = M->ray_r0 + r * RL;
+        const double* u = M->ray_dir + 3 * r;
+        int64_t a = 0;
+        for (int64_t b = 1; b < RL; ++b) {
+            if (b != RL - 1 && !node_surf[rn[b]]) continue;
+            const double* xa = xyz2 + 3 * (int64_t)rn[a];
+            const double* xb = xyz2 + 3 * (int64_t)rn[b];
+            const double ra = std::sqrt(xa[0] * xa[0] + xa[1] * xa[1] + xa[2] * xa[2]);
+            const double rb = std::sqrt(xb[0] * xb[0] + xb[1] * xb[1] + xb[2] * xb[2]);
+            for (int64_t j = a + 1; j < b; ++j) {
+                const double rj = ra + (r0[j] - r0[a]) / (r0[b] - r0[a]) * (rb - ra);
+                for (int k = 0; k < 3; ++k) xyz2[3 * (int64_t)rn[j] + k] = rj * u[k];
+            }
+            a = b;
+        }
+    }
+    return err;
+}
+
 // Second-order neighbours of every face, restating Setka::Init_TVD
 // (Setka_physics.cpp:646-738) on the geometry of `xyz`: beyond each side,
 // the neighbour through another face of that cell whose centre direction
@@ -1671,14 +1901,20 @@ int oracle_go(const OMesh* M, const OParams* P, double* state, double* xyz, cons
     for (int64_t step = 0; step < nsteps; ++step) {
         const double* X2 = xyz;
         const double* V2 = vol1.data();
+        int err = 0;
         if (P->move) {
-            oracle_move_nodes(M, P, xyz, xyz2.data(), tphys, time);
+            if (P->surface_motion) {
+                int64_t bad = -1;
+                err = o_surface_motion(M, P, state, xyz, xyz2.data(), cc1.data(), fc1.data(), fn1.data(), time, &bad);
+                if (err) info->err_index = bad;
+            } else {
+                oracle_move_nodes(M, P, xyz, xyz2.data(), tphys, time);
+            }
             oracle_geometry(M, xyz2.data(), cc2.data(), vol2.data(), fc2.data(), fn2.data(), fa2.data());
             X2 = xyz2.data();
             V2 = vol2.data();
         }
         double loc = 100000000.0;
-        int err = 0;
 #pragma omp parallel for schedule(static) reduction(min : loc)
         for (int64_t f = 0; f < nf; ++f) {
             int e = 0;

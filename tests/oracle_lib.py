@@ -42,6 +42,7 @@ class OMesh(ctypes.Structure):
         ("face_nodes", I32), ("face_cells", I32), ("face_type", I8), ("face_surf", I8),
         ("face_method", I8), ("face_bc", I32), ("bc_vals", D), ("node_amp", D), ("node_phase", D),
         ("face_tvd", I32),
+        ("ray_nodes", I32), ("ray_r0", D), ("ray_dir", D), ("nray", ctypes.c_int64), ("ray_len", ctypes.c_int64),
     ]
 
 
@@ -53,8 +54,14 @@ class OParams(ctypes.Structure):
         ("move", ctypes.c_int32), ("soft_fixups", ctypes.c_int32), ("method_policy", ctypes.c_int32),
         ("npassive", ctypes.c_int32), ("nh", ctypes.c_int32), ("TS_hard", ctypes.c_int32),
         ("contact_hard", ctypes.c_int32), ("tvd", ctypes.c_int32), ("snos_on_hp", ctypes.c_int32),
-        ("bn_in_p_on_hp", ctypes.c_int32), ("pad", ctypes.c_int32),
+        ("bn_in_p_on_hp", ctypes.c_int32), ("surface_motion", ctypes.c_int32),
+        ("move_TS", ctypes.c_int32), ("move_HP", ctypes.c_int32), ("move_BS", ctypes.c_int32),
+        ("null_bn_on_HP", ctypes.c_int32), ("pad2", ctypes.c_int32),
+        ("velocity_TS", ctypes.c_double), ("velocity_HP", ctypes.c_double), ("velocity_BS", ctypes.c_double),
     ]
+
+# The surface-tracking fields of OParams (titan_surface_params on the library side).
+SURFACE_KEYS = ("move_TS", "move_HP", "move_BS", "null_bn_on_HP", "velocity_TS", "velocity_HP", "velocity_BS")
 
 
 class OStepInfo(ctypes.Structure):
@@ -95,6 +102,7 @@ def oracle():
                                           ctypes.c_double, ctypes.c_double]
         lib.oracle_num_threads.restype = ctypes.c_int
         lib.oracle_tvd_neighbours.argtypes = [ctypes.POINTER(OMesh), D, I32]
+        lib.oracle_ray_geometry.argtypes = [ctypes.POINTER(OMesh), D, D, D]
         lib.oracle_godunov.argtypes = [D, ctypes.c_double, D, D, ctypes.c_int, ctypes.c_double, D, D]
         lib.oracle_godunov.restype = ctypes.c_int
         lib.oracle_face_states.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D, D, I8]
@@ -219,7 +227,10 @@ def random_riemann_cases(n: int, seed: int, *, weak_bn_frac=0.15, x_normal_frac=
 class OracleRun:
     """The oracle's step loop (oracle_go) on a mesh dict of titan_c-_b200.mesh."""
 
-    def __init__(self, mesh: dict, params: dict):
+    def __init__(self, mesh: dict, params: dict, surface: dict | None = None, rays: np.ndarray | None = None):
+        """surface / rays: surface-tracking node motion (the SURFACE_KEYS of
+        `surface`, rays [nray, ray_len] node ids from the inner end) instead of
+        the prescribed radial law."""
         self._keep = {}
 
         def keep(name, a, dt):
@@ -249,8 +260,19 @@ class OracleRun:
         self.mesh = m
         p = OParams()
         for k, _ in OParams._fields_:
-            if k != "pad":
+            if k not in ("pad2", "surface_motion") + SURFACE_KEYS:
                 setattr(p, k, params[k])
+        if surface is not None:
+            p.surface_motion = 1
+            for k in SURFACE_KEYS:
+                setattr(p, k, surface[k])
+            rn = keep("rays", rays, np.int32)
+            m.ray_nodes = _p(rn, I32)
+            m.nray, m.ray_len = rn.shape
+            r0 = keep("ray_r0", np.empty(rn.shape), np.float64)
+            rd = keep("ray_dir", np.empty((rn.shape[0], 3)), np.float64)
+            oracle().oracle_ray_geometry(ctypes.byref(m), _p(self.xyz), _p(r0), _p(rd))
+            m.ray_r0, m.ray_dir = _p(r0), _p(rd)
         self.params = p
         self.face_tvd = None
         if p.tvd:

@@ -1,0 +1,130 @@
+"""The oracle's surface-tracking node motion (Setka::Culc_Velocity_surface,
+TITAN/source/Setka_move.cpp:111-1358, and Luch::dvigenie, Luch.cpp:6-739)
+pinned by construction on the CPU:
+
+* with every surface held still the step equals the step on a mesh whose
+  nodes do not move, up to rounding (the rays place their nodes again from
+  the segment rule every step, as Luch::dvigenie does);
+* in a uniform flow every face's contact speed is the flow's normal speed, so
+  each HP node moves by dt times velocity_HP times the mean of (u . n) n over
+  its faces, projected on its radial direction — formed here in numpy from
+  the oracle's own face normals;
+* the other nodes of each ray stay on the ray, in order, at their initial
+  fraction of the segment between the surface nodes and the ray's ends;
+* null_bn_on_HP leaves the cells next to the HP without normal B."""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+
+def _shell(titan, nq=6, nlayer=10):
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=nq, nlayer=nlayer, move=True)
+    m["node_amp"] = np.zeros(m["node_xyz"].shape[0])
+    m["node_phase"] = np.zeros(m["node_xyz"].shape[0])
+    return m, p, st
+
+
+SURF = dict(velocity_TS=1.0, velocity_HP=1.0, velocity_BS=1.0, move_TS=1, move_HP=1, move_BS=1, null_bn_on_HP=0)
+
+
+def test_still_surfaces_give_the_fixed_mesh_step(titan, oracle_lib):
+    m, p, st = _shell(titan)
+    for layer, kind in ((4, 1), (6, 2), (8, 3)):
+        titan.mesh.mark_shell_surface(m, layer, kind)
+    rays = titan.mesh.shell_rays(m)
+    still = dict(SURF, move_TS=0, move_HP=0, move_BS=0)
+    a, b = np.ascontiguousarray(st.copy()), np.ascontiguousarray(st.copy())
+    ra = ol.OracleRun(m, p, surface=still, rays=rays)
+    rb = ol.OracleRun(m, p)            # prescribed motion with zero amplitude
+    x0 = ra.xyz.copy()
+    assert ra.go(a, 5).err_code == 0
+    assert rb.go(b, 5).err_code == 0
+    assert np.abs(ra.xyz - x0).max() <= 1e-15 * np.abs(x0).max()
+    for k in range(8):
+        assert np.abs(a[k] - b[k]).max() <= 1e-11 * np.abs(b[k]).max(), k
+
+
+def _uniform(m, u=(0.3, -0.2, 0.1), B=(0.05, 0.0, 0.1)):
+    C = m["cell_nodes"].shape[0]
+    st = np.zeros((10, C))
+    st[0], st[4] = 1.0, 1.0
+    st[1:4] = np.asarray(u)[:, None]
+    st[5:8] = np.asarray(B)[:, None]
+    return st
+
+
+def test_hp_nodes_move_with_the_contact_speed_of_a_uniform_flow(titan, oracle_lib):
+    m, p, _ = _shell(titan)
+    titan.mesh.mark_shell_surface(m, 5, 2)
+    rays = titan.mesh.shell_rays(m)
+    u = np.array([0.3, -0.2, 0.1])
+    st = np.ascontiguousarray(_uniform(m, u))
+    vel = 0.7
+    run = ol.OracleRun(m, p, surface=dict(SURF, velocity_HP=vel, move_TS=0, move_BS=0), rays=rays)
+    x0 = run.xyz.copy()
+    fn = run.geometry()["face_normal"]
+    dt = run.clock[0]
+    assert run.go(st, 1).err_code == 0
+    x1 = run.xyz
+    # numpy: mean over each HP node's faces of vel (u . n) n, projected on x/|x|
+    hp = np.nonzero(m["face_surf"] == 2)[0]
+    V = np.zeros_like(x0)
+    cnt = np.zeros(len(x0))
+    for f in hp:
+        for i in m["face_nodes"][f]:
+            V[i] += vel * (fn[f] @ u) * fn[f]
+            cnt[i] += 1
+    moved = cnt > 0
+    V[moved] /= cnt[moved, None]
+    B = x0[moved] / np.linalg.norm(x0[moved], axis=1, keepdims=True)
+    expect = x0[moved] + (np.sum(V[moved] * B, axis=1) * dt)[:, None] * B
+    np.testing.assert_allclose(x1[moved], expect, rtol=0, atol=1e-13 * np.abs(x0).max())
+    assert np.abs(x1[moved] - x0[moved]).max() > 1e-9 * dt * 1e5   # they did move
+
+
+def test_ray_nodes_keep_their_segment_fractions(titan, oracle_lib):
+    m, p, st = _shell(titan)
+    for layer, kind in ((4, 1), (6, 2), (8, 3)):
+        titan.mesh.mark_shell_surface(m, layer, kind)
+    rays = titan.mesh.shell_rays(m)
+    run = ol.OracleRun(m, p, surface=dict(SURF, velocity_TS=50.0, velocity_HP=50.0, velocity_BS=50.0), rays=rays)
+    x0 = run.xyz.copy()
+    s = np.ascontiguousarray(st.copy())
+    assert run.go(s, 3).err_code == 0
+    x1 = run.xyz
+    r0 = np.linalg.norm(x0[rays], axis=2)
+    r1 = np.linalg.norm(x1[rays], axis=2)
+    anchors = [0, 4, 6, 8, rays.shape[1] - 1]
+    assert np.abs(r1[:, [4, 6, 8]] - r0[:, [4, 6, 8]]).max() > 0     # the surfaces moved
+    assert np.array_equal(x1[rays[:, 0]], x0[rays[:, 0]])              # the ends did not
+    assert np.array_equal(x1[rays[:, -1]], x0[rays[:, -1]])
+    assert (np.diff(r1, axis=1) > 0).all()                             # order kept
+    d = x0[rays[:, 0]] / np.linalg.norm(x0[rays[:, 0]], axis=1, keepdims=True)
+    for a, b in zip(anchors[:-1], anchors[1:]):
+        for j in range(a + 1, b):
+            f0 = (r0[:, j] - r0[:, a]) / (r0[:, b] - r0[:, a])
+            f1 = (r1[:, j] - r1[:, a]) / (r1[:, b] - r1[:, a])
+            np.testing.assert_allclose(f1, f0, rtol=0, atol=1e-12)
+            cross = np.cross(x1[rays[:, j]], d)
+            assert np.abs(cross).max() <= 1e-12 * r1[:, j].max()
+
+
+def test_null_bn_on_hp_removes_the_normal_field_of_the_hp_cells(titan, oracle_lib):
+    m, p, _ = _shell(titan)
+    titan.mesh.mark_shell_surface(m, 5, 2)
+    rays = titan.mesh.shell_rays(m)
+    st = np.ascontiguousarray(_uniform(m, B=(0.3, -0.1, 0.2)))
+    run = ol.OracleRun(m, p, surface=dict(SURF, move_TS=0, move_BS=0, null_bn_on_HP=1), rays=rays)
+    fn = run.geometry()["face_normal"]
+    # after one step the HP cells' B . n is far below that of the same step
+    # without null_bn_on_HP (the step's own fluxes change B only a little)
+    ref = np.ascontiguousarray(st.copy())
+    run2 = ol.OracleRun(m, p, surface=dict(SURF, move_TS=0, move_BS=0, null_bn_on_HP=0), rays=rays)
+    assert run.go(st, 1).err_code == 0
+    assert run2.go(ref, 1).err_code == 0
+    hp = np.nonzero(m["face_surf"] == 2)[0]
+    cells = m["face_cells"][hp]
+    bn_null = np.abs(np.einsum("ij,ij->i", st[5:8, cells[:, 0]].T, fn[hp]))
+    bn_ref = np.abs(np.einsum("ij,ij->i", ref[5:8, cells[:, 0]].T, fn[hp]))
+    assert bn_null.mean() < 0.2 * bn_ref.mean(), (bn_null.mean(), bn_ref.mean())

@@ -317,7 +317,7 @@ namespace titan {
 
 struct GodunovFlux {
     double q[5];
-    double dsl, dsr;
+    double dsl, dsc, dsr;
     int rc;
 };
 
@@ -337,6 +337,7 @@ static __device__ __noinline__ GodunovFlux godunov_hp_face(double n0, double n1,
     double ds[3] = {0.0, 0.0, 0.0};
     g.rc = godunov_exact(nrm, w, q1, q2, contact, gamma, g.q, ds);
     g.dsl = ds[0];
+    g.dsc = ds[1];
     g.dsr = ds[2];
     return g;
 }

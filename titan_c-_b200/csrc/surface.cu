@@ -1,0 +1,194 @@
+// Surface-tracking node motion (-fmad=false, like the FP64 step): the
+// reference's Setka::Culc_Velocity_surface (TITAN/source/Setka_move.cpp:111-1358)
+// and Luch::dvigenie (Luch.cpp:6-739) for meshes whose rays are straight lines
+// of nodes.
+//
+//  1. Per moving surface, in the reference's order TS, HP, BS (so BS sees the
+//     HP cells' B as null_bn_on_HP left it): one thread per surface face forms
+//     the face's geometry on this layer and its reconstructed states, solves
+//     the Riemann problem at w = 0 and keeps velocity_X * ds * n, ds = dsl on
+//     TS, dsc on HP (the exact gas-dynamic solver with bn_in_p_on_HP), dsr on
+//     BS (Setka_move.cpp:128-447). HP faces with fewer than four surface
+//     neighbours are left out of the list (:192).
+//  2. One thread per surface node: the mean of its faces' contributions,
+//     summed in ascending original face order, and the move
+//     x' = x + (V . x/|x|) dt x/|x| (:1213-1265).
+//  3. One thread per ray: every node between two anchors (the ray's ends and
+//     its surface nodes) keeps its initial fraction of that segment, on the
+//     ray's direction.
+// The smoothing terms of the reference (sglag_*) are not part of this motion.
+#include "launch.h"
+#include "step_kernels.cuh"
+#include "surface.h"
+
+namespace titan {
+namespace surf {
+
+template <int NK, bool TVD>
+__global__ void __launch_bounds__(128) speed_kernel(FaceArgs a, SurfaceDev S, double* state_rw, int s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int pos = S.off[s] + i;
+    if (pos >= S.off[s + 1] || a.st->err_kind != 0) return;
+    const MeshView& M = a.M;
+    const Params& P = a.P;
+    const int nf = M.nface, nc = M.ncell, nn = M.nnode;
+    const int f = S.face_list[pos];
+    const int c0 = M.face_c0[f], c1 = M.face_c1[f];
+    // this layer's geometry of the face (Gran::Culc_measure)
+    double X[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) load_node(a.L1.xyz, nn, M.face_nodes[k * nf + f], X[k]);
+    double cA[3], cB[3];
+    load_cc(a.L1.cc, nc, c0, cA);
+    load_cc(a.L1.cc, nc, c1, cB);
+    const FaceGeom g = face_geometry(X, cA, cB);
+    const double n[3] = {g.n[0], g.n[1], g.n[2]};
+    double gc[3] = {g.c[0], g.c[1], g.c[2]};
+    const bool nullbn = (s == 2 && S.null_bn_on_hp);
+    if (nullbn) {
+        // the cells' own B loses its normal part (Setka_move.cpp:196-224)
+        const int cs[2] = {c0, c1};
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            double* bx = state_rw + 5 * nc + cs[j];
+            double* by = state_rw + 6 * nc + cs[j];
+            double* bz = state_rw + 7 * nc + cs[j];
+            const double dtpr = n[0] * *bx + n[1] * *by + n[2] * *bz;
+            *bx -= dtpr * n[0];
+            *by -= dtpr * n[1];
+            *bz -= dtpr * n[2];
+        }
+    }
+    double Ls[NV], Rs[NV];
+    face_states<NK, true, TVD, false>(a, f, 0, c0, n, gc, Ls, Rs);
+    int method;
+    if (P.method_policy == 1) {
+        const double bb =
+            ((Ls[5] * Ls[5] + Ls[6] * Ls[6] + Ls[7] * Ls[7]) + (Rs[5] * Rs[5] + Rs[6] * Rs[6] + Rs[7] * Rs[7])) / 2.0;
+        const double pp = (Ls[4] + Rs[4]) / 2.0;
+        method = (bb / (4.0 * kPi) / (2.0 * pp) > P.beta_switch) ? 3 : 2;
+    } else {
+        method = M.face_method[f];
+    }
+    if (nullbn) {
+        // and so do the face states (:279-295)
+        double* qs[2] = {Ls, Rs};
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            double* q = qs[j];
+            const double dtpr = n[0] * q[5] + n[1] * q[6] + n[2] * q[7];
+            q[5] -= dtpr * n[0];
+            q[6] -= dtpr * n[1];
+            q[7] -= dtpr * n[2];
+        }
+    }
+    double dsl = 0.0, dsc = 0.0, dsr = 0.0;
+    if (s == 2 && P.bn_in_p_on_hp) {
+        const GodunovFlux gd = godunov_hp_face(n[0], n[1], n[2], 0.0, Ls[0], Ls[1], Ls[2], Ls[3], Ls[4], Ls[5], Ls[6],
+                                               Ls[7], Rs[0], Rs[1], Rs[2], Rs[3], Rs[4], Rs[5], Rs[6], Rs[7], 0, P.gamma);
+        if (gd.rc) record_error(a.st, 14 + gd.rc, f);
+        dsl = gd.dsl;
+        dsc = gd.dsc;
+        dsr = gd.dsr;
+    } else {
+        double qd[8];
+        RiemannFlags fl;
+        fl.null_bn = false;
+        fl.left_ydar = false;
+        fl.contact = false;
+        fl.n_disc = 0;
+        const int rc = riemann_flux<double, 0>(method, n, 0.0, Ls, Rs, nullptr, nullptr, qd, nullptr, dsl, dsc, dsr,
+                                               fl, P.gamma);
+        if (rc) record_error(a.st, 10 + rc, f);
+    }
+    if (s == 2 && (isnan(dsc) || (dsc != 0.0 && fabs(dsc) < 2.2250738585072014e-308))) record_error(a.st, 19, f);
+    const double d = (s == 1) ? dsl : ((s == 2) ? dsc : dsr);
+    const double vd = S.vel[s] * d;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) S.vf[k * S.nlist + pos] = vd * n[k];
+}
+
+__global__ void node_kernel(FaceArgs a, SurfaceDev S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n_node || a.st->err_kind != 0) return;
+    const int nn = a.M.nnode;
+    const int id = S.node_id[i];
+    double v[3] = {0.0, 0.0, 0.0};
+    const int j0 = S.node_ptr[i], j1 = S.node_ptr[i + 1];
+    for (int j = j0; j < j1; ++j) {
+        const int pos = S.node_face[j];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) v[k] += S.vf[k * S.nlist + pos];
+    }
+    const int num = j1 - j0;
+    if (num > 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) v[k] /= num;
+    }
+    double A[3];
+    load_node(a.L1.xyz, nn, id, A);
+    const double an = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+    const double B[3] = {A[0] / an, A[1] / an, A[2] / an};
+    const double vb = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];
+    const double time = a.st->dt;
+    double* x2 = const_cast<double*>(a.xyz2);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) x2[k * nn + id] = A[k] + vb * time * B[k];
+}
+
+__global__ void ray_kernel(FaceArgs a, SurfaceDev S) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= S.nray || a.st->err_kind != 0) return;
+    const int nn = a.M.nnode, L = S.ray_len;
+    const int* rn = S.ray_nodes + (size_t)r * L;
+    const double* r0 = S.ray_r0 + (size_t)r * L;
+    const unsigned char* an = S.ray_anchor + (size_t)r * L;
+    const double u[3] = {S.ray_dir[3 * r], S.ray_dir[3 * r + 1], S.ray_dir[3 * r + 2]};
+    double* x2 = const_cast<double*>(a.xyz2);
+    int ja = 0;
+    double xa[3];
+    load_node(x2, nn, rn[0], xa);
+    double ra = sqrt(xa[0] * xa[0] + xa[1] * xa[1] + xa[2] * xa[2]);
+    for (int jb = 1; jb < L; ++jb) {
+        if (!an[jb]) continue;
+        double xb[3];
+        load_node(x2, nn, rn[jb], xb);
+        const double rb = sqrt(xb[0] * xb[0] + xb[1] * xb[1] + xb[2] * xb[2]);
+        for (int j = ja + 1; j < jb; ++j) {
+            const double rj = ra + (r0[j] - r0[ja]) / (r0[jb] - r0[ja]) * (rb - ra);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) x2[k * nn + rn[j]] = rj * u[k];
+        }
+        ja = jb;
+        ra = rb;
+    }
+}
+
+}  // namespace surf
+
+template <int NK, bool TVD>
+static void launch_speeds(const FaceArgs& fa, double* state_rw, const SurfaceDev& S, cudaStream_t s) {
+    for (int sf = 1; sf <= 3; ++sf) {
+        const int n = S.off[sf + 1] - S.off[sf];
+        if (n > 0) surf::speed_kernel<NK, TVD><<<blocks_for(n, 128), 128, 0, s>>>(fa, S, state_rw, sf);
+    }
+}
+
+cudaError_t launch_surface_motion(const FaceArgs& fa, double* state_rw, const SurfaceDev& S, int nk, bool tvd,
+                                  cudaStream_t s) {
+    const int nn = fa.M.nnode;
+    // nodes that neither a surface nor a ray moves keep their place
+    cudaError_t e = cudaMemcpyAsync(const_cast<double*>(fa.xyz2), fa.L1.xyz, sizeof(double) * 3 * (size_t)nn,
+                                    cudaMemcpyDeviceToDevice, s);
+    if (e) return e;
+    if (nk == 0 && !tvd) launch_speeds<0, false>(fa, state_rw, S, s);
+    else if (nk == 0 && tvd) launch_speeds<0, true>(fa, state_rw, S, s);
+    else if (nk == 2 && !tvd) launch_speeds<2, false>(fa, state_rw, S, s);
+    else if (nk == 2 && tvd) launch_speeds<2, true>(fa, state_rw, S, s);
+    else return cudaErrorInvalidValue;
+    if (S.n_node > 0) surf::node_kernel<<<blocks_for(S.n_node, 128), 128, 0, s>>>(fa, S);
+    if (S.nray > 0) surf::ray_kernel<<<blocks_for(S.nray, 128), 128, 0, s>>>(fa, S);
+    return cudaGetLastError();
+}
+
+}  // namespace titan

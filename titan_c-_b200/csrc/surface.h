@@ -1,0 +1,41 @@
+// Surface-tracking node motion (surface.cu): the device tables built by
+// titan_set_surface_motion and the launcher that replaces the prescribed
+// node motion of a step.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "step_types.h"
+
+namespace titan {
+
+struct SurfaceDev {
+    // moving surface faces, grouped by surface (1 TS, 2 HP, 3 BS): positions
+    // off[s] .. off[s+1]-1 of face_list hold surface s's faces (device ids)
+    int off[5];
+    const int* face_list;
+    double* vf;             // [3][nlist]: velocity_X * ds * n of each listed face
+    int nlist;
+    // moving surface nodes and, per node, its faces' list positions in
+    // ascending original face index
+    int n_node;
+    const int* node_id;     // [n_node] device node ids
+    const int* node_ptr;    // [n_node + 1]
+    const int* node_face;   // list positions
+    // rays: device node ids from the inner end, radii and direction at the
+    // start of tracking, anchors (ends and surface nodes)
+    int nray, ray_len;
+    const int* ray_nodes;
+    const double* ray_r0;
+    const double* ray_dir;  // [nray][3]
+    const unsigned char* ray_anchor;
+    double vel[4];          // velocity_TS / _HP / _BS at [1] / [2] / [3]
+    int null_bn_on_hp;
+};
+
+// xyz2 of `fa` from xyz of fa.L1 by surface tracking, with the step's dt from
+// the status word. state_rw is fa.state, writable: null_bn_on_HP removes the
+// normal B of the HP cells.
+cudaError_t launch_surface_motion(const FaceArgs& fa, double* state_rw, const SurfaceDev& S, int nk, bool tvd,
+                                  cudaStream_t s);
+
+}  // namespace titan

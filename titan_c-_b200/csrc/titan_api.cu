@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -16,6 +17,7 @@
 #include "launch.h"
 #include "mc.h"
 #include "renumber.h"
+#include "surface.h"
 
 using namespace titan;
 
@@ -112,6 +114,11 @@ struct titan_ctx {
     double closure_ninf = 0.0, closure_lambda = 0.0;
     int sm_count = 148;
 
+    // surface-tracking node motion (titan_set_surface_motion)
+    bool use_surface = false;
+    SurfaceDev surf{};
+    void* surf_buf[9] = {};  // face_list, vf, node_id, node_ptr, node_face, ray_nodes, ray_r0, ray_dir, ray_anchor
+
     // Monte-Carlo pass buffers (titan_mc_sources), allocated by the first pass
     McCell* d_mc_cells = nullptr;       // [ncell] tracing records
     double* d_mc_cdf = nullptr;         // [nface] inflow CDF
@@ -197,7 +204,23 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     const bool move = ctx->prm.move != 0;
     const int nxt = ctx->cur ^ 1;
     cudaError_t e = cudaSuccess;
-    if (move) {
+    if (move && ctx->use_surface) {
+        // nodes follow the TS / HP / BS surfaces (Setka::Culc_Velocity_surface,
+        // Luch::dvigenie) on this state; null_bn_on_HP may edit the HP cells' B
+        FaceArgs sa;
+        sa.M = M;
+        sa.P = ctx->P;
+        sa.L1 = ctx->layer[ctx->cur];
+        sa.xyz2 = ctx->layer[nxt].xyz;
+        sa.state = ctx->d_state[ctx->scur];
+        sa.flux = nullptr;
+        sa.st = ctx->d_status;
+        e = timed(ctx, "surface_motion", [&] {
+            return launch_surface_motion(sa, ctx->d_state[ctx->scur], ctx->surf, ctx->prm.npassive, ctx->P.tvd != 0,
+                                         ctx->stream);
+        });
+        if (e) return e;
+    } else if (move) {
         // the geometry of the next layer is formed inside face_flux (faces of
         // this layer) and cell_update (cells of the next layer)
         e = timed(ctx, "move_nodes", [&] {
@@ -367,6 +390,27 @@ std::string validate(const titan_mesh* m, const titan_params* p) {
 
 }  // namespace
 
+namespace {
+
+void drop_surface(titan_ctx* ctx) {
+    for (void*& p : ctx->surf_buf) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    ctx->surf = SurfaceDev{};
+    ctx->use_surface = false;
+}
+
+template <typename T>
+cudaError_t upload_vec(void** slot, const std::vector<T>& v) {
+    if (v.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc(slot, sizeof(T) * v.size());
+    if (!e) e = cudaMemcpy(*slot, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    return e;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* titan_version(void) { return "titan-b200 0.1 (sm_100a)"; }
@@ -385,6 +429,8 @@ int titan_destroy(titan_ctx* ctx) {
                     ctx->d_env, ctx->d_fallback, ctx->d_n_outside, ctx->d_mc_cells, ctx->d_mc_cdf,
                     ctx->d_mc_blocks, ctx->d_mc_tally, ctx->d_mc_lost};
     for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (void* p : ctx->surf_buf)
         if (p) cudaFree(p);
     // without node motion layer[1] aliases layer[0]: free it once
     const int nlayers = (ctx->layer[1].xyz != ctx->layer[0].xyz) ? 2 : 1;
@@ -1134,6 +1180,132 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, tit
         info->inflow_rate = total;
         info->gpu_ms = ms;
     }
+    return TITAN_OK;
+}
+
+int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int64_t nray, int32_t ray_len,
+                             const int32_t* ray_nodes) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    drop_graph(ctx);
+    drop_surface(ctx);
+    if (!sp) return TITAN_OK;
+    if (!ctx->prm.move) return fail(TITAN_EINVAL, "surface tracking needs a context created with move = 1");
+    if (nray <= 0 || ray_len < 2 || !ray_nodes) return fail(TITAN_EINVAL, "rays: nray > 0, ray_len >= 2 and ids");
+    const int64_t nf = ctx->nface, nn = ctx->nnode;
+    const Renumbering& R = ctx->R;
+    // mesh tables in device numbering
+    std::vector<int8_t> surf(nf), ftype(nf);
+    std::vector<int32_t> fnodes(4 * nf);
+    CK(cudaMemcpy(surf.data(), ctx->d_face_surf, nf, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ftype.data(), ctx->d_face_type, nf, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(fnodes.data(), ctx->d_face_nodes, sizeof(int32_t) * 4 * nf, cudaMemcpyDeviceToHost));
+    auto moves = [&](int s) {
+        return (s == 1 && sp->move_TS) || (s == 2 && sp->move_HP) || (s == 3 && sp->move_BS);
+    };
+    // surface neighbours of each surface face (Gran::grans_surf): faces of the
+    // same surface across each edge
+    std::map<std::tuple<int32_t, int32_t, int>, int> edges;
+    auto edge = [&](int64_t f, int k) {
+        int32_t a = fnodes[k * nf + f], b = fnodes[((k + 1) % 4) * nf + f];
+        if (a > b) std::swap(a, b);
+        return std::make_tuple(a, b, (int)surf[f]);
+    };
+    for (int64_t f = 0; f < nf; ++f)
+        if (surf[f] >= 1 && surf[f] <= 3)
+            for (int k = 0; k < 4; ++k) edges[edge(f, k)]++;
+    std::vector<int8_t> node_surf(nn, 0);
+    std::vector<std::vector<int32_t>> by_surf(4);
+    for (int64_t f = 0; f < nf; ++f) {
+        const int s = surf[f];
+        if (s < 1 || s > 3) continue;
+        for (int k = 0; k < 4; ++k) node_surf[fnodes[k * nf + f]] = (int8_t)s;
+        if (!moves(s) || ftype[f] != 0) continue;
+        if (s == 2) {
+            int nb = 0;
+            for (int k = 0; k < 4; ++k) nb += edges[edge(f, k)] - 1;
+            if (nb < 4) continue;
+        }
+        by_surf[s].push_back((int32_t)f);
+    }
+    SurfaceDev S{};
+    std::vector<int32_t> face_list;
+    S.off[0] = S.off[1] = 0;
+    for (int s = 1; s <= 3; ++s) {
+        face_list.insert(face_list.end(), by_surf[s].begin(), by_surf[s].end());
+        S.off[s + 1] = (int)face_list.size();
+    }
+    S.nlist = (int)face_list.size();
+    // per moving surface node: its faces' list positions, ascending original face index
+    std::vector<std::vector<std::pair<int32_t, int32_t>>> nf_of(nn);
+    for (int pos = 0; pos < S.nlist; ++pos) {
+        const int64_t f = face_list[pos];
+        for (int k = 0; k < 4; ++k) nf_of[fnodes[k * nf + f]].push_back({R.face_n2o[f], pos});
+    }
+    std::vector<int32_t> node_id, node_ptr{0}, node_face;
+    for (int64_t i = 0; i < nn; ++i) {
+        if (!node_surf[i] || !moves(node_surf[i])) continue;
+        auto& v = nf_of[i];
+        std::sort(v.begin(), v.end());
+        node_id.push_back((int32_t)i);
+        for (auto& pr : v) node_face.push_back(pr.second);
+        node_ptr.push_back((int32_t)node_face.size());
+    }
+    S.n_node = (int)node_id.size();
+    // rays in device numbering, with the radii and directions of this layer
+    std::vector<double> xyz(3 * nn);
+    CK(cudaMemcpy(xyz.data(), ctx->layer[ctx->cur].xyz, sizeof(double) * 3 * nn, cudaMemcpyDeviceToHost));
+    const int64_t L = ray_len;
+    std::vector<int32_t> rn(nray * L);
+    std::vector<double> r0(nray * L), dir(3 * nray);
+    std::vector<uint8_t> anchor(nray * L), seen(nn, 0);
+    for (int64_t r = 0; r < nray; ++r) {
+        for (int64_t j = 0; j < L; ++j) {
+            const int32_t o = ray_nodes[r * L + j];
+            if (o < 0 || o >= nn) return fail(TITAN_EINVAL, "ray node id out of range");
+            const int32_t d = R.node_o2n[o];
+            if (seen[d]++) return fail(TITAN_EINVAL, "a node lies on two rays, or twice on one");
+            rn[r * L + j] = d;
+            const double x = xyz[d], y = xyz[nn + d], z = xyz[2 * nn + d];
+            r0[r * L + j] = std::sqrt(x * x + y * y + z * z);
+            anchor[r * L + j] = (j == 0 || j == L - 1 || node_surf[d] != 0) ? 1 : 0;
+        }
+        const int32_t d0 = rn[r * L];
+        const double x = xyz[d0], y = xyz[nn + d0], z = xyz[2 * nn + d0];
+        const double n0 = std::sqrt(x * x + y * y + z * z);
+        dir[3 * r] = x / n0;
+        dir[3 * r + 1] = y / n0;
+        dir[3 * r + 2] = z / n0;
+    }
+    S.nray = (int)nray;
+    S.ray_len = ray_len;
+    S.vel[1] = sp->velocity_TS;
+    S.vel[2] = sp->velocity_HP;
+    S.vel[3] = sp->velocity_BS;
+    S.null_bn_on_hp = sp->null_bn_on_HP;
+    cudaError_t e = upload_vec(&ctx->surf_buf[0], face_list);
+    if (!e && S.nlist) e = cudaMalloc(&ctx->surf_buf[1], sizeof(double) * 3 * S.nlist);
+    if (!e) e = upload_vec(&ctx->surf_buf[2], node_id);
+    if (!e) e = upload_vec(&ctx->surf_buf[3], node_ptr);
+    if (!e) e = upload_vec(&ctx->surf_buf[4], node_face);
+    if (!e) e = upload_vec(&ctx->surf_buf[5], rn);
+    if (!e) e = upload_vec(&ctx->surf_buf[6], r0);
+    if (!e) e = upload_vec(&ctx->surf_buf[7], dir);
+    if (!e) e = upload_vec(&ctx->surf_buf[8], anchor);
+    if (e) {
+        drop_surface(ctx);
+        return fail(TITAN_ECUDA, std::string("surface tables: ") + cudaGetErrorString(e));
+    }
+    S.face_list = (const int*)ctx->surf_buf[0];
+    S.vf = (double*)ctx->surf_buf[1];
+    S.node_id = (const int*)ctx->surf_buf[2];
+    S.node_ptr = (const int*)ctx->surf_buf[3];
+    S.node_face = (const int*)ctx->surf_buf[4];
+    S.ray_nodes = (const int*)ctx->surf_buf[5];
+    S.ray_r0 = (const double*)ctx->surf_buf[6];
+    S.ray_dir = (const double*)ctx->surf_buf[7];
+    S.ray_anchor = (const unsigned char*)ctx->surf_buf[8];
+    ctx->surf = S;
+    ctx->use_surface = true;
     return TITAN_OK;
 }
 

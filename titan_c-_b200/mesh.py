@@ -180,6 +180,23 @@ def shell_mesh(nq: int, nlayer: int, r0: float = 1.0, r1: float = 100.0, outer_h
     return mesh
 
 
+def shell_rays(mesh: dict) -> np.ndarray:
+    """The shell's rays (Luch): node ids [6 nq^2 + 2, nlayer + 1], each a radial
+    line of nodes from the inner sphere outwards."""
+    layer, ray = mesh["node_layer"], mesh["node_ray"]
+    out = np.empty((int(ray.max()) + 1, int(layer.max()) + 1), dtype=np.int32)
+    out[ray, layer] = np.arange(len(ray), dtype=np.int32)
+    return out
+
+
+def mark_shell_surface(mesh: dict, layer: int, kind: int) -> None:
+    """face_surf = kind (1 TS, 2 HP, 3 BS, Type_Gran_surf) on the spherical
+    faces whose nodes all lie on node layer `layer` (an interior layer)."""
+    on = np.all(mesh["node_layer"][mesh["face_nodes"]] == layer, axis=1)
+    assert on.any() and not (mesh["face_type"][on] != 0).any(), "an interior node layer"
+    mesh["face_surf"][on] = kind
+
+
 def hex_geometry(mesh: dict, xyz: np.ndarray | None = None):
     """numpy geometry (cell centres, volumes, face centres, normals, areas) for tests."""
     xyz = mesh["node_xyz"] if xyz is None else xyz

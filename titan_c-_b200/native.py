@@ -63,6 +63,12 @@ class TitanDevMesh(ctypes.Structure):
             "face_half_dist", "hfluids")]
 
 
+class TitanSurfaceParams(ctypes.Structure):
+    _fields_ = [("velocity_TS", ctypes.c_double), ("velocity_HP", ctypes.c_double), ("velocity_BS", ctypes.c_double),
+                ("move_TS", ctypes.c_int32), ("move_HP", ctypes.c_int32), ("move_BS", ctypes.c_int32),
+                ("null_bn_on_HP", ctypes.c_int32)]
+
+
 class TitanMcParams(ctypes.Structure):
     _fields_ = [("n_H", ctypes.c_double), ("u_H", ctypes.c_double * 3), ("cp_H", ctypes.c_double),
                 ("n_particles", ctypes.c_int64), ("seed", ctypes.c_uint64), ("max_cells", ctypes.c_int32),
@@ -99,6 +105,8 @@ SIGNATURES = {
                      ctypes.c_int),
     "titan_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "titan_set_face_method": ([ctypes.c_void_p, I8], ctypes.c_int),
+    "titan_set_surface_motion": ([ctypes.c_void_p, ctypes.POINTER(TitanSurfaceParams), ctypes.c_int64,
+                                  ctypes.c_int32, I32], ctypes.c_int),
     "titan_upload_state": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_download_state": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_upload_hfluids": ([ctypes.c_void_p, D], ctypes.c_int),

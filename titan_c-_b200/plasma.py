@@ -95,6 +95,20 @@ class PlasmaStep:
         a = np.ascontiguousarray(n_state, dtype=np.int8)
         N.check(self._lib.titan_set_face_method(self._ctx, N.ptr(a, N.I8)))
 
+    def set_surface_motion(self, rays: np.ndarray | None, **surface):
+        """Surface-tracking node motion (titan_set_surface_motion): rays [nray,
+        ray_len] node ids from the inner end; surface: velocity_TS/_HP/_BS,
+        move_TS/_HP/_BS, null_bn_on_HP. rays None returns to the prescribed motion."""
+        if rays is None:
+            N.check(self._lib.titan_set_surface_motion(self._ctx, None, 0, 0, None))
+            return
+        sp = N.TitanSurfaceParams()
+        for k, _ in N.TitanSurfaceParams._fields_:
+            setattr(sp, k, surface.get(k, 0))
+        r = np.ascontiguousarray(rays, dtype=np.int32)
+        N.check(self._lib.titan_set_surface_motion(self._ctx, ctypes.byref(sp), r.shape[0], r.shape[1],
+                                                   N.ptr(r, N.I32)))
+
     def upload_state(self, state: np.ndarray):
         a = np.ascontiguousarray(state, dtype=np.float64)
         assert a.shape == (N.NV, self.ncell)

@@ -1557,7 +1557,7 @@ void oracle_move_nodes(const OMesh* M, const OParams* P, const double* xyz1, dou
 //  * Along each ray the end nodes and the surface nodes are anchors; every
 //    other node keeps its initial fraction of the segment between the
 //    anchors around it, on the ray's direction (the reference's A_Luch
-//    spacing is a fixed function of that fraction, Luch.cpp:47-200).
+//    spacing is a fixed function of that fraction, Luch.cpp:9-152).
 // ---------------------------------------------------------------------------
 
 // Radii and directions of the rays at `xyz` (the start of tracking).

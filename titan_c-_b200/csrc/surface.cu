@@ -13,9 +13,9 @@
 //  2. One thread per surface node: the mean of its faces' contributions,
 //     summed in ascending original face order, and the move
 //     x' = x + (V . x/|x|) dt x/|x| (:1213-1265).
-//  3. One thread per ray: every node between two anchors (the ray's ends and
-//     its surface nodes) keeps its initial fraction of that segment, on the
-//     ray's direction.
+//  3. One thread per ray node: every node between two anchors (the ray's ends
+//     and its surface nodes) keeps its initial fraction of that segment, on
+//     the ray's direction.
 // The smoothing terms of the reference (sglag_*) are not part of this motion.
 #include "launch.h"
 #include "step_kernels.cuh"
@@ -24,11 +24,13 @@
 namespace titan {
 namespace surf {
 
+// Surfaces s_lo..s_hi in one launch (their list positions are contiguous).
 template <int NK, bool TVD>
-__global__ void __launch_bounds__(128) speed_kernel(FaceArgs a, SurfaceDev S, double* state_rw, int s) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int pos = S.off[s] + i;
-    if (pos >= S.off[s + 1] || a.st->err_kind != 0) return;
+__global__ void __launch_bounds__(128) speed_kernel(FaceArgs a, SurfaceDev S, double* state_rw, int s_lo, int s_hi) {
+    const int pos = S.off[s_lo] + blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= S.off[s_hi + 1] || a.st->err_kind != 0) return;
+    int s = s_lo;
+    while (pos >= S.off[s + 1]) ++s;
     const MeshView& M = a.M;
     const Params& P = a.P;
     const int nf = M.nface, nc = M.ncell, nn = M.nnode;
@@ -136,41 +138,43 @@ __global__ void node_kernel(FaceArgs a, SurfaceDev S) {
     for (int k = 0; k < 3; ++k) x2[k * nn + id] = A[k] + vb * time * B[k];
 }
 
+// One thread per ray slot: a node that is not an anchor takes its place
+// between the anchors around it (ray_seg: their slots, set up once).
 __global__ void ray_kernel(FaceArgs a, SurfaceDev S) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= S.nray || a.st->err_kind != 0) return;
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= (long long)S.nray * S.ray_len || a.st->err_kind != 0) return;
+    const int2 seg = S.ray_seg[q];
+    if (seg.x < 0) return;  // an anchor
     const int nn = a.M.nnode, L = S.ray_len;
-    const int* rn = S.ray_nodes + (size_t)r * L;
-    const double* r0 = S.ray_r0 + (size_t)r * L;
-    const unsigned char* an = S.ray_anchor + (size_t)r * L;
-    const double u[3] = {S.ray_dir[3 * r], S.ray_dir[3 * r + 1], S.ray_dir[3 * r + 2]};
+    const int r = (int)(q / L);
+    const long long base = (long long)r * L;
+    const double* x2c = a.xyz2;
+    double xa[3], xb[3];
+    load_node(x2c, nn, S.ray_nodes[base + seg.x], xa);
+    load_node(x2c, nn, S.ray_nodes[base + seg.y], xb);
+    const double ra = sqrt(xa[0] * xa[0] + xa[1] * xa[1] + xa[2] * xa[2]);
+    const double rb = sqrt(xb[0] * xb[0] + xb[1] * xb[1] + xb[2] * xb[2]);
+    const double r0a = S.ray_r0[base + seg.x], r0b = S.ray_r0[base + seg.y];
+    const double rj = ra + (S.ray_r0[q] - r0a) / (r0b - r0a) * (rb - ra);
     double* x2 = const_cast<double*>(a.xyz2);
-    int ja = 0;
-    double xa[3];
-    load_node(x2, nn, rn[0], xa);
-    double ra = sqrt(xa[0] * xa[0] + xa[1] * xa[1] + xa[2] * xa[2]);
-    for (int jb = 1; jb < L; ++jb) {
-        if (!an[jb]) continue;
-        double xb[3];
-        load_node(x2, nn, rn[jb], xb);
-        const double rb = sqrt(xb[0] * xb[0] + xb[1] * xb[1] + xb[2] * xb[2]);
-        for (int j = ja + 1; j < jb; ++j) {
-            const double rj = ra + (r0[j] - r0[ja]) / (r0[jb] - r0[ja]) * (rb - ra);
+    const int id = S.ray_nodes[q];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) x2[k * nn + rn[j]] = rj * u[k];
-        }
-        ja = jb;
-        ra = rb;
-    }
+    for (int k = 0; k < 3; ++k) x2[k * nn + id] = rj * S.ray_dir[3 * r + k];
 }
 
 }  // namespace surf
 
 template <int NK, bool TVD>
 static void launch_speeds(const FaceArgs& fa, double* state_rw, const SurfaceDev& S, cudaStream_t s) {
-    for (int sf = 1; sf <= 3; ++sf) {
-        const int n = S.off[sf + 1] - S.off[sf];
-        if (n > 0) surf::speed_kernel<NK, TVD><<<blocks_for(n, 128), 128, 0, s>>>(fa, S, state_rw, sf);
+    auto run = [&](int lo, int hi) {
+        const int n = S.off[hi + 1] - S.off[lo];
+        if (n > 0) surf::speed_kernel<NK, TVD><<<blocks_for(n, 128), 128, 0, s>>>(fa, S, state_rw, lo, hi);
+    };
+    if (S.null_bn_on_hp) {
+        // HP edits the cells' B: TS before it, BS after it, as the reference runs them
+        for (int sf = 1; sf <= 3; ++sf) run(sf, sf);
+    } else {
+        run(1, 3);
     }
 }
 
@@ -187,7 +191,7 @@ cudaError_t launch_surface_motion(const FaceArgs& fa, double* state_rw, const Su
     else if (nk == 2 && tvd) launch_speeds<2, true>(fa, state_rw, S, s);
     else return cudaErrorInvalidValue;
     if (S.n_node > 0) surf::node_kernel<<<blocks_for(S.n_node, 128), 128, 0, s>>>(fa, S);
-    if (S.nray > 0) surf::ray_kernel<<<blocks_for(S.nray, 128), 128, 0, s>>>(fa, S);
+    if (S.nray > 0) surf::ray_kernel<<<blocks_for((long long)S.nray * S.ray_len, 256), 256, 0, s>>>(fa, S);
     return cudaGetLastError();
 }
 

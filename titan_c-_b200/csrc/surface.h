@@ -27,7 +27,7 @@ struct SurfaceDev {
     const int* ray_nodes;
     const double* ray_r0;
     const double* ray_dir;  // [nray][3]
-    const unsigned char* ray_anchor;
+    const int2* ray_seg;    // [nray][ray_len]: slots of the anchors around a node, (-1, -1) for an anchor
     double vel[4];          // velocity_TS / _HP / _BS at [1] / [2] / [3]
     int null_bn_on_hp;
 };

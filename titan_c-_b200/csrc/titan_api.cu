@@ -117,7 +117,7 @@ struct titan_ctx {
     // surface-tracking node motion (titan_set_surface_motion)
     bool use_surface = false;
     SurfaceDev surf{};
-    void* surf_buf[9] = {};  // face_list, vf, node_id, node_ptr, node_face, ray_nodes, ray_r0, ray_dir, ray_anchor
+    void* surf_buf[9] = {};  // face_list, vf, node_id, node_ptr, node_face, ray_nodes, ray_r0, ray_dir, ray_seg
 
     // Monte-Carlo pass buffers (titan_mc_sources), allocated by the first pass
     McCell* d_mc_cells = nullptr;       // [ncell] tracing records
@@ -1258,6 +1258,7 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     std::vector<int32_t> rn(nray * L);
     std::vector<double> r0(nray * L), dir(3 * nray);
     std::vector<uint8_t> anchor(nray * L), seen(nn, 0);
+    std::vector<int2> seg(nray * L);
     for (int64_t r = 0; r < nray; ++r) {
         for (int64_t j = 0; j < L; ++j) {
             const int32_t o = ray_nodes[r * L + j];
@@ -1269,6 +1270,13 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
             r0[r * L + j] = std::sqrt(x * x + y * y + z * z);
             anchor[r * L + j] = (j == 0 || j == L - 1 || node_surf[d] != 0) ? 1 : 0;
         }
+        for (int64_t a = 0, b = 1; b < L; ++b) {
+            if (!anchor[r * L + b]) continue;
+            seg[r * L + a] = make_int2(-1, -1);
+            for (int64_t j = a + 1; j < b; ++j) seg[r * L + j] = make_int2((int)a, (int)b);
+            a = b;
+        }
+        seg[r * L + L - 1] = make_int2(-1, -1);
         const int32_t d0 = rn[r * L];
         const double x = xyz[d0], y = xyz[nn + d0], z = xyz[2 * nn + d0];
         const double n0 = std::sqrt(x * x + y * y + z * z);
@@ -1290,7 +1298,7 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     if (!e) e = upload_vec(&ctx->surf_buf[5], rn);
     if (!e) e = upload_vec(&ctx->surf_buf[6], r0);
     if (!e) e = upload_vec(&ctx->surf_buf[7], dir);
-    if (!e) e = upload_vec(&ctx->surf_buf[8], anchor);
+    if (!e) e = upload_vec(&ctx->surf_buf[8], seg);
     if (e) {
         drop_surface(ctx);
         return fail(TITAN_ECUDA, std::string("surface tables: ") + cudaGetErrorString(e));
@@ -1303,7 +1311,7 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     S.ray_nodes = (const int*)ctx->surf_buf[5];
     S.ray_r0 = (const double*)ctx->surf_buf[6];
     S.ray_dir = (const double*)ctx->surf_buf[7];
-    S.ray_anchor = (const unsigned char*)ctx->surf_buf[8];
+    S.ray_seg = (const int2*)ctx->surf_buf[8];
     ctx->surf = S;
     ctx->use_surface = true;
     return TITAN_OK;

@@ -144,8 +144,9 @@ int titan_set_face_method(titan_ctx* ctx, const int8_t* n_state);
  * faces use the exact gas-dynamic solver). The other nodes of each ray keep
  * their fraction of the segment between the surface nodes and the ray's
  * ends, on the ray's direction. rays: nray x ray_len node ids (original
- * numbering) from the inner end; no node on two rays; radii and directions are
- * taken from the current nodes. The reference's smoothing terms (sglag_*)
+ * numbering) from the inner end, a shorter ray padded with -1 after its last
+ * node; no node on two rays; radii and directions are taken from the current
+ * nodes. The reference's smoothing terms (sglag_*)
  * are not applied. params NULL returns to the prescribed motion. */
 typedef struct titan_surface_params {
     double velocity_TS, velocity_HP, velocity_BS; /* Phys_param::velocity_TS / _HP / _BS */

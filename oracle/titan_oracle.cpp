@@ -1554,10 +1554,11 @@ void oracle_move_nodes(const OMesh* M, const OParams* P, const double* xyz1, dou
 //    and moves along its own direction: x' = x + (V . x/|x|) dt x/|x|
 //    (:1213-1265; the reference's heliotail rays are parallel to the x axis
 //    and move HP nodes with x < 0 along (0, y, z); these rays are all radial).
-//  * Along each ray the end nodes and the surface nodes are anchors; every
-//    other node keeps its initial fraction of the segment between the
-//    anchors around it, on the ray's direction (the reference's A_Luch
-//    spacing is a fixed function of that fraction, Luch.cpp:9-152).
+//  * Along each ray (a shorter one padded with -1) the end nodes and the
+//    surface nodes are anchors; every other node keeps its initial fraction
+//    of the segment between the anchors around it, on the ray's direction
+//    (the reference's A_Luch spacing is a fixed function of that fraction,
+//    Luch.cpp:9-152).
 // ---------------------------------------------------------------------------
 
 // Radii and directions of the rays at `xyz` (the start of tracking).
@@ -1566,6 +1567,10 @@ void oracle_ray_geometry(const OMesh* M, const double* xyz, double* r0, double* 
     for (int64_t r = 0; r < M->nray; ++r) {
         for (int64_t j = 0; j < L; ++j) {
             const int64_t i = M->ray_nodes[r * L + j];
+            if (i < 0) {  // padding after a shorter ray's last node
+                r0[r * L + j] = 0.0;
+                continue;
+            }
             const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
             r0[r * L + j] = std::sqrt(x * x + y * y + z * z);
         }
@@ -1734,9 +1739,11 @@ static int o_surface_motion(const OMesh* M, const OParams* P, double* st, const 
         const int32_t* rn = M->ray_nodes + r * RL;
         const double* r0 = M->ray_r0 + r * RL;
         const double* u = M->ray_dir + 3 * r;
+        int64_t Lr = 0;
+        while (Lr < RL && rn[Lr] >= 0) ++Lr;
         int64_t a = 0;
-        for (int64_t b = 1; b < RL; ++b) {
-            if (b != RL - 1 && !node_surf[rn[b]]) continue;
+        for (int64_t b = 1; b < Lr; ++b) {
+            if (b != Lr - 1 && !node_surf[rn[b]]) continue;
             const double* xa = xyz2 + 3 * (int64_t)rn[a];
             const double* xb = xyz2 + 3 * (int64_t)rn[b];
             const double ra = std::sqrt(xa[0] * xa[0] + xa[1] * xa[1] + xa[2] * xa[2]);

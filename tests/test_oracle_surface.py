@@ -128,3 +128,22 @@ def test_null_bn_on_hp_removes_the_normal_field_of_the_hp_cells(titan, oracle_li
     bn_null = np.abs(np.einsum("ij,ij->i", st[5:8, cells[:, 0]].T, fn[hp]))
     bn_ref = np.abs(np.einsum("ij,ij->i", ref[5:8, cells[:, 0]].T, fn[hp]))
     assert bn_null.mean() < 0.2 * bn_ref.mean(), (bn_null.mean(), bn_ref.mean())
+
+
+def test_a_shorter_ray_ends_at_its_last_node(titan, oracle_lib):
+    """Rays of different lengths: a ray padded with -1 treats its last node as
+    its outer end; the node it leaves out stays where it is."""
+    m, p, st = _shell(titan)
+    for layer, kind in ((4, 1), (6, 2), (8, 3)):
+        titan.mesh.mark_shell_surface(m, layer, kind)
+    rays = titan.mesh.shell_rays(m)
+    short = rays.copy()
+    short[::2, -1] = -1
+    run = ol.OracleRun(m, p, surface=dict(SURF, velocity_TS=50.0, velocity_HP=50.0, velocity_BS=50.0), rays=short)
+    x0 = run.xyz.copy()
+    s = np.ascontiguousarray(st.copy())
+    assert run.go(s, 2).err_code == 0
+    x1 = run.xyz
+    assert np.array_equal(x1[rays[::2, -1]], x0[rays[::2, -1]])     # left out
+    assert np.array_equal(x1[rays[::2, -2]], x0[rays[::2, -2]])     # the new outer end
+    assert not np.array_equal(x1[rays[::2, -3]], x0[rays[::2, -3]])  # its BS node still moves

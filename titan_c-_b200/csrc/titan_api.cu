@@ -1260,23 +1260,32 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     std::vector<uint8_t> anchor(nray * L), seen(nn, 0);
     std::vector<int2> seg(nray * L);
     for (int64_t r = 0; r < nray; ++r) {
+        // a shorter ray ends at its first -1
+        int64_t Lr = 0;
+        while (Lr < L && ray_nodes[r * L + Lr] >= 0) ++Lr;
+        if (Lr < 2) return fail(TITAN_EINVAL, "a ray needs at least two nodes");
         for (int64_t j = 0; j < L; ++j) {
             const int32_t o = ray_nodes[r * L + j];
-            if (o < 0 || o >= nn) return fail(TITAN_EINVAL, "ray node id out of range");
+            seg[r * L + j] = make_int2(-1, -1);
+            if (j >= Lr) {
+                if (o != -1) return fail(TITAN_EINVAL, "a ray's padding after its first -1 must be -1");
+                rn[r * L + j] = -1;
+                r0[r * L + j] = 0.0;
+                continue;
+            }
+            if (o >= nn) return fail(TITAN_EINVAL, "ray node id out of range");
             const int32_t d = R.node_o2n[o];
             if (seen[d]++) return fail(TITAN_EINVAL, "a node lies on two rays, or twice on one");
             rn[r * L + j] = d;
             const double x = xyz[d], y = xyz[nn + d], z = xyz[2 * nn + d];
             r0[r * L + j] = std::sqrt(x * x + y * y + z * z);
-            anchor[r * L + j] = (j == 0 || j == L - 1 || node_surf[d] != 0) ? 1 : 0;
+            anchor[r * L + j] = (j == 0 || j == Lr - 1 || node_surf[d] != 0) ? 1 : 0;
         }
-        for (int64_t a = 0, b = 1; b < L; ++b) {
+        for (int64_t a = 0, b = 1; b < Lr; ++b) {
             if (!anchor[r * L + b]) continue;
-            seg[r * L + a] = make_int2(-1, -1);
             for (int64_t j = a + 1; j < b; ++j) seg[r * L + j] = make_int2((int)a, (int)b);
             a = b;
         }
-        seg[r * L + L - 1] = make_int2(-1, -1);
         const int32_t d0 = rn[r * L];
         const double x = xyz[d0], y = xyz[nn + d0], z = xyz[2 * nn + d0];
         const double n0 = std::sqrt(x * x + y * y + z * z);

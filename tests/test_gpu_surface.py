@@ -60,8 +60,8 @@ def test_surface_tracking_steps_match_oracle(titan, oracle_lib, variant):
     r0, r1 = np.linalg.norm(x0[rays], axis=2), np.linalg.norm(x[rays], axis=2)
     assert np.abs(r1[:, [7, 9, 11]] - r0[:, [7, 9, 11]]).max() > 0
     assert np.array_equal(x[rays[:, 0]], x0[rays[:, 0]])
-    ends = np.where(rays[:, -1] >= 0, rays[:, -1], rays[:, -2])
-    assert np.array_equal(x[ends], x0[ends])
+    full = rays[:, -1] >= 0
+    assert np.array_equal(x[rays[full, -1]], x0[rays[full, -1]])
     gpu.close()
 
 

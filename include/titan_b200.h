@@ -158,6 +158,19 @@ typedef struct titan_surface_params {
 int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* params, int64_t nray, int32_t ray_len,
                              const int32_t* ray_nodes);
 
+/* Halo exchange of a sharded step (several contexts, one per GPU, each on the
+ * cells one rank owns plus a layer of copies of its neighbours' cells; no
+ * reference counterpart: the reference runs one OpenMP process per mesh).
+ * send_ids: this context's cells that other ranks keep copies of; recv_ids:
+ * its copies, both in the context's original numbering and in the order the
+ * peers agree on. titan_pack_halo writes the send cells' states, whole cells
+ * of 8 + npassive doubles each ([n_send][ns]), to a DEVICE buffer on this
+ * context's GPU; titan_unpack_halo writes a device buffer of the same form
+ * into the copies. Both return when the copy is done. */
+int titan_set_halo(titan_ctx* ctx, int64_t n_send, const int32_t* send_ids, int64_t n_recv, const int32_t* recv_ids);
+int titan_pack_halo(titan_ctx* ctx, double* out_device);
+int titan_unpack_halo(titan_ctx* ctx, const double* in_device);
+
 /* Cell::parameters[now] for all cells, SoA [TITAN_NV][ncell], original order.
  * Only the rows the context carries (8 + npassive) travel: the download leaves
  * the others as the caller has them, as the reference's step leaves the

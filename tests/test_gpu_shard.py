@@ -1,0 +1,72 @@
+"""The sharded step's device side on one GPU: two contexts on the two halves
+of a shell (titan.shard sub-meshes), their halo cells moved through device
+buffers by titan_pack_halo / titan_unpack_halo, stepped one after the other
+with the minimum dt, give the owned cells bit for bit as one context on the
+whole shell. (Ranks on separate GPUs move the same buffers with NCCL; the
+CPU tests run that protocol with gloo.)"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_two_contexts_exchanging_halos_match_one_context(titan, world):
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=8, nlayer=8, move=True, npassive=2)
+    S = titan.shard
+    dev = torch.device("cuda:0")
+    owner = S.partition(m, world)
+    ranks = []
+    for r in range(world):
+        sh = S.build_shard(m, owner, r)
+        step = titan.PlasmaStep(sh["mesh"], p)
+        step.upload_state(np.ascontiguousarray(st[:, sh["cells"]]))
+        bufs = {q: torch.empty((len(ids), 10), dtype=torch.float64, device=dev) for q, ids in sh["send"].items()}
+        ranks.append((sh, step, bufs))
+    ns = 8 + p["npassive"]
+    full = titan.PlasmaStep(m, p)
+    full.upload_state(st)
+    for _ in range(6):
+        # every rank packs what each peer needs, then unpacks what it receives
+        for sh, step, bufs in ranks:
+            for q, ids in sh["send"].items():
+                step.set_halo(ids, np.zeros(0, np.int32))
+                step.pack_halo(bufs[q].data_ptr())
+        for r, (sh, step, _) in enumerate(ranks):
+            for q, ids in sh["recv"].items():
+                src = ranks[q][2][r]
+                step.set_halo(np.zeros(0, np.int32), ids)
+                step.unpack_halo(src.data_ptr())
+        torch.cuda.synchronize()
+        for sh, step, _ in ranks:
+            step.go(1)
+        dt = min(step.dt for _, step, _ in ranks)
+        for _, step, _ in ranks:
+            step.dt = dt
+        full.go(1)
+        assert full.dt == dt
+    ref = full.download_state()
+    for sh, step, _ in ranks:
+        n = sh["n_owned"]
+        got = step.download_state()[:ns, :n]
+        assert np.array_equal(got, ref[:ns, sh["cells"][:n]])
+        step.close()
+    full.close()
+
+
+def test_pack_unpack_round_trip(titan):
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=6, nlayer=6, move=False)
+    g = titan.PlasmaStep(m, p)
+    g.upload_state(st)
+    ids = np.arange(0, g.ncell, 7, dtype=np.int32)
+    buf = torch.empty((len(ids), 8), dtype=torch.float64, device="cuda:0")
+    g.set_halo(ids, ids[::-1].copy())
+    g.pack_halo(buf.data_ptr())
+    np.testing.assert_array_equal(buf.cpu().numpy(), st[:8, ids].T)
+    g.unpack_halo(buf.data_ptr())                 # the same cells, in reverse order
+    got = g.download_state()
+    np.testing.assert_array_equal(got[:8, ids[::-1]], st[:8, ids])
+    with pytest.raises(titan.native.TitanError):
+        g.set_halo(np.array([g.ncell], np.int32), np.zeros(0, np.int32))
+    g.close()

@@ -8,7 +8,7 @@ learned charge-exchange closure's host side (`closure`), and the build
 script (`build`). The directory name is not a Python identifier, so it is
 imported with importlib: ``importlib.import_module("titan_c-_b200")``.
 """
-from . import closure, mesh, native, problems  # noqa: F401
+from . import closure, mesh, native, problems, shard  # noqa: F401
 from .native import FIELDS, NV, TitanError  # noqa: F401
 from .plasma import PlasmaStep, chlld  # noqa: F401
 

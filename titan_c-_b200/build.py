@@ -9,6 +9,7 @@ Translation units and their floating-point flags:
   kernels_tvd_fp64.cu, kernels_tvd_fp32.cu   the same with second-order faces
   kernels_cell.cu  -fmad=false  cell update (gather, update, sources, floors, next-layer geometry)
   surface.cu       -fmad=false  surface-tracking node motion (TS / HP / BS speeds, rays)
+  halo.cu                       whole-cell copies for the halo exchange of a sharded step
   mc_neutral.cu                 Monte-Carlo neutral hydrogen (source generator)
   closure_mlp.cu                closure inference on tcgen05 / TMEM (per step)
   closure_train.cu, closure_api.cu   closure training (BF16 tensor-core GEMMs), C ABI
@@ -38,6 +39,7 @@ UNITS = [
     ("kernels_tvd_fp64.cu", ["-fmad=false"]),
     ("kernels_cell.cu", ["-fmad=false"]),
     ("surface.cu", ["-fmad=false"]),
+    ("halo.cu", []),
     ("kernels_tvd_fp32.cu", ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("mc_neutral.cu", []),
     ("closure_mlp.cu", []),

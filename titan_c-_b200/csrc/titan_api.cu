@@ -14,6 +14,7 @@
 
 #include "../../include/titan_b200.h"
 #include "closure.h"
+#include "halo.h"
 #include "launch.h"
 #include "mc.h"
 #include "renumber.h"
@@ -113,6 +114,11 @@ struct titan_ctx {
     unsigned long long* d_n_outside = nullptr;
     double closure_ninf = 0.0, closure_lambda = 0.0;
     int sm_count = 148;
+
+    // halo exchange of a sharded step (titan_set_halo): renumbered cell ids
+    int32_t* d_halo_send = nullptr;
+    int32_t* d_halo_recv = nullptr;
+    int64_t n_halo_send = 0, n_halo_recv = 0;
 
     // surface-tracking node motion (titan_set_surface_motion)
     bool use_surface = false;
@@ -432,6 +438,8 @@ int titan_destroy(titan_ctx* ctx) {
         if (p) cudaFree(p);
     for (void* p : ctx->surf_buf)
         if (p) cudaFree(p);
+    if (ctx->d_halo_send) cudaFree(ctx->d_halo_send);
+    if (ctx->d_halo_recv) cudaFree(ctx->d_halo_recv);
     // without node motion layer[1] aliases layer[0]: free it once
     const int nlayers = (ctx->layer[1].xyz != ctx->layer[0].xyz) ? 2 : 1;
     for (int l = 0; l < nlayers; ++l) {
@@ -702,6 +710,54 @@ int titan_set_face_method(titan_ctx* ctx, const int8_t* ns) {
         h[f] = v;
     }
     CK(cudaMemcpyAsync(ctx->d_face_method, h.data(), h.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TITAN_OK;
+}
+
+int titan_set_halo(titan_ctx* ctx, int64_t n_send, const int32_t* send_ids, int64_t n_recv,
+                   const int32_t* recv_ids) {
+    if (!ctx || n_send < 0 || n_recv < 0 || (n_send && !send_ids) || (n_recv && !recv_ids))
+        return fail(TITAN_EINVAL, "bad argument");
+    const int64_t nc = ctx->ncell;
+    std::vector<int32_t> s(n_send), r(n_recv);
+    for (int64_t i = 0; i < n_send; ++i) {
+        if (send_ids[i] < 0 || send_ids[i] >= nc) return fail(TITAN_EINVAL, "halo cell id out of range");
+        s[i] = ctx->R.cell_o2n[send_ids[i]];
+    }
+    for (int64_t i = 0; i < n_recv; ++i) {
+        if (recv_ids[i] < 0 || recv_ids[i] >= nc) return fail(TITAN_EINVAL, "halo cell id out of range");
+        r[i] = ctx->R.cell_o2n[recv_ids[i]];
+    }
+    if (ctx->d_halo_send) cudaFree(ctx->d_halo_send);
+    if (ctx->d_halo_recv) cudaFree(ctx->d_halo_recv);
+    ctx->d_halo_send = ctx->d_halo_recv = nullptr;
+    ctx->n_halo_send = ctx->n_halo_recv = 0;
+    int64_t tmp = 0;
+    if (n_send) {
+        CK(dalloc(&ctx->d_halo_send, (size_t)n_send, &tmp));
+        CK(cudaMemcpy(ctx->d_halo_send, s.data(), sizeof(int32_t) * n_send, cudaMemcpyHostToDevice));
+    }
+    if (n_recv) {
+        CK(dalloc(&ctx->d_halo_recv, (size_t)n_recv, &tmp));
+        CK(cudaMemcpy(ctx->d_halo_recv, r.data(), sizeof(int32_t) * n_recv, cudaMemcpyHostToDevice));
+    }
+    ctx->n_halo_send = n_send;
+    ctx->n_halo_recv = n_recv;
+    return TITAN_OK;
+}
+
+int titan_pack_halo(titan_ctx* ctx, double* out) {
+    if (!ctx || (ctx->n_halo_send && !out)) return fail(TITAN_EINVAL, "bad argument");
+    CK(launch_halo_pack(ctx->d_state[ctx->scur], (int)ctx->ncell, ctx->d_halo_send, (int)ctx->n_halo_send, ctx->ns,
+                        out, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TITAN_OK;
+}
+
+int titan_unpack_halo(titan_ctx* ctx, const double* in) {
+    if (!ctx || (ctx->n_halo_recv && !in)) return fail(TITAN_EINVAL, "bad argument");
+    CK(launch_halo_unpack(ctx->d_state[ctx->scur], (int)ctx->ncell, ctx->d_halo_recv, (int)ctx->n_halo_recv,
+                          ctx->ns, in, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return TITAN_OK;
 }

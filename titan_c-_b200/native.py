@@ -136,6 +136,9 @@ SIGNATURES = {
     "titan_set_closure_fallback": ([ctypes.c_void_p, F32, F32, D], ctypes.c_int),
     "titan_closure_outside": ([ctypes.c_void_p, I64], ctypes.c_int),
     "titan_closure_fallback_from_mc": ([ctypes.c_void_p], ctypes.c_int),
+    "titan_set_halo": ([ctypes.c_void_p, ctypes.c_int64, I32, ctypes.c_int64, I32], ctypes.c_int),
+    "titan_pack_halo": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "titan_unpack_halo": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "titan_autotune": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p], ctypes.c_int),
     "titan_set_tuning": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
     "titan_get_tuning": ([ctypes.c_void_p, I32, I32, I32, I32, I32], ctypes.c_int),

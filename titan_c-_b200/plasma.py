@@ -109,6 +109,20 @@ class PlasmaStep:
         N.check(self._lib.titan_set_surface_motion(self._ctx, ctypes.byref(sp), r.shape[0], r.shape[1],
                                                    N.ptr(r, N.I32)))
 
+    def set_halo(self, send_ids: np.ndarray, recv_ids: np.ndarray):
+        """Cells this context sends to / receives from its peers in a sharded step (titan_set_halo)."""
+        s = np.ascontiguousarray(send_ids, dtype=np.int32)
+        r = np.ascontiguousarray(recv_ids, dtype=np.int32)
+        N.check(self._lib.titan_set_halo(self._ctx, len(s), N.ptr(s, N.I32), len(r), N.ptr(r, N.I32)))
+
+    def pack_halo(self, out_device_ptr: int):
+        """The send cells' states, [n_send][8 + npassive], into a device buffer (address)."""
+        N.check(self._lib.titan_pack_halo(self._ctx, ctypes.c_void_p(out_device_ptr)))
+
+    def unpack_halo(self, in_device_ptr: int):
+        """A device buffer [n_recv][8 + npassive] into the received cells."""
+        N.check(self._lib.titan_unpack_halo(self._ctx, ctypes.c_void_p(in_device_ptr)))
+
     def upload_state(self, state: np.ndarray):
         a = np.ascontiguousarray(state, dtype=np.float64)
         assert a.shape == (N.NV, self.ncell)

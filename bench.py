@@ -433,6 +433,59 @@ def cpu_baseline(args, m, p, st, steps=None):
                                       f"({dt:.1f} s), oracle/titan_oracle.cpp with OpenMP"}
 
 
+def run_sharded(args, rank, world):
+    """One shell split over the ranks (titan.shard: Morton ranges, one-cell halo
+    exchanged over NCCL each step, dt as the minimum over the ranks): strong
+    scaling of the FP64 or FP32-flux step. Opt-in (--shard); without it,
+    --gpus N runs N replicas."""
+    import torch
+
+    if args.mode not in ("fp64", "fp32"):
+        raise SystemExit("--shard runs the fp64 or fp32 step (the closure and the Monte-Carlo are not sharded)")
+    dev = rank % max(torch.cuda.device_count(), 1)
+    torch.cuda.set_device(dev)
+    pkg, m, p, st = build_problem(args)
+    C = m["cell_nodes"].shape[0]
+    flux = 64 if args.mode == "fp64" else 32
+    ss = pkg.shard.ShardedStep(pkg, m, dict(p, flux_precision=flux), rank, world, torch.device("cuda", dev))
+    ss.upload_state(st)
+    tuning = ss.step.step.autotune(reps=3) if args.tuning == "auto" else None
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    ss.go(max(args.warmup, 3))
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(dev) as clk:
+        ev0.record()
+        ss.go(args.steps)
+        ev1.record()
+        barrier()
+    t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms = float(t[0])
+    clocks = clk.summary()
+    ss.close()
+    if rank != 0:
+        return None
+    value = C * args.steps / (ms / 1e3)
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64" if flux == 64 else "f32-flux/f64-update",
+        "data": "synthetic (seeded heliosphere-like shell; no external data)",
+        "config": {"workload": f"heliosphere shell 6x{args.nq}x{args.nq}x{args.nlayer} = {C} cells split over "
+                               f"{world} GPUs (Morton ranges, one-cell halo over NCCL)",
+                   "cells": C, "mode": args.mode, "parallelism": f"sharded x{world}", "tuning": tuning},
+        "gpu_launches": None, "clocks": clocks,
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -472,6 +525,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--tuning", default="auto", help="auto, or 'face_variant,cell_variant'")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--shard", action="store_true",
+                    help="split one mesh over the GPUs (strong scaling) instead of N replicas")
     args = ap.parse_args()
     if args.impl == "reference":
         # a bounded sample of the workload: a full step is about 0.35 s on 16 host threads
@@ -486,7 +541,12 @@ def main():
 
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    line = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world)
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    elif args.shard:
+        line = run_sharded(args, rank, world)
+    else:
+        line = run_ours(args, rank, world)
     if world > 1 and args.impl == "ours":
         import torch
 

@@ -208,6 +208,9 @@ class ShardedStep:
         self.sbuf = torch.empty((max(len(send), 1), self.ns), dtype=torch.float64, device=device)
         self.rbuf = torch.empty((max(len(recv), 1), self.ns), dtype=torch.float64, device=device)
         self.n_send, self.n_recv = len(send), len(recv)
+        if torch.distributed.is_initialized():
+            # every rank meets here before the first point-to-point exchange
+            torch.distributed.barrier()
 
     def upload_state(self, state: np.ndarray):
         """The global state [10, C]; each rank takes its local cells."""
@@ -244,9 +247,10 @@ class ShardedStep:
         for _ in range(steps):
             self.exchange()
             self.step.go(1)
-            t = self.torch.tensor([self.step.dt], dtype=self.torch.float64, device=self.device)
-            dist.all_reduce(t, op=dist.ReduceOp.MIN)
-            self.step.dt = float(t.item())
+            if self.world > 1:
+                t = self.torch.tensor([self.step.dt], dtype=self.torch.float64, device=self.device)
+                dist.all_reduce(t, op=dist.ReduceOp.MIN)
+                self.step.dt = float(t.item())
 
     def close(self):
         self.step.close()

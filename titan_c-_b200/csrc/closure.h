@@ -142,4 +142,12 @@ struct ClosureDev {
 cudaError_t closure_create(const float* params, const float* norm, ClosureDev* d, cudaStream_t s);
 void closure_destroy(ClosureDev* d);
 
+// One training step of titan_mlp_train: the batch's first row, the learning
+// rate, Adam's bias corrections 1 - beta^t, and the epoch its loss adds to.
+struct TrainSched {
+    long long r0;
+    float lr, c1, c2;
+    int epoch;
+};
+
 }  // namespace titan

@@ -27,6 +27,12 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, int n, flo
                         float c1, float c2, const unsigned char* mask, cudaStream_t s);
 cudaError_t launch_to_bf16(const float* x, void* y, int n, cudaStream_t s);
 cudaError_t launch_input(const float* X, const float* mean, const float* istd, void* X0, int rows, cudaStream_t s);
+cudaError_t launch_input_sched(const float* X, const float* mean, const float* istd, void* X0, int rows,
+                               const TrainSched* sched, const int* step, cudaStream_t s);
+cudaError_t launch_loss_sched(const float* Y, const float* T, const float* w, const float* rw, int rows, void* dY,
+                              float* loss_epoch, const TrainSched* sched, const int* step, cudaStream_t s);
+cudaError_t launch_adam_sched(float* p, const float* g, float* m, float* v, int n, float b1, float b2, float eps,
+                              const unsigned char* mask, const TrainSched* sched, int* step, cudaStream_t s);
 cudaError_t launch_pack(const float* P, void* out, cudaStream_t s);
 
 namespace {
@@ -116,10 +122,12 @@ cudaError_t forward(Trainer& t, const float* params, cudaStream_t s) {
     return e;
 }
 
-cudaError_t backward(Trainer& t, const float* T, const float* w, const float* rw, cudaStream_t s) {
+// Gradients of one batch: `loss` forms dY (and adds up the loss); then the
+// layers backwards.
+template <typename Loss>
+cudaError_t backward_with(Trainer& t, Loss loss, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(t.grad, 0, sizeof(float) * kNParam, s);
-    if (!e) e = cudaMemsetAsync(t.loss, 0, sizeof(float), s);
-    if (!e) e = launch_loss(t.Z[4], T, w, rw, t.rows, t.dY, t.loss, s);
+    if (!e) e = loss();
     const char* Wb = static_cast<const char*>(t.Wb);
     const void* dZl = t.dY;
     const int split = t.rows >= 8192 ? 32 : (t.rows >= 1024 ? 8 : 1);
@@ -138,6 +146,13 @@ cudaError_t backward(Trainer& t, const float* T, const float* w, const float* rw
         }
     }
     return e;
+}
+
+cudaError_t backward(Trainer& t, const float* T, const float* w, const float* rw, cudaStream_t s) {
+    return backward_with(t, [&] {
+        cudaError_t e = cudaMemsetAsync(t.loss, 0, sizeof(float), s);
+        return e ? e : launch_loss(t.Z[4], T, w, rw, t.rows, t.dY, t.loss, s);
+    }, s);
 }
 
 bool alloc_trainer(Buf& b, Trainer& t, int rows) {
@@ -275,7 +290,29 @@ int titan_mlp_train(float* params, const float* norm, const float* X, const floa
     float* dw = b.get<float>(kOut);
     float* dnorm = b.get<float>(2 * kIn + kOut);
     float* drw = row_w ? b.get<float>((size_t)n) : nullptr;
+    const int64_t nb = n / B;  // full batches per epoch (rows are pre-shuffled by the caller)
+    // the schedule of every step: which batch, and Adam's scalars
+    std::vector<TrainSched> sched;
+    sched.reserve((size_t)(nb * o->epochs));
+    long long step = 0;
+    for (int ep = 0; ep < o->epochs; ++ep)
+        for (int64_t bi = 0; bi < nb; ++bi) {
+            ++step;
+            TrainSched q;
+            q.r0 = ((bi + (int64_t)ep * 7919) % nb) * B;
+            q.c1 = 1.0f - std::pow(o->beta1, (float)step);
+            q.c2 = 1.0f - std::pow(o->beta2, (float)step);
+            q.lr = o->lr * (o->lr_decay > 0.0f ? std::pow(o->lr_decay, (float)ep) : 1.0f);
+            q.epoch = ep;
+            sched.push_back(q);
+        }
+    TrainSched* dS = b.get<TrainSched>(sched.size() + 1);
+    int* dstep = b.get<int>(1);
+    float* dloss = b.get<float>((size_t)o->epochs);
     if (b.err) return mfail(TITAN_ENOMEM, "titan_mlp_train: device memory");
+    // a stream of its own: the batch is captured into a graph from it
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+        return mfail(TITAN_ECUDA, "titan_mlp_train: stream");
     const std::vector<unsigned char> mask = param_mask();
     cudaError_t e = cudaMemcpyAsync(dP, params, sizeof(float) * kNParam, cudaMemcpyHostToDevice, s);
     if (!e) e = cudaMemsetAsync(dm, 0, sizeof(float) * kNParam, s);
@@ -286,31 +323,38 @@ int titan_mlp_train(float* params, const float* norm, const float* X, const floa
     if (!e) e = cudaMemcpyAsync(dw, w, sizeof(float) * kOut, cudaMemcpyHostToDevice, s);
     if (!e) e = cudaMemcpyAsync(dnorm, norm, sizeof(float) * (2 * kIn + kOut), cudaMemcpyHostToDevice, s);
     if (!e && drw) e = cudaMemcpyAsync(drw, row_w, sizeof(float) * n, cudaMemcpyHostToDevice, s);
-    const int64_t nb = n / B;  // full batches per epoch (rows are pre-shuffled by the caller)
-    long long step = 0;
-    for (int ep = 0; ep < o->epochs && !e; ++ep) {
-        double ep_loss = 0.0;
-        for (int64_t bi = 0; bi < nb && !e; ++bi) {
-            const int64_t r0 = ((bi + (int64_t)ep * 7919) % nb) * B;
-            e = launch_input(dX + r0 * kIn, dnorm, dnorm + kIn, t.X0, B, s);
-            if (!e) e = forward(t, dP, s);
-            if (!e) e = backward(t, dT + r0 * kOut, dw, drw ? drw + r0 : nullptr, s);
-            ++step;
-            const float c1 = 1.0f - std::pow(o->beta1, (float)step), c2 = 1.0f - std::pow(o->beta2, (float)step);
-            const float lr = o->lr * (o->lr_decay > 0.0f ? std::pow(o->lr_decay, (float)ep) : 1.0f);
-            if (!e) e = launch_adam(dP, t.grad, dm, dv, kNParam, lr, o->beta1, o->beta2, 1e-8f, c1, c2, dmask, s);
-            if (!e && loss_per_epoch) {
-                float l = 0.0f;
-                e = cudaMemcpyAsync(&l, t.loss, sizeof(float), cudaMemcpyDeviceToHost, s);
-                if (!e) e = cudaStreamSynchronize(s);
-                ep_loss += l;
-            }
+    if (!e && !sched.empty())
+        e = cudaMemcpyAsync(dS, sched.data(), sizeof(TrainSched) * sched.size(), cudaMemcpyHostToDevice, s);
+    if (!e) e = cudaMemsetAsync(dstep, 0, sizeof(int), s);
+    if (!e) e = cudaMemsetAsync(dloss, 0, sizeof(float) * o->epochs, s);
+    // one batch captured once and replayed for every step
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    if (!e && !sched.empty()) {
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (!e) {
+            cudaError_t ec = launch_input_sched(dX, dnorm, dnorm + kIn, t.X0, B, dS, dstep, s);
+            if (!ec) ec = forward(t, dP, s);
+            if (!ec) ec = backward_with(t, [&] {
+                return launch_loss_sched(t.Z[4], dT, dw, drw, t.rows, t.dY, dloss, dS, dstep, s);
+            }, s);
+            if (!ec) ec = launch_adam_sched(dP, t.grad, dm, dv, kNParam, o->beta1, o->beta2, 1e-8f, dmask, dS, dstep, s);
+            e = cudaStreamEndCapture(s, &g);
+            if (!e) e = ec;
         }
-        if (loss_per_epoch) loss_per_epoch[ep] = (float)(ep_loss / (double)(nb > 0 ? nb : 1));
+        if (!e) e = cudaGraphInstantiate(&ge, g, 0);
+        for (size_t k = 0; k < sched.size() && !e; ++k) e = cudaGraphLaunch(ge, s);
     }
+    std::vector<float> el((size_t)o->epochs, 0.0f);
+    if (!e) e = cudaMemcpyAsync(el.data(), dloss, sizeof(float) * o->epochs, cudaMemcpyDeviceToHost, s);
     if (!e) e = cudaMemcpyAsync(params, dP, sizeof(float) * kNParam, cudaMemcpyDeviceToHost, s);
     if (!e) e = cudaStreamSynchronize(s);
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    if (s) cudaStreamDestroy(s);
     if (e) return mfail(TITAN_ECUDA, std::string("titan_mlp_train: ") + cudaGetErrorString(e));
+    if (loss_per_epoch)
+        for (int ep = 0; ep < o->epochs; ++ep) loss_per_epoch[ep] = el[ep] / (float)(nb > 0 ? nb : 1);
     return TITAN_OK;
 }
 

@@ -65,15 +65,17 @@ __global__ void __launch_bounds__(128) gemm_kernel(int M, int N, int K, const __
     const __nv_bfloat16 zero = __float2bfloat16(0.0f);
     for (int kc = kc0; kc < kc1; ++kc) {
         const int k0 = kc * BK;
+        // staging runs along the operand's contiguous dimension in memory, so
+        // that a warp's loads coalesce (m for A^T, k for A; n for B, k for B^T)
         for (int i = tid; i < BM * BK; i += 128) {
-            const int mm = i / BK, kk = i % BK;
+            const int mm = TA ? i % BM : i / BK, kk = TA ? i / BM : i % BK;
             const int gm = m0 + mm, gk = k0 + kk;
             __nv_bfloat16 v = zero;
             if (gm < M && gk < K) v = TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
             As[mm][kk] = v;
         }
         for (int i = tid; i < BN * BK; i += 128) {
-            const int nn = i / BK, kk = i % BK;
+            const int nn = TB ? i / BK : i % BN, kk = TB ? i % BK : i / BN;
             const int gn = n0 + nn, gk = k0 + kk;
             __nv_bfloat16 v = zero;
             if (gn < N && gk < K) v = TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
@@ -134,11 +136,13 @@ __global__ void dsilu_kernel(const float* dA, const float* Z, __nv_bfloat16* dZ,
     if (i < n) dZ[i] = __float2bfloat16(dA[i] * dsilu(Z[i]));
 }
 
-// Column sums of a bf16 matrix into db (atomic), for bias gradients.
+// Column sums of a bf16 matrix into db (atomic), for bias gradients; a block
+// sums kColsumRows rows, so a batch of a few thousand rows spreads over many SMs.
+constexpr int kColsumRows = 32;
 __global__ void colsum_kernel(const __nv_bfloat16* X, int rows, int cols, float* db) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cols) return;
-    const int r0 = blockIdx.y * 256, r1 = min(rows, r0 + 256);
+    const int r0 = blockIdx.y * kColsumRows, r1 = min(rows, r0 + kColsumRows);
     float s = 0.0f;
     for (int r = r0; r < r1; ++r) s += __bfloat162float(X[(size_t)r * cols + c]);
     atomicAdd(db + c, s);
@@ -184,6 +188,59 @@ __global__ void adam_kernel(float* p, const float* g, float* m, float* v, int n,
     v[i] = vi;
     p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
+
+// ---- graph-replayed training: the batch's row offset and Adam scalars come
+// from a schedule on the device, indexed by a step counter that the last
+// kernel of each batch advances, so one captured batch replays for all.
+
+__global__ void input_sched_kernel(const float* X, const float* mean, const float* istd, __nv_bfloat16* X0, int rows,
+                                   const TrainSched* sched, const int* step) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)rows * kInPad) return;
+    const long long r0 = sched[*step].r0;
+    const int r = (int)(i / kInPad), k = (int)(i % kInPad);
+    X0[i] = __float2bfloat16(k < kIn ? (X[(size_t)(r0 + r) * kIn + k] - mean[k]) * istd[k] : 0.0f);
+}
+
+__global__ void loss_sched_kernel(const float* Y, const float* T, const float* w, const float* rw, int rows,
+                                  __nv_bfloat16* dY, float* loss_epoch, const TrainSched* sched, const int* step) {
+    const TrainSched b = sched[*step];
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (r < rows) {
+        const float wr = rw ? rw[b.r0 + r] : 1.0f;
+        for (int k = 0; k < kOutPad; ++k) {
+            float g = 0.0f;
+            if (k < kOut) {
+                const float d = Y[(size_t)r * kOutPad + k] - T[(size_t)(b.r0 + r) * kOut + k];
+                l += wr * w[k] * d * d;
+                g = 2.0f * wr * w[k] * d / (float)rows;
+            }
+            dY[(size_t)r * kOutPad + k] = __float2bfloat16(g);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss_epoch + b.epoch, l / (float)rows);
+}
+
+__global__ void adam_sched_kernel(float* p, const float* g, float* m, float* v, int n, float b1, float b2, float eps,
+                                  const unsigned char* mask, const TrainSched* sched, const int* step) {
+    const TrainSched b = sched[*step];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!mask[i]) {
+        p[i] = 0.0f;
+        return;
+    }
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= b.lr * (mi / b.c1) / (sqrtf(vi / b.c2) + eps);
+}
+
+__global__ void advance_kernel(int* step) { *step += 1; }
 
 __global__ void to_bf16_kernel(const float* x, __nv_bfloat16* y, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -284,7 +341,7 @@ cudaError_t launch_dsilu(const float* dA, const float* Z, void* dZ, long long n,
 }
 
 cudaError_t launch_colsum(const void* X, int rows, int cols, float* db, cudaStream_t s) {
-    dim3 g((cols + 127) / 128, (rows + 255) / 256);
+    dim3 g((cols + 127) / 128, (rows + train::kColsumRows - 1) / train::kColsumRows);
     train::colsum_kernel<<<g, 128, 0, s>>>(static_cast<const __nv_bfloat16*>(X), rows, cols, db);
     return cudaGetLastError();
 }
@@ -303,6 +360,28 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, int n, flo
 
 cudaError_t launch_to_bf16(const float* x, void* y, int n, cudaStream_t s) {
     train::to_bf16_kernel<<<(n + 255) / 256, 256, 0, s>>>(x, static_cast<__nv_bfloat16*>(y), n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_input_sched(const float* X, const float* mean, const float* istd, void* X0, int rows,
+                               const TrainSched* sched, const int* step, cudaStream_t s) {
+    const long long n = (long long)rows * kInPad;
+    train::input_sched_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+        X, mean, istd, static_cast<__nv_bfloat16*>(X0), rows, sched, step);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_loss_sched(const float* Y, const float* T, const float* w, const float* rw, int rows, void* dY,
+                              float* loss_epoch, const TrainSched* sched, const int* step, cudaStream_t s) {
+    train::loss_sched_kernel<<<(rows + 255) / 256, 256, 0, s>>>(Y, T, w, rw, rows, static_cast<__nv_bfloat16*>(dY),
+                                                                loss_epoch, sched, step);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adam_sched(float* p, const float* g, float* m, float* v, int n, float b1, float b2, float eps,
+                              const unsigned char* mask, const TrainSched* sched, int* step, cudaStream_t s) {
+    train::adam_sched_kernel<<<(n + 255) / 256, 256, 0, s>>>(p, g, m, v, n, b1, b2, eps, mask, sched, step);
+    train::advance_kernel<<<1, 1, 0, s>>>(step);
     return cudaGetLastError();
 }
 

@@ -232,7 +232,9 @@ def error_study(pkg, m, p, st, tuning, closure, checkpoints=(100, 1000)):
 
 def face_flux_bytes(m, move: bool, fp32: bool) -> float:
     """Algorithmic DRAM bytes of one face-flux launch: every input read once,
-    every output written once (kernel K2)."""
+    every output written once — face data, the two cells' states, the node
+    coordinates of both layers when the mesh moves, and the 9 FP64 flux values
+    of each face (the record's 8-byte pad is not counted)."""
     C = m["cell_nodes"].shape[0]
     F = m["face_nodes"].shape[0]
     N = m["node_xyz"].shape[0]

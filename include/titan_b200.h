@@ -168,6 +168,11 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* params,
  * context's GPU; titan_unpack_halo writes a device buffer of the same form
  * into the copies. Both return when the copy is done. */
 int titan_set_halo(titan_ctx* ctx, int64_t n_send, const int32_t* send_ids, int64_t n_recv, const int32_t* recv_ids);
+/* Faces (original numbering, 1 = left out) whose CFL candidate does not enter
+ * dt: on a sharded rank, the faces between two halo cells, whose stencils can
+ * reach past the halo (their true candidates come from the rank that owns a
+ * side). NULL: every interior face counts, as in Setka::Go. */
+int titan_set_cfl_faces(titan_ctx* ctx, const int8_t* exclude);
 int titan_pack_halo(titan_ctx* ctx, double* out_device);
 int titan_unpack_halo(titan_ctx* ctx, const double* in_device);
 

@@ -82,6 +82,7 @@ struct OMesh {
     const double* ray_r0;        // nray*ray_len
     const double* ray_dir;       // nray*3
     int64_t nray, ray_len;
+    const int8_t* face_nodt;     // nface, 1: left out of the CFL minimum; may be null
 };
 
 struct OParams {
@@ -1329,7 +1330,7 @@ static double o_face(const OMesh* M, const OParams* P, const double* st, const d
         const int rc = o_chlld(method, n, w, L, R, 0, 0, nk, L + 8, R + 8, q, kq, ds, left_ydar, contact, P->gamma);
         if (rc) *err = 10 + rc;
     }
-    if (type == 0) {
+    if (type == 0 && !(M->face_nodt && M->face_nodt[f])) {
         const double dnt = P->KFL * dist / (mx(std::fabs(ds[0]), std::fabs(ds[2])) + std::fabs(w));
         if (dnt < loc_time) loc_time = mn(loc_time, dnt);
     }

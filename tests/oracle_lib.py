@@ -43,6 +43,7 @@ class OMesh(ctypes.Structure):
         ("face_method", I8), ("face_bc", I32), ("bc_vals", D), ("node_amp", D), ("node_phase", D),
         ("face_tvd", I32),
         ("ray_nodes", I32), ("ray_r0", D), ("ray_dir", D), ("nray", ctypes.c_int64), ("ray_len", ctypes.c_int64),
+        ("face_nodt", I8),
     ]
 
 
@@ -286,6 +287,12 @@ class OracleRun:
 
     def set_face_method(self, ns):
         self.face_method[:] = np.asarray(ns, dtype=np.int8)
+
+    def set_cfl_faces(self, exclude):
+        """Faces (1) left out of the CFL minimum; None: every interior face counts."""
+        a = None if exclude is None else np.ascontiguousarray(exclude, dtype=np.int8)
+        self._keep["nodt"] = a
+        self.mesh.face_nodt = _p(a, I8)
 
     def go(self, state: np.ndarray, steps: int) -> OStepInfo:
         """Advances `state` ([10, C], modified in place) by `steps` steps."""

@@ -11,16 +11,17 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_two_contexts_exchanging_halos_match_one_context(titan, world):
-    m, p, st, _ = titan.problems.heliosphere_shell(nq=8, nlayer=8, move=True, npassive=2)
+@pytest.mark.parametrize("world,kw", [(2, {}), (3, {}), (3, dict(tvd=True, zones=True))])
+def test_contexts_exchanging_halos_match_one_context(titan, world, kw):
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=8, nlayer=8, move=True, npassive=2, **kw)
     S = titan.shard
     dev = torch.device("cuda:0")
     owner = S.partition(m, world)
     ranks = []
     for r in range(world):
-        sh = S.build_shard(m, owner, r)
+        sh = S.build_shard(m, owner, r, layers=2 if p["tvd"] else 1)
         step = titan.PlasmaStep(sh["mesh"], p)
+        step.set_cfl_faces(sh["nodt"])
         step.upload_state(np.ascontiguousarray(st[:, sh["cells"]]))
         bufs = {q: torch.empty((len(ids), 10), dtype=torch.float64, device=dev) for q, ids in sh["send"].items()}
         ranks.append((sh, step, bufs))

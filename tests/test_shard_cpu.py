@@ -14,8 +14,8 @@ import torch.multiprocessing as mp
 import oracle_lib as ol
 
 
-def _problem(titan):
-    m, p, st, _ = titan.problems.heliosphere_shell(nq=6, nlayer=6, move=True)
+def _problem(titan, **kw):
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=6, nlayer=6, move=True, **kw)
     return m, p, np.ascontiguousarray(st)
 
 
@@ -40,6 +40,9 @@ class OracleStepper:
 
     def set_face_method(self, m):
         self.run.set_face_method(m)
+
+    def set_cfl_faces(self, exclude):
+        self.run.set_cfl_faces(exclude)
 
     def pack(self, buf):
         buf[: len(self.send)] = torch.from_numpy(np.ascontiguousarray(self.state[:, self.send].T[:, : buf.shape[1]]))
@@ -83,14 +86,16 @@ def test_sub_meshes_and_plans_are_consistent(titan):
                 assert np.array_equal(sh["cells"][ids], shards[q]["cells"][shards[q]["recv"][r]])
 
 
-def _emulated(titan, world, steps):
-    m, p, st = _problem(titan)
+def _emulated(titan, world, steps, **kw):
+    m, p, st = _problem(titan, **kw)
     S = titan.shard
     owner = S.partition(m, world)
     ranks = []
+    layers = 2 if p["tvd"] else 1
     for r in range(world):
-        sh = S.build_shard(m, owner, r)
+        sh = S.build_shard(m, owner, r, layers=layers)
         o = OracleStepper(None, sh["mesh"], p)
+        o.set_cfl_faces(sh["nodt"])
         o.upload_state(st[:, sh["cells"]])
         ranks.append((sh, o))
     full = ol.OracleRun(m, p)
@@ -111,9 +116,9 @@ def _emulated(titan, world, steps):
     return ranks, ref
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_emulated_ranks_match_the_single_domain_step_bit_for_bit(titan, oracle_lib, world):
-    ranks, ref = _emulated(titan, world, 4)
+@pytest.mark.parametrize("world,kw", [(2, {}), (4, {}), (3, dict(tvd=True, zones=True, npassive=2))])
+def test_emulated_ranks_match_the_single_domain_step_bit_for_bit(titan, oracle_lib, world, kw):
+    ranks, ref = _emulated(titan, world, 4, **kw)
     for sh, o in ranks:
         n = sh["n_owned"]
         assert np.array_equal(o.state[:, :n], ref[:, sh["cells"][:n]])

@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
         dsl_d = double(dsl);
         dsr_d = double(dsr);
         }
-        if (type == 0) {
+        if (type == 0 && !(M.face_nodt && M.face_nodt[f])) {
             if (!MOVE) dist = a.L1.fd[f];
             const double dnt = P.KFL * dist / (rmax(fabs(dsl_d), fabs(dsr_d)) + fabs(w));
             contrib = 10000000.0;

@@ -50,6 +50,7 @@ struct MeshView {
                                       // 3-bit indices into the cell's 8 nodes (ALE)
     const int* face_aa;           // [nface] second-order neighbour beyond cells[0] or -1
     const int* face_bb;           // [nface] second-order neighbour beyond cells[1] or -1
+    const signed char* face_nodt = nullptr;  // [nface] 1: left out of the CFL minimum, or null
 };
 
 struct Layer {  // geometry of one time layer (the reference's [2] arrays)

@@ -115,6 +115,8 @@ struct titan_ctx {
     double closure_ninf = 0.0, closure_lambda = 0.0;
     int sm_count = 148;
 
+    signed char* d_face_nodt = nullptr;  // faces left out of the CFL minimum (titan_set_cfl_faces)
+
     // halo exchange of a sharded step (titan_set_halo): renumbered cell ids
     int32_t* d_halo_send = nullptr;
     int32_t* d_halo_recv = nullptr;
@@ -167,6 +169,7 @@ struct titan_ctx {
         M.cell_fmap = d_cell_fmap;
         M.face_aa = d_face_aa;
         M.face_bb = d_face_bb;
+        M.face_nodt = d_face_nodt;
         return M;
     }
 };
@@ -440,6 +443,7 @@ int titan_destroy(titan_ctx* ctx) {
         if (p) cudaFree(p);
     if (ctx->d_halo_send) cudaFree(ctx->d_halo_send);
     if (ctx->d_halo_recv) cudaFree(ctx->d_halo_recv);
+    if (ctx->d_face_nodt) cudaFree(ctx->d_face_nodt);
     // without node motion layer[1] aliases layer[0]: free it once
     const int nlayers = (ctx->layer[1].xyz != ctx->layer[0].xyz) ? 2 : 1;
     for (int l = 0; l < nlayers; ++l) {
@@ -743,6 +747,21 @@ int titan_set_halo(titan_ctx* ctx, int64_t n_send, const int32_t* send_ids, int6
     }
     ctx->n_halo_send = n_send;
     ctx->n_halo_recv = n_recv;
+    return TITAN_OK;
+}
+
+int titan_set_cfl_faces(titan_ctx* ctx, const int8_t* exclude) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    drop_graph(ctx);  // the captured step reads the table's address
+    if (ctx->d_face_nodt) cudaFree(ctx->d_face_nodt);
+    ctx->d_face_nodt = nullptr;
+    if (!exclude) return TITAN_OK;
+    const int64_t nf = ctx->nface;
+    std::vector<signed char> h(nf);
+    for (int64_t f = 0; f < nf; ++f) h[f] = exclude[ctx->R.face_n2o[f]] ? 1 : 0;
+    int64_t tmp = 0;
+    CK(dalloc(&ctx->d_face_nodt, (size_t)nf, &tmp));
+    CK(cudaMemcpy(ctx->d_face_nodt, h.data(), nf, cudaMemcpyHostToDevice));
     return TITAN_OK;
 }
 

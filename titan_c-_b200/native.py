@@ -137,6 +137,7 @@ SIGNATURES = {
     "titan_closure_outside": ([ctypes.c_void_p, I64], ctypes.c_int),
     "titan_closure_fallback_from_mc": ([ctypes.c_void_p], ctypes.c_int),
     "titan_set_halo": ([ctypes.c_void_p, ctypes.c_int64, I32, ctypes.c_int64, I32], ctypes.c_int),
+    "titan_set_cfl_faces": ([ctypes.c_void_p, I8], ctypes.c_int),
     "titan_pack_halo": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "titan_unpack_halo": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "titan_autotune": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p], ctypes.c_int),

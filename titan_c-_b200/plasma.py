@@ -115,6 +115,11 @@ class PlasmaStep:
         r = np.ascontiguousarray(recv_ids, dtype=np.int32)
         N.check(self._lib.titan_set_halo(self._ctx, len(s), N.ptr(s, N.I32), len(r), N.ptr(r, N.I32)))
 
+    def set_cfl_faces(self, exclude: np.ndarray | None):
+        """Faces (1) whose CFL candidate is left out of dt (titan_set_cfl_faces); None: all count."""
+        a = None if exclude is None else np.ascontiguousarray(exclude, dtype=np.int8)
+        N.check(self._lib.titan_set_cfl_faces(self._ctx, N.ptr(a, N.I8)))
+
     def pack_halo(self, out_device_ptr: int):
         """The send cells' states, [n_send][8 + npassive], into a device buffer (address)."""
         N.check(self._lib.titan_pack_halo(self._ctx, ctypes.c_void_p(out_device_ptr)))

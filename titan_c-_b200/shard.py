@@ -10,8 +10,9 @@ same step:
   across their faces (the halo), every face of those cells and their nodes.
   A face of a halo cell whose other cell is not on the rank becomes an
   Outer_Soft boundary face there: the halo cells' own update is thrown away,
-  since the next exchange overwrites them, and boundary faces take no part in
-  the CFL minimum;
+  since the next exchange overwrites them; only faces with an owned cell
+  enter the rank's CFL minimum (titan_set_cfl_faces), and every face of the
+  mesh has an owned cell on some rank;
 * each step: the owners send their halo cells' states, every rank steps its
   sub-mesh with the dt of the previous step's global minimum, then the ranks
   take the minimum of their CFL candidates.
@@ -19,8 +20,11 @@ same step:
 Every face of an owned cell is on the rank with both its cells' true states,
 and the cell update gathers the faces in the cell's own order, so the owned
 cells come out bit for bit as in a single-domain step, whatever the split.
-Second-order faces (which reach two cells deep), surface tracking (rays that
-cross ranks) and Monte-Carlo passes are not sharded.
+Second-order faces take two halo layers: the cells beyond both sides of every
+face of an owned cell, and all their faces, are then on the rank, so the
+second-order neighbours (chosen on the rank's sub-mesh) are the global ones.
+Surface tracking (rays that cross ranks) and Monte-Carlo passes are not
+sharded.
 """
 from __future__ import annotations
 
@@ -50,8 +54,10 @@ def partition(mesh: dict, nranks: int) -> np.ndarray:
     return owner
 
 
-def build_shard(mesh: dict, owner: np.ndarray, rank: int) -> dict:
-    """Rank `rank`'s sub-mesh and halo plan.
+def build_shard(mesh: dict, owner: np.ndarray, rank: int, layers: int = 1) -> dict:
+    """Rank `rank`'s sub-mesh and halo plan, with `layers` layers of halo cells
+    (2 for second-order faces, whose reconstruction reaches the cells beyond
+    both sides of a face).
 
     Returns dict(mesh=local mesh dict, cells=global ids of the local cells
     (owned first, ascending, then the halo, ascending), n_owned, faces, nodes
@@ -61,10 +67,11 @@ def build_shard(mesh: dict, owner: np.ndarray, rank: int) -> dict:
     fc = mesh["face_cells"]
     cf = mesh["cell_faces"]
     owned = np.nonzero(owner == rank)[0]
-    f_own = np.unique(cf[owned].ravel())
-    nb = fc[f_own].ravel()
-    nb = nb[nb >= 0]
-    halo = np.setdiff1d(np.unique(nb), owned)
+    inner = owned
+    for _ in range(layers):
+        nb = fc[np.unique(cf[inner].ravel())].ravel()
+        inner = np.union1d(inner, nb[nb >= 0])
+    halo = np.setdiff1d(inner, owned)
     cells = np.concatenate([owned, halo]).astype(np.int64)
     lc = -np.ones(len(owner), dtype=np.int64)
     lc[cells] = np.arange(len(cells))
@@ -120,17 +127,22 @@ def build_shard(mesh: dict, owner: np.ndarray, rank: int) -> dict:
     n_owned = len(owned)
     for peer in np.unique(owner[halo]):
         recv[int(peer)] = lc[halo[owner[halo] == peer]]
-    # cells of mine in another rank's halo: neighbours of that rank's cells across my faces
+    # cells of mine in another rank's halo: within `layers` faces of that rank's cells
     for peer in range(int(owner.max()) + 1):
         if peer == rank:
             continue
-        theirs = np.nonzero(owner == peer)[0]
-        nbp = fc[np.unique(cf[theirs].ravel())].ravel()
-        mine = np.unique(nbp[(nbp >= 0)])
-        mine = mine[owner[mine] == rank]
+        reach = np.nonzero(owner == peer)[0]
+        for _ in range(layers):
+            nbp = fc[np.unique(cf[reach].ravel())].ravel()
+            reach = np.union1d(reach, nbp[nbp >= 0])
+        mine = reach[owner[reach] == rank]
         if len(mine):
             send[peer] = lc[mine]
-    return dict(mesh=local, cells=cells, n_owned=n_owned, faces=faces, nodes=nodes, recv=recv, send=send)
+    # faces with no owned cell: their stencils can reach past the halo, and the
+    # rank owning a side supplies their CFL candidate
+    nodt = ((c0 < 0) | (c0 >= n_owned)) & ((c1 < 0) | (c1 >= n_owned))
+    return dict(mesh=local, cells=cells, n_owned=n_owned, faces=faces, nodes=nodes, recv=recv, send=send,
+                nodt=np.ascontiguousarray(nodt.astype(np.int8)))
 
 
 def local_face_method(shard: dict, method: np.ndarray) -> np.ndarray:
@@ -157,6 +169,9 @@ class DeviceStepper:
 
     def set_face_method(self, m):
         self.step.set_face_method(m)
+
+    def set_cfl_faces(self, exclude):
+        self.step.set_cfl_faces(exclude)
 
     def pack(self, buf):
         self.step.pack_halo(buf.data_ptr())
@@ -188,13 +203,13 @@ class ShardedStep:
                  method: np.ndarray | None = None):
         import torch
 
-        if params.get("tvd"):
-            raise ValueError("second-order faces are not sharded (their reconstruction reaches two cells deep)")
         self.torch = torch
         self.rank, self.world, self.device = rank, world, device
         owner = partition(mesh, world)
-        self.shard = build_shard(mesh, owner, rank)
+        # second-order faces reconstruct from the cells beyond both sides: two halo layers
+        self.shard = build_shard(mesh, owner, rank, layers=2 if params.get("tvd") else 1)
         self.step = (stepper or DeviceStepper)(pkg, self.shard["mesh"], params)
+        self.step.set_cfl_faces(self.shard["nodt"])
         if method is not None:
             self.step.set_face_method(local_face_method(self.shard, method))
         self.ns = 8 + params["npassive"]

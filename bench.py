@@ -442,8 +442,8 @@ def run_sharded(args, rank, world):
     --gpus N runs N replicas."""
     import torch
 
-    if args.mode not in ("fp64", "fp32"):
-        raise SystemExit("--shard runs the fp64 or fp32 step (the closure and the Monte-Carlo are not sharded)")
+    if args.mode == "coupled":
+        raise SystemExit("--shard runs the fp64, fp32 or mixed-mlp step (the Monte-Carlo is not sharded)")
     dev = rank % max(torch.cuda.device_count(), 1)
     torch.cuda.set_device(dev)
     pkg, m, p, st = build_problem(args)
@@ -451,7 +451,14 @@ def run_sharded(args, rank, world):
     flux = 64 if args.mode == "fp64" else 32
     ss = pkg.shard.ShardedStep(pkg, m, dict(p, flux_precision=flux), rank, world, torch.device("cuda", dev))
     ss.upload_state(st)
-    tuning = ss.step.step.autotune(reps=3) if args.tuning == "auto" else None
+    plasma = ss.step.step
+    if args.mode == "mixed-mlp":
+        # the closure runs per rank on its sub-mesh's cells
+        closure, _ = load_closure(pkg, m, st)
+        closure.install(plasma)
+    tuning = plasma.autotune(reps=3) if args.tuning == "auto" else None
+    kernels = (3 if p["move"] else 2) + (1 if args.mode == "mixed-mlp" else 0)
+    kernels += (1 if ss.n_send else 0) + (1 if ss.n_recv else 0)  # halo pack / unpack
 
     def barrier():
         if world > 1:
@@ -467,10 +474,24 @@ def run_sharded(args, rank, world):
         ss.go(args.steps)
         ev1.record()
         barrier()
-    t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device="cuda")
+    # end to end: every step each rank's cells in from pinned host memory, the owned cells back
+    ns = 8 + p["npassive"]
+    n_loc = len(ss.shard["cells"])
+    host = torch.empty((10, n_loc), dtype=torch.float64, pin_memory=True).numpy()
+    host[:] = st[:, ss.shard["cells"]]
+    e2e_steps = max(3, min(args.steps, 20))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        plasma.upload_state(host)
+        ss.go(1)
+        plasma.download_state(host)
+    barrier()
+    e2e_wall = time.perf_counter() - t0
+    t = torch.tensor([ev0.elapsed_time(ev1), e2e_wall], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms = float(t[0])
+    ms, e2e_wall = float(t[0]), float(t[1])
     clocks = clk.summary()
     ss.close()
     if rank != 0:
@@ -479,12 +500,16 @@ def run_sharded(args, rank, world):
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f64" if flux == 64 else "f32-flux/f64-update",
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": {"fp64": "f64", "fp32": "f32-flux/f64-update", "mixed-mlp": "f32-flux/f64-update, bf16 MLP"}[args.mode],
         "data": "synthetic (seeded heliosphere-like shell; no external data)",
         "config": {"workload": f"heliosphere shell 6x{args.nq}x{args.nq}x{args.nlayer} = {C} cells split over "
                                f"{world} GPUs (Morton ranges, one-cell halo over NCCL)",
                    "cells": C, "mode": args.mode, "parallelism": f"sharded x{world}", "tuning": tuning},
-        "gpu_launches": None, "clocks": clocks,
+        "e2e": {"value": C * e2e_steps / e2e_wall, "unit": UNIT,
+                "h2d_bytes_per_step": 8 * ns * n_loc, "d2h_bytes_per_step": 8 * ns * n_loc,
+                "note": "rank 0's bytes; every rank moves its own cells"},
+        "gpu_launches": kernels * args.steps, "clocks": clocks,
     }
 
 

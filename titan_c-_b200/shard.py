@@ -47,6 +47,8 @@ def _morton3(p: np.ndarray) -> np.ndarray:
 def partition(mesh: dict, nranks: int) -> np.ndarray:
     """Owner rank of every cell: equal contiguous ranges of the Morton order of the centres."""
     cc = mesh["node_xyz"][mesh["cell_nodes"]].mean(axis=1)
+    if not 1 <= nranks <= len(cc):
+        raise ValueError(f"cannot split {len(cc)} cells over {nranks} ranks")
     order = np.argsort(_morton3(cc), kind="stable")
     owner = np.empty(len(cc), dtype=np.int32)
     for r, idx in enumerate(np.array_split(order, nranks)):

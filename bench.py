@@ -343,7 +343,7 @@ def run_ours(args, rank, world):
     step.close()
 
     # the plain all-FP64 step on the same mesh, and the mixed step's error against it
-    plain = None
+    plain = fp32_only = None
     if args.mode in ("mixed-mlp", "coupled"):
         s64, tun64 = make_step(pkg, m, p, st, 64, args.tuning)
         s64.go(max(args.warmup, 3))
@@ -351,15 +351,23 @@ def run_ours(args, rank, world):
         s64.close()
         plain = {"value": world * C * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
                  "tuning": tun64, "clocks": clk64}
+        # and the FP32-flux step without the closure (the mixed step's other half)
+        s32, tun32 = make_step(pkg, m, p, st, 32, args.tuning)
+        s32.go(max(args.warmup, 3))
+        ms32, clk32 = timed_steps(s32, args.steps, barrier, torch.cuda.ExternalStream(s32.stream()), dev)
+        s32.close()
+        fp32_only = {"ms_per_step": ms32 / args.steps, "tuning": tun32, "clocks": clk32}
 
-    t = torch.tensor([ms, e2e_wall] + ([plain["ms_per_step"]] if plain else []), dtype=torch.float64,
-                     device="cuda")
+    t = torch.tensor([ms, e2e_wall] + ([plain["ms_per_step"], fp32_only["ms_per_step"]] if plain else []),
+                     dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     ms, e2e_wall = float(t[0]), float(t[1])
     if plain:
         plain["ms_per_step"] = float(t[2])
         plain["value"] = world * C / (plain["ms_per_step"] / 1e3)
+        fp32_only["ms_per_step"] = float(t[3])
+        fp32_only["value"] = world * C / (fp32_only["ms_per_step"] / 1e3)
     if rank != 0:
         return None
     value = world * C * args.steps / (ms / 1e3)
@@ -409,6 +417,7 @@ def run_ours(args, rank, world):
                            "peak_source": tf_src, "tensor_frac": flops / (mlp_ms / 1e3) / 1e12 / tf_peak}
     if plain:
         line["plain_fp64"] = plain
+        line["fp32_flux_no_closure"] = fp32_only
         line["speedup_vs_plain_fp64"] = plain["ms_per_step"] / (ms / args.steps)
         if world == 1 and args.error_study:
             line["error_vs_fp64"] = error_study(pkg, m, p, st, tuning, closure)

@@ -4,29 +4,42 @@ buffers by titan_pack_halo / titan_unpack_halo, stepped one after the other
 with the minimum dt, give the owned cells bit for bit as one context on the
 whole shell. (Ranks on separate GPUs move the same buffers with NCCL; the
 CPU tests run that protocol with gloo.)"""
+import os
+
 import numpy as np
 import pytest
 import torch
 
 pytestmark = pytest.mark.gpu
 
+NET = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "titan_c-_b200", "data",
+                   "closure_shell.npz")
 
-@pytest.mark.parametrize("world,kw", [(2, {}), (3, {}), (3, dict(tvd=True, zones=True))])
-def test_contexts_exchanging_halos_match_one_context(titan, world, kw):
+
+@pytest.mark.parametrize("world,kw,closure", [(2, {}, False), (3, {}, False), (3, dict(tvd=True, zones=True), False),
+                                              (2, dict(flux_precision=32), True)])
+def test_contexts_exchanging_halos_match_one_context(titan, world, kw, closure):
+    """closure: the mixed step with the trained network's sources, per rank on
+    its own cells (each cell's sources depend on that cell alone)."""
     m, p, st, _ = titan.problems.heliosphere_shell(nq=8, nlayer=8, move=True, npassive=2, **kw)
     S = titan.shard
     dev = torch.device("cuda:0")
+    net = titan.closure.Closure.load(NET) if closure else None
     owner = S.partition(m, world)
     ranks = []
     for r in range(world):
         sh = S.build_shard(m, owner, r, layers=2 if p["tvd"] else 1)
         step = titan.PlasmaStep(sh["mesh"], p)
         step.set_cfl_faces(sh["nodt"])
+        if net is not None:
+            net.install(step)
         step.upload_state(np.ascontiguousarray(st[:, sh["cells"]]))
         bufs = {q: torch.empty((len(ids), 10), dtype=torch.float64, device=dev) for q, ids in sh["send"].items()}
         ranks.append((sh, step, bufs))
     ns = 8 + p["npassive"]
     full = titan.PlasmaStep(m, p)
+    if net is not None:
+        net.install(full)
     full.upload_state(st)
     for _ in range(6):
         # every rank packs what each peer needs, then unpacks what it receives

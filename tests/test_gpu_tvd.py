@@ -87,10 +87,10 @@ def test_every_launch_shape_gives_identical_second_order_results(T):
     m, p, st, _ = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, zones=True, npassive=2)
     p = dict(p, tvd=1)
     ref = None
-    for fv in range(6):
+    for fv in range(7):
         g = T.PlasmaStep(m, p)
         g.upload_state(st)
-        g.set_tuning(fv, fv % 5)
+        g.set_tuning(fv, fv % 6)
         g.go(4)
         out = g.download_state()
         g.close()

@@ -24,6 +24,7 @@ static cudaError_t face_flux_variant(const FaceArgs& a, int v, cudaStream_t s) {
         TITAN_FACE_CASE(3)
         TITAN_FACE_CASE(4)
         TITAN_FACE_CASE(5)
+        TITAN_FACE_CASE(6)
 #undef TITAN_FACE_CASE
         default:
             return cudaErrorInvalidValue;

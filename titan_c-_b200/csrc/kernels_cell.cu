@@ -200,6 +200,7 @@ static cudaError_t cell_update_variant(const CellArgs& a, int src, int v, cudaSt
         TITAN_CELL_CASE(2)
         TITAN_CELL_CASE(3)
         TITAN_CELL_CASE(4)
+        TITAN_CELL_CASE(5)
 #undef TITAN_CELL_CASE
         default:
             return cudaErrorInvalidValue;

@@ -15,13 +15,14 @@ constexpr int kGeomBlock = 256;
 struct FaceVariant {
     int block, min_blocks;
 };
-constexpr int kFaceVariants = 6;
-constexpr FaceVariant kFaceVariant[kFaceVariants] = {{128, 1}, {128, 3}, {128, 4}, {256, 2}, {64, 8}, {128, 5}};
+constexpr int kFaceVariants = 7;
+constexpr FaceVariant kFaceVariant[kFaceVariants] = {{128, 1}, {128, 3}, {128, 4}, {256, 2}, {64, 8}, {128, 5},
+                                                     {128, 6}};
 struct CellVariant {
     int block, min_blocks;
 };
-constexpr int kCellVariants = 5;
-constexpr CellVariant kCellVariant[kCellVariants] = {{256, 1}, {128, 1}, {512, 1}, {256, 4}, {128, 8}};
+constexpr int kCellVariants = 6;
+constexpr CellVariant kCellVariant[kCellVariants] = {{256, 1}, {128, 1}, {512, 1}, {256, 4}, {128, 8}, {256, 3}};
 
 cudaError_t launch_move_nodes(const MeshView& M, const Params& P, const double* xyz1, double* xyz2,
                               const DevStatus* st, cudaStream_t s);

@@ -137,6 +137,23 @@ def test_brio_wu_cube_steps_match_oracle(T, oracle_lib, steps):
     gpu.close()
 
 
+def test_brio_wu_config0_full_run_is_bit_exact(T, oracle_lib):
+    """The reference's CPU-runnable case in full: the 32^3 Brio-Wu cube, HLLD on
+    every face, 200 steps. No transcendental function enters this problem, so
+    the GPU's state, dt and time equal the oracle's bit for bit."""
+    m, p, st, meth = T.problems.brio_wu_cube(32)
+    gpu, run = _pair(T, m, p, meth)
+    gpu.upload_state(st)
+    s_or = np.ascontiguousarray(st.copy())
+    info = gpu.go(200)
+    oi = run.go(s_or, 200)
+    assert info["steps_done"] == 200 and oi.err_code == 0
+    s_gpu = gpu.download_state()
+    assert np.array_equal(s_gpu[:8].view(np.uint64), s_or[:8].view(np.uint64))
+    assert gpu.dt == run.clock[0] and gpu.t == run.clock[1]
+    gpu.close()
+
+
 def test_brio_wu_face_fluxes_match_oracle(T, oracle_lib):
     m, p, st, meth = T.problems.brio_wu_cube(10)
     gpu, run = _pair(T, m, p, meth)

@@ -154,6 +154,30 @@ def test_brio_wu_config0_full_run_is_bit_exact(T, oracle_lib):
     gpu.close()
 
 
+def test_config1_full_size_steps_match_oracle(T, oracle_lib):
+    """The measured workload at its full size: the 6x96x96x40 shell (2,211,840
+    cells, node motion), three FP64 steps against the oracle, each step from
+    the same state. Node motion calls sin, where CUDA and glibc may differ by an
+    ulp, so the bar is the contract's 1e-12; nearly every value is identical."""
+    m, p, st, _ = T.problems.heliosphere_shell(nq=96, nlayer=40, move=True)
+    gpu = T.PlasmaStep(m, p)
+    run = ol.OracleRun(m, p)
+    gpu.upload_state(st)
+    worst, same = 0.0, []
+    for _ in range(3):
+        before = np.ascontiguousarray(gpu.download_state())
+        run.xyz[:] = gpu.nodes()
+        run.clock[:] = (gpu.dt, gpu.t)
+        gpu.go(1)
+        assert run.go(before, 1).err_code == 0
+        after = gpu.download_state()
+        worst = max(worst, rel_err(after[:8], before[:8]))
+        same.append(float(np.mean(after[:8] == before[:8])))
+    gpu.close()
+    assert worst <= REL, worst
+    assert min(same) > 0.99, same
+
+
 def test_brio_wu_face_fluxes_match_oracle(T, oracle_lib):
     m, p, st, meth = T.problems.brio_wu_cube(10)
     gpu, run = _pair(T, m, p, meth)

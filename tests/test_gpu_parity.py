@@ -154,17 +154,19 @@ def test_brio_wu_config0_full_run_is_bit_exact(T, oracle_lib):
     gpu.close()
 
 
-def test_config1_full_size_steps_match_oracle(T, oracle_lib):
-    """The measured workload at its full size: the 6x96x96x40 shell (2,211,840
-    cells, node motion), three FP64 steps against the oracle, each step from
-    the same state. Node motion calls sin, where CUDA and glibc may differ by an
-    ulp, so the bar is the contract's 1e-12; nearly every value is identical."""
-    m, p, st, _ = T.problems.heliosphere_shell(nq=96, nlayer=40, move=True)
+@pytest.mark.parametrize("nq,steps", [(96, 3), (192, 1)])
+def test_config1_full_size_steps_match_oracle(T, oracle_lib, nq, steps):
+    """The measured workloads at their full sizes: the 6x96x96x40 shell
+    (2,211,840 cells) and the 6x192x192x40 one (8,847,360 cells), node motion,
+    FP64 steps against the oracle, each step from the same state. Node motion
+    calls sin, where CUDA and glibc may differ by an ulp, so the bar is the
+    contract's 1e-12; nearly every value is identical."""
+    m, p, st, _ = T.problems.heliosphere_shell(nq=nq, nlayer=40, move=True)
     gpu = T.PlasmaStep(m, p)
     run = ol.OracleRun(m, p)
     gpu.upload_state(st)
     worst, same = 0.0, []
-    for _ in range(3):
+    for _ in range(steps):
         before = np.ascontiguousarray(gpu.download_state())
         run.xyz[:] = gpu.nodes()
         run.clock[:] = (gpu.dt, gpu.t)

@@ -154,16 +154,30 @@ def test_brio_wu_config0_full_run_is_bit_exact(T, oracle_lib):
     gpu.close()
 
 
-@pytest.mark.parametrize("nq,steps", [(96, 3), (192, 1)])
-def test_config1_full_size_steps_match_oracle(T, oracle_lib, nq, steps):
+@pytest.mark.parametrize("nq,steps,extra", [(96, 3, {}), (192, 1, {}), (96, 2, dict(tvd=True)), (96, 2, "surface")])
+def test_config1_full_size_steps_match_oracle(T, oracle_lib, nq, steps, extra):
     """The measured workloads at their full sizes: the 6x96x96x40 shell
     (2,211,840 cells) and the 6x192x192x40 one (8,847,360 cells), node motion,
-    FP64 steps against the oracle, each step from the same state. Node motion
-    calls sin, where CUDA and glibc may differ by an ulp, so the bar is the
-    contract's 1e-12; nearly every value is identical."""
-    m, p, st, _ = T.problems.heliosphere_shell(nq=nq, nlayer=40, move=True)
+    FP64 steps against the oracle, each step from the same state; and the
+    2.2M-cell shell with second-order faces, and with surface tracking of three
+    surfaces (nodes compared too). Node motion calls sin, where CUDA and glibc
+    may differ by an ulp, so the bar is the contract's 1e-12; nearly every
+    value is identical."""
+    surface = extra == "surface"
+    m, p, st, _ = T.problems.heliosphere_shell(nq=nq, nlayer=40, move=True, **({} if surface else extra))
+    if surface:
+        # three surfaces on node layers 20, 28 and 34, rays along the radial node columns
+        for layer, kind in ((20, 1), (28, 2), (34, 3)):
+            T.mesh.mark_shell_surface(m, layer, kind)
+        sp = dict(velocity_TS=1.0, velocity_HP=1.0, velocity_BS=1.0, move_TS=1, move_HP=1, move_BS=1,
+                  null_bn_on_HP=0)
     gpu = T.PlasmaStep(m, p)
-    run = ol.OracleRun(m, p)
+    if surface:
+        rays = T.mesh.shell_rays(m)
+        gpu.set_surface_motion(rays, **sp)
+        run = ol.OracleRun(m, p, surface=sp, rays=rays)
+    else:
+        run = ol.OracleRun(m, p)
     gpu.upload_state(st)
     worst, same = 0.0, []
     for _ in range(steps):
@@ -175,6 +189,9 @@ def test_config1_full_size_steps_match_oracle(T, oracle_lib, nq, steps):
         after = gpu.download_state()
         worst = max(worst, rel_err(after[:8], before[:8]))
         same.append(float(np.mean(after[:8] == before[:8])))
+        if surface:
+            x = gpu.nodes()
+            worst = max(worst, float(np.abs(x - run.xyz).max() / np.abs(run.xyz).max()))
     gpu.close()
     assert worst <= REL, worst
     assert min(same) > 0.99, same

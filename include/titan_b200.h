@@ -146,13 +146,26 @@ int titan_set_face_method(titan_ctx* ctx, const int8_t* n_state);
  * ends, on the ray's direction. rays: nray x ray_len node ids (original
  * numbering) from the inner end, a shorter ray padded with -1 after its last
  * node; no node on two rays; radii and directions are taken from the current
- * nodes. The reference's smoothing terms (sglag_*)
- * are not applied. params NULL returns to the prescribed motion. */
+ * nodes. Smoothing (each adds one more term to a node's mean velocity,
+ * Setka_move.cpp:454-1211): on TS and HP, with sglag_TS / sglag_HP, a node
+ * moves toward the sphere that best fits it and its surface neighbours,
+ * velocity_X * k_sphere * (B2 - x) / dt, B2 = c + (mean |x_j - c| / |x - c|)
+ * (x - c); the centre c is fitted when this function is called (the reference
+ * refits between Go calls, TITAN/source/TITAN.cpp:109-124; call this again to
+ * refit); on BS, with sglag_BS, toward the mean of itself and its neighbours,
+ * velocity_BS * sglag_BS_k * (mean - x) / dt, for nodes with more than five
+ * neighbours. The reference's head-region limit on the HP sphere term and its
+ * smoothing along its own ray families are not applied. params NULL returns
+ * to the prescribed motion. */
 typedef struct titan_surface_params {
     double velocity_TS, velocity_HP, velocity_BS; /* Phys_param::velocity_TS / _HP / _BS */
     int32_t move_TS, move_HP, move_BS;            /* Phys_param::move_TS / _HP / _BS */
     int32_t null_bn_on_HP;                        /* Phys_param::null_bn_on_HP: the HP cells and face
                                                      states lose their normal B first */
+    int32_t sglag_TS, sglag_HP, sglag_BS;         /* Phys_param::sglag_*: surface smoothing (above) */
+    int32_t pad;
+    double sglag_TS_k_sphere, sglag_HP_k_sphere;  /* Phys_param::sglag_TS_k_sphere / sglag_HP_k_sphere */
+    double sglag_BS_k;                            /* Phys_param::sglag_BS_k */
 } titan_surface_params;
 
 int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* params, int64_t nray, int32_t ray_len,

@@ -19,6 +19,7 @@
 // evaluated in the same order and rounding as the reference's x86-64 build.
 // ============================================================================
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -83,6 +84,8 @@ struct OMesh {
     const double* ray_dir;       // nray*3
     int64_t nray, ray_len;
     const int8_t* face_nodt;     // nface, 1: left out of the CFL minimum; may be null
+    const double* surf_centre;   // nnode*3, fitted sphere centres of smoothed surface nodes
+                                 // (oracle_surface_centres); may be null
 };
 
 struct OParams {
@@ -107,6 +110,8 @@ struct OParams {
     int32_t null_bn_on_HP;  // Phys_param::null_bn_on_HP
     int32_t pad2;
     double velocity_TS, velocity_HP, velocity_BS;  // Phys_param::velocity_TS / _HP / _BS
+    int32_t sglag_TS, sglag_HP, sglag_BS, pad3;     // Phys_param::sglag_*: surface smoothing
+    double sglag_TS_k_sphere, sglag_HP_k_sphere, sglag_BS_k;
 };
 
 struct OStepInfo {
@@ -1548,13 +1553,16 @@ void oracle_move_nodes(const OMesh* M, const OParams* P, const double* xyz1, dou
 //    pressure goes into p and Godunov_Solver_Alexashov gives dsc (:298-327).
 //    A non-finite or subnormal dsc is an error (:329-342; error kind 19).
 //    The three surfaces run in the reference's order, so BS sees the HP
-//    cells' B as null_bn_on_HP left it. The smoothing terms (sglag_*) are not
-//    part of this restatement.
+//    cells' B as null_bn_on_HP left it.
 //  * Each node sums its faces' contributions in ascending face order (the
 //    reference sums under a mutex in thread order), divides by their number
 //    and moves along its own direction: x' = x + (V . x/|x|) dt x/|x|
 //    (:1213-1265; the reference's heliotail rays are parallel to the x axis
 //    and move HP nodes with x < 0 along (0, y, z); these rays are all radial).
+//    With sglag_TS / sglag_HP a TS / HP node's mean also takes a term toward
+//    the sphere fitted through it and its neighbours (centres from
+//    oracle_surface_centres); with sglag_BS a BS node with more than five
+//    neighbours one toward their mean with its own position.
 //  * Along each ray (a shorter one padded with -1) the end nodes and the
 //    surface nodes are anchors; every other node keeps its initial fraction
 //    of the segment between the anchors around it, on the ray's direction
@@ -1581,6 +1589,123 @@ void oracle_ray_geometry(const OMesh* M, const double* xyz, double* r0, double* 
         dir[3 * r] = x / n0;
         dir[3 * r + 1] = y / n0;
         dir[3 * r + 2] = z / n0;
+    }
+}
+
+// A surface node's neighbours for smoothing: the other nodes of its
+// surface's faces (Setka::Find_Yzel_Sosed_for_BS, Setka_move.cpp:2365-2397, and
+// the same sets in Smooth_head_TS3 / _HP3), ascending node id.
+static std::vector<std::vector<int64_t>> o_surface_neighbours_of_nodes(const OMesh* M) {
+    const int64_t nn = M->nnode, nf = M->nface;
+    std::vector<std::vector<int64_t>> nb(nn);
+    for (int64_t f = 0; f < nf; ++f) {
+        const int s = M->face_surf[f];
+        if (s < 1 || s > 3) continue;
+        for (int k = 0; k < 4; ++k)
+            for (int j = 0; j < 4; ++j)
+                if (j != k) nb[M->face_nodes[4 * f + k]].push_back(M->face_nodes[4 * f + j]);
+    }
+    for (int64_t i = 0; i < nn; ++i) {
+        auto& v = nb[i];
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        v.erase(std::remove(v.begin(), v.end(), i), v.end());
+    }
+    return nb;
+}
+
+// Weighted least squares of 2 p . c = |p|^2 (normal equations, partial
+// pivoting); singular (all weights zero): the zero vector.
+static void o_fit_weighted(const std::vector<std::array<double, 3>>& P, const std::vector<double>& w, double c[3]) {
+    double M[3][4] = {};
+    for (size_t i = 0; i < P.size(); ++i) {
+        const double a[3] = {2.0 * P[i][0], 2.0 * P[i][1], 2.0 * P[i][2]};
+        const double b = P[i][0] * P[i][0] + P[i][1] * P[i][1] + P[i][2] * P[i][2];
+        const double ww = w[i] * w[i];
+        for (int j = 0; j < 3; ++j) {
+            for (int k = 0; k < 3; ++k) M[j][k] += ww * a[j] * a[k];
+            M[j][3] += ww * a[j] * b;
+        }
+    }
+    double scale = 0.0;
+    for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k) scale = mx(scale, std::fabs(M[j][k]));
+    c[0] = c[1] = c[2] = 0.0;
+    if (!(scale > 0.0)) return;
+    for (int col = 0; col < 3; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 3; ++r)
+            if (std::fabs(M[r][col]) > std::fabs(M[piv][col])) piv = r;
+        if (std::fabs(M[piv][col]) <= 1e-14 * scale) return;
+        if (piv != col)
+            for (int k = 0; k < 4; ++k) std::swap(M[col][k], M[piv][k]);
+        for (int r = col + 1; r < 3; ++r) {
+            const double f = M[r][col] / M[col][col];
+            for (int k = col; k < 4; ++k) M[r][k] -= f * M[col][k];
+        }
+    }
+    for (int j = 2; j >= 0; --j) {
+        double v = M[j][3];
+        for (int k = j + 1; k < 3; ++k) v -= M[j][k] * c[k];
+        c[j] = v / M[j][j];
+    }
+}
+
+// Sphere centre of Setka::Smooth_head_TS3 / _HP3 (Setka_move.cpp:2205-2362):
+// the least-squares c of 2 p . c = |p|^2 over the node and its neighbours, then
+// up to 8 fits re-weighted by Tukey's biweight of the distance residuals
+// (cutoff 2.5 standard deviations) until the RMS residual changes by less than
+// 1e-6 (the reference solves each fit by SVD).
+static void o_fit_centre(const std::vector<std::array<double, 3>>& P, double c[3]) {
+    const size_t n = P.size();
+    std::vector<double> w(n, 1.0), res(n);
+    o_fit_weighted(P, w, c);
+    double prev = 1e308;
+    for (int iter = 0; iter < 8; ++iter) {
+        double radius = 0.0;
+        for (const auto& p : P)
+            radius += std::sqrt((p[0] - c[0]) * (p[0] - c[0]) + (p[1] - c[1]) * (p[1] - c[1]) +
+                                (p[2] - c[2]) * (p[2] - c[2]));
+        radius /= (double)n;
+        double total = 0.0;
+        for (size_t i = 0; i < n; ++i) {
+            const double d = std::sqrt((P[i][0] - c[0]) * (P[i][0] - c[0]) + (P[i][1] - c[1]) * (P[i][1] - c[1]) +
+                                       (P[i][2] - c[2]) * (P[i][2] - c[2]));
+            res[i] = std::fabs(d - radius);
+            total += res[i] * res[i];
+        }
+        const double rms = std::sqrt(total / (double)n);
+        if (std::fabs(prev - rms) < 1e-6) break;
+        prev = rms;
+        double mean = 0.0;
+        for (double r : res) mean += r;
+        mean /= (double)n;
+        double var = 0.0;
+        for (double r : res) var += (r - mean) * (r - mean);
+        const double cutoff = 2.5 * std::sqrt(var / (double)n);
+        for (size_t i = 0; i < n; ++i) {
+            if (res[i] < cutoff) {
+                const double t = res[i] / cutoff;
+                w[i] = (1.0 - t * t) * (1.0 - t * t);
+            } else {
+                w[i] = 0.0;
+            }
+        }
+        o_fit_weighted(P, w, c);
+    }
+}
+
+// Fitted centres of the surface nodes at `xyz` (out: nnode*3, zero elsewhere).
+void oracle_surface_centres(const OMesh* M, const double* xyz, double* out) {
+    const int64_t nn = M->nnode;
+    const auto nb = o_surface_neighbours_of_nodes(M);
+    std::fill(out, out + 3 * nn, 0.0);
+    for (int64_t i = 0; i < nn; ++i) {
+        if (nb[i].empty()) continue;
+        std::vector<std::array<double, 3>> P;
+        P.push_back({xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]});
+        for (int64_t j : nb[i]) P.push_back({xyz[3 * j], xyz[3 * j + 1], xyz[3 * j + 2]});
+        o_fit_centre(P, out + 3 * i);
     }
 }
 
@@ -1722,12 +1847,47 @@ static int o_surface_motion(const OMesh* M, const OParams* P, double* st, const 
         }
     }
     std::memcpy(xyz2, xyz, sizeof(double) * 3 * nn);
+    const bool smooth = P->sglag_TS || P->sglag_HP || P->sglag_BS;
+    const auto nbs = smooth ? o_surface_neighbours_of_nodes(M) : std::vector<std::vector<int64_t>>();
     for (int64_t i = 0; i < nn; ++i) {
-        if (!node_surf[i] || !o_surface_moves(P, node_surf[i])) continue;
+        const int s = node_surf[i];
+        if (!s || !o_surface_moves(P, s)) continue;
         double v[3] = {V[3 * i], V[3 * i + 1], V[3 * i + 2]};
-        if (num[i] > 0)
-            for (double& c : v) c /= num[i];
+        int cnt = num[i];
         const double* A = xyz + 3 * i;
+        // smoothing (Setka_move.cpp:454-1211): one more term of the mean
+        const bool sphere = (s == 1 && P->sglag_TS) || (s == 2 && P->sglag_HP);
+        if (sphere && !nbs[i].empty() && M->surf_centre) {
+            const double coef = s == 1 ? P->velocity_TS * P->sglag_TS_k_sphere : P->velocity_HP * P->sglag_HP_k_sphere;
+            const double* B = M->surf_centre + 3 * i;
+            const double rr = std::sqrt((A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) +
+                                        (A[2] - B[2]) * (A[2] - B[2]));
+            double r = 0.0;
+            for (int64_t j : nbs[i]) {
+                const double* X = xyz + 3 * j;
+                r += std::sqrt((X[0] - B[0]) * (X[0] - B[0]) + (X[1] - B[1]) * (X[1] - B[1]) +
+                               (X[2] - B[2]) * (X[2] - B[2]));
+            }
+            r /= (int)nbs[i].size();
+            const double kk = r / rr;
+            for (int k = 0; k < 3; ++k) {
+                const double b2 = kk * (A[k] - B[k]) + B[k];
+                v[k] += coef * (b2 - A[k]) / time;
+            }
+            ++cnt;
+        } else if (s == 3 && P->sglag_BS && nbs[i].size() > 5) {
+            const double coef = P->velocity_BS * P->sglag_BS_k;
+            double B[3] = {A[0], A[1], A[2]};
+            for (int64_t j : nbs[i])
+                for (int k = 0; k < 3; ++k) B[k] += xyz[3 * j + k];
+            for (int k = 0; k < 3; ++k) {
+                B[k] /= ((int)nbs[i].size() + 1.0);
+                v[k] += coef * (B[k] - A[k]) / time;
+            }
+            ++cnt;
+        }
+        if (cnt > 0)
+            for (double& c : v) c /= cnt;
         const double an = std::sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
         const double B[3] = {A[0] / an, A[1] / an, A[2] / an};
         const double vb = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];

@@ -43,7 +43,7 @@ class OMesh(ctypes.Structure):
         ("face_method", I8), ("face_bc", I32), ("bc_vals", D), ("node_amp", D), ("node_phase", D),
         ("face_tvd", I32),
         ("ray_nodes", I32), ("ray_r0", D), ("ray_dir", D), ("nray", ctypes.c_int64), ("ray_len", ctypes.c_int64),
-        ("face_nodt", I8),
+        ("face_nodt", I8), ("surf_centre", D),
     ]
 
 
@@ -59,10 +59,14 @@ class OParams(ctypes.Structure):
         ("move_TS", ctypes.c_int32), ("move_HP", ctypes.c_int32), ("move_BS", ctypes.c_int32),
         ("null_bn_on_HP", ctypes.c_int32), ("pad2", ctypes.c_int32),
         ("velocity_TS", ctypes.c_double), ("velocity_HP", ctypes.c_double), ("velocity_BS", ctypes.c_double),
+        ("sglag_TS", ctypes.c_int32), ("sglag_HP", ctypes.c_int32), ("sglag_BS", ctypes.c_int32),
+        ("pad3", ctypes.c_int32), ("sglag_TS_k_sphere", ctypes.c_double), ("sglag_HP_k_sphere", ctypes.c_double),
+        ("sglag_BS_k", ctypes.c_double),
     ]
 
 # The surface-tracking fields of OParams (titan_surface_params on the library side).
-SURFACE_KEYS = ("move_TS", "move_HP", "move_BS", "null_bn_on_HP", "velocity_TS", "velocity_HP", "velocity_BS")
+SURFACE_KEYS = ("move_TS", "move_HP", "move_BS", "null_bn_on_HP", "velocity_TS", "velocity_HP", "velocity_BS",
+                "sglag_TS", "sglag_HP", "sglag_BS", "sglag_TS_k_sphere", "sglag_HP_k_sphere", "sglag_BS_k")
 
 
 class OStepInfo(ctypes.Structure):
@@ -104,6 +108,7 @@ def oracle():
         lib.oracle_num_threads.restype = ctypes.c_int
         lib.oracle_tvd_neighbours.argtypes = [ctypes.POINTER(OMesh), D, I32]
         lib.oracle_ray_geometry.argtypes = [ctypes.POINTER(OMesh), D, D, D]
+        lib.oracle_surface_centres.argtypes = [ctypes.POINTER(OMesh), D, D]
         lib.oracle_godunov.argtypes = [D, ctypes.c_double, D, D, ctypes.c_int, ctypes.c_double, D, D]
         lib.oracle_godunov.restype = ctypes.c_int
         lib.oracle_face_states.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D, D, I8]
@@ -261,12 +266,12 @@ class OracleRun:
         self.mesh = m
         p = OParams()
         for k, _ in OParams._fields_:
-            if k not in ("pad2", "surface_motion") + SURFACE_KEYS:
+            if k not in ("pad2", "pad3", "surface_motion") + SURFACE_KEYS:
                 setattr(p, k, params[k])
         if surface is not None:
             p.surface_motion = 1
             for k in SURFACE_KEYS:
-                setattr(p, k, surface[k])
+                setattr(p, k, surface.get(k, 0))
             rn = keep("rays", rays, np.int32)
             m.ray_nodes = _p(rn, I32)
             m.nray, m.ray_len = rn.shape
@@ -274,6 +279,10 @@ class OracleRun:
             rd = keep("ray_dir", np.empty((rn.shape[0], 3)), np.float64)
             oracle().oracle_ray_geometry(ctypes.byref(m), _p(self.xyz), _p(r0), _p(rd))
             m.ray_r0, m.ray_dir = _p(r0), _p(rd)
+            if p.sglag_TS or p.sglag_HP:
+                sc = keep("surf_centre", np.zeros((m.nnode, 3)), np.float64)
+                oracle().oracle_surface_centres(ctypes.byref(m), _p(self.xyz), _p(sc))
+                m.surf_centre = _p(sc)
         self.params = p
         self.face_tvd = None
         if p.tvd:

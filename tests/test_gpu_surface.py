@@ -3,8 +3,8 @@ Setka::Culc_Velocity_surface, TITAN/source/Setka_move.cpp:111-1358, and
 Luch::dvigenie, Luch.cpp:6-739) against the oracle, step by step: the nodes
 and the state after each step within the contract's 1e-12 relative, with TS,
 HP and BS surfaces moving on a shell, and with the options that change the
-HP faces (null_bn_on_HP, bn_in_p_on_HP), second-order faces and passive
-scalars. The exact HP solver calls pow, which CUDA and glibc may round
+HP faces (null_bn_on_HP, bn_in_p_on_HP), second-order faces, passive
+scalars, rays of different lengths and the smoothing terms (sglag_*). The exact HP solver calls pow, which CUDA and glibc may round
 differently by an ulp."""
 import numpy as np
 import pytest
@@ -30,6 +30,8 @@ def _surface_shell(T, **kw):
     dict(params=dict(bn_in_p_on_hp=1)),
     dict(shell=dict(tvd=True, zones=True, npassive=2), surface=dict(velocity_HP=0.5)),
     dict(ragged=True),
+    dict(surface=dict(sglag_TS=1, sglag_HP=1, sglag_BS=1, sglag_TS_k_sphere=0.3, sglag_HP_k_sphere=0.3,
+                      sglag_BS_k=0.3, null_bn_on_HP=1)),
 ])
 def test_surface_tracking_steps_match_oracle(titan, oracle_lib, variant):
     m, p, st, rays = _surface_shell(titan, **variant.get("shell", {}))

@@ -147,3 +147,78 @@ def test_a_shorter_ray_ends_at_its_last_node(titan, oracle_lib):
     assert np.array_equal(x1[rays[::2, -1]], x0[rays[::2, -1]])     # left out
     assert np.array_equal(x1[rays[::2, -2]], x0[rays[::2, -2]])     # the new outer end
     assert not np.array_equal(x1[rays[::2, -3]], x0[rays[::2, -3]])  # its BS node still moves
+
+
+def _bumped_shell(titan, layer, kind, bump):
+    """A shell with one surface and one of its nodes pushed outward by `bump` (relative)."""
+    m, p, st = _shell(titan)
+    titan.mesh.mark_shell_surface(m, layer, kind)
+    node = int(np.nonzero(m["node_layer"] == layer)[0][17])
+    m["node_xyz"] = m["node_xyz"].copy()
+    m["node_xyz"][node] *= 1.0 + bump
+    return m, p, st, node
+
+
+def test_bs_smoothing_pulls_a_bumped_node_back(titan, oracle_lib):
+    """sglag_BS (Setka_move.cpp:1136-1211): a BS node pushed out of the surface
+    moves inward relative to the same step without smoothing, toward the mean
+    of itself and its neighbours."""
+    m, p, st, node = _bumped_shell(titan, 5, 3, 0.02)
+    rays = titan.mesh.shell_rays(m)
+    out = {}
+    for on in (0, 1):
+        run = ol.OracleRun(m, p, surface=dict(SURF, sglag_BS=on, sglag_BS_k=0.5), rays=rays)
+        s = np.ascontiguousarray(st.copy())
+        assert run.go(s, 1).err_code == 0
+        out[on] = np.linalg.norm(run.xyz[node])
+    assert out[1] < out[0], out
+
+
+@pytest.mark.parametrize("layer,kind,key,vel", [(4, 1, "sglag_TS", "velocity_TS"), (6, 2, "sglag_HP", "velocity_HP")])
+def test_sphere_smoothing_term_as_numpy_forms_it(titan, oracle_lib, layer, kind, key, vel):
+    """sglag_TS / sglag_HP (Setka_move.cpp:454-558, 559-620): the node's mean
+    velocity takes one more term, v_s = velocity_X k (B2 - x) / dt with
+    B2 = c + (mean |x_j - c| / |x - c|) (x - c), c the sphere centre fitted at
+    set-up; the node's radial displacement is then (n_f d_off + dt v_s . x/|x|)
+    / (n_f + 1), n_f its surface faces, d_off the displacement without it. The
+    reference's fit passes the sphere through the origin (it solves
+    2 p . c = |p|^2), so on an origin-centred surface the term points outward."""
+    m, p, st, node = _bumped_shell(titan, layer, kind, 0.02)
+    rays = titan.mesh.shell_rays(m)
+    k_sph, velo = 0.5, 1.0
+    d, runs = {}, {}
+    for on in (0, 1):
+        run = ol.OracleRun(m, p, surface=dict(SURF, **{key: on, key + "_k_sphere": k_sph, vel: velo}), rays=rays)
+        x0 = run.xyz.copy()
+        dt = run.clock[0]
+        s = np.ascontiguousarray(st.copy())
+        assert run.go(s, 1).err_code == 0
+        d[on] = np.linalg.norm(run.xyz[node]) - np.linalg.norm(x0[node])
+        runs[on] = run
+    c = np.zeros((m["node_xyz"].shape[0], 3))
+    import ctypes
+    ol.oracle().oracle_surface_centres(ctypes.byref(runs[1].mesh), ol._p(np.ascontiguousarray(x0)), ol._p(c))
+    faces = np.nonzero((m["face_surf"] == kind) & np.any(m["face_nodes"] == node, axis=1))[0]
+    nbs = np.setdiff1d(np.unique(m["face_nodes"][faces]), [node])
+    A, C = x0[node], c[node]
+    r = np.mean(np.linalg.norm(x0[nbs] - C, axis=1))
+    B2 = C + (r / np.linalg.norm(A - C)) * (A - C)
+    v_s = velo * k_sph * (B2 - A) / dt
+    nf = len(faces)
+    expect = (nf * d[0] + dt * (v_s @ (A / np.linalg.norm(A)))) / (nf + 1)
+    assert abs(d[1] - expect) <= 1e-9 * abs(expect), (d, expect)
+
+
+def test_smoothing_off_changes_nothing(titan, oracle_lib):
+    """All smoothing flags off: the same step as before smoothing existed, bit for bit."""
+    m, p, st = _shell(titan)
+    for layer, kind in ((4, 1), (6, 2), (8, 3)):
+        titan.mesh.mark_shell_surface(m, layer, kind)
+    rays = titan.mesh.shell_rays(m)
+    res = []
+    for extra in ({}, dict(sglag_TS=0, sglag_HP=0, sglag_BS=0, sglag_TS_k_sphere=0.3, sglag_BS_k=0.3)):
+        run = ol.OracleRun(m, p, surface=dict(SURF, **extra), rays=rays)
+        s = np.ascontiguousarray(st.copy())
+        assert run.go(s, 2).err_code == 0
+        res.append((s, run.xyz.copy()))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])

@@ -16,7 +16,9 @@
 //  3. One thread per ray node: every node between two anchors (the ray's ends
 //     and its surface nodes) keeps its initial fraction of that segment, on
 //     the ray's direction.
-// The smoothing terms of the reference (sglag_*) are not part of this motion.
+// With smoothing on, a node's mean also takes one smoothing term (sglag_*): toward
+// the sphere fitted through it and its neighbours (TS, HP) or toward the mean of
+// them (BS).
 #include "launch.h"
 #include "step_kernels.cuh"
 #include "surface.h"
@@ -122,17 +124,59 @@ __global__ void node_kernel(FaceArgs a, SurfaceDev S) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) v[k] += S.vf[k * S.nlist + pos];
     }
-    const int num = j1 - j0;
+    int num = j1 - j0;
+    double A[3];
+    load_node(a.L1.xyz, nn, id, A);
+    const double time = a.st->dt;
+    const int kind = S.sm_kind[i];
+    if (kind) {
+        // smoothing (Setka_move.cpp:454-1211): one more term of the mean
+        const int b0 = S.nb_ptr[i], b1 = S.nb_ptr[i + 1], nb = b1 - b0;
+        const double coef = S.sm_coef[i];
+        if (kind == 1) {
+            // toward the sphere fitted at set-up through the node and its neighbours
+            const double B[3] = {S.sm_centre[i], S.sm_centre[S.n_node + i], S.sm_centre[2 * S.n_node + i]};
+            const double rr = sqrt((A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) +
+                                   (A[2] - B[2]) * (A[2] - B[2]));
+            double r = 0.0;
+            for (int j = b0; j < b1; ++j) {
+                double X[3];
+                load_node(a.L1.xyz, nn, S.nb_id[j], X);
+                r += sqrt((X[0] - B[0]) * (X[0] - B[0]) + (X[1] - B[1]) * (X[1] - B[1]) +
+                          (X[2] - B[2]) * (X[2] - B[2]));
+            }
+            r /= nb;
+            const double kk = r / rr;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double b2 = kk * (A[k] - B[k]) + B[k];
+                v[k] += coef * (b2 - A[k]) / time;
+            }
+            ++num;
+        } else if (nb > 5) {
+            // toward the mean of the node and its neighbours
+            double B[3] = {A[0], A[1], A[2]};
+            for (int j = b0; j < b1; ++j) {
+                double X[3];
+                load_node(a.L1.xyz, nn, S.nb_id[j], X);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) B[k] += X[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                B[k] /= (nb + 1.0);
+                v[k] += coef * (B[k] - A[k]) / time;
+            }
+            ++num;
+        }
+    }
     if (num > 0) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) v[k] /= num;
     }
-    double A[3];
-    load_node(a.L1.xyz, nn, id, A);
     const double an = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
     const double B[3] = {A[0] / an, A[1] / an, A[2] / an};
     const double vb = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];
-    const double time = a.st->dt;
     double* x2 = const_cast<double*>(a.xyz2);
 #pragma unroll
     for (int k = 0; k < 3; ++k) x2[k * nn + id] = A[k] + vb * time * B[k];

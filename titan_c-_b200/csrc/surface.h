@@ -30,6 +30,15 @@ struct SurfaceDev {
     const int2* ray_seg;    // [nray][ray_len]: slots of the anchors around a node, (-1, -1) for an anchor
     double vel[4];          // velocity_TS / _HP / _BS at [1] / [2] / [3]
     int null_bn_on_hp;
+    // smoothing of each moving node (the reference's sglag_* terms): 0 none,
+    // 1 toward its fitted sphere (centre sm_centre), 2 toward the mean of it
+    // and its neighbours; coefficient velocity_X * k; neighbours in ascending
+    // original node order
+    const signed char* sm_kind;   // [n_node]
+    const double* sm_coef;        // [n_node]
+    const double* sm_centre;      // [3][n_node]
+    const int* nb_ptr;            // [n_node + 1]
+    const int* nb_id;             // device node ids
 };
 
 // xyz2 of `fa` from xyz of fa.L1 by surface tracking, with the step's dt from

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <array>
 #include <map>
 #include <tuple>
 #include <string>
@@ -125,7 +126,8 @@ struct titan_ctx {
     // surface-tracking node motion (titan_set_surface_motion)
     bool use_surface = false;
     SurfaceDev surf{};
-    void* surf_buf[9] = {};  // face_list, vf, node_id, node_ptr, node_face, ray_nodes, ray_r0, ray_dir, ray_seg
+    void* surf_buf[14] = {};  // face_list, vf, node_id, node_ptr, node_face, ray_nodes, ray_r0, ray_dir, ray_seg,
+                              // sm_kind, sm_coef, sm_centre, nb_ptr, nb_id
 
     // Monte-Carlo pass buffers (titan_mc_sources), allocated by the first pass
     McCell* d_mc_cells = nullptr;       // [ncell] tracing records
@@ -408,6 +410,90 @@ void drop_surface(titan_ctx* ctx) {
     }
     ctx->surf = SurfaceDev{};
     ctx->use_surface = false;
+}
+
+// Least squares of 2 p . c = |p|^2 over the points with weights w (normal
+// equations, Gaussian elimination with partial pivoting); a singular system
+// (all weights zero) gives the zero vector.
+void fit_weighted(const std::vector<std::array<double, 3>>& P, const std::vector<double>& w, double c[3]) {
+    double M[3][4] = {};
+    for (size_t i = 0; i < P.size(); ++i) {
+        const double a[3] = {2.0 * P[i][0], 2.0 * P[i][1], 2.0 * P[i][2]};
+        const double b = P[i][0] * P[i][0] + P[i][1] * P[i][1] + P[i][2] * P[i][2];
+        const double ww = w[i] * w[i];
+        for (int j = 0; j < 3; ++j) {
+            for (int k = 0; k < 3; ++k) M[j][k] += ww * a[j] * a[k];
+            M[j][3] += ww * a[j] * b;
+        }
+    }
+    double scale = 0.0;
+    for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k) scale = std::max(scale, std::fabs(M[j][k]));
+    c[0] = c[1] = c[2] = 0.0;
+    if (!(scale > 0.0)) return;
+    for (int col = 0; col < 3; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 3; ++r)
+            if (std::fabs(M[r][col]) > std::fabs(M[piv][col])) piv = r;
+        if (std::fabs(M[piv][col]) <= 1e-14 * scale) return;
+        if (piv != col)
+            for (int k = 0; k < 4; ++k) std::swap(M[col][k], M[piv][k]);
+        for (int r = col + 1; r < 3; ++r) {
+            const double f = M[r][col] / M[col][col];
+            for (int k = col; k < 4; ++k) M[r][k] -= f * M[col][k];
+        }
+    }
+    for (int j = 2; j >= 0; --j) {
+        double v = M[j][3];
+        for (int k = j + 1; k < 3; ++k) v -= M[j][k] * c[k];
+        c[j] = v / M[j][j];
+    }
+}
+
+// Centre of the sphere that best fits a node and its surface neighbours, as
+// Setka::Smooth_head_TS3 / Smooth_head_HP3 form it (Setka_move.cpp:2205-2362,
+// 2046-2203): the least-squares c of 2 p . c = |p|^2, then up to 8 fits
+// re-weighted by Tukey's biweight of the distance residuals (cutoff 2.5
+// standard deviations), until the RMS residual changes by less than 1e-6.
+// The reference solves each fit by SVD; the normal equations here give the
+// same centre up to rounding.
+void fit_centre(const std::vector<std::array<double, 3>>& P, double c[3]) {
+    const size_t n = P.size();
+    std::vector<double> w(n, 1.0), res(n);
+    fit_weighted(P, w, c);
+    double prev = 1e308;
+    for (int iter = 0; iter < 8; ++iter) {
+        double radius = 0.0;
+        for (const auto& p : P)
+            radius += std::sqrt((p[0] - c[0]) * (p[0] - c[0]) + (p[1] - c[1]) * (p[1] - c[1]) +
+                                (p[2] - c[2]) * (p[2] - c[2]));
+        radius /= (double)n;
+        double total = 0.0;
+        for (size_t i = 0; i < n; ++i) {
+            const double d = std::sqrt((P[i][0] - c[0]) * (P[i][0] - c[0]) + (P[i][1] - c[1]) * (P[i][1] - c[1]) +
+                                       (P[i][2] - c[2]) * (P[i][2] - c[2]));
+            res[i] = std::fabs(d - radius);
+            total += res[i] * res[i];
+        }
+        const double rms = std::sqrt(total / (double)n);
+        if (std::fabs(prev - rms) < 1e-6) break;
+        prev = rms;
+        double mean = 0.0;
+        for (double r : res) mean += r;
+        mean /= (double)n;
+        double var = 0.0;
+        for (double r : res) var += (r - mean) * (r - mean);
+        const double cutoff = 2.5 * std::sqrt(var / (double)n);
+        for (size_t i = 0; i < n; ++i) {
+            if (res[i] < cutoff) {
+                const double t = res[i] / cutoff;
+                w[i] = (1.0 - t * t) * (1.0 - t * t);
+            } else {
+                w[i] = 0.0;
+            }
+        }
+        fit_weighted(P, w, c);
+    }
 }
 
 template <typename T>
@@ -1329,6 +1415,49 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     // rays in device numbering, with the radii and directions of this layer
     std::vector<double> xyz(3 * nn);
     CK(cudaMemcpy(xyz.data(), ctx->layer[ctx->cur].xyz, sizeof(double) * 3 * nn, cudaMemcpyDeviceToHost));
+    // smoothing: each moving node's surface neighbours (the nodes of its
+    // surface's faces), ascending original id, and the fitted sphere centre
+    std::vector<std::vector<int32_t>> faces_of(nn);
+    for (int64_t f = 0; f < nf; ++f)
+        if (surf[f] >= 1 && surf[f] <= 3)
+            for (int k = 0; k < 4; ++k) faces_of[fnodes[k * nf + f]].push_back((int32_t)f);
+    std::vector<signed char> sm_kind(S.n_node, 0);
+    std::vector<double> sm_coef(S.n_node, 0.0), sm_centre(3 * (size_t)S.n_node, 0.0);
+    std::vector<int32_t> nb_ptr{0}, nb_id;
+    for (int i = 0; i < S.n_node; ++i) {
+        const int32_t d = node_id[i];
+        const int s = node_surf[d];
+        const bool sphere = (s == 1 && sp->sglag_TS) || (s == 2 && sp->sglag_HP);
+        const bool laplace = (s == 3 && sp->sglag_BS);
+        std::vector<int32_t> nbs;
+        if (sphere || laplace) {
+            for (int32_t f : faces_of[d]) {
+                if (surf[f] != s) continue;
+                for (int k = 0; k < 4; ++k) {
+                    const int32_t j = fnodes[k * nf + f];
+                    if (j != d) nbs.push_back(j);
+                }
+            }
+            std::sort(nbs.begin(), nbs.end(),
+                      [&](int32_t x, int32_t y) { return R.node_n2o[x] < R.node_n2o[y]; });
+            nbs.erase(std::unique(nbs.begin(), nbs.end()), nbs.end());
+        }
+        if (sphere && !nbs.empty()) {
+            sm_kind[i] = 1;
+            sm_coef[i] = (s == 1 ? sp->velocity_TS * sp->sglag_TS_k_sphere : sp->velocity_HP * sp->sglag_HP_k_sphere);
+            std::vector<std::array<double, 3>> P;
+            P.push_back({xyz[d], xyz[nn + d], xyz[2 * nn + d]});
+            for (int32_t j : nbs) P.push_back({xyz[j], xyz[nn + j], xyz[2 * nn + j]});
+            double c[3];
+            fit_centre(P, c);
+            for (int k = 0; k < 3; ++k) sm_centre[(size_t)k * S.n_node + i] = c[k];
+        } else if (laplace) {
+            sm_kind[i] = 2;
+            sm_coef[i] = sp->velocity_BS * sp->sglag_BS_k;
+        }
+        if (sm_kind[i]) nb_id.insert(nb_id.end(), nbs.begin(), nbs.end());
+        nb_ptr.push_back((int32_t)nb_id.size());
+    }
     const int64_t L = ray_len;
     std::vector<int32_t> rn(nray * L);
     std::vector<double> r0(nray * L), dir(3 * nray);
@@ -1383,6 +1512,11 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     if (!e) e = upload_vec(&ctx->surf_buf[6], r0);
     if (!e) e = upload_vec(&ctx->surf_buf[7], dir);
     if (!e) e = upload_vec(&ctx->surf_buf[8], seg);
+    if (!e) e = upload_vec(&ctx->surf_buf[9], sm_kind);
+    if (!e) e = upload_vec(&ctx->surf_buf[10], sm_coef);
+    if (!e) e = upload_vec(&ctx->surf_buf[11], sm_centre);
+    if (!e) e = upload_vec(&ctx->surf_buf[12], nb_ptr);
+    if (!e) e = upload_vec(&ctx->surf_buf[13], nb_id);
     if (e) {
         drop_surface(ctx);
         return fail(TITAN_ECUDA, std::string("surface tables: ") + cudaGetErrorString(e));
@@ -1396,6 +1530,11 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     S.ray_r0 = (const double*)ctx->surf_buf[6];
     S.ray_dir = (const double*)ctx->surf_buf[7];
     S.ray_seg = (const int2*)ctx->surf_buf[8];
+    S.sm_kind = (const signed char*)ctx->surf_buf[9];
+    S.sm_coef = (const double*)ctx->surf_buf[10];
+    S.sm_centre = (const double*)ctx->surf_buf[11];
+    S.nb_ptr = (const int*)ctx->surf_buf[12];
+    S.nb_id = (const int*)ctx->surf_buf[13];
     ctx->surf = S;
     ctx->use_surface = true;
     return TITAN_OK;

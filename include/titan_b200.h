@@ -396,10 +396,15 @@ int64_t titan_device_bytes(titan_ctx* ctx);
  * that loads the library until the process exits), so at most
  * TITAN_NOALLOC_MAX_FACES faces; larger meshes get TITAN_EINVAL. Stationary
  * meshes only (params->move = 0). The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress) and caches it: make that first
- * call before any stream capture. All calls share the array, which keeps the
+ * array's device address (cudaGetSymbolAddress) and caches it with the
+ * device's current context: make that first call before any stream capture.
+ * A device reset (cudaDeviceReset) gives the device a new context; the next
+ * call then looks the address up again, so after a reset, too, the first call
+ * comes before any capture. All calls share the array, which keeps the
  * previous call's contents (each call resets the status word itself), so calls
- * that overlap on the GPU race; run them one at a time.
+ * that overlap on the GPU race; run them one at a time. ncell must satisfy
+ * 3 ncell <= nface (6 faces per cell, 2 cells per face); other sizes get
+ * TITAN_EINVAL.
  *
  * All pointers in titan_dev_mesh and state_in/state_out are DEVICE memory,
  * in the library's kernel layout, in any consistent cell/face numbering:

@@ -16,6 +16,10 @@ Translation units and their floating-point flags:
   titan_api.cu, renumber.cpp    host side of the C ABI
   checkpoint.cpp                cell-parameter files in the reference's layout
   noalloc.cu       -fmad=false  titan_step_noalloc (fixed scratch array, no allocation)
+
+It also builds tests/cpp/setka_consumer.cpp (g++, host only) into _build/: a
+C++ program that drives the library through include/titan_b200.h the way the
+binding inside the reference's Setka does (used by the GPU tests).
 """
 from __future__ import annotations
 
@@ -107,7 +111,28 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_consumer(force, verbose)
     return LIB
+
+
+CONSUMER_SRC = os.path.join(os.path.dirname(HERE), "tests", "cpp", "setka_consumer.cpp")
+CONSUMER = os.path.join(BUILD, "setka_consumer")
+
+
+def build_consumer(force: bool = False, verbose: bool = False) -> str | None:
+    """The C++ consumer of the ABI, linked against the in-tree library (rpath
+    relative to the binary, so the tree can move)."""
+    if not os.path.exists(CONSUMER_SRC):
+        return None
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    if force or _stale(CONSUMER, [CONSUMER_SRC, LIB, os.path.join(inc, "titan_b200.h")]):
+        cxx = shutil.which("g++") or "g++"
+        cmd = [cxx, "-O2", "-std=c++17", f"-I{inc}", CONSUMER_SRC, "-o", CONSUMER, f"-L{HERE}", "-ltitan_b200",
+               "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return CONSUMER
 
 
 if __name__ == "__main__":

@@ -16,8 +16,10 @@
 // that overlap on the GPU (different streams or threads at the same time)
 // race; the array keeps the previous call's contents, and each call resets
 // the status word it needs zeroed before its kernels run.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -48,22 +50,43 @@ int nfail(int code, const std::string& msg) {
     return code;
 }
 
-// Device address of the scratch on the current device, looked up once per
-// device (with that device current) and cached.
+// Device address of the scratch on the current device, looked up with that
+// device current and cached together with the context it belongs to. A device
+// reset (cudaDeviceReset) destroys the context and the module with the array;
+// the next call then sees a different current context and looks the address
+// up again instead of using the stale one. The current context comes from the
+// driver's cuCtxGetCurrent, fetched through the runtime (no libcuda link).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
 std::mutex g_mu;
 void* g_addr[256] = {};
+CUcontext g_ctx[256] = {};
+CtxGetCurrentFn g_ctx_get = nullptr;
 
 int scratch_on_device(unsigned char** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 256) return nfail(TITAN_ECUDA, "titan_step_noalloc: no current device");
+    e = cudaSetDevice(dev);  // makes the device's primary context current on this thread
+    if (e != cudaSuccess)
+        return nfail(TITAN_ECUDA, std::string("titan_step_noalloc: no context: ") + cudaGetErrorString(e));
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    if (!g_ctx_get) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return nfail(TITAN_ECUDA, "titan_step_noalloc: cuCtxGetCurrent not available");
+        g_ctx_get = reinterpret_cast<CtxGetCurrentFn>(fn);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get(&ctx) != CUDA_SUCCESS || !ctx) return nfail(TITAN_ECUDA, "titan_step_noalloc: no current context");
+    if (!g_addr[dev] || g_ctx[dev] != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return nfail(TITAN_ECUDA, std::string("titan_step_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         g_addr[dev] = p;
+        g_ctx[dev] = ctx;
     }
     *out = static_cast<unsigned char*>(g_addr[dev]);
     return TITAN_OK;
@@ -87,6 +110,11 @@ extern "C" int titan_step_noalloc(const titan_dev_mesh* m, const titan_params* p
                                   double* state_out, double* dt_next, int32_t* err_kind, void* stream) {
     if (!m || !p || !state_in || !state_out || !dt_next) return nfail(TITAN_EINVAL, "titan_step_noalloc: null argument");
     if (m->nface <= 0 || m->ncell <= 0) return nfail(TITAN_EINVAL, "titan_step_noalloc: empty mesh");
+    // every cell lists 6 faces and a face belongs to at most 2 cells, so
+    // 3 ncell <= nface; this also keeps ncell far inside the kernels' int range
+    if (m->ncell > INT_MAX / 3 || 3 * m->ncell > m->nface)
+        return nfail(TITAN_EINVAL, "titan_step_noalloc: ncell inconsistent with nface (6 faces per cell, 2 cells per face)");
+    if (m->nbc < 0 || m->nbc > INT_MAX) return nfail(TITAN_EINVAL, "titan_step_noalloc: nbc out of range");
     if (m->nface > TITAN_NOALLOC_MAX_FACES) {
         char buf[200];
         snprintf(buf, sizeof buf, "titan_step_noalloc: %lld faces exceed the fixed scratch of %d faces",

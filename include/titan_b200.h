@@ -296,6 +296,9 @@ typedef struct titan_mc_params {
     uint64_t seed;
     int32_t max_cells;   /* cell visits before a particle counts as lost (0: 1000000) */
     int32_t face_types;  /* e.g. (1 << TITAN_FACE_OUTER_HARD) | (1 << TITAN_FACE_OUTER_SOFT) */
+    double* trace_out;   /* NULL, or host [n_particles][8]: each neutral's end — position (3),
+                            velocity (3), charge exchanges, 4 * cell visits + end kind (0 left
+                            through the boundary, 1 lost after max_cells, 2 no outgoing face) */
 } titan_mc_params;
 
 typedef struct titan_mc_info {
@@ -309,8 +312,10 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* params, double* out,
 /* ---------------------------------------------------------------------------
  * Learned charge-exchange closure (no reference counterpart: it stands in for
  * re-running the Monte-Carlo neutral solver between plasma steps).
- * An MLP 8 -> 128 -> 128 -> 128 -> 128 -> 5 with SiLU, BF16 weights and
- * activations, FP32 accumulation. Parameters: FP32 masters, TITAN_MLP_NPARAM
+ * An MLP 8 -> 128 -> 128 -> 128 -> 128 -> 5 with SiLU, BF16 weights, FP32
+ * accumulation; training rounds activations to BF16, inference carries each
+ * activation as a BF16 hi + lo pair (about 16 bits) with SiLU in FP32, so the
+ * sources are a smooth function of the cell state. Parameters: FP32 masters, TITAN_MLP_NPARAM
  * floats [W1 16x128 | b1 128 | W2 128x128 | b2 | W3 | b3 | W4 | b4 |
  * W5 128x16 | b5 16], W stored [in][out]; inputs 8..15 and outputs 5..15 are
  * padding kept at zero. norm: feature mean[8], 1/std[8], output scale[5].

@@ -66,14 +66,21 @@ def standardise(X, norm):
     return x0
 
 
-def forward(params, norm, X, emulate_bf16: bool = True):
-    """Outputs Y [n][5] (network units) and the cache for backward."""
-    r = bf16 if emulate_bf16 else (lambda a: np.asarray(a, np.float64))
+def forward(params, norm, X, emulate_bf16: bool = True, inference: bool = False):
+    """Outputs Y [n][5] (network units) and the cache for backward.
+
+    inference=True models the tcgen05 inference kernel instead of the training
+    path: weights and biases rounded to BF16, inputs and activations kept at
+    full precision (the kernel carries each as a BF16 hi + lo pair, about 16
+    significant bits, and evaluates SiLU in FP32)."""
+    r = bf16 if emulate_bf16 and not inference else (lambda a: np.asarray(a, np.float64))
     a = r(standardise(X, norm))
     cache = {"A": [a], "Z": [], "W": []}
     layers = unpack(params)
     for li, (W, b) in enumerate(layers):
-        Wr = r(W)
+        Wr = bf16(W) if inference else r(W)
+        if inference:
+            b = bf16(b)
         z = a @ Wr + b
         cache["W"].append(Wr)
         cache["Z"].append(z)

@@ -2164,4 +2164,332 @@ int oracle_num_threads(void) {
 #endif
 }
 
+// ---------------------------------------------------------------------------
+// Monte-Carlo neutral hydrogen pass (the closure's source generator), a CPU
+// restatement of the device pass of titan_mc_sources on the same numbering:
+//  * the neutral physics of Setka::MK_fly_immit (TITAN/source/Setka_MK.cpp:
+//    1752-2314): straight flight through the cells, the charge-exchange rate
+//    nu = rho_Th uz sigma(uz) / Kn with uz = Velosity_1(|v - V_p|, cp)
+//    (Setka_MK.cpp:40-50, 1976-1988), sigma(u) = (1 - a2 ln u)^2
+//    (Phys_param.h:177-180), the optical depth against -ln(1 - xi), the new
+//    velocity by the rejection scheme of Setka::M_K_Change_Velosity
+//    (Setka_MK.cpp:2788-2852), rho_Th / p_Th of Phys_param::Plasma_components_1
+//    (Phys_param.cpp:628-665) with the cell type as zone (Setka_MK.cpp:1956),
+//    floored as at Setka_MK.cpp:1966-1967;
+//  * the momentum and energy tallies mu (v_old - v_new), mu (|v_old|^2 -
+//    |v_new|^2) / 2 per exchange, and mu t per cell (n_H), divided by the
+//    cell volume at the end;
+//  * inflow: a drifting Maxwellian through the faces whose type is selected,
+//    faces chosen by the inflow CDF (stratified by particle id), positions
+//    uniform on the quad, velocities flux-weighted by rejection;
+//  * random numbers: the counter-based SplitMix64 finaliser over (seed,
+//    particle id, draw counter), so every neutral's history is a function of
+//    its id alone, and the CDF summed in the same fixed tree as the device
+//    scan (warp shuffles of 32, warp totals in order, 256-face rounds of
+//    4096-face blocks, blocks combined by 1024 segments).
+// The device tracer is compiled with FMA contraction and CUDA's libm, this
+// one without contraction and with glibc: a neutral's history agrees to
+// rounding until a decision (exchange or not, which face it leaves by, a
+// rejection test) falls within rounding of its threshold, so the test
+// compares neutrals one by one and requires nearly all to agree.
+// ---------------------------------------------------------------------------
+namespace {
+
+const double kMcSqrtPi = 1.77245385;                 // sqrtpi_ of TITAN/source/Header.h:94
+const double kMcSqrtPiFull = 1.7724538509055160273;  // sqrt(pi) of the inflow flux
+
+struct OMcRng {
+    uint64_t key, ctr;
+    double uniform() {
+        uint64_t z = key + 0x9E3779B97F4A7C15ull * (++ctr);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z = z ^ (z >> 31);
+        return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    }
+};
+
+double o_velosity_1(double u, double cp) {
+    if (u < 0.00001)
+        return 2.0 * cp / kMcSqrtPi + 2.0 * u * u / (3.0 * cp * kMcSqrtPi) - u * u * u * u / (15.0 * cp * cp * cp * kMcSqrtPi);
+    return std::exp(-u * u / (cp * cp)) * cp / kMcSqrtPi + (u + (cp * cp) / (2.0 * u)) * std::erf(u / cp);
+}
+
+double o_mc_sigma(double a2, double x) {
+    const double s = 1.0 - a2 * std::log(x);
+    return s * s;
+}
+
+void o_change_velocity(OMcRng& rng, double a2, double cp, const double U[3], const double Vn[3], double W[3]) {
+    const double X = std::sqrt((Vn[0] - U[0]) * (Vn[0] - U[0]) + (Vn[1] - U[1]) * (Vn[1] - U[1]) +
+                               (Vn[2] - U[2]) * (Vn[2] - U[2]));
+    const double p4 = 0.5 * kMcSqrtPi * X / (1.0 + 0.5 * kMcSqrtPi * X);
+    double v1 = U[0], v2 = U[1], v3 = U[2];
+    for (int it = 0; it < 1000; ++it) {
+        const double k1 = rng.uniform(), k2 = rng.uniform(), k3 = rng.uniform();
+        const double k4 = rng.uniform(), k5 = rng.uniform(), k6 = rng.uniform();
+        double y1, y2, y3;
+        if (p4 < k1) {
+            const double om1 = 1.0 - 2.0 * k4;
+            const double so = std::sqrt(1.0 - om1 * om1);
+            const double om2 = so * std::cos(2.0 * kPi * k5), om3 = so * std::sin(2.0 * kPi * k5);
+            const double lo = std::sqrt(-std::log(k2 * k3));
+            y1 = lo * om1;
+            y2 = lo * om2;
+            y3 = lo * om3;
+        } else {
+            y1 = std::sqrt(-std::log(k2)) * std::cos(kPi * k3);
+            y2 = std::sqrt(-std::log(k4)) * std::cos(2.0 * kPi * k5);
+            y3 = std::sqrt(-std::log(k4)) * std::sin(2.0 * kPi * k5);
+        }
+        v1 = y1 + U[0];
+        v2 = y2 + U[1];
+        v3 = y3 + U[2];
+        const double u1 = Vn[0] - v1, u2 = Vn[1] - v2, u3 = Vn[2] - v3;
+        const double uuu = std::sqrt(u1 * u1 + u2 * u2 + u3 * u3);
+        const double yy = std::sqrt(y1 * y1 + y2 * y2 + y3 * y3);
+        const double h = (uuu * o_mc_sigma(a2, uuu * cp)) / (o_mc_sigma(a2, X * cp) * (X + yy));
+        if (!(h < k6)) break;
+    }
+    W[0] = v1;
+    W[1] = v2;
+    W[2] = v3;
+}
+
+// The device's block scan of NT values v[0..NT): inclusive scan within each
+// warp of 32 (shuffle steps 1, 2, 4, 8, 16), then each warp adds the totals of
+// the warps before it, summed in ascending order. Returns the block total.
+double o_block_scan(std::vector<double>& v) {
+    const size_t nt = v.size(), nw = nt / 32;
+    std::vector<double> prev(nt), wt(nw);
+    for (int o = 1; o < 32; o <<= 1) {
+        prev = v;
+        for (size_t t = 0; t < nt; ++t)
+            if ((int)(t & 31) >= o) v[t] = prev[t] + prev[t - o];
+    }
+    for (size_t w = 0; w < nw; ++w) wt[w] = v[32 * w + 31];
+    double all = 0.0;
+    for (size_t k = 0; k < nw; ++k) all += wt[k];
+    for (size_t t = 0; t < nt; ++t) {
+        double before = 0.0;
+        for (size_t k = 0; k < t / 32; ++k) before += wt[k];
+        v[t] = before + v[t];
+    }
+    return all;
+}
+
+}  // namespace
+
+// One pass over a stationary mesh (its geometry formed here as
+// oracle_geometry does). tally [5][ncell] (n_H, S_m (3), S_E per unit volume),
+// trace [nparticles][8] or null (the device's per-neutral end record),
+// *inflow_total the neutrals entering per unit time, *lost the neutrals that
+// ended other than through the boundary. Returns 0, or 1 when no face lets
+// neutrals in.
+int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32_t npassive, double par_a_2,
+                   double par_Kn, double nH, const double* uH, double cpH, uint32_t face_types, uint64_t seed,
+                   int64_t nparticles, int32_t max_cells, double* tally, double* trace, double* inflow_total,
+                   int64_t* lost_out) {
+    const int64_t nc = M->ncell, nf = M->nface;
+    std::vector<double> cc(3 * nc), vol(nc), fc(3 * nf), fn(3 * nf), fa(nf);
+    oracle_geometry(M, xyz, cc.data(), vol.data(), fc.data(), fn.data(), fa.data());
+    // inflow weights and their CDF, in the device's summation tree
+    auto weight = [&](int64_t f) {
+        const int t = M->face_type[f];
+        if (t <= 0 || t > 31 || !((face_types >> t) & 1u)) return 0.0;
+        const double un = -(uH[0] * fn[3 * f] + uH[1] * fn[3 * f + 1] + uH[2] * fn[3 * f + 2]);
+        const double sr = un / cpH;
+        const double flux = nH * (cpH * std::exp(-sr * sr) / (2.0 * kMcSqrtPiFull) + 0.5 * un * (1.0 + std::erf(sr)));
+        return flux * fa[f];
+    };
+    const int64_t kChunk = 4096, kRound = 256, kSeg = 1024;
+    const int64_t nb = (nf + kChunk - 1) / kChunk;
+    std::vector<double> cdf(nf), bs(nb);
+    std::vector<double> v(kRound);
+    for (int64_t b = 0; b < nb; ++b) {
+        double carry = 0.0;
+        for (int64_t r = 0; r < kChunk / kRound; ++r) {
+            for (int64_t t = 0; t < kRound; ++t) {
+                const int64_t f = b * kChunk + r * kRound + t;
+                v[t] = f < nf ? weight(f) : 0.0;
+            }
+            const double all = o_block_scan(v);
+            for (int64_t t = 0; t < kRound; ++t) {
+                const int64_t f = b * kChunk + r * kRound + t;
+                if (f < nf) cdf[f] = carry + v[t];
+            }
+            carry += all;
+        }
+        bs[b] = carry;
+    }
+    const int64_t per = (nb + kSeg - 1) / kSeg;
+    std::vector<double> seg(kSeg), incl(kSeg);
+    for (int64_t t = 0; t < kSeg; ++t) {
+        const int64_t b0 = std::min(nb, t * per), b1 = std::min(nb, b0 + per);
+        double sg = 0.0;
+        for (int64_t b = b0; b < b1; ++b) {
+            const double x = bs[b];
+            bs[b] = sg;
+            sg += x;
+        }
+        seg[t] = sg;
+    }
+    incl = seg;
+    const double total = o_block_scan(incl);
+    for (int64_t t = 0; t < kSeg; ++t) {
+        const int64_t b0 = std::min(nb, t * per), b1 = std::min(nb, b0 + per);
+        const double before = incl[t] - seg[t];
+        for (int64_t b = b0; b < b1; ++b) bs[b] += before;
+    }
+    if (!(total > 0.0)) return 1;
+    for (int64_t f = 0; f < nf; ++f) cdf[f] = (f == nf - 1) ? 1.0 : (cdf[f] + bs[f / kChunk]) / total;
+    *inflow_total = total;
+    const double mu = total / (double)nparticles;
+    // the tracing records: outward face planes, neighbours, proton fluid
+    std::vector<double> plane(24 * nc), fluid(5 * nc);
+    std::vector<int32_t> nbr(6 * nc);
+    for (int64_t c = 0; c < nc; ++c) {
+        for (int sl = 0; sl < 6; ++sl) {
+            const int64_t f = M->cell_faces[6 * c + sl];
+            const bool first = M->face_cells[2 * f] == c;
+            const double sg = first ? 1.0 : -1.0;
+            const double n0 = sg * fn[3 * f], n1 = sg * fn[3 * f + 1], n2 = sg * fn[3 * f + 2];
+            double* P = &plane[24 * c + 4 * sl];
+            P[0] = n0;
+            P[1] = n1;
+            P[2] = n2;
+            P[3] = fc[3 * f] * n0 + fc[3 * f + 1] * n1 + fc[3 * f + 2] * n2;
+            nbr[6 * c + sl] = first ? M->face_cells[2 * f + 1] : M->face_cells[2 * f];
+        }
+        const double rho = state[c], p = state[4 * nc + c];
+        const double rho_He = npassive ? state[9 * nc + c] : 0.0;
+        const int al = (M->cell_type[c] <= 2) ? 2 : 1;
+        double r = -(kMeDmp * al * rho_He + 4.0 * (-rho + rho_He)) / (4.0 * (1.0 + kMeDmp));
+        double pt = p * (4.0 * rho - (4.0 + al * kMeDmp) * rho_He) / (8.0 * rho + (-7.0 + al + (1.0 - al) * kMeDmp) * rho_He);
+        if (r <= 1e-8) r = 1e-8;
+        if (pt <= 1e-8 / 2.0) pt = 1e-8 / 2.0;
+        fluid[5 * c] = r;
+        fluid[5 * c + 1] = std::sqrt(2.0 * pt / r);
+        fluid[5 * c + 2] = state[nc + c];
+        fluid[5 * c + 3] = state[2 * nc + c];
+        fluid[5 * c + 4] = state[3 * nc + c];
+    }
+    std::fill(tally, tally + 5 * nc, 0.0);
+    int64_t lost = 0;
+    for (int64_t pid = 0; pid < nparticles; ++pid) {
+        OMcRng rng{seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(pid + 1)), 0ull};
+        const double s = ((double)pid + rng.uniform()) / (double)nparticles;
+        int64_t lo = 0, hi = nf - 1;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (cdf[mid] < s)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        const int64_t f0 = lo;
+        double P[4][3];
+        for (int k = 0; k < 4; ++k)
+            for (int d = 0; d < 3; ++d) P[k][d] = xyz[3 * M->face_nodes[4 * f0 + k] + d];
+        const double A1 = tri_area(P[0], P[1], P[2]);
+        const double A2 = tri_area(P[0], P[3], P[2]);
+        const int tb = (rng.uniform() * (A1 + A2) < A1) ? 1 : 3;
+        double b1 = rng.uniform(), b2 = rng.uniform();
+        if (b1 + b2 > 1.0) {
+            b1 = 1.0 - b1;
+            b2 = 1.0 - b2;
+        }
+        double x[3];
+        for (int k = 0; k < 3; ++k) x[k] = P[0][k] + b1 * (P[tb][k] - P[0][k]) + b2 * (P[2][k] - P[0][k]);
+        const double nin[3] = {-fn[3 * f0], -fn[3 * f0 + 1], -fn[3 * f0 + 2]};
+        const double un = uH[0] * nin[0] + uH[1] * nin[1] + uH[2] * nin[2];
+        const double vmax = std::fmax(un, 0.0) + 6.0 * cpH;
+        double v[3] = {uH[0], uH[1], uH[2]};
+        for (int it = 0; it < 4096; ++it) {
+            const double r1 = std::sqrt(-std::log(rng.uniform())), t1 = 2.0 * kPi * rng.uniform();
+            const double r2 = std::sqrt(-std::log(rng.uniform())), t2 = 2.0 * kPi * rng.uniform();
+            v[0] = uH[0] + cpH * r1 * std::cos(t1);
+            v[1] = uH[1] + cpH * r1 * std::sin(t1);
+            v[2] = uH[2] + cpH * r2 * std::cos(t2);
+            const double vn = v[0] * nin[0] + v[1] * nin[1] + v[2] * nin[2];
+            if (vn > 0.0 && rng.uniform() * vmax < vn) break;
+        }
+        int64_t cell = M->face_cells[2 * f0];
+        double ksi = -std::log(1.0 - rng.uniform());
+        double I = 0.0;
+        int nex = 0, visit = 0, kind = 1;
+        for (; visit < max_cells; ++visit) {
+            const double* R = &plane[24 * cell];
+            double t_exit = 1e300;
+            int64_t next = -2;
+            for (int sl = 0; sl < 6; ++sl) {
+                const double vn = v[0] * R[4 * sl] + v[1] * R[4 * sl + 1] + v[2] * R[4 * sl + 2];
+                if (vn <= 0.0) continue;
+                const double d = R[4 * sl + 3] - (x[0] * R[4 * sl] + x[1] * R[4 * sl + 1] + x[2] * R[4 * sl + 2]);
+                const double t = std::fmax(d, 0.0) / vn;
+                if (t < t_exit) {
+                    t_exit = t;
+                    next = nbr[6 * cell + sl];
+                }
+            }
+            if (next == -2) {
+                kind = 2;
+                break;
+            }
+            const double* Fl = &fluid[5 * cell];
+            const double rho_th = Fl[0], cp = Fl[1];
+            const double du0 = v[0] - Fl[2], du1 = v[1] - Fl[3], du2 = v[2] - Fl[4];
+            const double u = std::sqrt(du0 * du0 + du1 * du1 + du2 * du2);
+            const double uz = o_velosity_1(u, cp);
+            const double nu = rho_th * uz * o_mc_sigma(par_a_2, uz) / par_Kn;
+            const double dI = nu * t_exit;
+            if (I + dI < ksi) {
+                tally[cell] += mu * t_exit;
+                I += dI;
+                for (int k = 0; k < 3; ++k) x[k] += t_exit * v[k];
+                if (next < 0) {
+                    kind = 0;
+                    break;
+                }
+                cell = next;
+                continue;
+            }
+            const double t_ex = (ksi - I) / nu;
+            tally[cell] += mu * t_ex;
+            for (int k = 0; k < 3; ++k) x[k] += t_ex * v[k];
+            const double U[3] = {Fl[2] / cp, Fl[3] / cp, Fl[4] / cp};
+            const double Vn[3] = {v[0] / cp, v[1] / cp, v[2] / cp};
+            double W[3];
+            o_change_velocity(rng, par_a_2, cp, U, Vn, W);
+            const double w0 = W[0] * cp, w1 = W[1] * cp, w2 = W[2] * cp;
+            tally[nc + cell] += mu * (v[0] - w0);
+            tally[2 * nc + cell] += mu * (v[1] - w1);
+            tally[3 * nc + cell] += mu * (v[2] - w2);
+            tally[4 * nc + cell] += mu * 0.5 * ((v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) - (w0 * w0 + w1 * w1 + w2 * w2));
+            v[0] = w0;
+            v[1] = w1;
+            v[2] = w2;
+            I = 0.0;
+            ksi = -std::log(1.0 - rng.uniform());
+            ++nex;
+        }
+        if (kind != 0) ++lost;
+        if (trace) {
+            double* r = trace + 8 * pid;
+            r[0] = x[0];
+            r[1] = x[1];
+            r[2] = x[2];
+            r[3] = v[0];
+            r[4] = v[1];
+            r[5] = v[2];
+            r[6] = (double)nex;
+            r[7] = 4.0 * (double)(visit + (kind == 0 ? 1 : 0)) + (double)kind;
+        }
+    }
+    for (int64_t c = 0; c < nc; ++c)
+        for (int k = 0; k < 5; ++k) tally[k * nc + c] /= vol[c];
+    *lost_out = lost;
+    return 0;
+}
+
 }  // extern "C"

@@ -335,3 +335,52 @@ class OracleRun:
         dtn = oracle().oracle_face_fluxes(ctypes.byref(self.mesh), ctypes.byref(self.params), _p(state),
                                           _p(self.xyz), _p(self.xyz), float(time), _p(fl), ctypes.byref(err))
         return fl, dtn, err.value
+
+
+def renumbered_mesh(mesh: dict, cell_n2o, face_n2o, node_n2o) -> dict:
+    """The mesh in a context's renumbering (new index -> original index arrays,
+    PlasmaStep.permutation()): every object moved to its new index and every
+    reference rewritten, the per-face node order and per-cell face order kept."""
+    c_o2n = np.empty_like(cell_n2o)
+    c_o2n[cell_n2o] = np.arange(len(cell_n2o), dtype=cell_n2o.dtype)
+    f_o2n = np.empty_like(face_n2o)
+    f_o2n[face_n2o] = np.arange(len(face_n2o), dtype=face_n2o.dtype)
+    n_o2n = np.empty_like(node_n2o)
+    n_o2n[node_n2o] = np.arange(len(node_n2o), dtype=node_n2o.dtype)
+    fcl = mesh["face_cells"][face_n2o]
+    fcl = np.where(fcl >= 0, c_o2n[np.maximum(fcl, 0)], -1).astype(np.int32)
+    out = dict(
+        node_xyz=np.ascontiguousarray(mesh["node_xyz"][node_n2o]),
+        cell_nodes=n_o2n[mesh["cell_nodes"][cell_n2o]].astype(np.int32),
+        cell_faces=f_o2n[mesh["cell_faces"][cell_n2o]].astype(np.int32),
+        cell_type=mesh["cell_type"][cell_n2o], cell_tvd=mesh["cell_tvd"][cell_n2o],
+        face_nodes=n_o2n[mesh["face_nodes"][face_n2o]].astype(np.int32), face_cells=fcl,
+        face_type=mesh["face_type"][face_n2o], face_surf=mesh["face_surf"][face_n2o],
+        face_bc=mesh["face_bc"][face_n2o], bc_vals=mesh["bc_vals"], node_amp=None, node_phase=None)
+    return out, c_o2n
+
+
+def mc_pass(mesh: dict, state: np.ndarray, params: dict, n_H: float, u_H, cp_H: float, n_particles: int,
+            seed: int = 1, face_types: int = (1 << 2) | (1 << 3), max_cells: int = 1000000):
+    """The oracle's Monte-Carlo pass on a stationary mesh: (tally [5, ncell],
+    trace [n_particles, 8], inflow rate, lost)."""
+    run = OracleRun(mesh, params)
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    C = run.mesh.ncell
+    tally = np.empty((5, C))
+    trace = np.empty((n_particles, 8))
+    total = ctypes.c_double(0.0)
+    lost = ctypes.c_int64(0)
+    uH = np.ascontiguousarray(u_H, dtype=np.float64)
+    L = oracle()
+    L.oracle_mc_pass.restype = ctypes.c_int
+    L.oracle_mc_pass.argtypes = [ctypes.POINTER(OMesh), D, D, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, D, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint64,
+                                 ctypes.c_int64, ctypes.c_int32, D, D, D, ctypes.POINTER(ctypes.c_int64)]
+    rc = L.oracle_mc_pass(ctypes.byref(run.mesh), _p(run.xyz), _p(st), int(params["npassive"]),
+                          float(params["par_a_2"]), float(params["par_Kn"]), float(n_H), _p(uH), float(cp_H),
+                          int(face_types), int(seed), int(n_particles), int(max_cells), _p(tally), _p(trace),
+                          ctypes.byref(total), ctypes.byref(lost))
+    if rc:
+        raise RuntimeError("oracle_mc_pass: no inflow faces")
+    return tally, trace, total.value, lost.value

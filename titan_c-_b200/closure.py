@@ -52,7 +52,8 @@ def features(state: np.ndarray, cc: np.ndarray, n_inf: float, lam: float) -> np.
     X = np.empty((rho.shape[0], NIN), dtype=np.float32)
     X[:, 0] = np.log(np.maximum(rho, 1e-30))
     X[:, 1] = ur
-    X[:, 2] = np.sqrt(np.maximum(v2 - ur * ur, 0.0))
+    # |u_t| = |v x r| / r: no cancellation for a nearly radial flow
+    X[:, 2] = np.sqrt((vy * z - vz * y) ** 2 + (vz * x - vx * z) ** 2 + (vx * y - vy * x) ** 2) / r
     X[:, 3] = np.log(np.maximum(p / rho, 1e-30))
     X[:, 4] = np.log(r)
     X[:, 5] = np.arccos(np.clip(x / r, -1.0, 1.0))

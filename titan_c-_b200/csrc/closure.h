@@ -23,14 +23,21 @@ constexpr int kIn = 8, kInPad = 16, kHid = 128, kOut = 5, kOutPad = 16, kTile = 
 constexpr int kModeRaw = 0, kModeSources = 1;
 // Packed bf16 operands of the inference kernel, each an N x K block in the
 // canonical K-major layout, in this order:
-//   W1'  128 x 16: 0.5 W1 for k < 8, 0.5 b1 at k = 8 (the input tile carries 1 there)
+//   W1'  128 x 16: 0.5 W1 for k < 8 and again for 8 <= k < 16 (the input
+//        operand carries the features' high BF16 parts at k < 8 and their
+//        low parts at k >= 8, so one K = 16 step multiplies both)
 //   W2'..W4'  128 x 128: 0.5 W
 //   W5   16 x 128
-//   B2'..B4'  128 x 16: 0.5 b at k = 0 (multiplied by a constant tile with 1 at k = 0)
+//   B1'..B4'  128 x 16: 0.5 b at k = 0 (multiplied by a constant tile with 1 at k = 0)
 //   B5   16 x 16: b5 at k = 0
 // The 0.5 makes the hidden-layer accumulator h = (z + b) / 2, so the epilogue
 // forms SiLU(z + b) = h (1 + tanh h) without a bias add or a scaling.
-constexpr int kWPack = kHid * kInPad + 3 * kHid * kHid + kOutPad * kHid + 3 * kHid * kInPad + kOutPad * kInPad;
+// Activations are never rounded to a single BF16: each is carried as a BF16
+// pair hi + lo (about 16 significant bits) and every layer multiplies both
+// halves by the same weights, which keeps the network a smooth function of
+// the cell state (a single BF16 rounding makes it a staircase with steps of
+// 2^-8 that turn rounding-level state differences into source jumps).
+constexpr int kWPack = kHid * kInPad + 3 * kHid * kHid + kOutPad * kHid + 4 * kHid * kInPad + kOutPad * kInPad;
 
 struct MlpNet {
     const void* wpack;   // kWPack bf16 (above)
@@ -70,57 +77,58 @@ __device__ __forceinline__ float log_nh_proxy_f(float n_inf, float lambda, float
     return __logf(n_inf) + fmaxf(-lambda * th / (r * s), -30.0f);
 }
 
-// Sources from the network outputs of one cell (sources mode), formed in FP32
-// and stored as FP64: m_x, m_y, m_z in the frame e1 = V/|V| (radial when V =
-// 0), e2 = the inflow direction -x made orthogonal to e1, e3 = e1 x e2; E.
+// Sources from the network outputs of one cell (sources mode), formed in FP64:
+// m_x, m_y, m_z in the frame e1 = V/|V| (radial when V = 0), e2 = the inflow
+// direction -x made orthogonal to e1, e3 = e1 x e2; E. For a flow nearly along
+// x, e2 = -x - (-x . e1) e1 is a cancellation residue of the transverse
+// velocity; in FP32 its direction would be set by rounding noise that the
+// flux arithmetic perturbs every step, so the frame is formed in FP64 with the
+// same degenerate-case threshold as the training side (closure.py frame()).
 __device__ inline void write_sources(const MlpArgs& a, int c, const float* y) {
     const int nc = a.ncell;
-    const float rho = (float)a.state[c], vx = (float)a.state[nc + c], vy = (float)a.state[2 * nc + c];
-    const float vz = (float)a.state[3 * nc + c];
-    const float x = (float)a.cc[c], yy = (float)a.cc[nc + c], z = (float)a.cc[2 * nc + c];
-    const float r = sqrtf(x * x + yy * yy + z * z);
-    const float norm = rho * __expf(log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, x, r));
-    const float vm = sqrtf(vx * vx + vy * vy + vz * vz);
-    float e1[3], e2[3], e3[3];
-    if (vm > 0.0f) {
-        const float iv = 1.0f / vm;
-        e1[0] = vx * iv;
-        e1[1] = vy * iv;
-        e1[2] = vz * iv;
+    const double rho = a.state[c], vx = a.state[nc + c], vy = a.state[2 * nc + c];
+    const double vz = a.state[3 * nc + c];
+    const double x = a.cc[c], yy = a.cc[nc + c], z = a.cc[2 * nc + c];
+    const double r = sqrt(x * x + yy * yy + z * z);
+    const double norm = rho * (double)__expf(log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, (float)x, (float)r));
+    const double vm = sqrt(vx * vx + vy * vy + vz * vz);
+    double e1[3], e2[3], e3[3];
+    if (vm > 0.0) {
+        e1[0] = vx / vm;
+        e1[1] = vy / vm;
+        e1[2] = vz / vm;
     } else {
-        const float ir = 1.0f / r;
-        e1[0] = x * ir;
-        e1[1] = yy * ir;
-        e1[2] = z * ir;
+        e1[0] = x / r;
+        e1[1] = yy / r;
+        e1[2] = z / r;
     }
-    const float d = -e1[0];
-    e2[0] = -1.0f - d * e1[0];
+    const double d = -e1[0];
+    e2[0] = -1.0 - d * e1[0];
     e2[1] = -d * e1[1];
     e2[2] = -d * e1[2];
-    float n2 = sqrtf(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
-    if (n2 < 1e-6f) {  // flow along x: any perpendicular
-        e2[0] = 0.0f;
-        e2[1] = 1.0f;
-        e2[2] = 0.0f;
-        n2 = 1.0f;
+    double n2 = sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+    if (n2 < 1e-12) {  // flow along x: any perpendicular
+        e2[0] = 0.0;
+        e2[1] = 1.0;
+        e2[2] = 0.0;
+        n2 = 1.0;
     }
-    const float in2 = 1.0f / n2;
-    e2[0] *= in2;
-    e2[1] *= in2;
-    e2[2] *= in2;
+    e2[0] /= n2;
+    e2[1] /= n2;
+    e2[2] /= n2;
     e3[0] = e1[1] * e2[2] - e1[2] * e2[1];
     e3[1] = e1[2] * e2[0] - e1[0] * e2[2];
     e3[2] = e1[0] * e2[1] - e1[1] * e2[0];
-    const float s1 = norm * y[1] * a.net.oscale[1], s2 = norm * y[2] * a.net.oscale[2];
-    const float s3 = norm * y[3] * a.net.oscale[3];
-    a.src[c] = (double)(s1 * e1[0] + s2 * e2[0] + s3 * e3[0]);
-    a.src[nc + c] = (double)(s1 * e1[1] + s2 * e2[1] + s3 * e3[1]);
-    a.src[2 * nc + c] = (double)(s1 * e1[2] + s2 * e2[2] + s3 * e3[2]);
-    a.src[3 * nc + c] = (double)(norm * y[4] * a.net.oscale[4]);
+    const double s1 = norm * (double)(y[1] * a.net.oscale[1]), s2 = norm * (double)(y[2] * a.net.oscale[2]);
+    const double s3 = norm * (double)(y[3] * a.net.oscale[3]);
+    a.src[c] = s1 * e1[0] + s2 * e2[0] + s3 * e3[0];
+    a.src[nc + c] = s1 * e1[1] + s2 * e2[1] + s3 * e3[1];
+    a.src[2 * nc + c] = s1 * e1[2] + s2 * e2[2] + s3 * e3[2];
+    a.src[3 * nc + c] = norm * (double)(y[4] * a.net.oscale[4]);
 }
 
 cudaError_t mlp_prepare();  // once per process, before any launch (sets the shared-memory size)
-// grid: one CTA per SM at most (sm_count), three tiles of 128 rows in flight per CTA
+// grid: one CTA per SM at most (sm_count), two tiles of 128 rows in flight per CTA
 cudaError_t launch_mlp_forward(const MlpArgs& a, int mode, int sm_count, cudaStream_t s);
 size_t mlp_forward_smem_bytes();
 

@@ -1,26 +1,36 @@
 // Learned charge-exchange closure: an MLP 8 -> 128 -> 128 -> 128 -> 128 -> 5
 // (SiLU) that maps the local plasma state to the sources the Monte-Carlo
 // neutral solver would produce (titan_mc_sources), so the step can run without
-// re-tracing neutrals. BF16 weights and activations, FP32 accumulation.
+// re-tracing neutrals. BF16 weights, FP32 accumulation.
 //
 // Inference (every step) runs on the 5th-generation tensor cores. A CTA holds
-// the layer operands in shared memory for the whole kernel, in the canonical
-// K-major "interleave" layout (8x16-byte core matrices), and runs three
-// warpgroups, each with its own tile of 128 cells in flight and its own
-// 128-column TMEM accumulator: while one warpgroup turns its accumulator into
-// the next layer's BF16 activations (tcgen05.ld, SiLU), the tensor core works
-// on the other warpgroups' layers. Each layer is M=128 x N x K=16
-// tcgen05.mma instructions issued by one thread of the warpgroup; completion
-// goes through the warpgroup's mbarrier; waiting threads sleep (try_wait with
-// a suspend hint) and the waits are bounded: a wait that runs out records an
-// error and the warpgroup stops issuing work; the CTA releases TMEM and
-// returns.
+// the layer weights in shared memory for the whole kernel, in the canonical
+// K-major "interleave" layout (8x16-byte core matrices), and runs two
+// warpgroups, each with its own tile of 128 cells in flight. A warpgroup's
+// activations live in tensor memory next to its accumulator and are the A
+// operand of the next layer's tcgen05.mma (the TMEM-A form), so shared memory
+// holds only the weights: while one warpgroup turns its accumulator into the
+// next layer's activations (tcgen05.ld, SiLU, tcgen05.st), the tensor core
+// works on the other warpgroup's layer. One thread of the warpgroup issues
+// the M=128 x N x K=16 instructions; completion goes through the warpgroup's
+// mbarrier; waiting threads sleep (try_wait with a suspend hint) and the waits
+// are bounded: a wait that runs out records an error and the warpgroup stops
+// issuing work; the CTA releases TMEM and returns.
 //
-// The hidden-layer operands carry a factor 0.5 and the biases (closure.h), so
-// the accumulator holds h = (z + b) / 2 and the epilogue turns a pair of
-// columns into SiLU(z + b) = h (1 + tanh h) with one conversion to bf16x2,
-// one tanh.approx.bf16x2 and one bf16x2 FMA. Features and sources are formed
-// in FP32 (the network itself is BF16).
+// Precision: the network must be a smooth function of the cell state. Two
+// runs whose states differ at rounding level (the FP64 step and the mixed
+// step) must get sources that differ at the same level; a network whose
+// activations are rounded once to BF16 is a staircase with 2^-8 steps, and
+// its sources jump wherever a state difference crosses a step. So every
+// activation and every standardised input is carried as a BF16 pair hi + lo
+// (hi = the nearest BF16, lo = the BF16 nearest the exact remainder, together
+// about 16 significant bits), each layer multiplies both halves by the same
+// BF16 weights (K = 256 per hidden layer: 128 hi columns, then 128 lo
+// columns), and SiLU is evaluated in FP32. The hidden-layer operands carry 0.5
+// and the biases (closure.h), so the accumulator holds h = (z + b) / 2 and
+// SiLU(z + b) = h (1 + tanh h): one tanh.approx.f32 and one FMA per column;
+// the hi/lo split is integer arithmetic on the FP32 bits (no conversion
+// instructions). Features and sources are formed in FP32.
 //
 // Training uses the same networks through mma.sync tiles (closure_train.cu).
 #include <cuda_bf16.h>
@@ -99,33 +109,82 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// D (TMEM) += A (TMEM, M=128 rows in lanes, 2 bf16 per column along K) . B (shared memory)
+__device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bd, uint32_t idesc,
+                                            uint32_t accum) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bd), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+// 16 / 8 consecutive 32-bit columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* r) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// SiLU of a pair of columns from the accumulator h = (z + b) / 2 (FP32):
-// h (1 + tanh h) in bf16x2 — one conversion, one tanh, one FMA.
-__device__ __forceinline__ uint32_t silu_pair(float h0, float h1) {
-    uint32_t hb, t, y;
-    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hb) : "f"(h1), "f"(h0));
-    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(hb));
-    asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(hb), "r"(t));
+__device__ __forceinline__ float tanh_f32(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 
-constexpr int kGroups = 3;  // warpgroups per CTA, one tile in flight each
+// Two FP32 values as BF16 pairs: hi = the nearest BF16 of each (ties away
+// from zero), lo = the BF16 nearest the exact remainder v - hi. Returns the
+// two packed words {hi(v0), hi(v1)} and {lo(v0), lo(v1)}, element 0 in the
+// low half. Integer operations on the bits: adding 2^15 and keeping the top
+// 16 bits rounds to nearest; v - hi is exact in FP32.
+__device__ __forceinline__ void split_pair(float v0, float v1, uint32_t& hi, uint32_t& lo) {
+    const uint32_t r0 = __float_as_uint(v0) + 0x8000u, r1 = __float_as_uint(v1) + 0x8000u;
+    const float l0 = v0 - __uint_as_float(r0 & 0xFFFF0000u);
+    const float l1 = v1 - __uint_as_float(r1 & 0xFFFF0000u);
+    hi = __byte_perm(r0, r1, 0x7632);
+    lo = __byte_perm(__float_as_uint(l0) + 0x8000u, __float_as_uint(l1) + 0x8000u, 0x7632);
+}
+
+// SiLU of a pair of columns from the accumulator h = (z + b) / 2 (FP32):
+// h (1 + tanh h), split into BF16 hi / lo words.
+__device__ __forceinline__ void silu_pair(float h0, float h1, uint32_t& hi, uint32_t& lo) {
+    const float a0 = fmaf(h0, tanh_f32(h0), h0);
+    const float a1 = fmaf(h1, tanh_f32(h1), h1);
+    split_pair(a0, a1, hi, lo);
+}
+
+constexpr int kGroups = 2;  // warpgroups per CTA, one tile in flight each
+// TMEM columns of one warpgroup: its FP32 accumulator (128 columns), then its
+// activations as the next layer's A operand (128 rows in the lanes, two bf16
+// per column along K: columns 0..63 the hi halves of K = 0..127, columns
+// 64..127 the lo halves; the input tile uses columns 0..7: hi at K < 8, lo at
+// K >= 8).
+constexpr uint32_t kColsPerGroup = 256, kAccCols = 128, kActLoCols = 64;
+constexpr uint32_t kCols = kGroups * kColsPerGroup;  // 512: the whole TMEM of the SM
+static_assert(kCols <= 512, "tensor memory holds 512 columns");
 
 // Shared memory of one CTA. The operand blocks (w1 .. bw5) are contiguous in
 // the order of the packed array (closure.h).
 struct alignas(128) Smem {
-    __nv_bfloat16 w1[kHid * kInPad];           // W1'  N=128 x K=16
+    __nv_bfloat16 w1[kHid * kInPad];           // W1'  N=128 x K=16 (hi and lo inputs)
     __nv_bfloat16 w[3][kHid * kHid];           // W2'..W4'  N=128 x K=128
     __nv_bfloat16 w5[kOutPad * kHid];          // W5   N=16 x K=128
-    __nv_bfloat16 bw[3][kHid * kInPad];        // B2'..B4'  N=128 x K=16
+    __nv_bfloat16 bw[4][kHid * kInPad];        // B1'..B4'  N=128 x K=16
     __nv_bfloat16 bw5[kOutPad * kInPad];       // B5   N=16 x K=16
     __nv_bfloat16 ones[kTile * kInPad];        // M=128 x K=16, 1 at k = 0
-    __nv_bfloat16 a[kGroups][kTile * kHid];    // activations M=128 x K=128; the input
-                                               // tile (K=16) aliases its first 4 KB
     float fmean[kIn], fistd[kIn];
     float env_lo[kIn], env_hi[kIn];
     uint64_t mbar[kGroups];
@@ -133,25 +192,33 @@ struct alignas(128) Smem {
     int abort[kGroups];  // written by the group's own threads before its barrier, read after it
 };
 
-// Input features of one cell from its state and centre (closure.h), in FP32.
+// Input features of one cell from its state and centre (closure.h). The
+// vector parts are formed in FP64 and rounded once: in FP32 the tangential
+// speed sqrt(v^2 - u_r^2) of a nearly radial flow is the square root of a
+// cancellation residue (~1e-7 |v|^2, so ~3e-4 |v| of noise with an infinite
+// slope), which would make the feature, and the sources, jump with
+// rounding-level state changes. |u_t| = |v x r| / r has no cancellation. The
+// logarithms take FP32 arguments rounded once from FP64 and use the accurate
+// logf, which is continuous at FP32 resolution.
 __device__ __forceinline__ void cell_features(const MlpArgs& a, int c, float* f) {
     const int nc = a.ncell;
-    const float rho = (float)a.state[c], vx = (float)a.state[nc + c], vy = (float)a.state[2 * nc + c];
-    const float vz = (float)a.state[3 * nc + c], p = (float)a.state[4 * nc + c];
-    const float x = (float)a.cc[c], y = (float)a.cc[nc + c], z = (float)a.cc[2 * nc + c];
-    const float r = sqrtf(x * x + y * y + z * z);
-    const float ir = 1.0f / r;
-    const float ur = (vx * x + vy * y + vz * z) * ir;
-    const float v2 = vx * vx + vy * vy + vz * vz;
-    const float vmag = sqrtf(v2);
-    f[0] = __logf(fmaxf(rho, 1e-30f));
-    f[1] = ur;
-    f[2] = sqrtf(fmaxf(v2 - ur * ur, 0.0f));
-    f[3] = __logf(fmaxf(p / rho, 1e-30f));
-    f[4] = __logf(r);
-    f[5] = acosf(fminf(fmaxf(x * ir, -1.0f), 1.0f));
-    f[6] = vmag > 0.0f ? -vx / vmag : 0.0f;
-    f[7] = log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, x, r);
+    const double rho = a.state[c], vx = a.state[nc + c], vy = a.state[2 * nc + c];
+    const double vz = a.state[3 * nc + c], p = a.state[4 * nc + c];
+    const double x = a.cc[c], y = a.cc[nc + c], z = a.cc[2 * nc + c];
+    const double r = sqrt(x * x + y * y + z * z);
+    const double ir = 1.0 / r;
+    const double ur = (vx * x + vy * y + vz * z) * ir;
+    const double cx = vy * z - vz * y, cy = vz * x - vx * z, cz = vx * y - vy * x;
+    const double ut = sqrt(cx * cx + cy * cy + cz * cz) * ir;
+    const double vmag = sqrt(vx * vx + vy * vy + vz * vz);
+    f[0] = logf((float)fmax(rho, 1e-30));
+    f[1] = (float)ur;
+    f[2] = (float)ut;
+    f[3] = logf((float)fmax(p / rho, 1e-30));
+    f[4] = logf((float)r);
+    f[5] = acosf((float)fmin(fmax(x * ir, -1.0), 1.0));
+    f[6] = vmag > 0.0 ? (float)(-vx / vmag) : 0.0f;
+    f[7] = log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, (float)x, (float)r);
 }
 
 // Named barrier of one warpgroup (ids 1..kGroups; 0 is __syncthreads).
@@ -187,10 +254,10 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
     const int g = tid >> 7;          // warpgroup
-    const int row = tid & 127;       // this thread's row of the group's tile
+    const int row = tid & 127;       // this thread's row of the group's tile (its TMEM lane)
     const bool leader = row == 0;    // issues the group's MMAs
 
-    // operands (pre-packed in the canonical layout), the constant tile, normalisation
+    // weights (pre-packed in the canonical layout), the constant tile, normalisation
     {
         const uint4* src = reinterpret_cast<const uint4*>(args.net.wpack);
         uint4* dst = reinterpret_cast<uint4*>(S.w1);
@@ -215,7 +282,6 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.mbar[i])), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    constexpr uint32_t kCols = kGroups <= 2 ? 256u : 512u;  // power of two >= 128 x groups
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
                      "r"(kCols));
@@ -225,23 +291,24 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
     fence_before();
     __syncthreads();
     fence_after();
-    // this group's accumulator: columns [128 g, 128 g + 128); this warp's 32 lanes
-    const uint32_t tmem = S.tmem + (uint32_t)(g * kHid);
-    const uint32_t tmem_row = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    // this group's accumulator and activation columns (lane 0), and this
+    // warp's lane quarter (a warp reaches lanes 32 (warp % 4) .. + 31)
+    const uint32_t acc = S.tmem + (uint32_t)g * kColsPerGroup;
+    const uint32_t act = acc + kAccCols;
+    const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;
     const uint32_t mbar = smem_u32(&S.mbar[g]);
     uint32_t phase = 0;
 
     const uint32_t idesc_h = instr_desc(kTile, kHid);
     const uint32_t idesc_o = instr_desc(kTile, kOutPad);
-    const uint32_t a_base = smem_u32(S.a[g]), ones_base = smem_u32(S.ones);
-    const uint32_t w1_base = smem_u32(S.w1), w5_base = smem_u32(S.w5), bw5_base = smem_u32(S.bw5);
+    const uint64_t ones_d = smem_desc(smem_u32(S.ones), kTile * 16, 128);
+    const uint32_t w5_base = smem_u32(S.w5);
     const int ntiles = (args.n + kTile - 1) / kTile;
-    uint4* ar = reinterpret_cast<uint4*>(S.a[g]);
 
     for (int tile = blockIdx.x + g * gridDim.x; tile < ntiles; tile += kGroups * gridDim.x) {
         const int cell = tile * kTile + row;
         const bool valid = cell < args.n;
-        // ---- input features -> input tile (bf16; k = 8 carries 1 for the bias, 9..15 zero)
+        // ---- input features -> standardised, as BF16 pairs: hi at K < 8, lo at K >= 8
         float f[kIn];
         bool outside = false;
         if (MODE == kModeRaw) {
@@ -258,67 +325,61 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
             }
         }
         {
-            uint32_t packed[kIn / 2];
+            uint32_t w8[8];
 #pragma unroll
             for (int k = 0; k < kIn; k += 2) {
-                const float f0 = valid ? (f[k] - S.fmean[k]) * S.fistd[k] : 0.0f;
-                const float f1 = valid ? (f[k + 1] - S.fmean[k + 1]) * S.fistd[k + 1] : 0.0f;
-                __nv_bfloat162 v = __floats2bfloat162_rn(f0, f1);
-                packed[k / 2] = *reinterpret_cast<uint32_t*>(&v);
+                const float x0 = valid ? (f[k] - S.fmean[k]) * S.fistd[k] : 0.0f;
+                const float x1 = valid ? (f[k + 1] - S.fmean[k + 1]) * S.fistd[k + 1] : 0.0f;
+                split_pair(x0, x1, w8[k / 2], w8[kIn / 2 + k / 2]);
             }
-            ar[canon_index(row, 0, kTile) / 8] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-            ar[canon_index(row, 8, kTile) / 8] = make_uint4(0x3F80u, 0u, 0u, 0u);
+            tmem_st8(act + lane, w8);
+            tmem_wait_st();
         }
-        fence_async_smem();
         fence_before();
         group_sync(g);
         fence_after();
         if (S.abort[g]) break;
-        // ---- layer 1: H = X' (128x16) . W1'^T  (bias through the 1 at k = 8)
+        // ---- layer 1: H = [X_hi X_lo] (128x16) . W1'^T + 1 . B1'^T
         if (leader) {
-            mma_bf16(tmem, smem_desc(a_base, kTile * 16, 128), smem_desc(w1_base, kHid * 16, 128), idesc_h, 0);
+            mma_bf16_ts(acc, act, smem_desc(smem_u32(S.w1), kHid * 16, 128), idesc_h, 0);
+            mma_bf16(acc, ones_d, smem_desc(smem_u32(S.bw[0]), kHid * 16, 128), idesc_h, 1);
             commit(mbar);
         }
         for (int layer = 0; layer < 4; ++layer) {
             if (!mbar_sleep_wait(mbar, phase)) S.abort[g] = 1;
             phase ^= 1;
             fence_after();
-            // h -> SiLU -> next activations (this thread's row)
+            // h -> SiLU -> next layer's A operand (this thread's lane)
 #pragma unroll
             for (int c0 = 0; c0 < kHid; c0 += 32) {
                 float v[32];
-                tmem_ld32(tmem_row + c0, v);
+                tmem_ld32(acc + lane + c0, v);
                 tmem_wait_ld();
+                uint32_t hi[16], lo[16];
 #pragma unroll
-                for (int j = 0; j < 32; j += 8) {
-                    uint32_t q[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) q[e] = silu_pair(v[j + 2 * e], v[j + 2 * e + 1]);
-                    ar[canon_index(row, c0 + j, kTile) / 8] = make_uint4(q[0], q[1], q[2], q[3]);
-                }
+                for (int j = 0; j < 16; ++j) silu_pair(v[2 * j], v[2 * j + 1], hi[j], lo[j]);
+                tmem_st16(act + lane + c0 / 2, hi);
+                tmem_st16(act + lane + kActLoCols + c0 / 2, lo);
             }
-            fence_async_smem();
+            tmem_wait_st();
             fence_before();
             group_sync(g);
             fence_after();
             if (S.abort[g]) break;
             if (leader) {
-                if (layer < 3) {
-                    const uint32_t wb = smem_u32(S.w[layer]);
+                // K = 256: the hi halves, then the lo halves, against the same weight block
+                const bool hidden = layer < 3;
+                const uint32_t wb = hidden ? smem_u32(S.w[layer]) : w5_base;
+                const uint32_t R = hidden ? kHid : kOutPad;
+                const uint32_t idesc = hidden ? idesc_h : idesc_o;
+#pragma unroll
+                for (int half = 0; half < 2; ++half)
 #pragma unroll
                     for (int s = 0; s < kHid / 16; ++s)
-                        mma_bf16(tmem, smem_desc(a_base + s * 2 * kTile * 16, kTile * 16, 128),
-                                 smem_desc(wb + s * 2 * kHid * 16, kHid * 16, 128), idesc_h, s > 0);
-                    mma_bf16(tmem, smem_desc(ones_base, kTile * 16, 128),
-                             smem_desc(smem_u32(S.bw[layer]), kHid * 16, 128), idesc_h, 1);
-                } else {
-#pragma unroll
-                    for (int s = 0; s < kHid / 16; ++s)
-                        mma_bf16(tmem, smem_desc(a_base + s * 2 * kTile * 16, kTile * 16, 128),
-                                 smem_desc(w5_base + s * 2 * kOutPad * 16, kOutPad * 16, 128), idesc_o, s > 0);
-                    mma_bf16(tmem, smem_desc(ones_base, kTile * 16, 128), smem_desc(bw5_base, kOutPad * 16, 128),
-                             idesc_o, 1);
-                }
+                        mma_bf16_ts(acc, act + half * kActLoCols + s * 8,
+                                    smem_desc(wb + s * 2 * R * 16, R * 16, 128), idesc, (half | s) != 0);
+                const uint32_t bb = hidden ? smem_u32(S.bw[layer + 1]) : smem_u32(S.bw5);
+                mma_bf16(acc, ones_d, smem_desc(bb, R * 16, 128), idesc, 1);
                 commit(mbar);
             }
         }
@@ -328,7 +389,7 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
         phase ^= 1;
         fence_after();
         float y[16];
-        tmem_ld16(tmem_row, y);
+        tmem_ld16(acc + lane, y);
         tmem_wait_ld();
         if (valid) {
             if (MODE == kModeRaw) {

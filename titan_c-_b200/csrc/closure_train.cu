@@ -275,19 +275,19 @@ __global__ void pack_kernel(const float* P, __nv_bfloat16* out) {
         region = 1 + j / sW, R = kHid, j %= sW;
     } else if ((j -= 3 * sW) < sW5) {
         region = 4, R = kOutPad;
-    } else if ((j -= sW5) < 3 * sB) {
+    } else if ((j -= sW5) < 4 * sB) {
         region = 5 + j / sB, R = kHid, j %= sB;
     } else {
-        j -= 3 * sB;
-        region = 8, R = kOutPad;
+        j -= 4 * sB;
+        region = 9, R = kOutPad;
     }
     const int core = j / 64, within = j % 64;
     const int rgroups = R / 8;
     const int n = (core % rgroups) * 8 + within / 8, k = (core / rgroups) * 8 + within % 8;
     float v = 0.0f;
     switch (region) {
-        case 0:  // W1' (K = 16): 0.5 W1 for k < 8, 0.5 b1 at k = 8
-            v = k < kIn ? 0.5f * P[oW1 + k * kHid + n] : (k == kIn ? 0.5f * P[ob1 + n] : 0.0f);
+        case 0:  // W1' (K = 16): 0.5 W1 for the features' high parts (k < 8) and low parts (k >= 8)
+            v = 0.5f * P[oW1 + (k % kIn) * kHid + n];
             break;
         case 1:
         case 2:
@@ -301,8 +301,9 @@ __global__ void pack_kernel(const float* P, __nv_bfloat16* out) {
             break;
         case 5:
         case 6:
-        case 7: {  // B2'..B4'
-            const int ob = region == 5 ? ob2 : (region == 6 ? ob3 : ob4);
+        case 7:
+        case 8: {  // B1'..B4'
+            const int ob = region == 5 ? ob1 : (region == 6 ? ob2 : (region == 7 ? ob3 : ob4));
             v = k == 0 ? 0.5f * P[ob + n] : 0.0f;
             break;
         }

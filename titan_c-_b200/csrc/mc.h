@@ -21,6 +21,7 @@ struct McArgs {
     int max_cells;
     double* tally;            // [5][ncell]: sum mu*t, sum mu*dv (3), sum mu*d(v^2)/2
     unsigned long long* lost;
+    double* trace;            // null, or [nparticles][8]: each neutral's end (titan_mc_params.trace_out)
 };
 
 // One cell's tracing record, built once per Monte-Carlo pass: the six face

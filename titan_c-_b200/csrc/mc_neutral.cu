@@ -293,7 +293,8 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
     double ksi = -log(1.0 - rng.uniform());
     double I = 0.0;
     double* T = a.tally;
-    for (int visit = 0; visit < a.max_cells; ++visit) {
+    int nex = 0, visit = 0, kind = 1;  // end kind: 0 left, 1 lost, 2 no outgoing face
+    for (; visit < a.max_cells; ++visit) {
         // the cell's record: its face planes, neighbours and proton fluid; the
         // ray leaves through the face it reaches first
         const McCell* R = cells + cell;
@@ -312,7 +313,10 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
                 next = __ldg(R->nbr + sl);
             }
         }
-        if (next == -2) break;  // no outgoing face (degenerate): give up on this particle
+        if (next == -2) {  // no outgoing face (degenerate): give up on this particle
+            kind = 2;
+            break;
+        }
         const double rho_th = __ldg(&R->rho_th), cp = __ldg(&R->cp);
         const double Vp[3] = {__ldg(R->V), __ldg(R->V + 1), __ldg(R->V + 2)};
         const double du0 = v[0] - Vp[0], du1 = v[1] - Vp[1], du2 = v[2] - Vp[2];
@@ -324,7 +328,10 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
             atomicAdd(&T[cell], a.mu * t_exit);
             I += dI;
             for (int k = 0; k < 3; ++k) x[k] += t_exit * v[k];
-            if (next < 0) return;  // left through the boundary
+            if (next < 0) {  // left through the boundary
+                kind = 0;
+                break;
+            }
             cell = next;
             continue;
         }
@@ -347,8 +354,20 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
         v[2] = w2;
         I = 0.0;
         ksi = -log(1.0 - rng.uniform());
+        ++nex;
     }
-    atomicAdd(a.lost, 1ull);
+    if (kind != 0) atomicAdd(a.lost, 1ull);
+    if (a.trace) {
+        double* r = a.trace + 8 * pid;
+        r[0] = x[0];
+        r[1] = x[1];
+        r[2] = x[2];
+        r[3] = v[0];
+        r[4] = v[1];
+        r[5] = v[2];
+        r[6] = (double)nex;
+        r[7] = 4.0 * (double)(visit + (kind == 0 ? 1 : 0)) + (double)kind;
+    }
 }
 
 // Divides the tallies by the cell volumes: n_H and the source densities.

@@ -1312,6 +1312,19 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, tit
     a.max_cells = mp->max_cells > 0 ? mp->max_cells : 1000000;
     a.tally = ctx->d_mc_tally;
     a.lost = ctx->d_mc_lost;
+    // per-neutral end records (tests and diagnostics): a buffer for this pass only
+    struct TraceBuf {
+        double* p = nullptr;
+        ~TraceBuf() {
+            if (p) cudaFree(p);
+        }
+    } trace;
+    if (mp->trace_out) {
+        int64_t tmp = 0;
+        cudaError_t e = dalloc(&trace.p, (size_t)8 * (size_t)mp->n_particles, &tmp);
+        if (e) return fail(TITAN_ENOMEM, std::string("mc trace buffer: ") + cudaGetErrorString(e));
+        a.trace = trace.p;
+    }
     // inflow CDF on the device; its total sets the particle weight
     double total = 0.0;
     CK(cudaEventRecord(ctx->ev[0], s));
@@ -1331,6 +1344,9 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, tit
     unsigned long long lost = 0;
     if (out) CK(cudaMemcpyAsync(out, ctx->d_stage, sizeof(double) * 5 * nc, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&lost, ctx->d_mc_lost, sizeof(lost), cudaMemcpyDeviceToHost, s));
+    if (mp->trace_out)
+        CK(cudaMemcpyAsync(mp->trace_out, trace.p, sizeof(double) * 8 * (size_t)mp->n_particles,
+                           cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));

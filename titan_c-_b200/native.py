@@ -74,7 +74,7 @@ class TitanSurfaceParams(ctypes.Structure):
 class TitanMcParams(ctypes.Structure):
     _fields_ = [("n_H", ctypes.c_double), ("u_H", ctypes.c_double * 3), ("cp_H", ctypes.c_double),
                 ("n_particles", ctypes.c_int64), ("seed", ctypes.c_uint64), ("max_cells", ctypes.c_int32),
-                ("face_types", ctypes.c_int32)]
+                ("face_types", ctypes.c_int32), ("trace_out", ctypes.c_void_p)]
 
 
 class TitanMcInfo(ctypes.Structure):

@@ -230,10 +230,17 @@ class PlasmaStep:
         return mp
 
     def mc_sources(self, n_H: float, u_H, cp_H: float, n_particles: int, seed: int = 1,
-                   face_types: int = (1 << 2) | (1 << 3), max_cells: int = 0, out: np.ndarray | None = None):
+                   face_types: int = (1 << 2) | (1 << 3), max_cells: int = 0, out: np.ndarray | None = None,
+                   trace: np.ndarray | None = None):
         """Monte-Carlo neutrals through the current state: ([5, ncell] = n_H, S_m (3), S_E; info).
-        `out`, a C-contiguous float64 [5, ncell] array, is filled in place when given."""
+        `out`, a C-contiguous float64 [5, ncell] array, is filled in place when given;
+        `trace`, a C-contiguous float64 [n_particles, 8] array, receives each neutral's end
+        record (titan_mc_params.trace_out)."""
         mp = self._mc_params(n_H, u_H, cp_H, n_particles, seed, face_types, max_cells)
+        if trace is not None:
+            if trace.shape != (n_particles, 8) or trace.dtype != np.float64 or not trace.flags.c_contiguous:
+                raise ValueError("trace must be a C-contiguous float64 array of shape (n_particles, 8)")
+            mp.trace_out = trace.ctypes.data
         if out is None:
             out = np.empty((5, self.ncell))
         elif out.shape != (5, self.ncell) or out.dtype != np.float64 or not out.flags.c_contiguous:

@@ -404,10 +404,11 @@ def step_roofline(m, move, closure, ms_per_step, kernels):
     ach = total / (ms_per_step / 1e3) / 1e9
     C = m["cell_nodes"].shape[0]
     tr = [traffic(k, C, closure) for k in kernels]
-    traffic = sum(tr) if tr and all(t is not None for t in tr) else None
+    step_traffic = sum(tr) if tr and all(t is not None for t in tr) else None
     return {"bound": "hbm", "bytes_per_cell_update": per_cell, "algorithmic_bytes_per_step": total,
             "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "peak_source": src,
-            "traffic_per_step": traffic, "traffic_over_algorithmic": (traffic / total) if traffic else None}
+            "traffic_per_step": step_traffic,
+            "traffic_over_algorithmic": (step_traffic / total) if step_traffic else None}
 
 
 def run_ours(args, rank, world):

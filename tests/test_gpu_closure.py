@@ -120,13 +120,18 @@ def test_closure_inside_the_step_equals_its_sources(titan):
         assert rel < 2e-2, (k, rel)
 
 
-def test_trained_closure_is_within_monte_carlo_noise(titan):
+def test_trained_closure_beats_fixed_sources_against_a_denoised_target(titan):
     """Train on Monte-Carlo sources of three plasma snapshots, judge on a
-    fourth. Errors are volume-weighted L1 over cells (the sources enter the
-    conserved variables as S V): the closure's error against the mean of 4
-    Monte-Carlo seeds is below one seed's statistical scatter about that mean.
-    Rows are weighted by cell volume in training too, since the Monte-Carlo
-    samples a cell in proportion to the neutral path length inside it."""
+    fourth against a denoised target: the mean of 32 Monte-Carlo seeds of
+    that snapshot. Errors are volume-weighted L1 over cells (the sources enter
+    the conserved variables as S V); rows are weighted by cell volume in
+    training too, since the Monte-Carlo samples a cell in proportion to the
+    neutral path length inside it. Asserted:
+    * the closure beats the method without it — the previous snapshot's
+      Monte-Carlo sources held fixed, which is what the plasma loop uses
+      between Monte-Carlo passes;
+    * the closure is closer to the denoised target than one fresh
+      Monte-Carlo pass (a single seed at the training particle count)."""
     m, p, g = _shell_run(titan, 0, nq=10, nlayer=14)
     kw = dict(n_H=0.18, u_H=(-2.6, 0.0, 0.0), cp_H=1.424, n_particles=1_000_000)
     geo = g.geometry()
@@ -135,7 +140,8 @@ def test_trained_closure_is_within_monte_carlo_noise(titan):
     for s in range(4):
         g.go(60)
         st = g.download_state()
-        seeds = [g.mc_sources(seed=100 * s + k, **kw)[0] for k in range(4)]
+        nseed = 32 if s == 3 else 2
+        seeds = [g.mc_sources(seed=100 * s + k, **kw)[0] for k in range(nseed)]
         snaps.append((st, np.mean(seeds, axis=0), seeds))
     g.close()
     # the generator has charge exchange only, which conserves the neutrals:
@@ -147,17 +153,20 @@ def test_trained_closure_is_within_monte_carlo_noise(titan):
     c = titan.closure.Closure(n_inf, lam, seed=0)
     losses = c.fit(X, T, epochs=60, batch=2048, lr=2e-3, lr_decay=0.95, row_weights=np.tile(vol, 3))
     assert losses[-1] < losses[0]
-    st, mean, seeds = snaps[3]
+    st, target, seeds = snaps[3]
     pred = c.predict(st, cc)
 
     def l1(a, b):
         return float((np.abs(a[1:5] - b[1:5]) * vol).sum() / (np.abs(b[1:5]) * vol).sum())
 
-    err = l1(pred, mean)
-    noise = np.mean([l1(sd, mean) for sd in seeds]) * np.sqrt(4.0 / 3.0)
-    stale = l1(snaps[2][1], mean)
-    print(f"closure {err:.3e}  one-seed noise {noise:.3e}  previous snapshot's sources {stale:.3e}")
-    assert err < noise
+    err = l1(pred, target)
+    # one seed's distance to the 32-seed mean, corrected to its distance to the truth
+    one_pass = np.mean([l1(sd, target) for sd in seeds[:8]]) * np.sqrt(32.0 / 31.0)
+    stale = l1(snaps[2][2][0], target)
+    print(f"closure {err:.3e}  one fresh Monte-Carlo pass {one_pass:.3e}  "
+          f"previous snapshot's sources held fixed {stale:.3e}")
+    assert err < stale
+    assert err < one_pass
 
 
 def test_cells_outside_the_training_envelope_take_the_fallback_sources(titan):

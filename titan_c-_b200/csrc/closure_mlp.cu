@@ -108,6 +108,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 64 consecutive 32-bit columns of this thread's TMEM lane (one instruction, one wait)
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
+    uint32_t r[64];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* r) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+                 : "memory");
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
@@ -166,14 +180,21 @@ __device__ __forceinline__ void silu_pair(float h0, float h1, uint32_t& hi, uint
     split_pair(a0, a1, hi, lo);
 }
 
-constexpr int kGroups = 2;  // warpgroups per CTA, one tile in flight each
-// TMEM columns of one warpgroup: its FP32 accumulator (128 columns), then its
+// Two tiles of 128 cells in flight per CTA, each worked by a pair of
+// warpgroups: both share the tile's rows (a warp reaches only its lane
+// quarter of TMEM, so the two warpgroups take the same 128 lanes) and split
+// its 128 accumulator columns, 64 each. One warpgroup of the pair also forms
+// the next tile's features while the current tile's last layer runs on the
+// tensor core; the other turns the outputs into sources.
+constexpr int kPairs = 2;
+constexpr int kThreads = 256 * kPairs;
+// TMEM columns of one pair: its FP32 accumulator (128 columns), then its
 // activations as the next layer's A operand (128 rows in the lanes, two bf16
 // per column along K: columns 0..63 the hi halves of K = 0..127, columns
 // 64..127 the lo halves; the input tile uses columns 0..7: hi at K < 8, lo at
 // K >= 8).
-constexpr uint32_t kColsPerGroup = 256, kAccCols = 128, kActLoCols = 64;
-constexpr uint32_t kCols = kGroups * kColsPerGroup;  // 512: the whole TMEM of the SM
+constexpr uint32_t kColsPerPair = 256, kAccCols = 128, kActLoCols = 64;
+constexpr uint32_t kCols = kPairs * kColsPerPair;  // 512: the whole TMEM of the SM
 static_assert(kCols <= 512, "tensor memory holds 512 columns");
 
 // Shared memory of one CTA. The operand blocks (w1 .. bw5) are contiguous in
@@ -187,9 +208,10 @@ struct alignas(128) Smem {
     __nv_bfloat16 ones[kTile * kInPad];        // M=128 x K=16, 1 at k = 0
     float fmean[kIn], fistd[kIn];
     float env_lo[kIn], env_hi[kIn];
-    uint64_t mbar[kGroups];
+    uint64_t mbar[kPairs];
     uint32_t tmem;
-    int abort[kGroups];  // written by the group's own threads before its barrier, read after it
+    int abort[kPairs];                  // written by the pair's threads before its barrier, read after it
+    unsigned char outside[kPairs][2][kTile];  // per tile parity: the row left the training envelope
 };
 
 // Input features of one cell from its state and centre (closure.h). The
@@ -221,9 +243,9 @@ __device__ __forceinline__ void cell_features(const MlpArgs& a, int c, float* f)
     f[7] = log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, (float)x, (float)r);
 }
 
-// Named barrier of one warpgroup (ids 1..kGroups; 0 is __syncthreads).
-__device__ __forceinline__ void group_sync(int g) {
-    asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory");
+// Named barrier of one pair of warpgroups (ids 1..kPairs; 0 is __syncthreads).
+__device__ __forceinline__ void pair_sync(int p) {
+    asm volatile("bar.sync %0, 256;" ::"r"(p + 1) : "memory");
 }
 
 // Sleeping wait on an mbarrier phase: try_wait with a suspend-time hint of
@@ -248,14 +270,40 @@ __device__ __forceinline__ bool mbar_sleep_wait(uint32_t mbar, uint32_t phase) {
     return false;
 }
 
+// The standardised inputs of one row as BF16 pairs (hi at K < 8 in words
+// 0..3, lo at K >= 8 in words 4..7) and whether the row left the envelope.
 template <int MODE>
-__global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args) {
+__device__ __forceinline__ void input_words(const MlpArgs& args, const Smem& S, int cell, uint32_t* w8,
+                                            bool& outside) {
+    const bool valid = cell < args.n;
+    float f[kIn];
+    outside = false;
+    if (MODE == kModeRaw) {
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) f[k] = valid ? args.x[(size_t)cell * kIn + k] : 0.0f;
+    } else if (valid) {
+        cell_features(args, cell, f);
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) outside |= !(f[k] >= S.env_lo[k] && f[k] <= S.env_hi[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < kIn; k += 2) {
+        const float x0 = valid ? (f[k] - S.fmean[k]) * S.fistd[k] : 0.0f;
+        const float x1 = valid ? (f[k + 1] - S.fmean[k + 1]) * S.fistd[k + 1] : 0.0f;
+        split_pair(x0, x1, w8[k / 2], w8[kIn / 2 + k / 2]);
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1) mlp_forward_tc(MlpArgs args) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int g = tid >> 7;          // warpgroup
-    const int row = tid & 127;       // this thread's row of the group's tile (its TMEM lane)
-    const bool leader = row == 0;    // issues the group's MMAs
+    const int wg = tid >> 7;             // warpgroup
+    const int p = wg >> 1;               // pair: one tile in flight
+    const int h = wg & 1;                // accumulator columns 64 h .. 64 h + 63
+    const int row = tid & 127;           // this thread's row of the tile (its TMEM lane)
+    const bool leader = h == 0 && row == 0;  // issues the pair's MMAs
 
     // weights (pre-packed in the canonical layout), the constant tile, normalisation
     {
@@ -277,8 +325,8 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
         }
     }
     if (tid == 0) {
-        for (int i = 0; i < kGroups; ++i) S.abort[i] = 0;
-        for (int i = 0; i < kGroups; ++i)
+        for (int i = 0; i < kPairs; ++i) S.abort[i] = 0;
+        for (int i = 0; i < kPairs; ++i)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.mbar[i])), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -291,12 +339,12 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
     fence_before();
     __syncthreads();
     fence_after();
-    // this group's accumulator and activation columns (lane 0), and this
+    // this pair's accumulator and activation columns (lane 0), and this
     // warp's lane quarter (a warp reaches lanes 32 (warp % 4) .. + 31)
-    const uint32_t acc = S.tmem + (uint32_t)g * kColsPerGroup;
+    const uint32_t acc = S.tmem + (uint32_t)p * kColsPerPair;
     const uint32_t act = acc + kAccCols;
     const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;
-    const uint32_t mbar = smem_u32(&S.mbar[g]);
+    const uint32_t mbar = smem_u32(&S.mbar[p]);
     uint32_t phase = 0;
 
     const uint32_t idesc_h = instr_desc(kTile, kHid);
@@ -304,41 +352,25 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
     const uint64_t ones_d = smem_desc(smem_u32(S.ones), kTile * 16, 128);
     const uint32_t w5_base = smem_u32(S.w5);
     const int ntiles = (args.n + kTile - 1) / kTile;
+    const int stride = kPairs * gridDim.x;
 
-    for (int tile = blockIdx.x + g * gridDim.x; tile < ntiles; tile += kGroups * gridDim.x) {
+    uint32_t w8[8];
+    bool outside = false;
+    int tile = blockIdx.x + p * gridDim.x;
+    if (h == 1 && tile < ntiles) input_words<MODE>(args, S, tile * kTile + row, w8, outside);
+    for (int par = 0; tile < ntiles; tile += stride, par ^= 1) {
         const int cell = tile * kTile + row;
         const bool valid = cell < args.n;
-        // ---- input features -> standardised, as BF16 pairs: hi at K < 8, lo at K >= 8
-        float f[kIn];
-        bool outside = false;
-        if (MODE == kModeRaw) {
-#pragma unroll
-            for (int k = 0; k < kIn; ++k) f[k] = valid ? args.x[(size_t)cell * kIn + k] : 0.0f;
-        } else {
-            if (valid) {
-                cell_features(args, cell, f);
-#pragma unroll
-                for (int k = 0; k < kIn; ++k) outside |= !(f[k] >= S.env_lo[k] && f[k] <= S.env_hi[k]);
-            } else {
-#pragma unroll
-                for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
-            }
-        }
-        {
-            uint32_t w8[8];
-#pragma unroll
-            for (int k = 0; k < kIn; k += 2) {
-                const float x0 = valid ? (f[k] - S.fmean[k]) * S.fistd[k] : 0.0f;
-                const float x1 = valid ? (f[k + 1] - S.fmean[k + 1]) * S.fistd[k + 1] : 0.0f;
-                split_pair(x0, x1, w8[k / 2], w8[kIn / 2 + k / 2]);
-            }
+        // ---- the tile's inputs (formed by h = 1 during the previous tile's last layer)
+        if (h == 1) {
+            S.outside[p][par][row] = outside;
             tmem_st8(act + lane, w8);
             tmem_wait_st();
         }
         fence_before();
-        group_sync(g);
+        pair_sync(p);
         fence_after();
-        if (S.abort[g]) break;
+        if (S.abort[p]) break;
         // ---- layer 1: H = [X_hi X_lo] (128x16) . W1'^T + 1 . B1'^T
         if (leader) {
             mma_bf16_ts(acc, act, smem_desc(smem_u32(S.w1), kHid * 16, 128), idesc_h, 0);
@@ -346,26 +378,28 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
             commit(mbar);
         }
         for (int layer = 0; layer < 4; ++layer) {
-            if (!mbar_sleep_wait(mbar, phase)) S.abort[g] = 1;
+            if (!mbar_sleep_wait(mbar, phase)) S.abort[p] = 1;
             phase ^= 1;
             fence_after();
-            // h -> SiLU -> next layer's A operand (this thread's lane)
-#pragma unroll
-            for (int c0 = 0; c0 < kHid; c0 += 32) {
-                float v[32];
-                tmem_ld32(acc + lane + c0, v);
+            // h -> SiLU -> this half's columns of the next layer's A operand
+            {
+                float v[64];
+                tmem_ld64(acc + lane + 64 * h, v);
                 tmem_wait_ld();
-                uint32_t hi[16], lo[16];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) silu_pair(v[2 * j], v[2 * j + 1], hi[j], lo[j]);
-                tmem_st16(act + lane + c0 / 2, hi);
-                tmem_st16(act + lane + kActLoCols + c0 / 2, lo);
+                for (int q = 0; q < 2; ++q) {  // stored in two halves to keep fewer words live
+                    uint32_t hi[16], lo[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) silu_pair(v[32 * q + 2 * j], v[32 * q + 2 * j + 1], hi[j], lo[j]);
+                    tmem_st16(act + lane + 32 * h + 16 * q, hi);
+                    tmem_st16(act + lane + kActLoCols + 32 * h + 16 * q, lo);
+                }
+                tmem_wait_st();
             }
-            tmem_wait_st();
             fence_before();
-            group_sync(g);
+            pair_sync(p);
             fence_after();
-            if (S.abort[g]) break;
+            if (S.abort[p]) break;
             if (leader) {
                 // K = 256: the hi halves, then the lo halves, against the same weight block
                 const bool hidden = layer < 3;
@@ -383,35 +417,42 @@ __global__ void __launch_bounds__(128 * kGroups, 1) mlp_forward_tc(MlpArgs args)
                 commit(mbar);
             }
         }
-        if (S.abort[g]) break;
-        // ---- output layer (bias included)
-        if (!mbar_sleep_wait(mbar, phase)) S.abort[g] = 1;
+        if (S.abort[p]) break;
+        // ---- the output layer runs; h = 1 forms the next tile's inputs meanwhile
+        if (h == 1 && tile + stride < ntiles) input_words<MODE>(args, S, (tile + stride) * kTile + row, w8, outside);
+        if (!mbar_sleep_wait(mbar, phase)) S.abort[p] = 1;
         phase ^= 1;
         fence_after();
         float y[16];
-        tmem_ld16(acc + lane, y);
-        tmem_wait_ld();
-        if (valid) {
-            if (MODE == kModeRaw) {
-#pragma unroll
-                for (int k = 0; k < kOut; ++k) args.y[(size_t)cell * kOut + k] = y[k];
-            } else if (outside && args.fallback) {
-                // outside the training envelope: the last Monte-Carlo sources
-#pragma unroll
-                for (int k = 0; k < 4; ++k) args.src[k * args.ncell + cell] = args.fallback[k * args.ncell + cell];
-            } else {
-                write_sources(args, cell, y);
-            }
-        }
-        if (MODE == kModeSources && args.n_outside) {
-            const unsigned int bal = __ballot_sync(0xffffffffu, valid && outside);
-            if ((threadIdx.x & 31) == 0 && bal) atomicAdd(args.n_outside, (unsigned long long)__popc(bal));
+        if (h == 0) {
+            tmem_ld16(acc + lane, y);
+            tmem_wait_ld();
         }
         fence_before();
-        group_sync(g);
+        pair_sync(p);  // the accumulator is free for the next tile
         fence_after();
+        if (h == 0) {
+            const bool out_env = S.outside[p][par][row] != 0;
+            if (valid) {
+                if (MODE == kModeRaw) {
+#pragma unroll
+                    for (int k = 0; k < kOut; ++k) args.y[(size_t)cell * kOut + k] = y[k];
+                } else if (out_env && args.fallback) {
+                    // outside the training envelope: the last Monte-Carlo sources
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        args.src[k * args.ncell + cell] = args.fallback[k * args.ncell + cell];
+                } else {
+                    write_sources(args, cell, y);
+                }
+            }
+            if (MODE == kModeSources && args.n_outside) {
+                const unsigned int bal = __ballot_sync(0xffffffffu, valid && out_env);
+                if ((threadIdx.x & 31) == 0 && bal) atomicAdd(args.n_outside, (unsigned long long)__popc(bal));
+            }
+        }
     }
-    if (S.abort[g] && row == 0) atomicExch(args.error, 1);
+    if (S.abort[p] && tid == 256 * p) atomicExch(args.error, 1);
     fence_before();
     __syncthreads();
     fence_after();
@@ -432,13 +473,13 @@ cudaError_t mlp_prepare() {
 cudaError_t launch_mlp_forward(const MlpArgs& a, int mode, int sm_count, cudaStream_t s) {
     const size_t smem = sizeof(mlp::Smem) + 1024;
     const int ntiles = (a.n + kTile - 1) / kTile;
-    const int want = (ntiles + mlp::kGroups - 1) / mlp::kGroups;
+    const int want = (ntiles + mlp::kPairs - 1) / mlp::kPairs;
     const int grid = want < sm_count ? want : sm_count;
     if (grid <= 0) return cudaSuccess;
     if (mode == kModeRaw)
-        mlp::mlp_forward_tc<kModeRaw><<<grid, 128 * mlp::kGroups, smem, s>>>(a);
+        mlp::mlp_forward_tc<kModeRaw><<<grid, mlp::kThreads, smem, s>>>(a);
     else
-        mlp::mlp_forward_tc<kModeSources><<<grid, 128 * mlp::kGroups, smem, s>>>(a);
+        mlp::mlp_forward_tc<kModeSources><<<grid, mlp::kThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 

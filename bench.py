@@ -125,10 +125,14 @@ def kernel_work(name: str, m, move: bool, sources: bool):
             return "hbm", float(F * (16 + 8 + 3) + C * (64 + 24) + N * 48)
         return "hbm", float(F * (8 + 3 + 24 + 8 + 8) + C * 64)
     if name == "cell_update":
-        b = C * (24 + 64 + 64 + 8 + 2) + (32 if sources else 0) * C
+        b = C * (24 + 64 + 64 + 8 + 2)
+        if sources:  # the closure: its 5 FP32 outputs and the centres in, the next step's 8 input words and flag out
+            b += C * (20 + 24 + 1 + 32 + 1)
         if move:   # next layer: cell nodes, face->node map, new coordinates; centres and volumes out
             b += C * (32 + 12 + 8 + 24) + N * 24
         return "hbm", float(b)
+    if name == "closure_inputs":
+        return "hbm", float(C * (40 + 24 + 32 + 1))
     if name == "move_nodes":
         return "hbm", float(N * (24 + 24 + 16))
     if name == "closure_mlp":

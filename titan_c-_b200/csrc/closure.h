@@ -17,6 +17,8 @@
 
 #include <cstdint>
 
+#include "step_types.h"
+
 namespace titan {
 
 constexpr int kIn = 8, kInPad = 16, kHid = 128, kOut = 5, kOutPad = 16, kTile = 128;
@@ -52,20 +54,12 @@ struct MlpArgs {
     // raw mode
     const float* x;        // [n][kIn] unstandardised features
     float* y;              // [n][kOut]
-    // sources mode
+    // step mode (kModeSources): inputs formed by the previous step's cell
+    // update (or closure_inputs), outputs turned into sources by this step's
     int ncell;
-    const double* state;   // [ns][ncell]
-    const double* cc;      // [3][ncell] cell centres
-    double* src;           // [4][ncell] m_x, m_y, m_z, E
-    double nH_inf, lambda; // cold-model proxy
+    const uint32_t* in_words;  // [8][ncell] standardised inputs as BF16 hi / lo words
+    float* y_out;              // [kOut][ncell] network outputs (scaled units)
     int* error;
-    // training envelope (sources mode; env_lo null: none): a cell whose
-    // features leave [env_lo, env_hi] takes fallback[4][ncell] as its sources
-    // (the last Monte-Carlo pass) and is counted in *n_outside
-    const float* env_lo;
-    const float* env_hi;
-    const double* fallback;
-    unsigned long long* n_outside;
 };
 
 // log of the cold-model neutral density n_inf exp(-lambda theta / (r sin theta)),
@@ -77,20 +71,75 @@ __device__ __forceinline__ float log_nh_proxy_f(float n_inf, float lambda, float
     return __logf(n_inf) + fmaxf(-lambda * th / (r * s), -30.0f);
 }
 
-// Sources from the network outputs of one cell (sources mode), formed in FP64:
-// m_x, m_y, m_z in the frame e1 = V/|V| (radial when V = 0), e2 = the inflow
-// direction -x made orthogonal to e1, e3 = e1 x e2; E. For a flow nearly along
-// x, e2 = -x - (-x . e1) e1 is a cancellation residue of the transverse
-// velocity; in FP32 its direction would be set by rounding noise that the
-// flux arithmetic perturbs every step, so the frame is formed in FP64 with the
-// same degenerate-case threshold as the training side (closure.py frame()).
-__device__ inline void write_sources(const MlpArgs& a, int c, const float* y) {
-    const int nc = a.ncell;
-    const double rho = a.state[c], vx = a.state[nc + c], vy = a.state[2 * nc + c];
-    const double vz = a.state[3 * nc + c];
-    const double x = a.cc[c], yy = a.cc[nc + c], z = a.cc[2 * nc + c];
+// Two FP32 values as BF16 pairs: hi = the nearest BF16 of each (ties away
+// from zero), lo = the BF16 nearest the exact remainder v - hi. Returns the
+// two packed words {hi(v0), hi(v1)} and {lo(v0), lo(v1)}, element 0 in the
+// low half. Integer operations on the bits: adding 2^15 and keeping the top
+// 16 bits rounds to nearest; v - hi is exact in FP32.
+__device__ __forceinline__ void split_pair(float v0, float v1, uint32_t& hi, uint32_t& lo) {
+    const uint32_t r0 = __float_as_uint(v0) + 0x8000u, r1 = __float_as_uint(v1) + 0x8000u;
+    const float l0 = v0 - __uint_as_float(r0 & 0xFFFF0000u);
+    const float l1 = v1 - __uint_as_float(r1 & 0xFFFF0000u);
+    hi = __byte_perm(r0, r1, 0x7632);
+    lo = __byte_perm(__float_as_uint(l0) + 0x8000u, __float_as_uint(l1) + 0x8000u, 0x7632);
+}
+
+// Input features of one cell (the list above) from its primitives and centre.
+// The vector parts are formed in FP64 and rounded once: in FP32 the tangential
+// speed sqrt(v^2 - u_r^2) of a nearly radial flow is the square root of a
+// cancellation residue (~1e-7 |v|^2, so ~3e-4 |v| of noise with an infinite
+// slope), which would make the feature, and the sources, jump with
+// rounding-level state changes. |u_t| = |v x r| / r has no cancellation. The
+// logarithms take FP32 arguments rounded once from FP64 and use the accurate
+// logf, which is continuous at FP32 resolution.
+__device__ __forceinline__ void closure_features(double rho, double vx, double vy, double vz, double p, double x,
+                                                 double y, double z, double nH_inf, double lambda, float* f) {
+    const double r = sqrt(x * x + y * y + z * z);
+    const double ir = 1.0 / r;
+    const double ur = (vx * x + vy * y + vz * z) * ir;
+    const double cx = vy * z - vz * y, cy = vz * x - vx * z, cz = vx * y - vy * x;
+    const double ut = sqrt(cx * cx + cy * cy + cz * cz) * ir;
+    const double vmag = sqrt(vx * vx + vy * vy + vz * vz);
+    f[0] = logf((float)fmax(rho, 1e-30));
+    f[1] = (float)ur;
+    f[2] = (float)ut;
+    f[3] = logf((float)fmax(p / rho, 1e-30));
+    f[4] = logf((float)r);
+    f[5] = acosf((float)fmin(fmax(x * ir, -1.0), 1.0));
+    f[6] = vmag > 0.0 ? (float)(-vx / vmag) : 0.0f;
+    f[7] = log_nh_proxy_f((float)nH_inf, (float)lambda, (float)x, (float)r);
+}
+
+// The standardised features as the network's input words (hi at K < 8 in
+// words 0..3, lo at K >= 8 in words 4..7); whether they leave the envelope.
+__device__ __forceinline__ void closure_words(const float* f, const float* norm, const float* env, uint32_t* w8,
+                                              bool& outside) {
+    outside = false;
+    if (env) {
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) outside |= !(f[k] >= env[k] && f[k] <= env[kIn + k]);
+    }
+#pragma unroll
+    for (int k = 0; k < kIn; k += 2) {
+        const float x0 = (f[k] - norm[k]) * norm[kIn + k];
+        const float x1 = (f[k + 1] - norm[k + 1]) * norm[kIn + k + 1];
+        split_pair(x0, x1, w8[k / 2], w8[kIn / 2 + k / 2]);
+    }
+}
+
+// Sources m_x, m_y, m_z, E of one cell from the network outputs y (scaled
+// units), formed in FP64: momentum in the frame e1 = V/|V| (radial when V = 0),
+// e2 = the inflow direction -x made orthogonal to e1, e3 = e1 x e2. For a flow
+// nearly along x, e2 = -x - (-x . e1) e1 is a cancellation residue of the
+// transverse velocity; in FP32 its direction would be set by rounding noise
+// that the flux arithmetic perturbs every step, so the frame is formed in FP64
+// with the same degenerate-case threshold as the training side (closure.py
+// frame()).
+__device__ __forceinline__ void closure_sources(const float* y, const float* oscale, double rho, double vx, double vy,
+                                                double vz, double x, double yy, double z, double nH_inf, double lambda,
+                                                double* S) {
     const double r = sqrt(x * x + yy * yy + z * z);
-    const double norm = rho * (double)__expf(log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, (float)x, (float)r));
+    const double norm = rho * (double)__expf(log_nh_proxy_f((float)nH_inf, (float)lambda, (float)x, (float)r));
     const double vm = sqrt(vx * vx + vy * vy + vz * vz);
     double e1[3], e2[3], e3[3];
     if (vm > 0.0) {
@@ -119,15 +168,20 @@ __device__ inline void write_sources(const MlpArgs& a, int c, const float* y) {
     e3[0] = e1[1] * e2[2] - e1[2] * e2[1];
     e3[1] = e1[2] * e2[0] - e1[0] * e2[2];
     e3[2] = e1[0] * e2[1] - e1[1] * e2[0];
-    const double s1 = norm * (double)(y[1] * a.net.oscale[1]), s2 = norm * (double)(y[2] * a.net.oscale[2]);
-    const double s3 = norm * (double)(y[3] * a.net.oscale[3]);
-    a.src[c] = s1 * e1[0] + s2 * e2[0] + s3 * e3[0];
-    a.src[nc + c] = s1 * e1[1] + s2 * e2[1] + s3 * e3[1];
-    a.src[2 * nc + c] = s1 * e1[2] + s2 * e2[2] + s3 * e3[2];
-    a.src[3 * nc + c] = norm * (double)(y[4] * a.net.oscale[4]);
+    const double s1 = norm * (double)(y[1] * oscale[1]), s2 = norm * (double)(y[2] * oscale[2]);
+    const double s3 = norm * (double)(y[3] * oscale[3]);
+    S[0] = s1 * e1[0] + s2 * e2[0] + s3 * e3[0];
+    S[1] = s1 * e1[1] + s2 * e2[1] + s3 * e3[1];
+    S[2] = s1 * e1[2] + s2 * e2[2] + s3 * e3[2];
+    S[3] = norm * (double)(y[4] * oscale[4]);
 }
 
 cudaError_t mlp_prepare();  // once per process, before any launch (sets the shared-memory size)
+// The closure's input words and envelope flags of every cell from a state and
+// its centres (the first step after the state changed outside the step loop).
+cudaError_t launch_closure_inputs(const double* state, const double* cc, int ncell, const float* norm,
+                                  const float* env, double nH_inf, double lambda, uint32_t* in, unsigned char* outside,
+                                  cudaStream_t s);
 // grid: one CTA per SM at most (sm_count), two tiles of 128 rows in flight per CTA
 cudaError_t launch_mlp_forward(const MlpArgs& a, int mode, int sm_count, cudaStream_t s);
 size_t mlp_forward_smem_bytes();

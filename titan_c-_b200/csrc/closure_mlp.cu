@@ -159,19 +159,6 @@ __device__ __forceinline__ float tanh_f32(float x) {
     return y;
 }
 
-// Two FP32 values as BF16 pairs: hi = the nearest BF16 of each (ties away
-// from zero), lo = the BF16 nearest the exact remainder v - hi. Returns the
-// two packed words {hi(v0), hi(v1)} and {lo(v0), lo(v1)}, element 0 in the
-// low half. Integer operations on the bits: adding 2^15 and keeping the top
-// 16 bits rounds to nearest; v - hi is exact in FP32.
-__device__ __forceinline__ void split_pair(float v0, float v1, uint32_t& hi, uint32_t& lo) {
-    const uint32_t r0 = __float_as_uint(v0) + 0x8000u, r1 = __float_as_uint(v1) + 0x8000u;
-    const float l0 = v0 - __uint_as_float(r0 & 0xFFFF0000u);
-    const float l1 = v1 - __uint_as_float(r1 & 0xFFFF0000u);
-    hi = __byte_perm(r0, r1, 0x7632);
-    lo = __byte_perm(__float_as_uint(l0) + 0x8000u, __float_as_uint(l1) + 0x8000u, 0x7632);
-}
-
 // SiLU of a pair of columns from the accumulator h = (z + b) / 2 (FP32):
 // h (1 + tanh h), split into BF16 hi / lo words.
 __device__ __forceinline__ void silu_pair(float h0, float h1, uint32_t& hi, uint32_t& lo) {
@@ -207,41 +194,10 @@ struct alignas(128) Smem {
     __nv_bfloat16 bw5[kOutPad * kInPad];       // B5   N=16 x K=16
     __nv_bfloat16 ones[kTile * kInPad];        // M=128 x K=16, 1 at k = 0
     float fmean[kIn], fistd[kIn];
-    float env_lo[kIn], env_hi[kIn];
     uint64_t mbar[kPairs];
     uint32_t tmem;
-    int abort[kPairs];                  // written by the pair's threads before its barrier, read after it
-    unsigned char outside[kPairs][2][kTile];  // per tile parity: the row left the training envelope
+    int abort[kPairs];  // written by the pair's threads before its barrier, read after it
 };
-
-// Input features of one cell from its state and centre (closure.h). The
-// vector parts are formed in FP64 and rounded once: in FP32 the tangential
-// speed sqrt(v^2 - u_r^2) of a nearly radial flow is the square root of a
-// cancellation residue (~1e-7 |v|^2, so ~3e-4 |v| of noise with an infinite
-// slope), which would make the feature, and the sources, jump with
-// rounding-level state changes. |u_t| = |v x r| / r has no cancellation. The
-// logarithms take FP32 arguments rounded once from FP64 and use the accurate
-// logf, which is continuous at FP32 resolution.
-__device__ __forceinline__ void cell_features(const MlpArgs& a, int c, float* f) {
-    const int nc = a.ncell;
-    const double rho = a.state[c], vx = a.state[nc + c], vy = a.state[2 * nc + c];
-    const double vz = a.state[3 * nc + c], p = a.state[4 * nc + c];
-    const double x = a.cc[c], y = a.cc[nc + c], z = a.cc[2 * nc + c];
-    const double r = sqrt(x * x + y * y + z * z);
-    const double ir = 1.0 / r;
-    const double ur = (vx * x + vy * y + vz * z) * ir;
-    const double cx = vy * z - vz * y, cy = vz * x - vx * z, cz = vx * y - vy * x;
-    const double ut = sqrt(cx * cx + cy * cy + cz * cz) * ir;
-    const double vmag = sqrt(vx * vx + vy * vy + vz * vz);
-    f[0] = logf((float)fmax(rho, 1e-30));
-    f[1] = (float)ur;
-    f[2] = (float)ut;
-    f[3] = logf((float)fmax(p / rho, 1e-30));
-    f[4] = logf((float)r);
-    f[5] = acosf((float)fmin(fmax(x * ir, -1.0), 1.0));
-    f[6] = vmag > 0.0 ? (float)(-vx / vmag) : 0.0f;
-    f[7] = log_nh_proxy_f((float)a.nH_inf, (float)a.lambda, (float)x, (float)r);
-}
 
 // Named barrier of one pair of warpgroups (ids 1..kPairs; 0 is __syncthreads).
 __device__ __forceinline__ void pair_sync(int p) {
@@ -270,27 +226,22 @@ __device__ __forceinline__ bool mbar_sleep_wait(uint32_t mbar, uint32_t phase) {
     return false;
 }
 
-// The standardised inputs of one row as BF16 pairs (hi at K < 8 in words
-// 0..3, lo at K >= 8 in words 4..7) and whether the row left the envelope.
+// The input words of one row (hi at K < 8 in words 0..3, lo at K >= 8 in
+// words 4..7): standardised and split from raw features, or, in step mode,
+// as the previous step's cell update (or closure_inputs) formed them.
 template <int MODE>
-__device__ __forceinline__ void input_words(const MlpArgs& args, const Smem& S, int cell, uint32_t* w8,
-                                            bool& outside) {
+__device__ __forceinline__ void input_words(const MlpArgs& args, const Smem& S, int cell, uint32_t* w8) {
     const bool valid = cell < args.n;
-    float f[kIn];
-    outside = false;
     if (MODE == kModeRaw) {
 #pragma unroll
-        for (int k = 0; k < kIn; ++k) f[k] = valid ? args.x[(size_t)cell * kIn + k] : 0.0f;
-    } else if (valid) {
-        cell_features(args, cell, f);
+        for (int k = 0; k < kIn; k += 2) {
+            const float x0 = valid ? (args.x[(size_t)cell * kIn + k] - S.fmean[k]) * S.fistd[k] : 0.0f;
+            const float x1 = valid ? (args.x[(size_t)cell * kIn + k + 1] - S.fmean[k + 1]) * S.fistd[k + 1] : 0.0f;
+            split_pair(x0, x1, w8[k / 2], w8[kIn / 2 + k / 2]);
+        }
+    } else {
 #pragma unroll
-        for (int k = 0; k < kIn; ++k) outside |= !(f[k] >= S.env_lo[k] && f[k] <= S.env_hi[k]);
-    }
-#pragma unroll
-    for (int k = 0; k < kIn; k += 2) {
-        const float x0 = valid ? (f[k] - S.fmean[k]) * S.fistd[k] : 0.0f;
-        const float x1 = valid ? (f[k + 1] - S.fmean[k + 1]) * S.fistd[k + 1] : 0.0f;
-        split_pair(x0, x1, w8[k / 2], w8[kIn / 2 + k / 2]);
+        for (int k = 0; k < 8; ++k) w8[k] = valid ? args.in_words[(size_t)k * args.ncell + cell] : 0u;
     }
 }
 
@@ -320,8 +271,6 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_tc(MlpArgs args) {
         if (tid < kIn) {
             S.fmean[tid] = args.net.fmean[tid];
             S.fistd[tid] = args.net.fistd[tid];
-            S.env_lo[tid] = args.env_lo ? args.env_lo[tid] : -3.0e38f;
-            S.env_hi[tid] = args.env_lo ? args.env_hi[tid] : 3.0e38f;
         }
     }
     if (tid == 0) {
@@ -354,16 +303,14 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_tc(MlpArgs args) {
     const int ntiles = (args.n + kTile - 1) / kTile;
     const int stride = kPairs * gridDim.x;
 
+    // h = 1 loads the next tile's input words during the last hidden layer's
+    // MMA, so their latency is off the pair's critical path.
     uint32_t w8[8];
-    bool outside = false;
     int tile = blockIdx.x + p * gridDim.x;
-    if (h == 1 && tile < ntiles) input_words<MODE>(args, S, tile * kTile + row, w8, outside);
-    for (int par = 0; tile < ntiles; tile += stride, par ^= 1) {
+    if (h == 1 && tile < ntiles) input_words<MODE>(args, S, tile * kTile + row, w8);
+    for (; tile < ntiles; tile += stride) {
         const int cell = tile * kTile + row;
-        const bool valid = cell < args.n;
-        // ---- the tile's inputs (formed by h = 1 during the previous tile's last layer)
         if (h == 1) {
-            S.outside[p][par][row] = outside;
             tmem_st8(act + lane, w8);
             tmem_wait_st();
         }
@@ -416,10 +363,11 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_tc(MlpArgs args) {
                 mma_bf16(acc, ones_d, smem_desc(bb, R * 16, 128), idesc, 1);
                 commit(mbar);
             }
+            if (layer == 2 && h == 1 && tile + stride < ntiles)
+                input_words<MODE>(args, S, (tile + stride) * kTile + row, w8);
         }
         if (S.abort[p]) break;
-        // ---- the output layer runs; h = 1 forms the next tile's inputs meanwhile
-        if (h == 1 && tile + stride < ntiles) input_words<MODE>(args, S, (tile + stride) * kTile + row, w8, outside);
+        // ---- the output layer (N = 16)
         if (!mbar_sleep_wait(mbar, phase)) S.abort[p] = 1;
         phase ^= 1;
         fence_after();
@@ -431,24 +379,13 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_tc(MlpArgs args) {
         fence_before();
         pair_sync(p);  // the accumulator is free for the next tile
         fence_after();
-        if (h == 0) {
-            const bool out_env = S.outside[p][par][row] != 0;
-            if (valid) {
-                if (MODE == kModeRaw) {
+        if (h == 0 && cell < args.n) {
+            if (MODE == kModeRaw) {
 #pragma unroll
-                    for (int k = 0; k < kOut; ++k) args.y[(size_t)cell * kOut + k] = y[k];
-                } else if (out_env && args.fallback) {
-                    // outside the training envelope: the last Monte-Carlo sources
+                for (int k = 0; k < kOut; ++k) args.y[(size_t)cell * kOut + k] = y[k];
+            } else {
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        args.src[k * args.ncell + cell] = args.fallback[k * args.ncell + cell];
-                } else {
-                    write_sources(args, cell, y);
-                }
-            }
-            if (MODE == kModeSources && args.n_outside) {
-                const unsigned int bal = __ballot_sync(0xffffffffu, valid && out_env);
-                if ((threadIdx.x & 31) == 0 && bal) atomicAdd(args.n_outside, (unsigned long long)__popc(bal));
+                for (int k = 0; k < kOut; ++k) args.y_out[(size_t)k * args.ncell + cell] = y[k];
             }
         }
     }
@@ -460,6 +397,33 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_tc(MlpArgs args) {
 }
 
 }  // namespace mlp
+
+namespace mlp {
+// closure_inputs: every cell's input words and envelope flag (closure.h).
+__global__ void closure_inputs_kernel(const double* __restrict__ state, const double* __restrict__ cc, int nc,
+                                      const float* __restrict__ norm, const float* __restrict__ env, double nH_inf,
+                                      double lambda, uint32_t* __restrict__ in, unsigned char* __restrict__ outside) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    float f[kIn];
+    closure_features(state[c], state[nc + c], state[2 * nc + c], state[3 * nc + c], state[4 * nc + c], cc[c],
+                     cc[nc + c], cc[2 * nc + c], nH_inf, lambda, f);
+    uint32_t w8[8];
+    bool out = false;
+    closure_words(f, norm, env, w8, out);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) in[(size_t)k * nc + c] = w8[k];
+    outside[c] = out ? 1 : 0;
+}
+}  // namespace mlp
+
+cudaError_t launch_closure_inputs(const double* state, const double* cc, int ncell, const float* norm,
+                                  const float* env, double nH_inf, double lambda, uint32_t* in, unsigned char* outside,
+                                  cudaStream_t s) {
+    mlp::closure_inputs_kernel<<<(ncell + 255) / 256, 256, 0, s>>>(state, cc, ncell, norm, env, nH_inf, lambda, in,
+                                                                   outside);
+    return cudaGetLastError();
+}
 
 cudaError_t mlp_prepare() {
     const int smem = (int)(sizeof(mlp::Smem) + 1024);

@@ -1,6 +1,7 @@
 // Cell-update translation unit (-fmad=false, like kernels_fp64.cu): the
 // per-cell gather of face fluxes, the conservative update with sources and
 // floors, the next layer's cell geometry, and the CFL rollover.
+#include "closure.h"
 #include "launch.h"
 #include "step_kernels.cuh"
 
@@ -79,6 +80,21 @@ __global__ void __launch_bounds__(BS, MINB) cell_update_kernel(CellArgs a) {
         } else if (SRC == 2) {
 #pragma unroll
             for (int k = 0; k < 4; ++k) S[k] = a.src[k * nc + c];
+        } else if (SRC == 3) {
+            // the closure's sources for this step's state, in its frame at the current centre
+            const ClosureCell& q = a.cl;
+            const bool out_env = q.outside[c] != 0;
+            if (out_env && q.fallback) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) S[k] = q.fallback[k * nc + c];
+            } else {
+                float y[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) y[k] = q.y[k * nc + c];
+                closure_sources(y, q.norm + 16, prim[0], prim[1], prim[2], prim[3], q.cc1[c], q.cc1[nc + c],
+                                q.cc1[2 * nc + c], q.nH_inf, q.lambda, S);
+            }
+            if (out_env && q.n_outside) atomicAdd(q.n_outside, 1ull);
         }
         const double g1 = a.P.gamma - 1.0;
         const double cpi4 = 4.0 * kPi;
@@ -154,6 +170,21 @@ __global__ void __launch_bounds__(BS, MINB) cell_update_kernel(CellArgs a) {
             o[8 * nc + c] = Q3;
             if (NK > 1) o[9 * nc + c] = rho_He3;
         }
+        if (SRC == 3) {
+            // the closure's inputs for the next step, from the state just written
+            const ClosureCell& q = a.cl;
+            float f[8];
+            // the centre the next step's closure sees: the next layer's (moving mesh) or this one
+            const double cx = MOVE ? C2[0] : q.cc1[c], cy = MOVE ? C2[1] : q.cc1[nc + c];
+            const double cz = MOVE ? C2[2] : q.cc1[2 * nc + c];
+            closure_features(rho3, u3, v3, w3, p3, cx, cy, cz, q.nH_inf, q.lambda, f);
+            uint32_t w8[8];
+            bool out = false;
+            closure_words(f, q.norm, q.env, w8, out);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) q.in[(size_t)k * nc + c] = w8[k];
+            q.outside[c] = out ? 1 : 0;
+        }
     }
     // Last block to finish rolls the clock: t += dt, dt = CFL minimum of this
     // step's faces (applied on the next step, Setka_physics.cpp:1606-1607).
@@ -185,7 +216,8 @@ static void cell_update_src(const CellArgs& a, int src, cudaStream_t s) {
     const unsigned int g = blocks_for(a.M.ncell, BS);
     if (src == 0) cell_update_kernel<FT, NK, MOVE, 0, BS, MINB><<<g, BS, 0, s>>>(a);
     else if (src == 1) cell_update_kernel<FT, NK, MOVE, 1, BS, MINB><<<g, BS, 0, s>>>(a);
-    else cell_update_kernel<FT, NK, MOVE, 2, BS, MINB><<<g, BS, 0, s>>>(a);
+    else if (src == 2) cell_update_kernel<FT, NK, MOVE, 2, BS, MINB><<<g, BS, 0, s>>>(a);
+    else cell_update_kernel<FT, NK, MOVE, 3, BS, MINB><<<g, BS, 0, s>>>(a);
 }
 
 template <typename FT, int NK, bool MOVE>

@@ -73,6 +73,22 @@ struct FaceArgs {
     DevStatus* st;
 };
 
+// What the cell update needs from the learned closure (source mode 3): this
+// step's network outputs, turned into sources with the frame of the state
+// they came from, and the next step's network inputs, formed from the state
+// it has just written (closure.h).
+struct ClosureCell {
+    const float* y;              // [5][ncell] this step's network outputs (scaled units)
+    uint32_t* in;                // [8][ncell] next step's input words (written)
+    unsigned char* outside;      // [ncell] outside the training envelope: this step's (read), the next step's (written)
+    const double* fallback;      // [4][ncell] sources of cells outside the envelope (last Monte-Carlo pass), or null
+    unsigned long long* n_outside;  // cells outside the envelope this step, or null
+    const float* norm;           // feature mean[8], 1/std[8], output scale[5]
+    const float* env;            // [2][8] envelope (lo, hi), or null
+    double nH_inf, lambda;       // cold-model proxy
+    const double* cc1;           // [3][ncell] cell centres of the current layer
+};
+
 struct CellArgs {
     MeshView M;
     Params P;
@@ -85,6 +101,7 @@ struct CellArgs {
     const void* flux;
     const double* hfl;     // [5*nh][ncell] frozen neutral fluids (Bera sources)
     const double* src;     // [4][ncell] external sources (m_x, m_y, m_z, E)
+    ClosureCell cl;        // source mode 3: the learned closure
     DevStatus* st;
 };
 

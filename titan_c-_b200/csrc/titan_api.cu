@@ -110,6 +110,10 @@ struct titan_ctx {
 
     ClosureDev closure;        // learned sources (titan_set_closure)
     bool use_closure = false;
+    uint32_t* d_cl_in = nullptr;        // [8][ncell] the network's input words for the next step
+    float* d_cl_y = nullptr;            // [5][ncell] the network's outputs of the current step
+    unsigned char* d_cl_out = nullptr;  // [ncell] the next step's cells outside the training envelope
+    bool cl_valid = false;              // d_cl_in / d_cl_out match the current state and centres
     float* d_env = nullptr;    // [2][8] training envelope (titan_set_closure_fallback)
     double* d_fallback = nullptr;       // [4][ncell] fallback sources, renumbered
     unsigned long long* d_n_outside = nullptr;
@@ -209,6 +213,26 @@ const char* face_kernel_name(const titan_ctx* ctx) {
     return ctx->fp32 ? "face_flux_fp32" : "face_flux_fp64";
 }
 
+// The closure's part of the cell update (source mode 3) for the current buffers.
+ClosureCell closure_cell(const titan_ctx* ctx) {
+    ClosureCell q{};
+    q.y = ctx->d_cl_y;
+    q.in = ctx->d_cl_in;
+    q.outside = ctx->d_cl_out;
+    q.fallback = ctx->d_fallback;
+    q.n_outside = ctx->d_n_outside;
+    q.norm = ctx->closure.norm;
+    q.env = ctx->d_env;
+    q.nH_inf = ctx->closure_ninf;
+    q.lambda = ctx->closure_lambda;
+    q.cc1 = ctx->layer[ctx->cur].cc;
+    return q;
+}
+
+int step_source_mode(const titan_ctx* ctx) {
+    return ctx->use_closure ? 3 : (ctx->use_src ? 2 : (ctx->prm.nh > 0 ? 1 : 0));
+}
+
 // Enqueue one step; flips the layer and state buffers.
 cudaError_t enqueue_step(titan_ctx* ctx) {
     const MeshView M = ctx->view();
@@ -241,21 +265,15 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
         if (e) return e;
     }
     if (ctx->use_closure) {
-        // sources of this step from the network, on the current state
+        // the network on this step's inputs (formed by the previous cell update);
+        // the cell update turns its outputs into sources
         MlpArgs ma{};
         ma.net = ctx->closure.view();
         ma.n = (int)ctx->ncell;
         ma.ncell = (int)ctx->ncell;
-        ma.state = ctx->d_state[ctx->scur];
-        ma.cc = ctx->layer[ctx->cur].cc;
-        ma.src = ctx->d_src;
-        ma.nH_inf = ctx->closure_ninf;
-        ma.lambda = ctx->closure_lambda;
+        ma.in_words = ctx->d_cl_in;
+        ma.y_out = ctx->d_cl_y;
         ma.error = ctx->closure.error;
-        ma.env_lo = ctx->d_env;
-        ma.env_hi = ctx->d_env ? ctx->d_env + kIn : nullptr;
-        ma.fallback = ctx->d_fallback;
-        ma.n_outside = ctx->d_n_outside;
         if (ctx->d_n_outside) {
             e = cudaMemsetAsync(ctx->d_n_outside, 0, sizeof(unsigned long long), ctx->stream);
             if (e) return e;
@@ -285,8 +303,9 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     ca.flux = ctx->d_flux;
     ca.hfl = ctx->d_hfl;
     ca.src = ctx->d_src;
+    ca.cl = closure_cell(ctx);
     ca.st = ctx->d_status;
-    const int src = (ctx->use_src || ctx->use_closure) ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
+    const int src = step_source_mode(ctx);
     e = timed(ctx, "cell_update",
               [&] { return launch_cell_update(ca, nk, move, src, ctx->cell_variant, ctx->stream); });
     if (e) return e;
@@ -527,6 +546,9 @@ int titan_destroy(titan_ctx* ctx) {
         if (p) cudaFree(p);
     for (void* p : ctx->surf_buf)
         if (p) cudaFree(p);
+    if (ctx->d_cl_in) cudaFree(ctx->d_cl_in);
+    if (ctx->d_cl_y) cudaFree(ctx->d_cl_y);
+    if (ctx->d_cl_out) cudaFree(ctx->d_cl_out);
     if (ctx->d_halo_send) cudaFree(ctx->d_halo_send);
     if (ctx->d_halo_recv) cudaFree(ctx->d_halo_recv);
     if (ctx->d_face_nodt) cudaFree(ctx->d_face_nodt);
@@ -863,12 +885,14 @@ int titan_unpack_halo(titan_ctx* ctx, const double* in) {
     if (!ctx || (ctx->n_halo_recv && !in)) return fail(TITAN_EINVAL, "bad argument");
     CK(launch_halo_unpack(ctx->d_state[ctx->scur], (int)ctx->ncell, ctx->d_halo_recv, (int)ctx->n_halo_recv,
                           ctx->ns, in, ctx->stream));
+    ctx->cl_valid = false;
     CK(cudaStreamSynchronize(ctx->stream));
     return TITAN_OK;
 }
 
 int titan_upload_state(titan_ctx* ctx, const double* state) {
     if (!ctx || !state) return fail(TITAN_EINVAL, "null argument");
+    ctx->cl_valid = false;
     const int64_t nc = ctx->ncell;
     cudaStream_t s = ctx->stream, x = ctx->xfer;
     // field by field: the copy of field k+1 overlaps the gather of field k
@@ -947,6 +971,16 @@ int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout
     cudaStream_t s = ctx->stream;
     std::memcpy(ctx->h_status, &init, sizeof(DevStatus));
     CK(cudaMemcpyAsync(ctx->d_status, ctx->h_status, sizeof(DevStatus), cudaMemcpyHostToDevice, s));
+    if (ctx->use_closure && !ctx->cl_valid && nsteps > 0) {
+        // the state or centres changed outside the step loop: the closure's
+        // inputs for the first step (every later step's come from the cell update)
+        CK(timed(ctx, "closure_inputs", [&] {
+            return launch_closure_inputs(ctx->d_state[ctx->scur], ctx->layer[ctx->cur].cc, (int)ctx->ncell,
+                                         ctx->closure.norm, ctx->d_env, ctx->closure_ninf, ctx->closure_lambda,
+                                         ctx->d_cl_in, ctx->d_cl_out, s);
+        }));
+        ctx->cl_valid = true;
+    }
     CK(cudaEventRecord(ctx->ev[0], s));
     int64_t done = 0;
     if (ctx->profiling) {
@@ -1014,6 +1048,7 @@ int titan_upload_nodes(titan_ctx* ctx, const double* xyz) {
     for (int64_t i = 0; i < nn; ++i)
         for (int k = 0; k < 3; ++k) h[k * nn + i] = xyz[3 * (int64_t)ctx->R.node_n2o[i] + k];
     drop_graph(ctx);
+    ctx->cl_valid = false;
     const Layer& L = ctx->layer[ctx->cur];
     CK(cudaMemcpyAsync(L.xyz, h.data(), sizeof(double) * 3 * nn, cudaMemcpyHostToDevice, ctx->stream));
     const MeshView M = ctx->view();
@@ -1154,11 +1189,15 @@ int titan_set_closure(titan_ctx* ctx, const float* params, const float* norm, do
     ctx->use_closure = false;
     if (!params) return TITAN_OK;
     if (!norm || !(n_inf > 0.0)) return fail(TITAN_EINVAL, "closure needs norm and n_inf > 0");
-    if (!ctx->d_src) {
-        int64_t dummy = 0;
-        CK(dalloc(&ctx->d_src, (size_t)4 * ctx->ncell, &dummy));
-        ctx->dev_bytes += dummy;
+    if (!ctx->d_cl_in) {
+        int64_t bytes = 0;
+        cudaError_t e = dalloc(&ctx->d_cl_in, (size_t)8 * ctx->ncell, &bytes);
+        if (!e) e = dalloc(&ctx->d_cl_y, (size_t)5 * ctx->ncell, &bytes);
+        if (!e) e = dalloc(&ctx->d_cl_out, (size_t)ctx->ncell, &bytes);
+        if (e) return fail(TITAN_ENOMEM, std::string("closure buffers: ") + cudaGetErrorString(e));
+        ctx->dev_bytes += bytes;
     }
+    ctx->cl_valid = false;
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, dev));
@@ -1211,6 +1250,7 @@ int titan_set_closure_fallback(titan_ctx* ctx, const float* lo, const float* hi,
     if (!ctx) return fail(TITAN_EINVAL, "null argument");
     if ((lo == nullptr) != (hi == nullptr)) return fail(TITAN_EINVAL, "lo and hi go together");
     drop_graph(ctx);
+    ctx->cl_valid = false;  // the envelope flags are formed with the inputs
     if (!lo) {
         void* ps[] = {ctx->d_env, ctx->d_fallback, ctx->d_n_outside};
         for (void* p : ps)
@@ -1579,7 +1619,7 @@ int titan_get_tuning(titan_ctx* ctx, int32_t* face_variant, int32_t* cell_varian
 
 int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     if (!ctx || reps <= 0) return fail(TITAN_EINVAL, "bad argument");
-    const int src = (ctx->use_src || ctx->use_closure) ? 2 : (ctx->prm.nh > 0 ? 1 : 0);
+    const int src = step_source_mode(ctx);
     char key[256];
     snprintf(key, sizeof key, "sm_100a cells=%lld faces=%lld move=%d flux=%d npassive=%d src=%d tvd=%d",
              (long long)ctx->ncell, (long long)ctx->nface, ctx->prm.move, ctx->prm.flux_precision,
@@ -1632,8 +1672,12 @@ int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     ca.flux = ctx->d_flux;
     ca.hfl = ctx->d_hfl;
     ca.src = ctx->d_src;
+    ca.cl = closure_cell(ctx);
     ca.st = ctx->d_status;
     const int nk = ctx->prm.npassive;
+    // the timed cell updates write the closure's next inputs from a state the
+    // context does not keep: they are formed again before the next step
+    ctx->cl_valid = false;
     auto time_it = [&](auto launch, float* ms_out) -> cudaError_t {
         std::memcpy(ctx->h_status, &init, sizeof(DevStatus));
         cudaError_t e = cudaMemcpyAsync(ctx->d_status, ctx->h_status, sizeof(DevStatus), cudaMemcpyHostToDevice, s);

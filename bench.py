@@ -81,17 +81,25 @@ def peak_tflops():
 # each kernel on the 6x96x96x40 shell itself (the workload of this benchmark;
 # ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum, one launch each).
 # Keyed by (kernel, cells, sources in the step); other sizes report no traffic.
-TRAFFIC = {}
+TRAFFIC = {
+    # the mixed step (FP32 Riemann arithmetic, closure sources)
+    ("move_nodes", 2211840, True): 107.85e6, ("closure_mlp", 2211840, True): 81.21e6,
+    ("face_flux_fp32", 2211840, True): 1066.71e6, ("cell_update", 2211840, True): 1433.49e6,
+    # the plain FP64 step
+    ("move_nodes", 2211840, False): 110.73e6, ("face_flux_fp64", 2211840, False): 1045.15e6,
+    ("cell_update", 2211840, False): 1164.85e6,
+}
 
 
 def traffic(name, C, sources):
     return TRAFFIC.get((name, C, bool(sources)))
 
 # FP64-pipe warp instructions per face of face_flux_fp64 on the moving shell,
-# counted by ncu (sm__inst_executed_pipe_fp64.sum / faces; 1,148 thread
-# instructions per face: 337 DFMA of the IEEE divisions and square roots,
-# 339 DMUL, 258 DADD, the rest compares and conversions).
-FP64_WARP_INST_PER_FACE = 35.87
+# counted by ncu at the benchmark's launch shape (sm__inst_executed_pipe_fp64.sum
+# / faces on the 6x64x64x40 shell; 1,173 thread instructions per face: 337 DFMA
+# of the IEEE divisions and square roots, 346 DMUL, 268 DADD, the rest compares
+# and conversions).
+FP64_WARP_INST_PER_FACE = 36.65
 FP64_WARP_INST_PER_CLK_PER_SM = 2.0  # 64 FP64 lanes per clock per SM
 
 
@@ -617,11 +625,12 @@ def run_sharded(args, rank, world):
     ss.go(max(args.warmup, 3))
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.ExternalStream(plasma.stream())  # the loop runs on the context's stream
     barrier()
     with ClockSampler(dev) as clk:
-        ev0.record()
+        ev0.record(stream)
         ss.go(args.steps)
-        ev1.record()
+        ev1.record(stream)
         barrier()
     # end to end: every step each rank's cells in from pinned host memory, the owned cells back
     ns = 8 + p["npassive"]

@@ -179,7 +179,10 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* params,
  * peers agree on. titan_pack_halo writes the send cells' states, whole cells
  * of 8 + npassive doubles each ([n_send][ns]), to a DEVICE buffer on this
  * context's GPU; titan_unpack_halo writes a device buffer of the same form
- * into the copies. Both return when the copy is done. */
+ * into the copies. Both are ordered on titan_stream(ctx) and return without
+ * waiting: work on another stream that reads a packed buffer, or writes one
+ * to be unpacked, orders itself against this stream (an event, or the
+ * stream itself as the exchange's stream). */
 int titan_set_halo(titan_ctx* ctx, int64_t n_send, const int32_t* send_ids, int64_t n_recv, const int32_t* recv_ids);
 /* Faces (original numbering, 1 = left out) whose CFL candidate does not enter
  * dt: on a sharded rank, the faces between two halo cells, whose stencils can
@@ -208,6 +211,28 @@ int titan_set_sources(titan_ctx* ctx, const double* src);
  * first step (the reference starts with 1e-5); out, the CFL dt of the next
  * step. t_inout: accumulated physical time (drives the node motion). */
 int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout, titan_step_info* info);
+
+/* The same loop paced by the device, for a mesh split over GPUs (no
+ * reference counterpart: the reference steps one mesh in one process). All
+ * four calls are ordered on titan_stream(ctx) and only titan_get_clock waits
+ * for it, so a caller can put its own work (an NCCL exchange of halo cells,
+ * an all-reduce of dt) on the same stream between steps without the host
+ * taking part:
+ *   titan_set_clock   the device clock of a run: dt of the next step, t, and
+ *                     cleared counters and error word (as titan_step does
+ *                     from dt_inout / t_inout);
+ *   titan_step_async  enqueues nsteps steps from the device clock; each step
+ *                     leaves its CFL minimum as the next step's dt;
+ *   titan_dt_copy     copies the clock's dt to (into_clock = 0) or from (1)
+ *                     one double of device memory, e.g. the buffer of an
+ *                     all-reduce(min) over the ranks;
+ *   titan_get_clock   waits for the stream and reports dt, t and the run's
+ *                     status as titan_step does (info may be NULL).
+ * titan_pack_halo / titan_unpack_halo are ordered on the same stream too. */
+int titan_set_clock(titan_ctx* ctx, double dt, double t);
+int titan_step_async(titan_ctx* ctx, int64_t nsteps);
+int titan_dt_copy(titan_ctx* ctx, double* dt_device, int32_t into_clock);
+int titan_get_clock(titan_ctx* ctx, double* dt, double* t, titan_step_info* info);
 
 /* Node coordinates [nnode*3] (original numbering) for the current layer; the
  * layer's geometry (and the second-order neighbours of a tvd context) is formed

@@ -877,7 +877,6 @@ int titan_pack_halo(titan_ctx* ctx, double* out) {
     if (!ctx || (ctx->n_halo_send && !out)) return fail(TITAN_EINVAL, "bad argument");
     CK(launch_halo_pack(ctx->d_state[ctx->scur], (int)ctx->ncell, ctx->d_halo_send, (int)ctx->n_halo_send, ctx->ns,
                         out, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
     return TITAN_OK;
 }
 
@@ -886,7 +885,6 @@ int titan_unpack_halo(titan_ctx* ctx, const double* in) {
     CK(launch_halo_unpack(ctx->d_state[ctx->scur], (int)ctx->ncell, ctx->d_halo_recv, (int)ctx->n_halo_recv,
                           ctx->ns, in, ctx->stream));
     ctx->cl_valid = false;
-    CK(cudaStreamSynchronize(ctx->stream));
     return TITAN_OK;
 }
 
@@ -960,17 +958,28 @@ int titan_set_sources(titan_ctx* ctx, const double* src) {
     return TITAN_OK;
 }
 
-int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout, titan_step_info* info) {
-    if (!ctx || !dt_inout || nsteps < 0) return fail(TITAN_EINVAL, "bad argument");
-    const double t0 = t_inout ? *t_inout : 0.0;
-    if (!(*dt_inout > 0.0) || !std::isfinite(*dt_inout)) return fail(TITAN_EINVAL, "dt must be positive");
-    DevStatus init{};
-    init.dt = *dt_inout;
-    init.t = t0;
-    init.dt_next_bits = 0x4197D78400000000ull;  // bits of 1e8, the identity of the CFL minimum
+}  // extern "C"
+
+namespace {
+
+// The device clock and status word of a run: dt, t, cleared counters and error
+// word, the identity of the CFL minimum; written by a kernel, so it is
+// ordered on the stream like the steps and needs no host buffer.
+__global__ void set_status_kernel(DevStatus* st, double dt, double t) {
+    st->err_kind = 0;
+    st->err_index = 0;
+    st->n_rho_floor = 0;
+    st->n_p_floor = 0;
+    st->steps_done = 0;
+    st->block_counter = 0;
+    st->dt_next_bits = 0x4197D78400000000ull;  // bits of 1e8, the identity of the CFL minimum
+    st->dt = dt;
+    st->t = t;
+}
+
+// Enqueues nsteps steps on the context's stream from the device clock; no host sync.
+int enqueue_steps(titan_ctx* ctx, int64_t nsteps) {
     cudaStream_t s = ctx->stream;
-    std::memcpy(ctx->h_status, &init, sizeof(DevStatus));
-    CK(cudaMemcpyAsync(ctx->d_status, ctx->h_status, sizeof(DevStatus), cudaMemcpyHostToDevice, s));
     if (ctx->use_closure && !ctx->cl_valid && nsteps > 0) {
         // the state or centres changed outside the step loop: the closure's
         // inputs for the first step (every later step's come from the cell update)
@@ -981,7 +990,6 @@ int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout
         }));
         ctx->cl_valid = true;
     }
-    CK(cudaEventRecord(ctx->ev[0], s));
     int64_t done = 0;
     if (ctx->profiling) {
         drop_graph(ctx);
@@ -997,14 +1005,17 @@ int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout
             CK(enqueue_step(ctx));
         }
     }
-    CK(cudaEventRecord(ctx->ev[1], s));
+    return TITAN_OK;
+}
+
+// Waits for the context's stream and reports the device clock and status.
+int finish_steps(titan_ctx* ctx, double* dt_out, double* t_out, titan_step_info* info, float ms) {
+    cudaStream_t s = ctx->stream;
     CK(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     const DevStatus& st = *ctx->h_status;
-    *dt_inout = st.dt;
-    if (t_inout) *t_inout = st.t;
+    if (dt_out) *dt_out = st.dt;
+    if (t_out) *t_out = st.t;
     int status = TITAN_OK;
     if (st.err_kind != 0) status = st.err_kind >= 20 ? TITAN_ENONFINITE : TITAN_ESOLVER;
     if (ctx->use_closure) {
@@ -1036,6 +1047,53 @@ int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout
                  st.err_index, (unsigned long long)st.steps_done);
         return fail(status, buf);
     }
+    return TITAN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int titan_step(titan_ctx* ctx, int64_t nsteps, double* dt_inout, double* t_inout, titan_step_info* info) {
+    if (!ctx || !dt_inout || nsteps < 0) return fail(TITAN_EINVAL, "bad argument");
+    const double t0 = t_inout ? *t_inout : 0.0;
+    if (!(*dt_inout > 0.0) || !std::isfinite(*dt_inout)) return fail(TITAN_EINVAL, "dt must be positive");
+    cudaStream_t s = ctx->stream;
+    set_status_kernel<<<1, 1, 0, s>>>(ctx->d_status, *dt_inout, t0);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[0], s));
+    const int rc = enqueue_steps(ctx, nsteps);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[1], s));
+    CK(cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    return finish_steps(ctx, dt_inout, t_inout, info, ms);
+}
+
+int titan_set_clock(titan_ctx* ctx, double dt, double t) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    if (!(dt > 0.0) || !std::isfinite(dt) || !std::isfinite(t)) return fail(TITAN_EINVAL, "dt must be positive");
+    set_status_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_status, dt, t);
+    CK(cudaGetLastError());
+    return TITAN_OK;
+}
+
+int titan_step_async(titan_ctx* ctx, int64_t nsteps) {
+    if (!ctx || nsteps < 0) return fail(TITAN_EINVAL, "bad argument");
+    return enqueue_steps(ctx, nsteps);
+}
+
+int titan_get_clock(titan_ctx* ctx, double* dt, double* t, titan_step_info* info) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    return finish_steps(ctx, dt, t, info, 0.f);
+}
+
+int titan_dt_copy(titan_ctx* ctx, double* dev, int32_t into_clock) {
+    if (!ctx || !dev) return fail(TITAN_EINVAL, "null argument");
+    double* clock_dt = &ctx->d_status->dt;
+    CK(cudaMemcpyAsync(into_clock ? clock_dt : dev, into_clock ? dev : clock_dt, sizeof(double),
+                       cudaMemcpyDeviceToDevice, ctx->stream));
     return TITAN_OK;
 }
 

@@ -114,6 +114,10 @@ SIGNATURES = {
     "titan_upload_hfluids": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_set_sources": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_step": ([ctypes.c_void_p, ctypes.c_int64, D, D, ctypes.POINTER(TitanStepInfo)], ctypes.c_int),
+    "titan_set_clock": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+    "titan_step_async": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "titan_get_clock": ([ctypes.c_void_p, D, D, ctypes.POINTER(TitanStepInfo)], ctypes.c_int),
+    "titan_dt_copy": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "titan_download_nodes": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_download_geometry": ([ctypes.c_void_p, D, D, D, D, D], ctypes.c_int),
     "titan_download_face_fluxes": ([ctypes.c_void_p, D], ctypes.c_int),

@@ -159,6 +159,30 @@ class PlasmaStep:
         N.check(rc)
         return self.last_info
 
+    # -- the loop paced by the device (titan_set_clock / titan_step_async /
+    # titan_dt_copy / titan_get_clock): ordered on self.stream(), no host wait
+    def set_clock(self, dt: float | None = None, t: float | None = None):
+        N.check(self._lib.titan_set_clock(self._ctx, float(self.dt if dt is None else dt),
+                                          float(self.t if t is None else t)))
+
+    def step_async(self, steps: int):
+        N.check(self._lib.titan_step_async(self._ctx, int(steps)))
+
+    def dt_copy(self, dev_ptr: int, into_clock: bool):
+        """The device clock's dt to (False) or from (True) one double at dev_ptr."""
+        N.check(self._lib.titan_dt_copy(self._ctx, ctypes.c_void_p(dev_ptr), int(into_clock)))
+
+    def get_clock(self) -> dict:
+        """Waits for the stream; dt and t of the device clock, and the run's info."""
+        dt, t = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        info = N.TitanStepInfo()
+        rc = self._lib.titan_get_clock(self._ctx, ctypes.byref(dt), ctypes.byref(t), ctypes.byref(info))
+        self.last_info = {k: getattr(info, k) for k, _ in N.TitanStepInfo._fields_}
+        if rc == N.TITAN_OK:
+            self.dt, self.t = dt.value, t.value
+        N.check(rc)
+        return self.last_info
+
     def nodes(self) -> np.ndarray:
         out = np.empty((self.nnode, 3))
         N.check(self._lib.titan_download_nodes(self._ctx, N.ptr(out)))

@@ -153,7 +153,11 @@ def local_face_method(shard: dict, method: np.ndarray) -> np.ndarray:
 
 
 class DeviceStepper:
-    """A PlasmaStep on a sub-mesh, with the halo copies through device tensors."""
+    """A PlasmaStep on a sub-mesh, with the halo copies through device tensors.
+    Its halo copies, steps and clock are ordered on the context's stream, so
+    ShardedStep drives it without host waits (device_paced)."""
+
+    device_paced = True
 
     def __init__(self, pkg, mesh: dict, params: dict):
         self.step = pkg.PlasmaStep(mesh, params)
@@ -237,9 +241,19 @@ class ShardedStep:
         return self.step.download_state()[:, : self.shard["n_owned"]]
 
     def exchange(self):
-        dist = self.torch.distributed
+        """The halo exchange of the host-paced loop (steppers without a device
+        stream, e.g. the oracle on CPU ranks)."""
         if self.n_send:
             self.step.pack(self.sbuf)
+        self._p2p()
+        if self.device.type == "cuda":
+            self.torch.cuda.current_stream(self.device).synchronize()
+        if self.n_recv:
+            self.step.unpack(self.rbuf)
+
+    def _p2p(self):
+        """The point-to-point halo messages on the current stream."""
+        dist = self.torch.distributed
         ops, off = [], 0
         for p in self.peers_send:
             n = len(self.shard["send"][p])
@@ -252,14 +266,12 @@ class ShardedStep:
             off += n
         if ops:
             for w in dist.batch_isend_irecv(ops):
-                w.wait()
-        if self.device.type == "cuda":
-            self.torch.cuda.current_stream(self.device).synchronize()
-        if self.n_recv:
-            self.step.unpack(self.rbuf)
+                w.wait()  # NCCL: the current stream waits; the host does not
 
     def go(self, steps: int):
         """`steps` steps; dt after each is the minimum over the ranks."""
+        if getattr(self.step, "device_paced", False) and self.device.type == "cuda":
+            return self._go_device(steps)
         dist = self.torch.distributed
         for _ in range(steps):
             self.exchange()
@@ -268,6 +280,32 @@ class ShardedStep:
                 t = self.torch.tensor([self.step.dt], dtype=self.torch.float64, device=self.device)
                 dist.all_reduce(t, op=dist.ReduceOp.MIN)
                 self.step.dt = float(t.item())
+
+    def _go_device(self, steps: int):
+        """The loop paced by the device: every step's pack, NCCL exchange,
+        unpack, step and all-reduce(min) of dt run on the context's stream in
+        order, and the host waits once, at the end (titan_get_clock)."""
+        torch = self.torch
+        dist = torch.distributed
+        ps = self.step.step
+        stream = torch.cuda.ExternalStream(ps.stream(), device=self.device)
+        reduce_dt = dist.is_initialized()
+        if reduce_dt and not hasattr(self, "dt_buf"):
+            self.dt_buf = torch.zeros(1, dtype=torch.float64, device=self.device)
+        with torch.cuda.stream(stream):
+            ps.set_clock()
+            for _ in range(steps):
+                if self.n_send:
+                    ps.pack_halo(self.sbuf.data_ptr())
+                self._p2p()
+                if self.n_recv:
+                    ps.unpack_halo(self.rbuf.data_ptr())
+                ps.step_async(1)
+                if reduce_dt:
+                    ps.dt_copy(self.dt_buf.data_ptr(), into_clock=False)
+                    dist.all_reduce(self.dt_buf, op=dist.ReduceOp.MIN)
+                    ps.dt_copy(self.dt_buf.data_ptr(), into_clock=True)
+        return ps.get_clock()
 
     def close(self):
         self.step.close()

@@ -111,7 +111,7 @@ typedef struct titan_step_info {
     int32_t err_kind;        /* 0, 11-14 solver region/branch, 15-18 exact HP solver (negative pressure,
                                 Newton / bisection without convergence, no wave pattern), 19 non-finite
                                 or subnormal contact speed of an HP face (surface tracking), 20
-                                non-finite density */
+                                non-finite density, 21 a staged cell update's copy wait ran out */
     double  dt_next;         /* CFL dt that the next step will use */
     double  t;               /* accumulated physical time */
     double  gpu_ms;          /* device time of this call's step loop (CUDA events) */
@@ -170,6 +170,26 @@ typedef struct titan_surface_params {
 
 int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* params, int64_t nray, int32_t ray_len,
                              const int32_t* ray_nodes);
+
+/* The A_Luch spacing law of Luch::dvigenie (TITAN/source/Luch.cpp:9-152) for
+ * the rays given to titan_set_surface_motion, in place of the fraction rule:
+ * every ray has M0 + M1 + M2 + M3 + M4 + 5 nodes, from the inner end: M0 at
+ * R0 + j (R1 - R0) / M0; the R1 node (left where it is); M1 evenly between R1
+ * and the TS node (slot M0 + M1 + 1); M11 after the TS at the same step; M2 -
+ * M11 up to the HP node (slot M0 + M1 + M2 + 2) by the cubic law of da1, da2;
+ * M3 up to the BS node (slot M0 + M1 + M2 + M3 + 3) by the law of da3, da4;
+ * M4 up to the end, placed at R5, by the law of da5. The TS, HP and BS radii
+ * are those of the ray's surface nodes after they have moved in the step.
+ * Geo_param's names (TITAN/source/Geo_param.h:22-63); one set for all rays
+ * (the reference's per-ray da1..da5 overrides are not taken). NULL returns to
+ * the fraction rule; titan_set_surface_motion clears the law. */
+typedef struct titan_ray_law {
+    int32_t M0, M1, M11, M2, M3, M4;
+    int32_t pad[2];
+    double R0, R1, R5;
+    double da1, da2, da3, da4, da5;
+} titan_ray_law;
+int titan_set_ray_law(titan_ctx* ctx, const titan_ray_law* law);
 
 /* Halo exchange of a sharded step (several contexts, one per GPU, each on the
  * cells one rank owns plus a layer of copies of its neighbours' cells; no
@@ -393,7 +413,12 @@ int titan_closure_outside(titan_ctx* ctx, int64_t* n_outside);
  * this context's mesh and state, `reps` launches each, and keeps the fastest.
  * Call after titan_upload_state. With a cache file, a line for the same mesh
  * size and step options is reused instead of timing, and new results are
- * appended. The device status is reset, so call it between runs. */
+ * appended. The device status is reset, so call it between runs.
+ * Face variants 0-6; cell variants 0-5 read each face record from global
+ * memory, 6-8 stage the records of a block's faces in shared memory (one bulk
+ * copy of the contiguous run its cells own, cp.async for the others) with
+ * identical results. A staged shape whose wait for its copy runs out sets
+ * err_kind 21 and the step returns TITAN_ETIMEOUT. */
 int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path);
 int titan_set_tuning(titan_ctx* ctx, int32_t face_variant, int32_t cell_variant);
 int titan_get_tuning(titan_ctx* ctx, int32_t* face_variant, int32_t* cell_variant, int32_t* face_block,

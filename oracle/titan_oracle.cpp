@@ -86,6 +86,9 @@ struct OMesh {
     const int8_t* face_nodt;     // nface, 1: left out of the CFL minimum; may be null
     const double* surf_centre;   // nnode*3, fitted sphere centres of smoothed surface nodes
                                  // (oracle_surface_centres); may be null
+    // The A_Luch spacing law for the rays (Luch.cpp:9-152), or null for the
+    // fraction rule: M0, M1, M11, M2, M3, M4 (as doubles), R0, R1, R5, da1..da5.
+    const double* ray_law;
 };
 
 struct OParams {
@@ -1565,10 +1568,64 @@ void oracle_move_nodes(const OMesh* M, const OParams* P, const double* xyz1, dou
 //    neighbours one toward their mean with its own position.
 //  * Along each ray (a shorter one padded with -1) the end nodes and the
 //    surface nodes are anchors; every other node keeps its initial fraction
-//    of the segment between the anchors around it, on the ray's direction
-//    (the reference's A_Luch spacing is a fixed function of that fraction,
-//    Luch.cpp:9-152).
+//    of the segment between the anchors around it, on the ray's direction.
+//    With M->ray_law the rays follow the reference's A_Luch law instead
+//    (o_a_luch_ray).
 // ---------------------------------------------------------------------------
+
+// One ray under the A_Luch law of Luch::dvigenie (Luch.cpp:9-152): walks the
+// ray's segments in order and places each node the law moves at r * u, from
+// the current radii R2, R3, R4 of the ray's TS, HP and BS nodes (their slots
+// follow from the node counts). The R1 node and the surface nodes stay.
+static void o_a_luch_ray(const double* law, const int32_t* rn, const double* u, double* xyz2) {
+    const int M0 = (int)law[0], M1 = (int)law[1], M11 = (int)law[2], M2 = (int)law[3], M3 = (int)law[4],
+              M4 = (int)law[5];
+    const double R0 = law[6], R1 = law[7], R5 = law[8];
+    auto radius = [&](int slot) {
+        const double* x = xyz2 + 3 * (int64_t)rn[slot];
+        return std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    };
+    const double R2 = radius(M0 + M1 + 1), R3 = radius(M0 + M1 + M2 + 2), R4 = radius(M0 + M1 + M2 + M3 + 3);
+    auto put = [&](int slot, double r) {
+        for (int k = 0; k < 3; ++k) xyz2[3 * (int64_t)rn[slot] + k] = r * u[k];
+    };
+    for (int j = 0; j < M0; ++j) put(j, R0 + j * (R1 - R0) / M0);
+    int num = M0 + 1;
+    for (int j = 0; j < M1; ++j) put(num + j, R1 + (j + 1) * (R2 - R1) / (M1 + 1));
+    num += M1 + 1;
+    const double dr = (R2 - R1) / (M1 + 1);
+    for (int j = 0; j < M11; ++j) put(num + j, R2 + dr * (j + 1));
+    num += M11;
+    {
+        const double a = law[9], b = law[10];
+        for (int j = 0; j < M2 - M11; ++j) {
+            const double s = (j + 1.0) / (M2 - M11 + 1.0);
+            const double q1 = 1.0 - 3.0 * s + 2.0 * (s * s), q2 = 1.0 - 2.0 * s;
+            const double ss = s * (a * (q1 * q1) +
+                                   s * (7.0 + b * (q2 * q2) * (-1.0 + s) - 2.0 * s * (9.0 + 2.0 * s * (-5.0 + 2.0 * s))));
+            put(num + j, R2 + dr * M11 + (R3 - R2 - dr * M11) * ss);
+        }
+    }
+    num += (M2 - M11) + 1;
+    {
+        const double a = law[11], b = law[12];
+        for (int j = 0; j < M3; ++j) {
+            const double s = (j + 1.0) / (M3 + 1.0);
+            const double ss = s * (a - (2.0 * a + b - 3.0) * s + (a + b - 2.0) * s * s);
+            put(num + j, R3 + (R4 - R3) * ss);
+        }
+    }
+    num += M3 + 1;
+    {
+        const double a = law[13], b = 2.0;
+        for (int j = 0; j < M4; ++j) {
+            const double s = (j + 1.0) / (M4 + 1.0);
+            const double ss = a * s - (3.0 * a + b - 4.0) * s * s * s + (2.0 * a + b - 3.0) * s * s * s * s;
+            put(num + j, R4 + (R5 - R4) * ss);
+        }
+    }
+    put(num + M4, R5);
+}
 
 // Radii and directions of the rays at `xyz` (the start of tracking).
 void oracle_ray_geometry(const OMesh* M, const double* xyz, double* r0, double* dir) {
@@ -1900,6 +1957,10 @@ static int o_surface_motion(const OMesh* M, const OParams* P, double* st, const 
         const int32_t* rn = M->ray_nodes + r * RL;
         const double* r0 = M->ray_r0 + r * RL;
         const double* u = M->ray_dir + 3 * r;
+        if (M->ray_law) {
+            o_a_luch_ray(M->ray_law, rn, u, xyz2);
+            continue;
+        }
         int64_t Lr = 0;
         while (Lr < RL && rn[Lr] >= 0) ++Lr;
         int64_t a = 0;

@@ -43,8 +43,11 @@ class OMesh(ctypes.Structure):
         ("face_method", I8), ("face_bc", I32), ("bc_vals", D), ("node_amp", D), ("node_phase", D),
         ("face_tvd", I32),
         ("ray_nodes", I32), ("ray_r0", D), ("ray_dir", D), ("nray", ctypes.c_int64), ("ray_len", ctypes.c_int64),
-        ("face_nodt", I8), ("surf_centre", D),
+        ("face_nodt", I8), ("surf_centre", D), ("ray_law", D),
     ]
+
+# The fields of titan_ray_law (the A_Luch law), in the oracle's order.
+RAY_LAW_KEYS = ("M0", "M1", "M11", "M2", "M3", "M4", "R0", "R1", "R5", "da1", "da2", "da3", "da4", "da5")
 
 
 class OParams(ctypes.Structure):
@@ -233,10 +236,12 @@ def random_riemann_cases(n: int, seed: int, *, weak_bn_frac=0.15, x_normal_frac=
 class OracleRun:
     """The oracle's step loop (oracle_go) on a mesh dict of titan_c-_b200.mesh."""
 
-    def __init__(self, mesh: dict, params: dict, surface: dict | None = None, rays: np.ndarray | None = None):
+    def __init__(self, mesh: dict, params: dict, surface: dict | None = None, rays: np.ndarray | None = None,
+                 ray_law: dict | None = None):
         """surface / rays: surface-tracking node motion (the SURFACE_KEYS of
         `surface`, rays [nray, ray_len] node ids from the inner end) instead of
-        the prescribed radial law."""
+        the prescribed radial law; ray_law: the A_Luch law (RAY_LAW_KEYS) for
+        the rays instead of the fraction rule."""
         self._keep = {}
 
         def keep(name, a, dt):
@@ -279,6 +284,8 @@ class OracleRun:
             rd = keep("ray_dir", np.empty((rn.shape[0], 3)), np.float64)
             oracle().oracle_ray_geometry(ctypes.byref(m), _p(self.xyz), _p(r0), _p(rd))
             m.ray_r0, m.ray_dir = _p(r0), _p(rd)
+            if ray_law is not None:
+                m.ray_law = _p(keep("ray_law", [float(ray_law[k]) for k in RAY_LAW_KEYS], np.float64))
             if p.sglag_TS or p.sglag_HP:
                 sc = keep("surf_centre", np.zeros((m.nnode, 3)), np.float64)
                 oracle().oracle_surface_centres(ctypes.byref(m), _p(self.xyz), _p(sc))

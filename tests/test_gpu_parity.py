@@ -320,7 +320,7 @@ def test_every_launch_shape_gives_identical_results(T):
     m, p, st, hf = T.problems.heliosphere_shell(nq=8, nlayer=6, move=True, zones=True, npassive=2)
     outs = []
     for fv in range(7):
-        for cv in range(6):
+        for cv in range(9):  # 6-8: the staged cell update
             if cv and fv:
                 continue
             g = T.PlasmaStep(m, p)
@@ -340,7 +340,7 @@ def test_autotune_picks_a_shape_and_caches_it(T, tmp_path):
     g.set_face_method(meth)
     g.upload_state(st)
     t1 = g.autotune(reps=2, cache=cache)
-    assert 0 <= t1["face_variant"] < 7 and 0 <= t1["cell_variant"] < 6
+    assert 0 <= t1["face_variant"] < 7 and 0 <= t1["cell_variant"] < 9
     assert open(cache).read().count("|") == 1
     g2 = T.PlasmaStep(m, p)
     g2.upload_state(st)

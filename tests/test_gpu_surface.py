@@ -95,3 +95,50 @@ def test_back_to_prescribed_motion_and_bad_rays(titan):
     g.go(2)
     assert np.isfinite(g.download_state()).all()
     g.close()
+
+
+def test_a_luch_ray_law_steps_match_oracle(titan, oracle_lib):
+    """The A_Luch spacing law (titan_set_ray_law, Luch.cpp:9-152) on a shell
+    built by that law: nodes and state after each step within 1e-12 of the
+    oracle; a ray of the wrong length or without a surface node on the law's
+    slots is refused."""
+    from test_oracle_surface import LAW, LAW_SLOTS, law_shell
+
+    m, p, st, rays = law_shell(titan, nq=8)
+    surf = dict(SURF, velocity_TS=30.0, velocity_HP=30.0, velocity_BS=30.0)
+    gpu = titan.PlasmaStep(m, p)
+    gpu.set_surface_motion(rays, **surf)
+    gpu.set_ray_law(LAW)
+    run = ol.OracleRun(m, p, surface=surf, rays=rays, ray_law=LAW)
+    gpu.upload_state(st)
+    x0 = gpu.nodes()
+    worst_s = worst_x = 0.0
+    for _ in range(6):
+        before = np.ascontiguousarray(gpu.download_state())
+        run.xyz[:] = gpu.nodes()
+        run.clock[:] = (gpu.dt, gpu.t)
+        gpu.go(1)
+        assert run.go(before, 1).err_code == 0
+        worst_s = max(worst_s, rel_err(gpu.download_state()[:8], before[:8]))
+        worst_x = max(worst_x, float(np.abs(gpu.nodes() - run.xyz).max() / np.abs(run.xyz).max()))
+    assert worst_s <= REL, worst_s
+    assert worst_x <= REL, worst_x
+    x = gpu.nodes()
+    r0, r1 = np.linalg.norm(x0[rays], axis=2), np.linalg.norm(x[rays], axis=2)
+    assert np.abs(r1[:, list(LAW_SLOTS)] - r0[:, list(LAW_SLOTS)]).max() > 1e-6
+    # the graph path (several steps per call) gives the same nodes
+    g2 = titan.PlasmaStep(m, p)
+    g2.set_surface_motion(rays, **surf)
+    g2.set_ray_law(LAW)
+    g2.upload_state(st)
+    g2.go(6)
+    assert np.array_equal(g2.nodes(), x)
+    g2.close()
+    # a law whose ray length differs, or whose TS slot holds no TS node, is refused
+    with pytest.raises(titan.TitanError):
+        gpu.set_ray_law(dict(LAW, M4=LAW["M4"] + 1))
+    with pytest.raises(titan.TitanError):
+        gpu.set_ray_law(dict(LAW, M0=LAW["M0"] + 1, M4=LAW["M4"] - 1))
+    gpu.set_ray_law(None)
+    gpu.go(1)
+    gpu.close()

@@ -222,3 +222,51 @@ def test_smoothing_off_changes_nothing(titan, oracle_lib):
         assert run.go(s, 2).err_code == 0
         res.append((s, run.xyz.copy()))
     assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+# The A_Luch spacing law (Luch::dvigenie, TITAN/source/Luch.cpp:9-152): node
+# counts and radii of Geo_param; a ray of M0 + M1 + M2 + M3 + M4 + 5 = 24 nodes.
+LAW = dict(M0=2, M1=4, M11=1, M2=5, M3=4, M4=4, R0=1.0, R1=2.0, R5=100.0,
+           da1=1.2, da2=0.8, da3=0.9, da4=1.1, da5=0.5)
+LAW_SLOTS = (7, 13, 18)   # TS, HP, BS
+
+
+def law_shell(titan, nq=6, R=(10.0, 20.0, 40.0), **kw):
+    """A shell whose layers sit where the A_Luch law puts them, with the
+    TS, HP and BS surfaces on the law's slots."""
+    radii = titan.mesh.a_luch_radii(LAW, *R)
+    m, p, st, hf = titan.problems.heliosphere_shell(nq=nq, nlayer=len(radii) - 1, move=True, radii=radii, **kw)
+    for slot, kind in zip(LAW_SLOTS, (1, 2, 3)):
+        titan.mesh.mark_shell_surface(m, slot, kind)
+    return m, p, st, titan.mesh.shell_rays(m)
+
+
+def test_a_luch_law_is_a_fixed_point_of_still_surfaces(titan, oracle_lib):
+    m, p, st, rays = law_shell(titan)
+    still = dict(SURF, move_TS=0, move_HP=0, move_BS=0)
+    run = ol.OracleRun(m, p, surface=still, rays=rays, ray_law=LAW)
+    x0 = run.xyz.copy()
+    assert run.go(np.ascontiguousarray(st.copy()), 3).err_code == 0
+    assert np.abs(run.xyz - x0).max() <= 1e-13 * np.abs(x0).max()
+
+
+def test_a_luch_law_places_ray_nodes_from_the_moved_surfaces(titan, oracle_lib):
+    """After steps that move the three surfaces, every ray's radii are the
+    law's radii for its current TS, HP and BS radii (mesh.a_luch_radii, a
+    separate numpy restatement), on the ray's own direction."""
+    m, p, st, rays = law_shell(titan)
+    surf = dict(SURF, velocity_TS=30.0, velocity_HP=30.0, velocity_BS=30.0)
+    run = ol.OracleRun(m, p, surface=surf, rays=rays, ray_law=LAW)
+    x0 = run.xyz.copy()
+    s = np.ascontiguousarray(st.copy())
+    assert run.go(s, 4).err_code == 0
+    r = np.linalg.norm(run.xyz[rays], axis=2)
+    moved = np.abs(r[:, list(LAW_SLOTS)] - np.linalg.norm(x0[rays][:, list(LAW_SLOTS)], axis=2))
+    assert moved.max() > 1e-6
+    for k in range(rays.shape[0]):
+        want = titan.mesh.a_luch_radii(LAW, *r[k, list(LAW_SLOTS)])
+        assert np.abs(r[k] - want).max() <= 1e-12 * want.max(), k
+    # every node of a ray on the ray's initial direction
+    d0 = x0[rays[:, 0]] / np.linalg.norm(x0[rays[:, 0]], axis=1)[:, None]
+    u = run.xyz[rays] / r[:, :, None]
+    assert np.abs(u - d0[:, None, :]).max() <= 1e-12

@@ -7,11 +7,12 @@
 
 namespace titan {
 
-template <typename FT, int NK, bool MOVE, int SRC, int BS, int MINB>
-__global__ void __launch_bounds__(BS, MINB) cell_update_kernel(CellArgs a) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool ok = a.st->err_kind == 0;
-    if (c < a.M.ncell && ok) {
+// The update of cell c. `gather(PO)` sums the cell's six face records into
+// PO in the cell's own face order (the flux gather of Setka_physics.cpp:
+// 1671-1733); the launch shapes differ only in where the records come from.
+template <int NK, bool MOVE, int SRC, typename Gather>
+__device__ __forceinline__ void update_cell(const CellArgs& a, const int c, Gather&& gather) {
+    {
         const MeshView& M = a.M;
         const int nc = M.ncell;
         const double time = a.st->dt;
@@ -31,38 +32,8 @@ __global__ void __launch_bounds__(BS, MINB) cell_update_kernel(CellArgs a) {
                 load_node(a.L2.xyz, nn, M.cell_nodes[li * nc + c], p);
             });
         }
-        using L = FluxLayout<FT, NK>;
         double PO[9 + NK];
-#pragma unroll
-        for (int k = 0; k < 9 + NK; ++k) PO[k] = 0.0;
-        const FT* fx = reinterpret_cast<const FT*>(a.flux);
-#pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            const int fs = M.cell_faces[s * nc + c];
-            const int f = fs & 0x7fffffff;
-            const double sign = (fs < 0) ? -1.0 : 1.0;
-            const FT* src = fx + size_t(f) * L::stride;
-            FT v[L::stride];
-            if (sizeof(FT) == 8) {
-#pragma unroll
-                for (int k = 0; k < L::stride; k += 2) {
-                    const double2 t = __ldg(reinterpret_cast<const double2*>(src) + k / 2);
-                    v[k] = FT(t.x);
-                    v[k + 1] = FT(t.y);
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < L::stride; k += 4) {
-                    const float4 t = __ldg(reinterpret_cast<const float4*>(src) + k / 4);
-                    v[k] = FT(t.x);
-                    v[k + 1] = FT(t.y);
-                    v[k + 2] = FT(t.z);
-                    v[k + 3] = FT(t.w);
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 9 + NK; ++k) PO[k] += sign * double(v[k]);
-        }
+        gather(PO);
         double prim[NV];
 #pragma unroll
         for (int k = 0; k < 8 + NK; ++k) prim[k] = a.state[k * nc + c];
@@ -186,8 +157,11 @@ __global__ void __launch_bounds__(BS, MINB) cell_update_kernel(CellArgs a) {
             q.outside[c] = out ? 1 : 0;
         }
     }
-    // Last block to finish rolls the clock: t += dt, dt = CFL minimum of this
-    // step's faces (applied on the next step, Setka_physics.cpp:1606-1607).
+}
+
+// Last block to finish rolls the clock: t += dt, dt = CFL minimum of this
+// step's faces (applied on the next step, Setka_physics.cpp:1606-1607).
+__device__ __forceinline__ void roll_clock(const CellArgs& a) {
     __shared__ bool last;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -211,41 +185,280 @@ __global__ void __launch_bounds__(BS, MINB) cell_update_kernel(CellArgs a) {
     }
 }
 
-template <typename FT, int NK, bool MOVE, int BS, int MINB>
-static void cell_update_src(const CellArgs& a, int src, cudaStream_t s) {
-    const unsigned int g = blocks_for(a.M.ncell, BS);
-    if (src == 0) cell_update_kernel<FT, NK, MOVE, 0, BS, MINB><<<g, BS, 0, s>>>(a);
-    else if (src == 1) cell_update_kernel<FT, NK, MOVE, 1, BS, MINB><<<g, BS, 0, s>>>(a);
-    else if (src == 2) cell_update_kernel<FT, NK, MOVE, 2, BS, MINB><<<g, BS, 0, s>>>(a);
-    else cell_update_kernel<FT, NK, MOVE, 3, BS, MINB><<<g, BS, 0, s>>>(a);
+
+
+// One face record (9 + NK fluxes times area, padded to 16 bytes) added into PO
+// with the face's sign: from global memory through the read-only path, or from
+// shared memory where the staged update put it.
+template <int NK>
+__device__ __forceinline__ void add_record_global(const double* src, double sign, double* PO) {
+    constexpr int S = FluxLayout<double, NK>::stride;
+    double v[S];
+#pragma unroll
+    for (int k = 0; k < S; k += 2) {
+        const double2 t = __ldg(reinterpret_cast<const double2*>(src) + k / 2);
+        v[k] = t.x;
+        v[k + 1] = t.y;
+    }
+#pragma unroll
+    for (int k = 0; k < 9 + NK; ++k) PO[k] += sign * v[k];
 }
 
-template <typename FT, int NK, bool MOVE>
-static cudaError_t cell_update_variant(const CellArgs& a, int src, int v, cudaStream_t s) {
+template <int NK>
+__device__ __forceinline__ void add_record_shared(const double* src, double sign, double* PO) {
+    constexpr int S = FluxLayout<double, NK>::stride;
+    double v[S];
+#pragma unroll
+    for (int k = 0; k < S; k += 2) {
+        const double2 t = reinterpret_cast<const double2*>(src)[k / 2];
+        v[k] = t.x;
+        v[k + 1] = t.y;
+    }
+#pragma unroll
+    for (int k = 0; k < 9 + NK; ++k) PO[k] += sign * v[k];
+}
+
+// One thread per cell; each record is read from global memory where it is
+// needed (two dependent loads per face: the face id, then the record).
+template <int NK, bool MOVE, int SRC, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) cell_update_kernel(CellArgs a) {
+    const int c = blockIdx.x * BS + threadIdx.x;
+    if (c < a.M.ncell && a.st->err_kind == 0) {
+        update_cell<NK, MOVE, SRC>(a, c, [&](double* PO) {
+            constexpr int S = FluxLayout<double, NK>::stride;
+            const double* fx = static_cast<const double*>(a.flux);
+            const int nc = a.M.ncell;
+#pragma unroll
+            for (int k = 0; k < 9 + NK; ++k) PO[k] = 0.0;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                const int fs = a.M.cell_faces[s * nc + c];
+                add_record_global<NK>(fx + size_t(fs & 0x7fffffff) * S, fs < 0 ? -1.0 : 1.0, PO);
+            }
+        });
+    }
+    roll_clock(a);
+}
+
+// Shared memory of the staged update: an mbarrier, then the records of the
+// faces the block's cells own (cells[0] in the block), at most `cap` of them
+// (4.25 per cell; the renumbered shells need at most 4.2), then OV slots per
+// thread for records of the cell's other faces.
+template <int NK, int BS, int OV>
+struct StagedSmem {
+    static constexpr int S = FluxLayout<double, NK>::stride;
+    static constexpr int cap = (17 * BS) / 4;
+    static constexpr size_t bytes = 16 + sizeof(double) * S * (size_t(cap) + size_t(OV) * BS);
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Sleeping wait on phase 0 of an mbarrier: try_wait with a 100 us suspend
+// hint, at most ~1 s (globaltimer) and 2^14 calls; false when it ran out.
+__device__ __forceinline__ bool stage_wait(uint32_t mbar) {
+    uint64_t t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (int it = 0; it < (1 << 14); ++it) {
+        uint32_t done = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0, %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(100000u)
+            : "memory");
+        if (done) return true;
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > 1000000000ull) return false;
+    }
+    return false;
+}
+
+// The block's wait for its staged records. A wait that runs out records
+// error kind 21 (the step then reports TITAN_ETIMEOUT) and waits once more,
+// so the block does not leave while its copy may still be writing.
+__device__ __forceinline__ void stage_wait_or_flag(uint32_t mbar, DevStatus* st, int index) {
+    if (!stage_wait(mbar)) {
+        record_error(st, 21, index);
+        stage_wait(mbar);
+    }
+}
+
+// The cell update with its face records staged in shared memory. Faces are
+// sorted by cells[0], so the faces owned by the block's cells are one
+// contiguous run of records: one elected thread copies it with a single bulk
+// TMA copy (cp.async.bulk, completion counted on an mbarrier) while every
+// thread gathers its cell's nodes, state and face ids. A record outside that
+// run (a face whose owner is in another block, about one per cell on the
+// shells) is copied by its thread with cp.async into its own slots, up to OV
+// of them; any beyond are read from global memory. The sums run in the cell's
+// own face order, as in cell_update_kernel, so results are identical.
+template <int NK, bool MOVE, int SRC, int BS, int MINB, int OV>
+__global__ void __launch_bounds__(BS, MINB) cell_update_staged_kernel(CellArgs a) {
+    using SM = StagedSmem<NK, BS, OV>;
+    constexpr int S = SM::S;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int go_s;
+    double* stage = reinterpret_cast<double*>(smem + 16);
+    double* ov = stage + size_t(SM::cap) * S;
+    const uint32_t mbar = smem_addr(smem);
+    const int nc = a.M.ncell;
+    const int tid = threadIdx.x;
+    const int cb = blockIdx.x * BS;
+    const int c = cb + tid;
+    const int nchunk = (nc + 31) >> 5;
+    const int fb = a.owner_start[cb >> 5];
+    const int fe = a.owner_start[min((cb + BS) >> 5, nchunk)];
+    const int nstage = min(fe - fb, SM::cap);
+    const double* fx = static_cast<const double*>(a.flux);
+    if (tid == 0) {
+        const int go = a.st->err_kind == 0;
+        go_s = go;
+        if (go && nstage > 0) {
+            const uint32_t bytes = uint32_t(nstage) * S * sizeof(double);
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile(
+                "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(mbar),
+                "r"(bytes)
+                : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(stage)),
+                "l"(fx + size_t(fb) * S), "r"(bytes), "r"(mbar)
+                : "memory");
+        }
+    }
+    __syncthreads();
+    const bool go = go_s != 0;
+    const bool staged = go && nstage > 0;
+    if (c < nc && go) {
+        int fs[6];
+#pragma unroll
+        for (int s = 0; s < 6; ++s) fs[s] = a.M.cell_faces[s * nc + c];
+        {
+            int k = 0;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                const int f = fs[s] & 0x7fffffff;
+                if ((unsigned)(f - fb) >= (unsigned)nstage && k < OV) {
+                    const uint32_t dst = smem_addr(ov + size_t(k * BS + tid) * S);
+                    const double* src = fx + size_t(f) * S;
+#pragma unroll
+                    for (int j = 0; j < S; j += 2)
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 8u * j), "l"(src + j)
+                                     : "memory");
+                    ++k;
+                }
+            }
+        }
+        update_cell<NK, MOVE, SRC>(a, c, [&](double* PO) {
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            if (staged) stage_wait_or_flag(mbar, a.st, cb);
+#pragma unroll
+            for (int k = 0; k < 9 + NK; ++k) PO[k] = 0.0;
+            int k = 0;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                const int f = fs[s] & 0x7fffffff;
+                const double sign = fs[s] < 0 ? -1.0 : 1.0;
+                if ((unsigned)(f - fb) < (unsigned)nstage) {
+                    add_record_shared<NK>(stage + size_t(f - fb) * S, sign, PO);
+                } else if (k < OV) {
+                    add_record_shared<NK>(ov + size_t(k * BS + tid) * S, sign, PO);
+                    ++k;
+                } else {
+                    add_record_global<NK>(fx + size_t(f) * S, sign, PO);
+                }
+            }
+        });
+    } else if (staged) {
+        stage_wait_or_flag(mbar, a.st, cb);
+    }
+    roll_clock(a);
+}
+
+template <int NK, bool MOVE, int SRC, int BS, int MINB>
+static cudaError_t plain_launch(const CellArgs* a, cudaStream_t s) {
+    if (!a) return cudaSuccess;
+    cell_update_kernel<NK, MOVE, SRC, BS, MINB><<<blocks_for(a->M.ncell, BS), BS, 0, s>>>(*a);
+    return cudaGetLastError();
+}
+
+// The staged kernels need more than 48 KB of dynamic shared memory: with a
+// null `a` this sets the attribute on the current device (cell_update_prepare,
+// called when a context is created, so never while a stream is captured).
+template <int NK, bool MOVE, int SRC, int BS, int MINB, int OV>
+static cudaError_t staged_launch(const CellArgs* a, cudaStream_t s) {
+    constexpr int bytes = (int)StagedSmem<NK, BS, OV>::bytes;
+    if (!a)
+        return cudaFuncSetAttribute(cell_update_staged_kernel<NK, MOVE, SRC, BS, MINB, OV>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (!a->owner_start) return cudaErrorInvalidValue;
+    cell_update_staged_kernel<NK, MOVE, SRC, BS, MINB, OV><<<blocks_for(a->M.ncell, BS), BS, bytes, s>>>(*a);
+    return cudaGetLastError();
+}
+
+template <int NK, bool MOVE, int BS, int MINB, int OV>
+static cudaError_t variant_src(const CellArgs* a, int src, cudaStream_t s) {
+    if constexpr (OV == 0) {
+        if (src == 0) return plain_launch<NK, MOVE, 0, BS, MINB>(a, s);
+        if (src == 1) return plain_launch<NK, MOVE, 1, BS, MINB>(a, s);
+        if (src == 2) return plain_launch<NK, MOVE, 2, BS, MINB>(a, s);
+        return plain_launch<NK, MOVE, 3, BS, MINB>(a, s);
+    } else {
+        if (src == 0) return staged_launch<NK, MOVE, 0, BS, MINB, OV>(a, s);
+        if (src == 1) return staged_launch<NK, MOVE, 1, BS, MINB, OV>(a, s);
+        if (src == 2) return staged_launch<NK, MOVE, 2, BS, MINB, OV>(a, s);
+        return staged_launch<NK, MOVE, 3, BS, MINB, OV>(a, s);
+    }
+}
+
+template <int NK, bool MOVE>
+static cudaError_t cell_update_variant(const CellArgs* a, int src, int v, cudaStream_t s) {
     switch (v) {
-#define TITAN_CELL_CASE(i)                                                                   \
-    case i:                                                                                \
-        cell_update_src<FT, NK, MOVE, kCellVariant[i].block, kCellVariant[i].min_blocks>(a, src, s); \
-        break;
+#define TITAN_CELL_CASE(i)                                                                                   \
+    case i:                                                                                                  \
+        return variant_src<NK, MOVE, kCellVariant[i].block, kCellVariant[i].min_blocks, kCellVariant[i].overflow>( \
+            a, src, s);
         TITAN_CELL_CASE(0)
         TITAN_CELL_CASE(1)
         TITAN_CELL_CASE(2)
         TITAN_CELL_CASE(3)
         TITAN_CELL_CASE(4)
         TITAN_CELL_CASE(5)
+        TITAN_CELL_CASE(6)
+        TITAN_CELL_CASE(7)
+        TITAN_CELL_CASE(8)
 #undef TITAN_CELL_CASE
         default:
             return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
+}
+
+static cudaError_t cell_update_dispatch(const CellArgs* a, int nk, bool move, int src, int variant, cudaStream_t s) {
+    if (nk == 0 && !move) return cell_update_variant<0, false>(a, src, variant, s);
+    if (nk == 0 && move) return cell_update_variant<0, true>(a, src, variant, s);
+    if (nk == 2 && !move) return cell_update_variant<2, false>(a, src, variant, s);
+    if (nk == 2 && move) return cell_update_variant<2, true>(a, src, variant, s);
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_cell_update(const CellArgs& a, int nk, bool move, int src, int variant, cudaStream_t s) {
-    if (nk == 0 && !move) return cell_update_variant<double, 0, false>(a, src, variant, s);
-    if (nk == 0 && move) return cell_update_variant<double, 0, true>(a, src, variant, s);
-    if (nk == 2 && !move) return cell_update_variant<double, 2, false>(a, src, variant, s);
-    if (nk == 2 && move) return cell_update_variant<double, 2, true>(a, src, variant, s);
-    return cudaErrorInvalidValue;
+    return cell_update_dispatch(&a, nk, move, src, variant, s);
+}
+
+cudaError_t cell_update_prepare() {
+    for (int nk = 0; nk <= 2; nk += 2)
+        for (int move = 0; move <= 1; ++move)
+            for (int src = 0; src <= 3; ++src)
+                for (int v = 0; v < kCellVariants; ++v) {
+                    const cudaError_t e = cell_update_dispatch(nullptr, nk, move != 0, src, v, nullptr);
+                    if (e) return e;
+                }
+    return cudaSuccess;
 }
 
 }  // namespace titan

@@ -103,6 +103,11 @@ struct CellArgs {
     const double* src;     // [4][ncell] external sources (m_x, m_y, m_z, E)
     ClosureCell cl;        // source mode 3: the learned closure
     DevStatus* st;
+    // [ceil(ncell / 32) + 1]: the first face whose cells[0] is >= 32 k (faces
+    // sorted by cells[0], as the renumbering leaves them), so the faces owned
+    // by a block of cells are one contiguous range of records; null when the
+    // faces are not in that order (the staged launch shapes need it)
+    const int* owner_start = nullptr;
 };
 
 }  // namespace titan

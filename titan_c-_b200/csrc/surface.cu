@@ -15,7 +15,8 @@
 //     x' = x + (V . x/|x|) dt x/|x| (:1213-1265).
 //  3. One thread per ray node: every node between two anchors (the ray's ends
 //     and its surface nodes) keeps its initial fraction of that segment, on
-//     the ray's direction.
+//     the ray's direction; or, with the A_Luch law (Luch.cpp:9-152), takes the
+//     radius that law gives it from the ray's TS, HP and BS radii.
 // With smoothing on, a node's mean also takes one smoothing term (sglag_*): toward
 // the sphere fitted through it and its neighbours (TS, HP) or toward the mean of
 // them (BS).
@@ -182,11 +183,90 @@ __global__ void node_kernel(FaceArgs a, SurfaceDev S) {
     for (int k = 0; k < 3; ++k) x2[k * nn + id] = A[k] + vb * time * B[k];
 }
 
+__device__ __forceinline__ double sq(double x) { return x * x; }
+
+// Radius of slot j of a ray under the A_Luch law, from the current radii R2,
+// R3, R4 of its TS, HP and BS nodes, with the reference's expressions
+// (Luch.cpp:17-152); false for the slots the law leaves where they are (the
+// R1 node and the three surface nodes).
+__device__ bool a_luch_radius(const RayLaw& g, int j, double R2, double R3, double R4, double* r) {
+    const int M0 = g.M0, M1 = g.M1, M11 = g.M11, M2 = g.M2, M3 = g.M3, M4 = g.M4;
+    const double R0 = g.R0, R1 = g.R1, R5 = g.R5;
+    if (j < M0) {
+        *r = R0 + j * (R1 - R0) / M0;
+        return true;
+    }
+    int num = M0 + 1;
+    if (j < num) return false;
+    if (j < num + M1) {
+        *r = R1 + (j - num + 1) * (R2 - R1) / (M1 + 1);
+        return true;
+    }
+    num += M1 + 1;
+    if (j < num) return false;
+    const double dr = (R2 - R1) / (M1 + 1);
+    if (j < num + M11) {
+        *r = R2 + dr * (j - num + 1);
+        return true;
+    }
+    num += M11;
+    if (j < num + (M2 - M11)) {
+        const double a = g.da1, b = g.da2;
+        const double s = (j - num + 1.0) / (M2 - M11 + 1.0);
+        const double ss = s * (a * sq(1.0 - 3.0 * s + 2.0 * sq(s)) +
+                               s * (7.0 + b * sq(1.0 - 2.0 * s) * (-1.0 + s) -
+                                    2.0 * s * (9.0 + 2.0 * s * (-5.0 + 2.0 * s))));
+        *r = R2 + dr * M11 + (R3 - R2 - dr * M11) * ss;
+        return true;
+    }
+    num += (M2 - M11) + 1;
+    if (j < num) return false;
+    if (j < num + M3) {
+        const double a = g.da3, b = g.da4;
+        const double s = (j - num + 1.0) / (M3 + 1.0);
+        const double ss = s * (a - (2.0 * a + b - 3.0) * s + (a + b - 2.0) * s * s);
+        *r = R3 + (R4 - R3) * ss;
+        return true;
+    }
+    num += M3 + 1;
+    if (j < num) return false;
+    if (j < num + M4) {
+        const double a = g.da5, b = 2.0;
+        const double s = (j - num + 1.0) / (M4 + 1.0);
+        const double ss = a * s - (3.0 * a + b - 4.0) * s * s * s + (2.0 * a + b - 3.0) * s * s * s * s;
+        *r = R4 + (R5 - R4) * ss;
+        return true;
+    }
+    *r = R5;
+    return true;
+}
+
+__device__ __forceinline__ double node_radius(const double* xyz, int nn, int id) {
+    double x[3];
+    load_node(xyz, nn, id, x);
+    return sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+}
+
 // One thread per ray slot: a node that is not an anchor takes its place
-// between the anchors around it (ray_seg: their slots, set up once).
+// between the anchors around it (ray_seg: their slots, set up once), or, with
+// the A_Luch law, the place the law gives it from the ray's surface nodes.
 __global__ void ray_kernel(FaceArgs a, SurfaceDev S) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= (long long)S.nray * S.ray_len || a.st->err_kind != 0) return;
+    if (S.law.on) {
+        const int L = S.ray_len, nn = a.M.nnode;
+        const int r = (int)(q / L), j = (int)(q % L);
+        const int* rn = S.ray_nodes + (long long)r * L;
+        const double R2 = node_radius(a.xyz2, nn, rn[S.law.ts_slot()]);
+        const double R3 = node_radius(a.xyz2, nn, rn[S.law.hp_slot()]);
+        const double R4 = node_radius(a.xyz2, nn, rn[S.law.bs_slot()]);
+        double rj;
+        if (!a_luch_radius(S.law, j, R2, R3, R4, &rj)) return;
+        double* x2 = const_cast<double*>(a.xyz2);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) x2[k * nn + rn[j]] = rj * S.ray_dir[3 * r + k];
+        return;
+    }
     const int2 seg = S.ray_seg[q];
     if (seg.x < 0) return;  // an anchor
     const int nn = a.M.nnode, L = S.ray_len;

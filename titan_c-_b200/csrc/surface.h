@@ -8,6 +8,21 @@
 
 namespace titan {
 
+// The A_Luch spacing law of Luch::dvigenie (TITAN/source/Luch.cpp:9-152):
+// node counts and radii of Geo_param (Geo_param.h:22-63). A ray then has
+// M0 + M1 + M2 + M3 + M4 + 5 nodes: M0 fixed from R0, the R1 node, M1 up to
+// the TS node, M11 at the step before the TS, M2 - M11 to the HP node, M3 to
+// the BS node, M4 to the outer end at R5.
+struct RayLaw {
+    int on;
+    int M0, M1, M11, M2, M3, M4;
+    double R0, R1, R5, da1, da2, da3, da4, da5;
+    __host__ __device__ int ts_slot() const { return M0 + M1 + 1; }
+    __host__ __device__ int hp_slot() const { return M0 + M1 + M2 + 2; }
+    __host__ __device__ int bs_slot() const { return M0 + M1 + M2 + M3 + 3; }
+    __host__ __device__ int length() const { return M0 + M1 + M2 + M3 + M4 + 5; }
+};
+
 struct SurfaceDev {
     // moving surface faces, grouped by surface (1 TS, 2 HP, 3 BS): positions
     // off[s] .. off[s+1]-1 of face_list hold surface s's faces (device ids)
@@ -28,6 +43,7 @@ struct SurfaceDev {
     const double* ray_r0;
     const double* ray_dir;  // [nray][3]
     const int2* ray_seg;    // [nray][ray_len]: slots of the anchors around a node, (-1, -1) for an anchor
+    RayLaw law;             // law.on: the A_Luch law places the ray's other nodes instead
     double vel[4];          // velocity_TS / _HP / _BS at [1] / [2] / [3]
     int null_bn_on_hp;
     // smoothing of each moving node (the reference's sglag_* terms): 0 none,

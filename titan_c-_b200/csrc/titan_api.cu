@@ -84,6 +84,7 @@ struct titan_ctx {
     int8_t *d_face_type = nullptr, *d_face_surf = nullptr, *d_face_method = nullptr;
     double* d_bc_vals = nullptr;
     int32_t *d_cell_faces = nullptr, *d_cell_nodes = nullptr;
+    int32_t* d_owner_start = nullptr;  // [ceil(ncell/32)+1] first face owned by each 32-cell chunk
     int8_t* d_cell_type = nullptr;
     uint8_t* d_cell_tvd = nullptr;
     double *d_node_amp = nullptr, *d_node_phase = nullptr;
@@ -130,6 +131,8 @@ struct titan_ctx {
     // surface-tracking node motion (titan_set_surface_motion)
     bool use_surface = false;
     SurfaceDev surf{};
+    std::vector<int32_t> h_ray_nodes;  // the rays of surf (device node ids, -1 padding)
+    std::vector<int8_t> h_node_surf;   // per device node: the surface (1 TS, 2 HP, 3 BS) it lies on, or 0
     void* surf_buf[14] = {};  // face_list, vf, node_id, node_ptr, node_face, ray_nodes, ray_r0, ray_dir, ray_seg,
                               // sm_kind, sm_coef, sm_centre, nb_ptr, nb_id
 
@@ -305,6 +308,7 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     ca.src = ctx->d_src;
     ca.cl = closure_cell(ctx);
     ca.st = ctx->d_status;
+    ca.owner_start = ctx->d_owner_start;
     const int src = step_source_mode(ctx);
     e = timed(ctx, "cell_update",
               [&] { return launch_cell_update(ca, nk, move, src, ctx->cell_variant, ctx->stream); });
@@ -541,7 +545,7 @@ int titan_destroy(titan_ctx* ctx) {
                     ctx->d_node_phase, ctx->d_state[0], ctx->d_state[1], ctx->d_flux, ctx->d_hfl, ctx->d_src,
                     ctx->d_stage, ctx->d_status, ctx->d_cell_fmap, ctx->d_face_aa, ctx->d_face_bb,
                     ctx->d_env, ctx->d_fallback, ctx->d_n_outside, ctx->d_mc_cells, ctx->d_mc_cdf,
-                    ctx->d_mc_blocks, ctx->d_mc_tally, ctx->d_mc_lost};
+                    ctx->d_mc_blocks, ctx->d_mc_tally, ctx->d_mc_lost, ctx->d_owner_start};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (void* p : ctx->surf_buf)
@@ -622,6 +626,9 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
         if (e) return bail(fail(TITAN_ECUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(e)));
     }
 
+    e = cell_update_prepare();
+    if (e) return bail(fail(TITAN_ECUDA, std::string("cell update kernels: ") + cudaGetErrorString(e)));
+
     // --- renumbering and remapped host arrays ---
     ctx->R = sfc_renumber(m->nnode, m->ncell, m->nface, m->node_xyz, m->cell_nodes, m->face_cells);
     const Renumbering& R = ctx->R;
@@ -638,6 +645,18 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
         face_method[f] = m->face_surf[o] != TITAN_SURF_US ? TITAN_HLLD : TITAN_LAX;  // Gran::Get_method
         face_bc[f] = m->face_bc[o];
         for (int k = 0; k < 4; ++k) face_nodes[k * nf + f] = R.node_o2n[m->face_nodes[4 * o + k]];
+    }
+    // The renumbering sorts faces by cells[0]: the first face owned by each
+    // 32-cell chunk, for the staged cell update (empty if the order did not hold)
+    std::vector<int32_t> owner_start;
+    if (std::is_sorted(face_c0.begin(), face_c0.end())) {
+        const int64_t nchunk = (nc + 31) / 32;
+        owner_start.resize(nchunk + 1);
+        int64_t f = 0;
+        for (int64_t k = 0; k <= nchunk; ++k) {
+            while (f < nf && face_c0[f] < 32 * k) ++f;
+            owner_start[k] = (int32_t)f;
+        }
     }
     std::vector<int32_t> cell_faces(6 * nc), cell_nodes(8 * nc);
     std::vector<int8_t> cell_type(nc);
@@ -714,6 +733,7 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     DA(ctx->d_face_method, nf);
     DA(ctx->d_bc_vals, bc.size());
     DA(ctx->d_cell_faces, 6 * nc);
+    if (!owner_start.empty()) DA(ctx->d_owner_start, owner_start.size());
     DA(ctx->d_cell_nodes, 8 * nc);
     DA(ctx->d_cell_type, nc);
     DA(ctx->d_cell_tvd, nc);
@@ -773,6 +793,7 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     put(ctx->d_face_method, face_method);
     put(ctx->d_bc_vals, bc);
     put(ctx->d_cell_faces, cell_faces);
+    if (!owner_start.empty()) put(ctx->d_owner_start, owner_start);
     put(ctx->d_cell_nodes, cell_nodes);
     put(ctx->d_cell_type, cell_type);
     put(ctx->d_cell_tvd, cell_tvd);
@@ -1017,7 +1038,8 @@ int finish_steps(titan_ctx* ctx, double* dt_out, double* t_out, titan_step_info*
     if (dt_out) *dt_out = st.dt;
     if (t_out) *t_out = st.t;
     int status = TITAN_OK;
-    if (st.err_kind != 0) status = st.err_kind >= 20 ? TITAN_ENONFINITE : TITAN_ESOLVER;
+    if (st.err_kind != 0)
+        status = st.err_kind == 21 ? TITAN_ETIMEOUT : st.err_kind >= 20 ? TITAN_ENONFINITE : TITAN_ESOLVER;
     if (ctx->use_closure) {
         int cerr = 0;
         CK(cudaMemcpy(&cerr, ctx->closure.error, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1032,7 +1054,7 @@ int finish_steps(titan_ctx* ctx, double* dt_out, double* t_out, titan_step_info*
         info->err_index = -1;
         if (st.err_kind != 0) {
             const int idx = st.err_index;
-            if (st.err_kind >= 20)
+            if (st.err_kind >= 20)  // a cell (20) or the first cell of a block (21)
                 info->err_index = (idx >= 0 && idx < ctx->ncell) ? ctx->R.cell_n2o[idx] : -1;
             else
                 info->err_index = (idx >= 0 && idx < ctx->nface) ? ctx->R.face_n2o[idx] : -1;
@@ -1651,6 +1673,57 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     S.nb_id = (const int*)ctx->surf_buf[13];
     ctx->surf = S;
     ctx->use_surface = true;
+    ctx->h_ray_nodes = std::move(rn);
+    ctx->h_node_surf = std::move(node_surf);
+    return TITAN_OK;
+}
+
+int titan_set_ray_law(titan_ctx* ctx, const titan_ray_law* law) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    if (!ctx->use_surface) return fail(TITAN_EINVAL, "the ray law needs titan_set_surface_motion first");
+    drop_graph(ctx);
+    if (!law) {
+        ctx->surf.law = RayLaw{};
+        return TITAN_OK;
+    }
+    RayLaw g{};
+    g.on = 1;
+    g.M0 = law->M0;
+    g.M1 = law->M1;
+    g.M11 = law->M11;
+    g.M2 = law->M2;
+    g.M3 = law->M3;
+    g.M4 = law->M4;
+    g.R0 = law->R0;
+    g.R1 = law->R1;
+    g.R5 = law->R5;
+    g.da1 = law->da1;
+    g.da2 = law->da2;
+    g.da3 = law->da3;
+    g.da4 = law->da4;
+    g.da5 = law->da5;
+    if (g.M0 < 1 || g.M1 < 0 || g.M11 < 0 || g.M2 < g.M11 || g.M3 < 0 || g.M4 < 0)
+        return fail(TITAN_EINVAL, "ray law: M0 >= 1, M1, M3, M4 >= 0 and 0 <= M11 <= M2");
+    const double v[] = {g.R0, g.R1, g.R5, g.da1, g.da2, g.da3, g.da4, g.da5};
+    for (double x : v)
+        if (!std::isfinite(x)) return fail(TITAN_EINVAL, "ray law: radii and da1..da5 must be finite");
+    const int L = ctx->surf.ray_len;
+    if (g.length() != L)
+        return fail(TITAN_EINVAL, "ray law: every ray needs M0 + M1 + M2 + M3 + M4 + 5 nodes");
+    const int slot[3] = {g.ts_slot(), g.hp_slot(), g.bs_slot()};
+    for (int64_t r = 0; r < ctx->surf.nray; ++r)
+        for (int k = 0; k < 3; ++k) {
+            const int32_t d = ctx->h_ray_nodes[r * L + slot[k]];
+            if (d < 0 || ctx->h_ray_nodes[r * L + L - 1] < 0)
+                return fail(TITAN_EINVAL, "ray law: a ray is shorter than the law's length");
+            if (ctx->h_node_surf[d] != k + 1) {
+                char buf[160];
+                snprintf(buf, sizeof buf, "ray law: node %d of ray %lld is not on the %s surface", slot[k],
+                         (long long)r, k == 0 ? "TS" : k == 1 ? "HP" : "BS");
+                return fail(TITAN_EINVAL, buf);
+            }
+        }
+    ctx->surf.law = g;
     return TITAN_OK;
 }
 
@@ -1658,6 +1731,8 @@ int titan_set_tuning(titan_ctx* ctx, int32_t face_variant, int32_t cell_variant)
     if (!ctx) return fail(TITAN_EINVAL, "null argument");
     if (face_variant < 0 || face_variant >= kFaceVariants || cell_variant < 0 || cell_variant >= kCellVariants)
         return fail(TITAN_EINVAL, "variant out of range");
+    if (kCellVariant[cell_variant].overflow > 0 && !ctx->d_owner_start)
+        return fail(TITAN_EINVAL, "staged cell update needs the faces sorted by cells[0]");
     ctx->face_variant = face_variant;
     ctx->cell_variant = cell_variant;
     drop_graph(ctx);
@@ -1732,6 +1807,7 @@ int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     ca.src = ctx->d_src;
     ca.cl = closure_cell(ctx);
     ca.st = ctx->d_status;
+    ca.owner_start = ctx->d_owner_start;
     const int nk = ctx->prm.npassive;
     // the timed cell updates write the closure's next inputs from a state the
     // context does not keep: they are formed again before the next step
@@ -1759,6 +1835,8 @@ int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path) {
     }
     best = 1e30f;
     for (int v = 0; v < kCellVariants; ++v) {
+        cms[v] = 1e30f;
+        if (kCellVariant[v].overflow > 0 && !ctx->d_owner_start) continue;
         CK(time_it([&] { return launch_cell_update(ca, nk, move, src, v, s); }, &cms[v]));
         if (cms[v] < best) {
             best = cms[v];

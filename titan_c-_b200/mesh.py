@@ -91,15 +91,22 @@ def _finish(node_xyz, cell_nodes, face_nodes, face_cells, cell_faces):
 
 def cube_mesh(n: int, length: float = 1.0) -> dict:
     """Unit cube of n^3 hexahedra on [0, length]^3; every boundary face Outer_Soft."""
-    m = n + 1
-    g = np.arange(m, dtype=np.float64) * (length / n)
-    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    return box_mesh(n, n, n, (length, length, length))
+
+
+def box_mesh(nx: int, ny: int, nz: int, lengths=(1.0, 1.0, 1.0)) -> dict:
+    """Box of nx x ny x nz hexahedra on [0, lx] x [0, ly] x [0, lz]; every
+    boundary face Outer_Soft."""
+    gx = np.arange(nx + 1, dtype=np.float64) * (lengths[0] / nx)
+    gy = np.arange(ny + 1, dtype=np.float64) * (lengths[1] / ny)
+    gz = np.arange(nz + 1, dtype=np.float64) * (lengths[2] / nz)
+    X, Y, Z = np.meshgrid(gx, gy, gz, indexing="ij")
     node_xyz = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
 
     def nid(i, j, k):
-        return (i * m + j) * m + k
+        return (i * (ny + 1) + j) * (nz + 1) + k
 
-    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
     i, j, k = i.ravel(), j.ravel(), k.ravel()
     cell_nodes = np.stack([nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k),
                            nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)],
@@ -148,8 +155,10 @@ def cubed_sphere_directions(nq: int):
     return dirs, np.concatenate(quads, axis=0)
 
 
-def shell_mesh(nq: int, nlayer: int, r0: float = 1.0, r1: float = 100.0, outer_hard_x: float = 0.0) -> dict:
-    """Spherical shell of 6 nq^2 x nlayer hexahedra with geometric radial spacing.
+def shell_mesh(nq: int, nlayer: int, r0: float = 1.0, r1: float = 100.0, outer_hard_x: float = 0.0,
+               radii: np.ndarray | None = None) -> dict:
+    """Spherical shell of 6 nq^2 x nlayer hexahedra with geometric radial spacing
+    (or the nlayer + 1 node radii `radii`, from the inner sphere outwards).
 
     Inner sphere faces are Inner_Hard, outer faces Outer_Hard where the face
     centre has x > outer_hard_x (the inflow side) and Outer_Soft elsewhere —
@@ -157,7 +166,11 @@ def shell_mesh(nq: int, nlayer: int, r0: float = 1.0, r1: float = 100.0, outer_h
     Returns the mesh plus `node_layer` and `node_ray` (per-node indices)."""
     dirs, quads = cubed_sphere_directions(nq)
     ns = dirs.shape[0]
-    radii = r0 * (r1 / r0) ** (np.arange(nlayer + 1) / nlayer)
+    if radii is None:
+        radii = r0 * (r1 / r0) ** (np.arange(nlayer + 1) / nlayer)
+    radii = np.asarray(radii, dtype=np.float64)
+    assert radii.shape == (nlayer + 1,) and np.all(np.diff(radii) > 0)
+    r0 = radii[0]
     node_xyz = (radii[:, None, None] * dirs[None, :, :]).reshape(-1, 3)
     nq_ = quads.shape[0]
     lay = np.arange(nlayer)
@@ -178,6 +191,37 @@ def shell_mesh(nq: int, nlayer: int, r0: float = 1.0, r1: float = 100.0, outer_h
     mesh["cell_layer"] = np.repeat(lay, nq_)
     mesh["radii"] = radii
     return mesh
+
+
+def a_luch_radii(law: dict, R2: float, R3: float, R4: float) -> np.ndarray:
+    """Node radii along a ray under the A_Luch law of Luch::dvigenie
+    (TITAN/source/Luch.cpp:9-152) with the TS, HP and BS at R2, R3, R4: the
+    M0 + M1 + M2 + M3 + M4 + 5 radii from R0 to R5 (Geo_param's M0..M4, R0,
+    R1, R5, da1..da5 in `law`), for building a mesh the law leaves in place."""
+    M0, M1, M11, M2, M3, M4 = (int(law[k]) for k in ("M0", "M1", "M11", "M2", "M3", "M4"))
+    R0, R1, R5 = law["R0"], law["R1"], law["R5"]
+    out = [R0 + j * (R1 - R0) / M0 for j in range(M0)] + [R1]
+    out += [R1 + (j + 1) * (R2 - R1) / (M1 + 1) for j in range(M1)] + [R2]
+    dr = (R2 - R1) / (M1 + 1)
+    out += [R2 + dr * (j + 1) for j in range(M11)]
+    a, b = law["da1"], law["da2"]
+    for j in range(M2 - M11):
+        s = (j + 1.0) / (M2 - M11 + 1.0)
+        ss = s * (a * (1.0 - 3.0 * s + 2.0 * s * s) ** 2 +
+                  s * (7.0 + b * (1.0 - 2.0 * s) ** 2 * (-1.0 + s) - 2.0 * s * (9.0 + 2.0 * s * (-5.0 + 2.0 * s))))
+        out.append(R2 + dr * M11 + (R3 - R2 - dr * M11) * ss)
+    out.append(R3)
+    a, b = law["da3"], law["da4"]
+    for j in range(M3):
+        s = (j + 1.0) / (M3 + 1.0)
+        out.append(R3 + (R4 - R3) * s * (a - (2.0 * a + b - 3.0) * s + (a + b - 2.0) * s * s))
+    out.append(R4)
+    a, b = law["da5"], 2.0
+    for j in range(M4):
+        s = (j + 1.0) / (M4 + 1.0)
+        out.append(R4 + (R5 - R4) * (a * s - (3.0 * a + b - 4.0) * s ** 3 + (2.0 * a + b - 3.0) * s ** 4))
+    out.append(R5)
+    return np.array(out)
 
 
 def shell_rays(mesh: dict) -> np.ndarray:

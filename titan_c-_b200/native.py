@@ -71,6 +71,14 @@ class TitanSurfaceParams(ctypes.Structure):
                 ("sglag_HP_k_sphere", ctypes.c_double), ("sglag_BS_k", ctypes.c_double)]
 
 
+class TitanRayLaw(ctypes.Structure):
+    _fields_ = [("M0", ctypes.c_int32), ("M1", ctypes.c_int32), ("M11", ctypes.c_int32), ("M2", ctypes.c_int32),
+                ("M3", ctypes.c_int32), ("M4", ctypes.c_int32), ("pad", ctypes.c_int32 * 2),
+                ("R0", ctypes.c_double), ("R1", ctypes.c_double), ("R5", ctypes.c_double),
+                ("da1", ctypes.c_double), ("da2", ctypes.c_double), ("da3", ctypes.c_double),
+                ("da4", ctypes.c_double), ("da5", ctypes.c_double)]
+
+
 class TitanMcParams(ctypes.Structure):
     _fields_ = [("n_H", ctypes.c_double), ("u_H", ctypes.c_double * 3), ("cp_H", ctypes.c_double),
                 ("n_particles", ctypes.c_int64), ("seed", ctypes.c_uint64), ("max_cells", ctypes.c_int32),
@@ -109,6 +117,7 @@ SIGNATURES = {
     "titan_set_face_method": ([ctypes.c_void_p, I8], ctypes.c_int),
     "titan_set_surface_motion": ([ctypes.c_void_p, ctypes.POINTER(TitanSurfaceParams), ctypes.c_int64,
                                   ctypes.c_int32, I32], ctypes.c_int),
+    "titan_set_ray_law": ([ctypes.c_void_p, ctypes.POINTER(TitanRayLaw)], ctypes.c_int),
     "titan_upload_state": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_download_state": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_upload_hfluids": ([ctypes.c_void_p, D], ctypes.c_int),

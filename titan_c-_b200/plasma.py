@@ -109,6 +109,19 @@ class PlasmaStep:
         N.check(self._lib.titan_set_surface_motion(self._ctx, ctypes.byref(sp), r.shape[0], r.shape[1],
                                                    N.ptr(r, N.I32)))
 
+    def set_ray_law(self, law: dict | None):
+        """The A_Luch spacing law for the rays of set_surface_motion
+        (titan_set_ray_law): M0, M1, M11, M2, M3, M4, R0, R1, R5, da1..da5;
+        None returns to the fraction rule."""
+        if law is None:
+            N.check(self._lib.titan_set_ray_law(self._ctx, None))
+            return
+        g = N.TitanRayLaw()
+        for k, _ in N.TitanRayLaw._fields_:
+            if k != "pad":
+                setattr(g, k, law[k])
+        N.check(self._lib.titan_set_ray_law(self._ctx, ctypes.byref(g)))
+
     def set_halo(self, send_ids: np.ndarray, recv_ids: np.ndarray):
         """Cells this context sends to / receives from its peers in a sharded step (titan_set_halo)."""
         s = np.ascontiguousarray(send_ids, dtype=np.int32)

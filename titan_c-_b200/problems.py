@@ -84,9 +84,11 @@ def _lism(n: int, rho=0.06, u=2.6, mach=2.0, b=0.3, angle_deg=60.0, gamma=GAMMA)
 
 def heliosphere_shell(nq: int = 96, nlayer: int = 40, seed: int = 20261203, move: bool = True,
                       zones: bool = False, npassive: int = 0, nh: int = 0, flux_precision: int = 64,
-                      r_mid: float = 25.0, width: float = 3.0, amp: float = 1e-3, tvd: bool = False):
-    """(mesh, params, state [10, C], hfluids [5 nh, C] or None)."""
-    m = _mesh.shell_mesh(nq, nlayer)
+                      r_mid: float = 25.0, width: float = 3.0, amp: float = 1e-3, tvd: bool = False,
+                      radii: np.ndarray | None = None):
+    """(mesh, params, state [10, C], hfluids [5 nh, C] or None); radii: the
+    nlayer + 1 node radii of the layers instead of geometric spacing."""
+    m = _mesh.shell_mesh(nq, nlayer, radii=radii)
     rng = np.random.default_rng(seed)
     xyz = m["node_xyz"]
     cc = xyz[m["cell_nodes"]].mean(axis=1)

@@ -354,6 +354,37 @@ typedef struct titan_mc_info {
 
 int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* params, double* out, titan_mc_info* info);
 
+/* Tabulated velocity distributions of the neutrals entering through chosen
+ * faces, the reference's face AMR functions (AMR_f, TITAN/source/AMR_f.h)
+ * as Monte-Carlo input: Setka::MK_go (TITAN/source/Setka_MK.cpp:1225-1575)
+ * launches the neutrals of an interface face from its AMR_f, where the
+ * others (and these faces without a table) take the drifting Maxwellian.
+ * Each face gives the frame of its AMR_f (Vn, Vt, Vm: a velocity with local
+ * coordinates (x, y, z) is x Vn + y Vt + z Vm, Vn pointing into the cell the
+ * neutrals enter) and its leaf cells in the reference's tree order, each a
+ * box [xL, xR] x [yL, yR] x [zL, zR] of local velocities (0 <= xL < xR) with
+ * the distribution's value f. A face's inflow is the sum over its leaves of
+ * box volume * f * |box centre x| times the face area (AMR_f::Culk_SpotokV,
+ * AMR_f.cpp:4-48), and it joins the other faces' inflow in one CDF. A neutral
+ * that starts on such a face takes a leaf by that weight (AMR_f::
+ * Get_random_velosity, AMR_f.cpp:50-96) and, in it, x = sqrt(xL^2 + r (xR^2 -
+ * xL^2)), y and z uniform (AMR_cell::Get_random_velosity_in_cell,
+ * AMR_cell.cpp:273-326). side: 0 the neutrals enter cells[0], 1 cells[1]
+ * (interior faces only). Kept by the context for the passes that follow; NULL
+ * (or nface = 0) removes the tables. The reference's per-face particle counts
+ * (N_particle and weight mu per face) are replaced by one stratified draw of
+ * all neutrals over the joint CDF, each with the same weight. */
+typedef struct titan_mc_face_dist {
+    int64_t nface;
+    const int32_t* face;      /* [nface] original face ids, each at most once */
+    const int8_t* side;       /* [nface] */
+    const double* frame;      /* [nface][9] Vn, Vt, Vm */
+    const int64_t* leaf_ptr;  /* [nface + 1] leaves of face i: leaf_ptr[i] .. leaf_ptr[i+1]-1 */
+    const double* leaf_box;   /* [nleaf][6] xL, xR, yL, yR, zL, zR */
+    const double* leaf_f;     /* [nleaf] */
+} titan_mc_face_dist;
+int titan_set_mc_face_dist(titan_ctx* ctx, const titan_mc_face_dist* dist);
+
 /* ---------------------------------------------------------------------------
  * Learned charge-exchange closure (no reference counterpart: it stands in for
  * re-running the Monte-Carlo neutral solver between plasma steps).

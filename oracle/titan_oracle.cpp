@@ -2347,15 +2347,51 @@ double o_block_scan(std::vector<double>& v) {
 // *inflow_total the neutrals entering per unit time, *lost the neutrals that
 // ended other than through the boundary. Returns 0, or 1 when no face lets
 // neutrals in.
+// Tabulated inflow of some faces (the reference's face AMR functions as
+// input, Setka_MK.cpp:1225-1575): per face its frame Vn, Vt, Vm, the side the
+// neutrals enter and its leaves (box in local velocities, value f) in tree order.
+struct OMcFaceDist {
+    int64_t nface;
+    const int32_t* face;
+    const int8_t* side;
+    const double* frame;
+    const int64_t* leaf_ptr;
+    const double* leaf_box;
+    const double* leaf_f;
+};
+
 int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32_t npassive, double par_a_2,
                    double par_Kn, double nH, const double* uH, double cpH, uint32_t face_types, uint64_t seed,
                    int64_t nparticles, int32_t max_cells, double* tally, double* trace, double* inflow_total,
-                   int64_t* lost_out) {
+                   int64_t* lost_out, const OMcFaceDist* fd) {
     const int64_t nc = M->ncell, nf = M->nface;
     std::vector<double> cc(3 * nc), vol(nc), fc(3 * nf), fn(3 * nf), fa(nf);
     oracle_geometry(M, xyz, cc.data(), vol.data(), fc.data(), fn.data(), fa.data());
+    // the tables: each leaf's weight box volume * f * |centre x| (Culk_SpotokV,
+    // AMR_f.cpp:4-48), the face's inflow per unit area and the leaves'
+    // cumulative shares (the last one 1)
+    std::vector<int64_t> tab_of(nf, -1);
+    std::vector<double> tab_flux, leaf_cum;
+    if (fd && fd->nface > 0) {
+        tab_flux.resize(fd->nface);
+        leaf_cum.resize(fd->leaf_ptr[fd->nface]);
+        for (int64_t i = 0; i < fd->nface; ++i) {
+            tab_of[fd->face[i]] = i;
+            double sum = 0.0;
+            for (int64_t l = fd->leaf_ptr[i]; l < fd->leaf_ptr[i + 1]; ++l) {
+                const double* b = fd->leaf_box + 6 * l;
+                const double dx = b[1] - b[0], dy = b[3] - b[2], dz = b[5] - b[4];
+                sum += dx * dy * dz * fd->leaf_f[l] * std::fabs((b[0] + b[1]) / 2.0);
+                leaf_cum[l] = sum;
+            }
+            tab_flux[i] = sum;
+            for (int64_t l = fd->leaf_ptr[i]; l < fd->leaf_ptr[i + 1]; ++l)
+                leaf_cum[l] = (l == fd->leaf_ptr[i + 1] - 1) ? 1.0 : leaf_cum[l] / sum;
+        }
+    }
     // inflow weights and their CDF, in the device's summation tree
     auto weight = [&](int64_t f) {
+        if (tab_of[f] >= 0) return tab_flux[tab_of[f]] * fa[f];
         const int t = M->face_type[f];
         if (t <= 0 || t > 31 || !((face_types >> t) & 1u)) return 0.0;
         const double un = -(uH[0] * fn[3 * f] + uH[1] * fn[3 * f + 1] + uH[2] * fn[3 * f + 2]);
@@ -2462,11 +2498,35 @@ int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32
         }
         double x[3];
         for (int k = 0; k < 3; ++k) x[k] = P[0][k] + b1 * (P[tb][k] - P[0][k]) + b2 * (P[2][k] - P[0][k]);
+        const int64_t tab = tab_of[f0];
+        double v[3] = {uH[0], uH[1], uH[2]};
+        int64_t cell = M->face_cells[2 * f0];
+        if (tab >= 0) {
+            // AMR_f::Get_random_velosity (AMR_f.cpp:50-96) over the flattened
+            // leaves, then AMR_cell::Get_random_velosity_in_cell (AMR_cell.cpp:273-326)
+            const double u = rng.uniform();
+            int64_t l = fd->leaf_ptr[tab], h = fd->leaf_ptr[tab + 1] - 1;
+            while (l < h) {
+                const int64_t mid = (l + h) >> 1;
+                if (leaf_cum[mid] < u)
+                    l = mid + 1;
+                else
+                    h = mid;
+            }
+            const double* B = fd->leaf_box + 6 * l;
+            const double L = B[0], R = B[1];
+            double w[3];
+            w[0] = std::sqrt(L * L + rng.uniform() * (R * R - L * L));
+            w[1] = B[2] + rng.uniform() * (B[3] - B[2]);
+            w[2] = B[4] + rng.uniform() * (B[5] - B[4]);
+            const double* E = fd->frame + 9 * tab;
+            for (int k = 0; k < 3; ++k) v[k] = w[0] * E[k] + w[1] * E[3 + k] + w[2] * E[6 + k];
+            if (fd->side[tab]) cell = M->face_cells[2 * f0 + 1];
+        }
         const double nin[3] = {-fn[3 * f0], -fn[3 * f0 + 1], -fn[3 * f0 + 2]};
         const double un = uH[0] * nin[0] + uH[1] * nin[1] + uH[2] * nin[2];
         const double vmax = std::fmax(un, 0.0) + 6.0 * cpH;
-        double v[3] = {uH[0], uH[1], uH[2]};
-        for (int it = 0; it < 4096; ++it) {
+        for (int it = 0; it < 4096 && tab < 0; ++it) {
             const double r1 = std::sqrt(-std::log(rng.uniform())), t1 = 2.0 * kPi * rng.uniform();
             const double r2 = std::sqrt(-std::log(rng.uniform())), t2 = 2.0 * kPi * rng.uniform();
             v[0] = uH[0] + cpH * r1 * std::cos(t1);
@@ -2475,7 +2535,6 @@ int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32
             const double vn = v[0] * nin[0] + v[1] * nin[1] + v[2] * nin[2];
             if (vn > 0.0 && rng.uniform() * vmax < vn) break;
         }
-        int64_t cell = M->face_cells[2 * f0];
         double ksi = -std::log(1.0 - rng.uniform());
         double I = 0.0;
         int nex = 0, visit = 0, kind = 1;

@@ -367,10 +367,18 @@ def renumbered_mesh(mesh: dict, cell_n2o, face_n2o, node_n2o) -> dict:
     return out, c_o2n
 
 
+class OMcFaceDist(ctypes.Structure):
+    _fields_ = [("nface", ctypes.c_int64), ("face", I32), ("side", I8), ("frame", D),
+                ("leaf_ptr", ctypes.POINTER(ctypes.c_int64)), ("leaf_box", D), ("leaf_f", D)]
+
+
 def mc_pass(mesh: dict, state: np.ndarray, params: dict, n_H: float, u_H, cp_H: float, n_particles: int,
-            seed: int = 1, face_types: int = (1 << 2) | (1 << 3), max_cells: int = 1000000):
+            seed: int = 1, face_types: int = (1 << 2) | (1 << 3), max_cells: int = 1000000,
+            face_dist: dict | None = None):
     """The oracle's Monte-Carlo pass on a stationary mesh: (tally [5, ncell],
-    trace [n_particles, 8], inflow rate, lost)."""
+    trace [n_particles, 8], inflow rate, lost). face_dist: tabulated inflow
+    of some faces (face, side, frame, leaf_ptr, leaf_box, leaf_f; face ids in
+    `mesh`'s numbering)."""
     run = OracleRun(mesh, params)
     st = np.ascontiguousarray(state, dtype=np.float64)
     C = run.mesh.ncell
@@ -383,11 +391,24 @@ def mc_pass(mesh: dict, state: np.ndarray, params: dict, n_H: float, u_H, cp_H: 
     L.oracle_mc_pass.restype = ctypes.c_int
     L.oracle_mc_pass.argtypes = [ctypes.POINTER(OMesh), D, D, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double, D, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint64,
-                                 ctypes.c_int64, ctypes.c_int32, D, D, D, ctypes.POINTER(ctypes.c_int64)]
+                                 ctypes.c_int64, ctypes.c_int32, D, D, D, ctypes.POINTER(ctypes.c_int64),
+                                 ctypes.POINTER(OMcFaceDist)]
+    fd, keep = None, []
+    if face_dist is not None:
+        arrs = dict(face=np.ascontiguousarray(face_dist["face"], dtype=np.int32),
+                    side=np.ascontiguousarray(face_dist["side"], dtype=np.int8),
+                    frame=np.ascontiguousarray(face_dist["frame"], dtype=np.float64),
+                    leaf_ptr=np.ascontiguousarray(face_dist["leaf_ptr"], dtype=np.int64),
+                    leaf_box=np.ascontiguousarray(face_dist["leaf_box"], dtype=np.float64),
+                    leaf_f=np.ascontiguousarray(face_dist["leaf_f"], dtype=np.float64))
+        keep.append(arrs)
+        fd = OMcFaceDist(len(arrs["face"]), _p(arrs["face"], I32), _p(arrs["side"], I8), _p(arrs["frame"]),
+                         arrs["leaf_ptr"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(arrs["leaf_box"]),
+                         _p(arrs["leaf_f"]))
     rc = L.oracle_mc_pass(ctypes.byref(run.mesh), _p(run.xyz), _p(st), int(params["npassive"]),
                           float(params["par_a_2"]), float(params["par_Kn"]), float(n_H), _p(uH), float(cp_H),
                           int(face_types), int(seed), int(n_particles), int(max_cells), _p(tally), _p(trace),
-                          ctypes.byref(total), ctypes.byref(lost))
+                          ctypes.byref(total), ctypes.byref(lost), ctypes.byref(fd) if fd is not None else None)
     if rc:
         raise RuntimeError("oracle_mc_pass: no inflow faces")
     return tally, trace, total.value, lost.value

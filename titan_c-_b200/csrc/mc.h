@@ -7,6 +7,21 @@
 
 namespace titan {
 
+// Tabulated inflow distributions (titan_set_mc_face_dist) in device numbering:
+// index[f] = the table of face f or -1; per table the AMR_f frame, the side
+// the neutrals enter, the inflow per unit area (sum of box volume * f * |x_c|
+// over the leaves) and its leaves; per leaf its box and the face's
+// cumulative share of the inflow up to it (the last leaf of a face holds 1).
+struct McFaceDist {
+    const int* index;        // [nface], or null: no tables
+    const double* frame;     // [ntab][9] Vn, Vt, Vm
+    const signed char* side; // [ntab]
+    const double* flux;      // [ntab] inflow per unit face area
+    const int* leaf_ptr;     // [ntab + 1]
+    const double* box;       // [nleaf][6]
+    const double* cum;       // [nleaf]
+};
+
 struct McArgs {
     MeshView M;
     Params P;
@@ -22,6 +37,7 @@ struct McArgs {
     double* tally;            // [5][ncell]: sum mu*t, sum mu*dv (3), sum mu*d(v^2)/2
     unsigned long long* lost;
     double* trace;            // null, or [nparticles][8]: each neutral's end (titan_mc_params.trace_out)
+    McFaceDist fd;            // tabulated inflow of some faces (fd.index null: none)
 };
 
 // One cell's tracing record, built once per Monte-Carlo pass: the six face

@@ -136,6 +136,10 @@ constexpr double kSqrtPiFull = 1.7724538509055160273;  // sqrt(pi)
 // Maxwellian through the inward normal, n [cp e^{-s^2} / (2 sqrt(pi)) + u_n (1 + erf s) / 2]
 // with s = u_n / cp, times the face area; 0 for faces that let no neutrals in.
 __device__ __forceinline__ double inflow_weight(const Args& a, int f) {
+    if (a.fd.index) {  // a tabulated face: its table's inflow (AMR_f::Culk_SpotokV)
+        const int d = a.fd.index[f];
+        if (d >= 0) return a.fd.flux[d] * a.L.fa[f];
+    }
     const int t = a.M.face_type[f];
     if (t <= 0 || t > 31 || !((a.face_types >> t) & 1u)) return 0.0;
     const int nf = a.M.nface;
@@ -274,12 +278,37 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
     }
     double x[3];
     for (int k = 0; k < 3; ++k) x[k] = P[0][k] + b1 * (P[tb][k] - P[0][k]) + b2 * (P[2][k] - P[0][k]);
+    const int tab = a.fd.index ? a.fd.index[f0] : -1;
+    double v[3] = {a.uH0, a.uH1, a.uH2};
+    int cell = M.face_c0[f0];
+    if (tab >= 0) {
+        // velocity from the face's table: a leaf by its share of the inflow,
+        // then the flux-weighted normal component and uniform tangential ones
+        // in the leaf's box, turned into the face's frame
+        const double u = rng.uniform();
+        int l = a.fd.leaf_ptr[tab], h = a.fd.leaf_ptr[tab + 1] - 1;
+        while (l < h) {
+            const int mid = (l + h) >> 1;
+            if (a.fd.cum[mid] < u)
+                l = mid + 1;
+            else
+                h = mid;
+        }
+        const double* B = a.fd.box + 6 * (size_t)l;
+        const double xL = B[0], xR = B[1];
+        const double w0 = sqrt(xL * xL + rng.uniform() * (xR * xR - xL * xL));
+        const double w1 = B[2] + rng.uniform() * (B[3] - B[2]);
+        const double w2 = B[4] + rng.uniform() * (B[5] - B[4]);
+        const double* E = a.fd.frame + 9 * (size_t)tab;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) v[k] = w0 * E[k] + w1 * E[3 + k] + w2 * E[6 + k];
+        if (a.fd.side[tab]) cell = M.face_c1[f0];
+    }
     // velocity: flux-weighted drifting Maxwellian through the inward normal
     const double nin[3] = {-a.L.fn[f0], -a.L.fn[nf + f0], -a.L.fn[2 * nf + f0]};
     const double un = a.uH0 * nin[0] + a.uH1 * nin[1] + a.uH2 * nin[2];
     const double vmax = fmax(un, 0.0) + 6.0 * a.cpH;
-    double v[3] = {a.uH0, a.uH1, a.uH2};
-    for (int it = 0; it < 4096; ++it) {
+    for (int it = 0; it < 4096 && tab < 0; ++it) {
         // Box-Muller pairs for exp(-y^2) per component
         const double r1 = sqrt(-log(rng.uniform())), t1 = 2.0 * kPi * rng.uniform();
         const double r2 = sqrt(-log(rng.uniform())), t2 = 2.0 * kPi * rng.uniform();
@@ -289,7 +318,6 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
         const double vn = v[0] * nin[0] + v[1] * nin[1] + v[2] * nin[2];
         if (vn > 0.0 && rng.uniform() * vmax < vn) break;
     }
-    int cell = M.face_c0[f0];
     double ksi = -log(1.0 - rng.uniform());
     double I = 0.0;
     double* T = a.tally;

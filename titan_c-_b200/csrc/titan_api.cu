@@ -139,6 +139,9 @@ struct titan_ctx {
     // Monte-Carlo pass buffers (titan_mc_sources), allocated by the first pass
     McCell* d_mc_cells = nullptr;       // [ncell] tracing records
     double* d_mc_cdf = nullptr;         // [nface] inflow CDF
+    // tabulated inflow distributions (titan_set_mc_face_dist): index, frame,
+    // side, flux, leaf_ptr, box, cum (McFaceDist)
+    void* fd_buf[7] = {};
     double* d_mc_blocks = nullptr;      // [mc_scan_blocks(nface)] + 1: block sums, total
     double* d_mc_tally = nullptr;       // [5][ncell]
     unsigned long long* d_mc_lost = nullptr;
@@ -549,6 +552,8 @@ int titan_destroy(titan_ctx* ctx) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (void* p : ctx->surf_buf)
+        if (p) cudaFree(p);
+    for (void* p : ctx->fd_buf)
         if (p) cudaFree(p);
     if (ctx->d_cl_in) cudaFree(ctx->d_cl_in);
     if (ctx->d_cl_y) cudaFree(ctx->d_cl_y);
@@ -1432,6 +1437,15 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, tit
     a.max_cells = mp->max_cells > 0 ? mp->max_cells : 1000000;
     a.tally = ctx->d_mc_tally;
     a.lost = ctx->d_mc_lost;
+    if (ctx->fd_buf[0]) {
+        a.fd.index = (const int*)ctx->fd_buf[0];
+        a.fd.frame = (const double*)ctx->fd_buf[1];
+        a.fd.side = (const signed char*)ctx->fd_buf[2];
+        a.fd.flux = (const double*)ctx->fd_buf[3];
+        a.fd.leaf_ptr = (const int*)ctx->fd_buf[4];
+        a.fd.box = (const double*)ctx->fd_buf[5];
+        a.fd.cum = (const double*)ctx->fd_buf[6];
+    }
     // per-neutral end records (tests and diagnostics): a buffer for this pass only
     struct TraceBuf {
         double* p = nullptr;
@@ -1476,6 +1490,74 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, tit
         info->lost = (int64_t)lost;
         info->inflow_rate = total;
         info->gpu_ms = ms;
+    }
+    return TITAN_OK;
+}
+
+int titan_set_mc_face_dist(titan_ctx* ctx, const titan_mc_face_dist* d) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    for (void*& p : ctx->fd_buf) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    if (!d || d->nface == 0) return TITAN_OK;
+    if (d->nface < 0 || !d->face || !d->side || !d->frame || !d->leaf_ptr || !d->leaf_box || !d->leaf_f)
+        return fail(TITAN_EINVAL, "face tables: nface >= 0 and every array");
+    const int64_t nf = ctx->nface, nt = d->nface;
+    const Renumbering& R = ctx->R;
+    if (d->leaf_ptr[0] != 0) return fail(TITAN_EINVAL, "face tables: leaf_ptr[0] must be 0");
+    const int64_t nleaf = d->leaf_ptr[nt];
+    if (nleaf < nt || nleaf > INT32_MAX) return fail(TITAN_EINVAL, "face tables: leaf_ptr[nface] out of range");
+    std::vector<int32_t> index(nf, -1), ptr(nt + 1, 0);
+    std::vector<int8_t> side(nt);
+    std::vector<double> flux(nt), cum(nleaf);
+    std::vector<int32_t> c1(nf);
+    CK(cudaMemcpy(c1.data(), ctx->d_face_c1, sizeof(int32_t) * nf, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nt; ++i) {
+        const int32_t fo = d->face[i];
+        if (fo < 0 || fo >= nf) return fail(TITAN_EINVAL, "face tables: face id out of range");
+        const int32_t f = R.face_o2n[fo];
+        if (index[f] >= 0) return fail(TITAN_EINVAL, "face tables: a face is listed twice");
+        index[f] = (int32_t)i;
+        if (d->side[i] != 0 && d->side[i] != 1) return fail(TITAN_EINVAL, "face tables: side is 0 or 1");
+        if (d->side[i] == 1 && c1[f] < 0) return fail(TITAN_EINVAL, "face tables: side 1 on a boundary face");
+        side[i] = d->side[i];
+        const int64_t l0 = d->leaf_ptr[i], l1 = d->leaf_ptr[i + 1];
+        if (!(l1 > l0) || l1 > nleaf) return fail(TITAN_EINVAL, "face tables: leaf_ptr must increase to leaf_ptr[nface]");
+        ptr[i + 1] = (int32_t)l1;
+        // inflow per unit area: leaf weights box volume * f * |centre x| summed
+        // in the given (tree) order, then each leaf's cumulative share
+        double sum = 0.0;
+        for (int64_t l = l0; l < l1; ++l) {
+            const double* b = d->leaf_box + 6 * l;
+            const double fl = d->leaf_f[l];
+            if (!(b[0] >= 0.0 && b[1] > b[0] && b[3] > b[2] && b[5] > b[4]) || !(fl >= 0.0) || !std::isfinite(fl) ||
+                !std::isfinite(b[1]) || !std::isfinite(b[2]) || !std::isfinite(b[3]) || !std::isfinite(b[4]) ||
+                !std::isfinite(b[5]))
+                return fail(TITAN_EINVAL, "face tables: leaves need 0 <= xL < xR, yL < yR, zL < zR, f >= 0");
+            const double V = ((b[1] - b[0]) * (b[3] - b[2])) * (b[5] - b[4]);
+            sum += V * fl * std::fabs((b[0] + b[1]) / 2.0);
+            cum[l] = sum;
+        }
+        if (!(sum > 0.0)) return fail(TITAN_EINVAL, "face tables: a face's distribution lets nothing in");
+        flux[i] = sum;
+        for (int64_t l = l0; l < l1; ++l) cum[l] = (l == l1 - 1) ? 1.0 : cum[l] / sum;
+    }
+    std::vector<double> frame(d->frame, d->frame + 9 * nt);
+    std::vector<double> box(d->leaf_box, d->leaf_box + 6 * nleaf);
+    cudaError_t e = upload_vec(&ctx->fd_buf[0], index);
+    if (!e) e = upload_vec(&ctx->fd_buf[1], frame);
+    if (!e) e = upload_vec(&ctx->fd_buf[2], side);
+    if (!e) e = upload_vec(&ctx->fd_buf[3], flux);
+    if (!e) e = upload_vec(&ctx->fd_buf[4], ptr);
+    if (!e) e = upload_vec(&ctx->fd_buf[5], box);
+    if (!e) e = upload_vec(&ctx->fd_buf[6], cum);
+    if (e) {
+        for (void*& p : ctx->fd_buf) {
+            if (p) cudaFree(p);
+            p = nullptr;
+        }
+        return fail(TITAN_ECUDA, std::string("face tables: ") + cudaGetErrorString(e));
     }
     return TITAN_OK;
 }

@@ -85,6 +85,12 @@ class TitanMcParams(ctypes.Structure):
                 ("face_types", ctypes.c_int32), ("trace_out", ctypes.c_void_p)]
 
 
+class TitanMcFaceDist(ctypes.Structure):
+    _fields_ = [("nface", ctypes.c_int64), ("face", ctypes.c_void_p), ("side", ctypes.c_void_p),
+                ("frame", ctypes.c_void_p), ("leaf_ptr", ctypes.c_void_p), ("leaf_box", ctypes.c_void_p),
+                ("leaf_f", ctypes.c_void_p)]
+
+
 class TitanMcInfo(ctypes.Structure):
     _fields_ = [("particles", ctypes.c_int64), ("lost", ctypes.c_int64), ("inflow_rate", ctypes.c_double),
                 ("gpu_ms", ctypes.c_double)]
@@ -118,6 +124,7 @@ SIGNATURES = {
     "titan_set_surface_motion": ([ctypes.c_void_p, ctypes.POINTER(TitanSurfaceParams), ctypes.c_int64,
                                   ctypes.c_int32, I32], ctypes.c_int),
     "titan_set_ray_law": ([ctypes.c_void_p, ctypes.POINTER(TitanRayLaw)], ctypes.c_int),
+    "titan_set_mc_face_dist": ([ctypes.c_void_p, ctypes.POINTER(TitanMcFaceDist)], ctypes.c_int),
     "titan_upload_state": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_download_state": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_upload_hfluids": ([ctypes.c_void_p, D], ctypes.c_int),

@@ -286,6 +286,24 @@ class PlasmaStep:
         N.check(self._lib.titan_mc_sources(self._ctx, ctypes.byref(mp), N.ptr(out), ctypes.byref(info)))
         return out, {k: getattr(info, k) for k, _ in N.TitanMcInfo._fields_}
 
+    def set_mc_face_dist(self, face_dist: dict | None):
+        """Tabulated velocity distributions of the neutrals entering through
+        some faces (titan_set_mc_face_dist): face (original ids), side, frame
+        [n, 9], leaf_ptr [n + 1], leaf_box [nleaf, 6], leaf_f [nleaf]; None
+        removes them."""
+        if face_dist is None:
+            N.check(self._lib.titan_set_mc_face_dist(self._ctx, None))
+            return
+        arrs = dict(face=np.ascontiguousarray(face_dist["face"], dtype=np.int32),
+                    side=np.ascontiguousarray(face_dist["side"], dtype=np.int8),
+                    frame=np.ascontiguousarray(face_dist["frame"], dtype=np.float64),
+                    leaf_ptr=np.ascontiguousarray(face_dist["leaf_ptr"], dtype=np.int64),
+                    leaf_box=np.ascontiguousarray(face_dist["leaf_box"], dtype=np.float64),
+                    leaf_f=np.ascontiguousarray(face_dist["leaf_f"], dtype=np.float64))
+        d = N.TitanMcFaceDist(len(arrs["face"]), *(arrs[k].ctypes.data for k in
+                                                   ("face", "side", "frame", "leaf_ptr", "leaf_box", "leaf_f")))
+        N.check(self._lib.titan_set_mc_face_dist(self._ctx, ctypes.byref(d)))
+
     def mc_pass(self, n_H: float, u_H, cp_H: float, n_particles: int, seed: int = 1,
                 face_types: int = (1 << 2) | (1 << 3), max_cells: int = 0) -> dict:
         """A Monte-Carlo pass whose sources stay on the device (for

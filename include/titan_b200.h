@@ -343,7 +343,8 @@ typedef struct titan_mc_params {
     int32_t face_types;  /* e.g. (1 << TITAN_FACE_OUTER_HARD) | (1 << TITAN_FACE_OUTER_SOFT) */
     double* trace_out;   /* NULL, or host [n_particles][8]: each neutral's end — position (3),
                             velocity (3), charge exchanges, 4 * cell visits + end kind (0 left
-                            through the boundary, 1 lost after max_cells, 2 no outgoing face) */
+                            through the boundary, 1 lost after max_cells, 2 no outgoing face,
+                            3 stopped on a tallied face, titan_set_mc_face_tally) */
 } titan_mc_params;
 
 typedef struct titan_mc_info {
@@ -384,6 +385,35 @@ typedef struct titan_mc_face_dist {
     const double* leaf_f;     /* [nleaf] */
 } titan_mc_face_dist;
 int titan_set_mc_face_dist(titan_ctx* ctx, const titan_mc_face_dist* dist);
+
+/* Outgoing velocity distributions tallied on chosen faces, the other half of
+ * the reference's face AMR coupling: a neutral that reaches a listed face
+ * from its side cell (side 0: leaving cells[0]; 1: leaving cells[1]) stops
+ * there (Setka_MK.cpp:2165-2182) and AMR_f::Add_particle (AMR_f.cpp:240-316)
+ * adds mu / |v . Vn|, mu and mu / (v . Vn)^2 to the face's moments n, Smu,
+ * nn, and mu to the first leaf (half-open boxes, in the given order) holding
+ * its local velocity (x, y, z) = (v . Vn, v . Vt, v . Vm), clamped 1e-7
+ * inside the leaves' bounding box (a velocity no leaf holds shrinks toward
+ * the origin by 0.995 per try, at most 30 tries, else it counts as
+ * unplaced). After each pass the moments are per unit face area and each
+ * leaf's weight per unit box volume, face area and box-centre x
+ * (AMR_f::Normir_velocity_volume, AMR_f.cpp:318-336), so a face's tallied
+ * leaves are a table titan_set_mc_face_dist takes for the zone beyond it.
+ * Vn points out of the side cell; leaves 0 <= xL < xR. Kept by the context
+ * for the passes that follow; NULL removes the tallies. The trace's end kind
+ * of such a neutral is 3. */
+typedef struct titan_mc_face_tally {
+    int64_t nface;
+    const int32_t* face;      /* [nface] original face ids, each at most once */
+    const int8_t* side;       /* [nface] */
+    const double* frame;      /* [nface][9] Vn, Vt, Vm */
+    const int64_t* leaf_ptr;  /* [nface + 1] */
+    const double* leaf_box;   /* [nleaf][6] xL, xR, yL, yR, zL, zR */
+} titan_mc_face_tally;
+int titan_set_mc_face_tally(titan_ctx* ctx, const titan_mc_face_tally* tally);
+/* The last pass's tallies: leaf_f [nleaf], moments [nface][3] (n, Smu, nn);
+ * either may be NULL. unplaced: neutrals no leaf held. */
+int titan_get_mc_face_tally(titan_ctx* ctx, double* leaf_f, double* moments, int64_t* unplaced);
 
 /* ---------------------------------------------------------------------------
  * Learned charge-exchange closure (no reference counterpart: it stands in for

@@ -2360,10 +2360,26 @@ struct OMcFaceDist {
     const double* leaf_f;
 };
 
+// Outgoing tallies on some faces (AMR_f::Add_particle, AMR_f.cpp:240-316, at
+// Setka_MK.cpp:2165-2182): per face the side whose leaving neutrals stop
+// there, the frame and the leaf boxes. Results: leaf weights, moments (n,
+// Smu, nn) per face, and the neutrals no leaf held.
+struct OMcFaceTally {
+    int64_t nface;
+    const int32_t* face;
+    const int8_t* side;
+    const double* frame;
+    const int64_t* leaf_ptr;
+    const double* leaf_box;
+    double* leaf_f;
+    double* moments;
+    int64_t* unplaced;
+};
+
 int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32_t npassive, double par_a_2,
                    double par_Kn, double nH, const double* uH, double cpH, uint32_t face_types, uint64_t seed,
                    int64_t nparticles, int32_t max_cells, double* tally, double* trace, double* inflow_total,
-                   int64_t* lost_out, const OMcFaceDist* fd) {
+                   int64_t* lost_out, const OMcFaceDist* fd, const OMcFaceTally* ft) {
     const int64_t nc = M->ncell, nf = M->nface;
     std::vector<double> cc(3 * nc), vol(nc), fc(3 * nf), fn(3 * nf), fa(nf);
     oracle_geometry(M, xyz, cc.data(), vol.data(), fc.data(), fn.data(), fa.data());
@@ -2457,6 +2473,9 @@ int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32
             P[2] = n2;
             P[3] = fc[3 * f] * n0 + fc[3 * f + 1] * n1 + fc[3 * f + 2] * n2;
             nbr[6 * c + sl] = first ? M->face_cells[2 * f + 1] : M->face_cells[2 * f];
+            if (ft)  // a tallied face seen from its side cell: neutrals stop there (table t as -3 - t)
+                for (int64_t t = 0; t < ft->nface; ++t)
+                    if (ft->face[t] == f && ft->side[t] == (first ? 0 : 1)) nbr[6 * c + sl] = (int32_t)(-3 - t);
         }
         const double rho = state[c], p = state[4 * nc + c];
         const double rho_He = npassive ? state[9 * nc + c] : 0.0;
@@ -2473,6 +2492,55 @@ int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32
     }
     std::fill(tally, tally + 5 * nc, 0.0);
     int64_t lost = 0;
+    // the tallied faces' bounds (the leaves' bounding box) and their accumulators
+    std::vector<double> ft_bounds;
+    if (ft) {
+        ft_bounds.resize(6 * ft->nface);
+        for (int64_t t = 0; t < ft->nface; ++t) {
+            double* B = &ft_bounds[6 * t];
+            for (int k = 0; k < 6; k += 2) {
+                B[k] = HUGE_VAL;
+                B[k + 1] = -HUGE_VAL;
+            }
+            for (int64_t l = ft->leaf_ptr[t]; l < ft->leaf_ptr[t + 1]; ++l)
+                for (int k = 0; k < 6; k += 2) {
+                    B[k] = std::min(B[k], ft->leaf_box[6 * l + k]);
+                    B[k + 1] = std::max(B[k + 1], ft->leaf_box[6 * l + k + 1]);
+                }
+        }
+        std::fill(ft->leaf_f, ft->leaf_f + ft->leaf_ptr[ft->nface], 0.0);
+        std::fill(ft->moments, ft->moments + 3 * ft->nface, 0.0);
+        *ft->unplaced = 0;
+    }
+    auto stop_on_face = [&](int64_t t, const double* v) {
+        const double* E = ft->frame + 9 * t;
+        const double Vnn = std::fabs(v[0] * E[0] + v[1] * E[1] + v[2] * E[2]);
+        ft->moments[3 * t] += mu / Vnn;
+        ft->moments[3 * t + 1] += mu;
+        ft->moments[3 * t + 2] += mu * ((1.0 / Vnn) * (1.0 / Vnn));
+        double q[3] = {v[0] * E[0] + v[1] * E[1] + v[2] * E[2], v[0] * E[3] + v[1] * E[4] + v[2] * E[5],
+                       v[0] * E[6] + v[1] * E[7] + v[2] * E[8]};
+        const double* B = &ft_bounds[6 * t];
+        for (int k = 0; k < 3; ++k) {
+            if (q[k] < B[2 * k]) q[k] = B[2 * k] + 1e-7;
+            if (q[k] > B[2 * k + 1]) q[k] = B[2 * k + 1] - 1e-7;
+        }
+        for (int kk = 1; kk <= 30; ++kk) {
+            for (int64_t l = ft->leaf_ptr[t]; l < ft->leaf_ptr[t + 1]; ++l) {
+                const double* b = ft->leaf_box + 6 * l;
+                if (b[0] <= q[0] && q[0] < b[1] && b[2] <= q[1] && q[1] < b[3] && b[4] <= q[2] && q[2] < b[5]) {
+                    ft->leaf_f[l] += mu;
+                    return;
+                }
+            }
+            q[0] *= 0.995;
+            if (kk < 20) {
+                q[1] *= 0.995;
+                q[2] *= 0.995;
+            }
+        }
+        ++*ft->unplaced;
+    };
     for (int64_t pid = 0; pid < nparticles; ++pid) {
         OMcRng rng{seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(pid + 1)), 0ull};
         const double s = ((double)pid + rng.uniform()) / (double)nparticles;
@@ -2569,6 +2637,10 @@ int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32
                 for (int k = 0; k < 3; ++k) x[k] += t_exit * v[k];
                 if (next < 0) {
                     kind = 0;
+                    if (next <= -3) {
+                        stop_on_face(-3 - (int64_t)next, v);
+                        kind = 3;
+                    }
                     break;
                 }
                 cell = next;
@@ -2593,7 +2665,7 @@ int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32
             ksi = -std::log(1.0 - rng.uniform());
             ++nex;
         }
-        if (kind != 0) ++lost;
+        if (kind == 1 || kind == 2) ++lost;
         if (trace) {
             double* r = trace + 8 * pid;
             r[0] = x[0];
@@ -2603,11 +2675,20 @@ int oracle_mc_pass(const OMesh* M, const double* xyz, const double* state, int32
             r[4] = v[1];
             r[5] = v[2];
             r[6] = (double)nex;
-            r[7] = 4.0 * (double)(visit + (kind == 0 ? 1 : 0)) + (double)kind;
+            r[7] = 4.0 * (double)(visit + (kind == 0 || kind == 3 ? 1 : 0)) + (double)kind;
         }
     }
     for (int64_t c = 0; c < nc; ++c)
         for (int k = 0; k < 5; ++k) tally[k * nc + c] /= vol[c];
+    if (ft)  // per unit face area; leaves also per box volume and centre x (Normir_velocity_volume)
+        for (int64_t t = 0; t < ft->nface; ++t) {
+            const double squ = fa[ft->face[t]];
+            for (int k = 0; k < 3; ++k) ft->moments[3 * t + k] /= squ;
+            for (int64_t l = ft->leaf_ptr[t]; l < ft->leaf_ptr[t + 1]; ++l) {
+                const double* b = ft->leaf_box + 6 * l;
+                ft->leaf_f[l] /= ((b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]) * squ * ((b[0] + b[1]) / 2.0));
+            }
+        }
     *lost_out = lost;
     return 0;
 }

@@ -372,13 +372,21 @@ class OMcFaceDist(ctypes.Structure):
                 ("leaf_ptr", ctypes.POINTER(ctypes.c_int64)), ("leaf_box", D), ("leaf_f", D)]
 
 
+class OMcFaceTally(ctypes.Structure):
+    _fields_ = [("nface", ctypes.c_int64), ("face", I32), ("side", I8), ("frame", D),
+                ("leaf_ptr", ctypes.POINTER(ctypes.c_int64)), ("leaf_box", D), ("leaf_f", D), ("moments", D),
+                ("unplaced", ctypes.POINTER(ctypes.c_int64))]
+
+
 def mc_pass(mesh: dict, state: np.ndarray, params: dict, n_H: float, u_H, cp_H: float, n_particles: int,
             seed: int = 1, face_types: int = (1 << 2) | (1 << 3), max_cells: int = 1000000,
-            face_dist: dict | None = None):
+            face_dist: dict | None = None, face_tally: dict | None = None):
     """The oracle's Monte-Carlo pass on a stationary mesh: (tally [5, ncell],
     trace [n_particles, 8], inflow rate, lost). face_dist: tabulated inflow
     of some faces (face, side, frame, leaf_ptr, leaf_box, leaf_f; face ids in
-    `mesh`'s numbering)."""
+    `mesh`'s numbering); face_tally: outgoing tallies (face, side, frame,
+    leaf_ptr, leaf_box), whose results (leaf_f, moments, unplaced) are added
+    to that dict."""
     run = OracleRun(mesh, params)
     st = np.ascontiguousarray(state, dtype=np.float64)
     C = run.mesh.ncell
@@ -392,7 +400,7 @@ def mc_pass(mesh: dict, state: np.ndarray, params: dict, n_H: float, u_H, cp_H: 
     L.oracle_mc_pass.argtypes = [ctypes.POINTER(OMesh), D, D, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double, D, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint64,
                                  ctypes.c_int64, ctypes.c_int32, D, D, D, ctypes.POINTER(ctypes.c_int64),
-                                 ctypes.POINTER(OMcFaceDist)]
+                                 ctypes.POINTER(OMcFaceDist), ctypes.POINTER(OMcFaceTally)]
     fd, keep = None, []
     if face_dist is not None:
         arrs = dict(face=np.ascontiguousarray(face_dist["face"], dtype=np.int32),
@@ -405,10 +413,30 @@ def mc_pass(mesh: dict, state: np.ndarray, params: dict, n_H: float, u_H, cp_H: 
         fd = OMcFaceDist(len(arrs["face"]), _p(arrs["face"], I32), _p(arrs["side"], I8), _p(arrs["frame"]),
                          arrs["leaf_ptr"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(arrs["leaf_box"]),
                          _p(arrs["leaf_f"]))
+    ft = None
+    if face_tally is not None:
+        t = dict(face=np.ascontiguousarray(face_tally["face"], dtype=np.int32),
+                 side=np.ascontiguousarray(face_tally["side"], dtype=np.int8),
+                 frame=np.ascontiguousarray(face_tally["frame"], dtype=np.float64),
+                 leaf_ptr=np.ascontiguousarray(face_tally["leaf_ptr"], dtype=np.int64),
+                 leaf_box=np.ascontiguousarray(face_tally["leaf_box"], dtype=np.float64))
+        nt = len(t["face"])
+        t["leaf_f"] = np.zeros(int(t["leaf_ptr"][-1]))
+        t["moments"] = np.zeros((nt, 3))
+        t["unplaced"] = np.zeros(1, dtype=np.int64)
+        keep.append(t)
+        ft = OMcFaceTally(nt, _p(t["face"], I32), _p(t["side"], I8), _p(t["frame"]),
+                          t["leaf_ptr"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(t["leaf_box"]),
+                          _p(t["leaf_f"]), _p(t["moments"]),
+                          t["unplaced"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
     rc = L.oracle_mc_pass(ctypes.byref(run.mesh), _p(run.xyz), _p(st), int(params["npassive"]),
                           float(params["par_a_2"]), float(params["par_Kn"]), float(n_H), _p(uH), float(cp_H),
                           int(face_types), int(seed), int(n_particles), int(max_cells), _p(tally), _p(trace),
-                          ctypes.byref(total), ctypes.byref(lost), ctypes.byref(fd) if fd is not None else None)
+                          ctypes.byref(total), ctypes.byref(lost), ctypes.byref(fd) if fd is not None else None,
+                          ctypes.byref(ft) if ft is not None else None)
     if rc:
         raise RuntimeError("oracle_mc_pass: no inflow faces")
+    if ft is not None:
+        face_tally.update(leaf_f=keep[-1]["leaf_f"], moments=keep[-1]["moments"],
+                          unplaced=int(keep[-1]["unplaced"][0]))
     return tally, trace, total.value, lost.value

@@ -151,3 +151,122 @@ def test_bad_face_tables_are_refused(titan):
             g.set_mc_face_dist(bad)
     g.set_mc_face_dist(None)
     g.close()
+
+
+def _sphere_faces(m, layer=9):
+    """The interior faces of node layer `layer`, the side of each face's
+    outer cell, and the unit vector from that cell through the face."""
+    on = np.all(m["node_layer"][m["face_nodes"]] == layer, axis=1) & (m["face_cells"][:, 1] >= 0)
+    faces = np.nonzero(on)[0]
+    cc = m["node_xyz"][m["cell_nodes"]].mean(axis=1)
+    fc = m["face_cells"][faces]
+    r0, r1 = np.linalg.norm(cc[fc[:, 0]], axis=1), np.linalg.norm(cc[fc[:, 1]], axis=1)
+    side = (r1 > r0).astype(np.int8)           # the outer cell's side
+    return faces, side
+
+
+def _tally_tables(g, faces, side, nx, ny, xmax=8.0, ymax=6.0):
+    """Leaf grids for faces, frame Vn pointing out of the side cell."""
+    nrm = g.geometry()["face_normal"]
+    xe = np.linspace(0.0, xmax, nx + 1)
+    ye = np.linspace(-ymax, ymax, ny + 1)
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(ny), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    b = np.stack([xe[i], xe[i + 1], ye[j], ye[j + 1], ye[k], ye[k + 1]], axis=1)
+    frame = np.array([_frame(nrm[f] * (1.0 if s == 0 else -1.0)) for f, s in zip(faces, side)])
+    return dict(face=faces.astype(np.int32), side=side.astype(np.int8), frame=frame,
+                leaf_ptr=np.arange(len(faces) + 1, dtype=np.int64) * len(b),
+                leaf_box=np.tile(b, (len(faces), 1)))
+
+
+def test_face_tallies_match_oracle(titan, oracle_lib):
+    m, p, st = _shell(titan)
+    p = dict(p, par_Kn=2.0)
+    g = titan.PlasmaStep(m, p)
+    g.upload_state(st)
+    faces, side = _sphere_faces(m)
+    ft = _tally_tables(g, faces, side, 4, 4)
+    g.set_mc_face_tally(ft)
+    n = 40000
+    trace = np.zeros((n, 8))
+    g.mc_sources(n_particles=n, seed=7, trace=trace, **MC)
+    got = g.mc_face_tally()
+    c_n2o, f_n2o, n_n2o = g.permutation()
+    g.close()
+    mr, c_o2n = ol.renumbered_mesh(m, c_n2o, f_n2o, n_n2o)
+    f_o2n = np.empty_like(f_n2o)
+    f_o2n[f_n2o] = np.arange(len(f_n2o))
+    fto = dict(ft, face=f_o2n[ft["face"]])
+    ol.mc_pass(mr, st[:, c_n2o], p, n_particles=n, seed=7, face_tally=fto, **MC)
+    kinds = trace[:, 7] % 4
+    assert (kinds == 3).mean() > 0.03              # many neutrals stopped on the sphere
+    assert got["unplaced"] == fto["unplaced"]
+    for a, b in ((got["leaf_f"], fto["leaf_f"]), (got["moments"], fto["moments"])):
+        scale = np.abs(b).max()
+        assert (np.abs(a - b) <= 1e-9 * scale).mean() >= 0.9
+        assert abs(a.sum() - b.sum()) <= 0.05 * np.abs(b).sum()
+
+
+def test_zone_coupling_through_face_tables(titan):
+    """Zone A (the whole mesh, neutrals stopped when they cross the layer-9
+    sphere inward) tallies its outgoing tables; zone B (launched only from
+    those tables, into the inner cells) then carries the neutrals on. Without
+    charge exchange a straight path crosses the sphere inward at most once, so
+    the inner zone's neutral content of B equals that of one pass with no
+    tallies, up to sampling and the tables' velocity resolution."""
+    m, p, st = _shell(titan)
+    p = dict(p, par_Kn=1e30)
+    g = titan.PlasmaStep(m, p)
+    g.upload_state(st)
+    cc = m["node_xyz"][m["cell_nodes"]].mean(axis=1)
+    rsph = np.linalg.norm(m["node_xyz"][m["node_layer"] == 9], axis=1).mean()
+    inner = np.linalg.norm(cc, axis=1) < rsph
+    geo = g.geometry()
+    vol, area = geo["cell_volume"], geo["face_area"]
+    n = 4000000
+    full, _ = g.mc_sources(n_particles=n, seed=21, face_types=1 << 2, **MC)
+    faces, side = _sphere_faces(m)
+    ft = _tally_tables(g, faces, side, 10, 12, xmax=8.0, ymax=6.0)
+    g.set_mc_face_tally(ft)
+    _, infoA = g.mc_sources(n_particles=n, seed=22, face_types=1 << 2, **MC)
+    tal = g.mc_face_tally()
+    g.set_mc_face_tally(None)
+    keep = np.zeros(len(faces), bool)
+    lp = ft["leaf_ptr"]
+    for i in range(len(faces)):
+        keep[i] = tal["leaf_f"][lp[i]:lp[i + 1]].sum() > 0
+    sel = np.nonzero(keep)[0]
+    nl = lp[1] - lp[0]
+    fd = dict(face=faces[sel], side=(1 - side[sel]).astype(np.int8), frame=ft["frame"][sel],
+              leaf_ptr=np.arange(len(sel) + 1, dtype=np.int64) * nl,
+              leaf_box=np.concatenate([ft["leaf_box"][lp[i]:lp[i + 1]] for i in sel]),
+              leaf_f=np.concatenate([tal["leaf_f"][lp[i]:lp[i + 1]] for i in sel]))
+    g.set_mc_face_dist(fd)
+    zoneB, infoB = g.mc_sources(n_particles=n, seed=23, face_types=0, **MC)
+    g.close()
+    # B's inflow is what A stopped on the sphere: sum of Smu times face area
+    assert tal["unplaced"] == 0
+    crossed = float((tal["moments"][:, 1] * area[faces]).sum())
+    assert abs(infoB["inflow_rate"] / crossed - 1.0) < 1e-9
+    content_full = float((full[0] * vol)[inner].sum())
+    content_B = float((zoneB[0] * vol)[inner].sum())
+    assert abs(content_B / content_full - 1.0) < 0.05, (content_B, content_full)
+
+
+def test_bad_face_tallies_are_refused(titan):
+    m, p, st = _shell(titan)
+    g = titan.PlasmaStep(m, p)
+    g.upload_state(st)
+    faces, side = _sphere_faces(m)
+    ft = _tally_tables(g, faces[:3], side[:3], 2, 2)
+    bnd = np.nonzero(m["face_cells"][:, 1] < 0)[0][:3]
+    with pytest.raises(titan.TitanError):
+        g.set_mc_face_tally(dict(ft, face=bnd.astype(np.int32), side=np.ones(3, np.int8)))
+    with pytest.raises(titan.TitanError):
+        g.set_mc_face_tally(dict(ft, leaf_box=ft["leaf_box"] * np.array([1, -1, 1, 1, 1, 1.0])))
+    g.set_mc_face_tally(ft)
+    with pytest.raises(titan.TitanError):
+        g.mc_face_tally()                      # no pass since the tallies were set
+    g.mc_sources(n_particles=1000, seed=1, **MC)
+    assert g.mc_face_tally()["leaf_f"].shape == (len(ft["leaf_box"]),)
+    g.close()

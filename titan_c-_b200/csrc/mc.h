@@ -22,6 +22,25 @@ struct McFaceDist {
     const double* cum;       // [nleaf]
 };
 
+// Tallied outgoing distributions (titan_set_mc_face_tally) in device
+// numbering: a neutral that reaches a listed face from the table's side cell
+// stops there and adds its weight to the leaf holding its local velocity
+// (clamped into the table's bounds), and mu / |v_n|, mu, mu / v_n^2 to the
+// face's moments. The pack kernel marks such a face in the side cell's record
+// as neighbour -3 - table.
+struct McFaceTally {
+    const int* index;        // [nface], or null: no tallies
+    const int* face;         // [ntab] device face ids
+    const signed char* side; // [ntab]
+    const double* frame;     // [ntab][9] Vn, Vt, Vm
+    const double* bounds;    // [ntab][6] the leaves' bounding box
+    const int* leaf_ptr;     // [ntab + 1]
+    const double* box;       // [nleaf][6]
+    double* f;               // [nleaf] summed weights
+    double* mom;             // [ntab][3] n, Smu, nn
+    unsigned long long* unplaced;  // neutrals whose velocity no leaf holds
+};
+
 struct McArgs {
     MeshView M;
     Params P;
@@ -38,6 +57,7 @@ struct McArgs {
     unsigned long long* lost;
     double* trace;            // null, or [nparticles][8]: each neutral's end (titan_mc_params.trace_out)
     McFaceDist fd;            // tabulated inflow of some faces (fd.index null: none)
+    McFaceTally ft;           // tallied outflow of some faces (ft.index null: none)
 };
 
 // One cell's tracing record, built once per Monte-Carlo pass: the six face
@@ -66,5 +86,8 @@ cudaError_t launch_mc_inflow_cdf(const McArgs& a, double* cdf, double* block_sum
 cudaError_t launch_mc_pack(const McArgs& a, McCell* cells, cudaStream_t s);
 cudaError_t launch_mc_trace_cells(const McArgs& a, const McCell* cells, cudaStream_t s);
 cudaError_t launch_mc_normalise(double* tally, const double* vol, int ncell, cudaStream_t s);
+// The outgoing tables' weights and moments per unit face area, and the
+// weights per unit box volume and normal speed (AMR_f::Normir_velocity_volume).
+cudaError_t launch_mc_tally_normalise(const McArgs& a, int ntab, cudaStream_t s);
 
 }  // namespace titan

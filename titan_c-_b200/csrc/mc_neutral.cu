@@ -241,9 +241,54 @@ __global__ void pack_kernel(Args a, McCell* __restrict__ cells) {
         R.plane[sl][2] = n2;
         R.plane[sl][3] = a.L.fc[f] * n0 + a.L.fc[nf + f] * n1 + a.L.fc[2 * nf + f] * n2;
         R.nbr[sl] = (fs < 0) ? M.face_c0[f] : M.face_c1[f];
+        if (a.ft.index) {  // a tallied face, reached from the table's side: the neutral stops there
+            const int t = a.ft.index[f];
+            if (t >= 0 && a.ft.side[t] == ((fs < 0) ? 1 : 0)) R.nbr[sl] = -3 - t;
+        }
     }
     plasma_in_cell(a, c, R.rho_th, R.cp, R.V);
     cells[c] = R;
+}
+
+// A neutral that stops on tallied face table t (AMR_f::Add_particle,
+// AMR_f.cpp:240-316): the moments mu / |v_n|, mu, mu / v_n^2, then its local
+// velocity, clamped 1e-7 inside the table's bounds, adds mu to the first leaf
+// that holds it (half-open boxes, the order of the table); where no leaf does,
+// the point shrinks toward the origin by 0.995 and is looked up again, as the
+// reference does, and after 30 tries counts as unplaced.
+__device__ void tally_outgoing(const Args& a, int t, const double v[3]) {
+    const McFaceTally& T = a.ft;
+    const double* E = T.frame + 9 * (size_t)t;
+    const double Vnn = fabs(v[0] * E[0] + v[1] * E[1] + v[2] * E[2]);
+    atomicAdd(&T.mom[3 * t], a.mu / Vnn);
+    atomicAdd(&T.mom[3 * t + 1], a.mu);
+    atomicAdd(&T.mom[3 * t + 2], a.mu * ((1.0 / Vnn) * (1.0 / Vnn)));
+    double x = v[0] * E[0] + v[1] * E[1] + v[2] * E[2];
+    double y = v[0] * E[3] + v[1] * E[4] + v[2] * E[5];
+    double z = v[0] * E[6] + v[1] * E[7] + v[2] * E[8];
+    const double* B = T.bounds + 6 * (size_t)t;
+    if (x < B[0]) x = B[0] + 1e-7;
+    if (x > B[1]) x = B[1] - 1e-7;
+    if (y < B[2]) y = B[2] + 1e-7;
+    if (y > B[3]) y = B[3] - 1e-7;
+    if (z < B[4]) z = B[4] + 1e-7;
+    if (z > B[5]) z = B[5] - 1e-7;
+    const int l0 = T.leaf_ptr[t], l1 = T.leaf_ptr[t + 1];
+    for (int kk = 1; kk <= 30; ++kk) {
+        for (int l = l0; l < l1; ++l) {
+            const double* b = T.box + 6 * (size_t)l;
+            if (b[0] <= x && x < b[1] && b[2] <= y && y < b[3] && b[4] <= z && z < b[5]) {
+                atomicAdd(&T.f[l], a.mu);
+                return;
+            }
+        }
+        x *= 0.995;
+        if (kk < 20) {
+            y *= 0.995;
+            z *= 0.995;
+        }
+    }
+    atomicAdd(T.unplaced, 1ull);
 }
 
 __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* __restrict__ cells) {
@@ -356,8 +401,12 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
             atomicAdd(&T[cell], a.mu * t_exit);
             I += dI;
             for (int k = 0; k < 3; ++k) x[k] += t_exit * v[k];
-            if (next < 0) {  // left through the boundary
+            if (next < 0) {  // left through the boundary, or stopped on a tallied face
                 kind = 0;
+                if (next <= -3) {
+                    tally_outgoing(a, -3 - next, v);
+                    kind = 3;
+                }
                 break;
             }
             cell = next;
@@ -384,7 +433,7 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
         ksi = -log(1.0 - rng.uniform());
         ++nex;
     }
-    if (kind != 0) atomicAdd(a.lost, 1ull);
+    if (kind == 1 || kind == 2) atomicAdd(a.lost, 1ull);
     if (a.trace) {
         double* r = a.trace + 8 * pid;
         r[0] = x[0];
@@ -394,7 +443,7 @@ __global__ void __launch_bounds__(128) trace_cells_kernel(Args a, const McCell* 
         r[4] = v[1];
         r[5] = v[2];
         r[6] = (double)nex;
-        r[7] = 4.0 * (double)(visit + (kind == 0 ? 1 : 0)) + (double)kind;
+        r[7] = 4.0 * (double)(visit + (kind == 0 || kind == 3 ? 1 : 0)) + (double)kind;
     }
 }
 
@@ -407,7 +456,27 @@ __global__ void normalise_kernel(double* T, const double* vol, int nc) {
     for (int k = 0; k < 5; ++k) T[k * nc + c] /= V;
 }
 
+// The outgoing tables per unit face area; each leaf's weight also per unit box
+// volume and box-centre normal speed (AMR_f::Normir_velocity_volume,
+// AMR_f.cpp:318-336). One thread per table.
+__global__ void tally_normalise_kernel(Args a, int ntab) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntab) return;
+    const McFaceTally& T = a.ft;
+    const double squ = a.L.fa[T.face[t]];
+    for (int k = 0; k < 3; ++k) T.mom[3 * t + k] /= squ;
+    for (int l = T.leaf_ptr[t]; l < T.leaf_ptr[t + 1]; ++l) {
+        const double* b = T.box + 6 * (size_t)l;
+        T.f[l] /= ((b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]) * squ * ((b[0] + b[1]) / 2.0));
+    }
+}
+
 }  // namespace mc
+
+cudaError_t launch_mc_tally_normalise(const McArgs& a, int ntab, cudaStream_t s) {
+    mc::tally_normalise_kernel<<<blocks_for(ntab, 128), 128, 0, s>>>(a, ntab);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_mc_inflow_cdf(const McArgs& a, double* cdf, double* block_sums, double* total_out,
                                  cudaStream_t s) {

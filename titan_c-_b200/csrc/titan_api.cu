@@ -142,6 +142,11 @@ struct titan_ctx {
     // tabulated inflow distributions (titan_set_mc_face_dist): index, frame,
     // side, flux, leaf_ptr, box, cum (McFaceDist)
     void* fd_buf[7] = {};
+    // tallied outgoing distributions (titan_set_mc_face_tally): index, face,
+    // side, frame, bounds, leaf_ptr, box, f, mom, unplaced (McFaceTally)
+    void* ft_buf[10] = {};
+    int64_t ft_ntab = 0, ft_nleaf = 0;
+    bool ft_valid = false;  // the tables hold a finished pass
     double* d_mc_blocks = nullptr;      // [mc_scan_blocks(nface)] + 1: block sums, total
     double* d_mc_tally = nullptr;       // [5][ncell]
     unsigned long long* d_mc_lost = nullptr;
@@ -554,6 +559,8 @@ int titan_destroy(titan_ctx* ctx) {
     for (void* p : ctx->surf_buf)
         if (p) cudaFree(p);
     for (void* p : ctx->fd_buf)
+        if (p) cudaFree(p);
+    for (void* p : ctx->ft_buf)
         if (p) cudaFree(p);
     if (ctx->d_cl_in) cudaFree(ctx->d_cl_in);
     if (ctx->d_cl_y) cudaFree(ctx->d_cl_y);
@@ -1446,6 +1453,19 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, tit
         a.fd.box = (const double*)ctx->fd_buf[5];
         a.fd.cum = (const double*)ctx->fd_buf[6];
     }
+    if (ctx->ft_buf[0]) {
+        a.ft.index = (const int*)ctx->ft_buf[0];
+        a.ft.face = (const int*)ctx->ft_buf[1];
+        a.ft.side = (const signed char*)ctx->ft_buf[2];
+        a.ft.frame = (const double*)ctx->ft_buf[3];
+        a.ft.bounds = (const double*)ctx->ft_buf[4];
+        a.ft.leaf_ptr = (const int*)ctx->ft_buf[5];
+        a.ft.box = (const double*)ctx->ft_buf[6];
+        a.ft.f = (double*)ctx->ft_buf[7];
+        a.ft.mom = (double*)ctx->ft_buf[8];
+        a.ft.unplaced = (unsigned long long*)ctx->ft_buf[9];
+        ctx->ft_valid = false;
+    }
     // per-neutral end records (tests and diagnostics): a buffer for this pass only
     struct TraceBuf {
         double* p = nullptr;
@@ -1469,9 +1489,15 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, tit
     a.mu = total / (double)mp->n_particles;
     CK(cudaMemsetAsync(ctx->d_mc_tally, 0, sizeof(double) * 5 * nc, s));
     CK(cudaMemsetAsync(ctx->d_mc_lost, 0, sizeof(unsigned long long), s));
+    if (a.ft.index) {
+        CK(cudaMemsetAsync(a.ft.f, 0, sizeof(double) * ctx->ft_nleaf, s));
+        CK(cudaMemsetAsync(a.ft.mom, 0, sizeof(double) * 3 * ctx->ft_ntab, s));
+        CK(cudaMemsetAsync(a.ft.unplaced, 0, sizeof(unsigned long long), s));
+    }
     CK(launch_mc_pack(a, ctx->d_mc_cells, s));
     CK(launch_mc_trace_cells(a, ctx->d_mc_cells, s));
     CK(launch_mc_normalise(ctx->d_mc_tally, L.vol, (int)nc, s));
+    if (a.ft.index) CK(launch_mc_tally_normalise(a, (int)ctx->ft_ntab, s));
     // back to the caller's cell numbering on the device, then one copy
     if (out) CK(launch_scatter(ctx->d_mc_tally, ctx->d_stage, ctx->d_cell_n2o, (int)nc, 5, s));
     CK(cudaEventRecord(ctx->ev[1], s));
@@ -1485,6 +1511,7 @@ int titan_mc_sources(titan_ctx* ctx, const titan_mc_params* mp, double* out, tit
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
     ctx->mc_valid = true;
+    ctx->ft_valid = a.ft.index != nullptr;
     if (info) {
         info->particles = mp->n_particles;
         info->lost = (int64_t)lost;
@@ -1558,6 +1585,96 @@ int titan_set_mc_face_dist(titan_ctx* ctx, const titan_mc_face_dist* d) {
             p = nullptr;
         }
         return fail(TITAN_ECUDA, std::string("face tables: ") + cudaGetErrorString(e));
+    }
+    return TITAN_OK;
+}
+
+namespace {
+void drop_face_tally(titan_ctx* ctx) {
+    for (void*& p : ctx->ft_buf) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    ctx->ft_ntab = ctx->ft_nleaf = 0;
+    ctx->ft_valid = false;
+}
+}  // namespace
+
+int titan_set_mc_face_tally(titan_ctx* ctx, const titan_mc_face_tally* d) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    drop_face_tally(ctx);
+    if (!d || d->nface == 0) return TITAN_OK;
+    if (d->nface < 0 || !d->face || !d->side || !d->frame || !d->leaf_ptr || !d->leaf_box)
+        return fail(TITAN_EINVAL, "face tallies: nface >= 0 and every array");
+    const int64_t nf = ctx->nface, nt = d->nface;
+    const Renumbering& R = ctx->R;
+    if (d->leaf_ptr[0] != 0) return fail(TITAN_EINVAL, "face tallies: leaf_ptr[0] must be 0");
+    const int64_t nleaf = d->leaf_ptr[nt];
+    if (nleaf < nt || nleaf > INT32_MAX) return fail(TITAN_EINVAL, "face tallies: leaf_ptr[nface] out of range");
+    std::vector<int32_t> index(nf, -1), face(nt), ptr(nt + 1, 0);
+    std::vector<int8_t> side(nt);
+    std::vector<double> bounds(6 * nt);
+    std::vector<int32_t> c1(nf);
+    CK(cudaMemcpy(c1.data(), ctx->d_face_c1, sizeof(int32_t) * nf, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nt; ++i) {
+        const int32_t fo = d->face[i];
+        if (fo < 0 || fo >= nf) return fail(TITAN_EINVAL, "face tallies: face id out of range");
+        const int32_t f = R.face_o2n[fo];
+        if (index[f] >= 0) return fail(TITAN_EINVAL, "face tallies: a face is listed twice");
+        index[f] = (int32_t)i;
+        face[i] = f;
+        if (d->side[i] != 0 && d->side[i] != 1) return fail(TITAN_EINVAL, "face tallies: side is 0 or 1");
+        if (d->side[i] == 1 && c1[f] < 0) return fail(TITAN_EINVAL, "face tallies: side 1 on a boundary face");
+        side[i] = d->side[i];
+        const int64_t l0 = d->leaf_ptr[i], l1 = d->leaf_ptr[i + 1];
+        if (!(l1 > l0) || l1 > nleaf) return fail(TITAN_EINVAL, "face tallies: leaf_ptr must increase to leaf_ptr[nface]");
+        ptr[i + 1] = (int32_t)l1;
+        double* B = &bounds[6 * i];
+        for (int k = 0; k < 6; k += 2) {
+            B[k] = INFINITY;
+            B[k + 1] = -INFINITY;
+        }
+        for (int64_t l = l0; l < l1; ++l) {
+            const double* b = d->leaf_box + 6 * l;
+            if (!(b[0] >= 0.0 && b[1] > b[0] && b[3] > b[2] && b[5] > b[4]) || !std::isfinite(b[1]) ||
+                !std::isfinite(b[2]) || !std::isfinite(b[3]) || !std::isfinite(b[4]) || !std::isfinite(b[5]))
+                return fail(TITAN_EINVAL, "face tallies: leaves need 0 <= xL < xR, yL < yR, zL < zR");
+            for (int k = 0; k < 6; k += 2) {
+                B[k] = std::min(B[k], b[k]);
+                B[k + 1] = std::max(B[k + 1], b[k + 1]);
+            }
+        }
+    }
+    std::vector<double> frame(d->frame, d->frame + 9 * nt);
+    std::vector<double> box(d->leaf_box, d->leaf_box + 6 * nleaf);
+    cudaError_t e = upload_vec(&ctx->ft_buf[0], index);
+    if (!e) e = upload_vec(&ctx->ft_buf[1], face);
+    if (!e) e = upload_vec(&ctx->ft_buf[2], side);
+    if (!e) e = upload_vec(&ctx->ft_buf[3], frame);
+    if (!e) e = upload_vec(&ctx->ft_buf[4], bounds);
+    if (!e) e = upload_vec(&ctx->ft_buf[5], ptr);
+    if (!e) e = upload_vec(&ctx->ft_buf[6], box);
+    if (!e) e = cudaMalloc(&ctx->ft_buf[7], sizeof(double) * nleaf);
+    if (!e) e = cudaMalloc(&ctx->ft_buf[8], sizeof(double) * 3 * nt);
+    if (!e) e = cudaMalloc(&ctx->ft_buf[9], sizeof(unsigned long long));
+    if (e) {
+        drop_face_tally(ctx);
+        return fail(TITAN_ECUDA, std::string("face tallies: ") + cudaGetErrorString(e));
+    }
+    ctx->ft_ntab = nt;
+    ctx->ft_nleaf = nleaf;
+    return TITAN_OK;
+}
+
+int titan_get_mc_face_tally(titan_ctx* ctx, double* leaf_f, double* moments, int64_t* unplaced) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    if (!ctx->ft_valid) return fail(TITAN_EINVAL, "face tallies: no Monte-Carlo pass since they were set");
+    if (leaf_f) CK(cudaMemcpy(leaf_f, ctx->ft_buf[7], sizeof(double) * ctx->ft_nleaf, cudaMemcpyDeviceToHost));
+    if (moments) CK(cudaMemcpy(moments, ctx->ft_buf[8], sizeof(double) * 3 * ctx->ft_ntab, cudaMemcpyDeviceToHost));
+    if (unplaced) {
+        unsigned long long u = 0;
+        CK(cudaMemcpy(&u, ctx->ft_buf[9], sizeof(u), cudaMemcpyDeviceToHost));
+        *unplaced = (int64_t)u;
     }
     return TITAN_OK;
 }

@@ -91,6 +91,11 @@ class TitanMcFaceDist(ctypes.Structure):
                 ("leaf_f", ctypes.c_void_p)]
 
 
+class TitanMcFaceTally(ctypes.Structure):
+    _fields_ = [("nface", ctypes.c_int64), ("face", ctypes.c_void_p), ("side", ctypes.c_void_p),
+                ("frame", ctypes.c_void_p), ("leaf_ptr", ctypes.c_void_p), ("leaf_box", ctypes.c_void_p)]
+
+
 class TitanMcInfo(ctypes.Structure):
     _fields_ = [("particles", ctypes.c_int64), ("lost", ctypes.c_int64), ("inflow_rate", ctypes.c_double),
                 ("gpu_ms", ctypes.c_double)]
@@ -125,6 +130,8 @@ SIGNATURES = {
                                   ctypes.c_int32, I32], ctypes.c_int),
     "titan_set_ray_law": ([ctypes.c_void_p, ctypes.POINTER(TitanRayLaw)], ctypes.c_int),
     "titan_set_mc_face_dist": ([ctypes.c_void_p, ctypes.POINTER(TitanMcFaceDist)], ctypes.c_int),
+    "titan_set_mc_face_tally": ([ctypes.c_void_p, ctypes.POINTER(TitanMcFaceTally)], ctypes.c_int),
+    "titan_get_mc_face_tally": ([ctypes.c_void_p, D, D, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "titan_upload_state": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_download_state": ([ctypes.c_void_p, D], ctypes.c_int),
     "titan_upload_hfluids": ([ctypes.c_void_p, D], ctypes.c_int),

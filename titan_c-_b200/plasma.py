@@ -304,6 +304,33 @@ class PlasmaStep:
                                                    ("face", "side", "frame", "leaf_ptr", "leaf_box", "leaf_f")))
         N.check(self._lib.titan_set_mc_face_dist(self._ctx, ctypes.byref(d)))
 
+    def set_mc_face_tally(self, face_tally: dict | None):
+        """Outgoing distributions tallied on some faces (titan_set_mc_face_tally):
+        face (original ids), side, frame [n, 9], leaf_ptr [n + 1], leaf_box
+        [nleaf, 6]; None removes them."""
+        if face_tally is None:
+            N.check(self._lib.titan_set_mc_face_tally(self._ctx, None))
+            self._ft_shape = None
+            return
+        arrs = dict(face=np.ascontiguousarray(face_tally["face"], dtype=np.int32),
+                    side=np.ascontiguousarray(face_tally["side"], dtype=np.int8),
+                    frame=np.ascontiguousarray(face_tally["frame"], dtype=np.float64),
+                    leaf_ptr=np.ascontiguousarray(face_tally["leaf_ptr"], dtype=np.int64),
+                    leaf_box=np.ascontiguousarray(face_tally["leaf_box"], dtype=np.float64))
+        d = N.TitanMcFaceTally(len(arrs["face"]), *(arrs[k].ctypes.data for k in
+                                                    ("face", "side", "frame", "leaf_ptr", "leaf_box")))
+        N.check(self._lib.titan_set_mc_face_tally(self._ctx, ctypes.byref(d)))
+        self._ft_shape = (len(arrs["face"]), int(arrs["leaf_ptr"][-1]))
+
+    def mc_face_tally(self) -> dict:
+        """The last pass's face tallies: leaf_f [nleaf], moments [n, 3] (n, Smu, nn), unplaced."""
+        nt, nl = self._ft_shape
+        f = np.empty(nl)
+        mom = np.empty((nt, 3))
+        u = ctypes.c_int64(0)
+        N.check(self._lib.titan_get_mc_face_tally(self._ctx, N.ptr(f), N.ptr(mom), ctypes.byref(u)))
+        return dict(leaf_f=f, moments=mom, unplaced=u.value)
+
     def mc_pass(self, n_H: float, u_H, cp_H: float, n_particles: int, seed: int = 1,
                 face_types: int = (1 << 2) | (1 << 3), max_cells: int = 0) -> dict:
         """A Monte-Carlo pass whose sources stay on the device (for

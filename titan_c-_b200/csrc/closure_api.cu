@@ -34,6 +34,7 @@ cudaError_t launch_loss_sched(const float* Y, const float* T, const float* w, co
 cudaError_t launch_adam_sched(float* p, const float* g, float* m, float* v, int n, float b1, float b2, float eps,
                               const unsigned char* mask, const TrainSched* sched, int* step, cudaStream_t s);
 cudaError_t launch_pack(const float* P, void* out, cudaStream_t s);
+int gemm_error_take();
 
 namespace {
 
@@ -130,7 +131,9 @@ cudaError_t backward_with(Trainer& t, Loss loss, cudaStream_t s) {
     if (!e) e = loss();
     const char* Wb = static_cast<const char*>(t.Wb);
     const void* dZl = t.dY;
-    const int split = t.rows >= 8192 ? 32 : (t.rows >= 1024 ? 8 : 1);
+    // dW = A^T dZ has K = the batch's rows: split it so a batch of a few
+    // thousand rows still spreads over tens of CTAs (two 32-row chunks or more each)
+    const int split = std::max(1, std::min(64, t.rows / 64));
     for (int l = 4; l >= 0 && !e; --l) {
         const void* Ain = l > 0 ? t.A[l - 1] : (const void*)t.X0;
         // dW_l = A_{l-1}^T dZ_l  ([in][out]), db_l = colsum dZ_l
@@ -269,6 +272,7 @@ int titan_mlp_grad(const float* params, const float* norm, const float* X, const
                                          sizeof(float) * kOut, n, cudaMemcpyDeviceToHost, s);
     if (!e) e = cudaStreamSynchronize(s);
     if (e) return mfail(TITAN_ECUDA, std::string("titan_mlp_grad: ") + cudaGetErrorString(e));
+    if (gemm_error_take()) return mfail(TITAN_ETIMEOUT, "titan_mlp_grad: a tensor-core wait ran out");
     return TITAN_OK;
 }
 
@@ -353,6 +357,7 @@ int titan_mlp_train(float* params, const float* norm, const float* X, const floa
     if (g) cudaGraphDestroy(g);
     if (s) cudaStreamDestroy(s);
     if (e) return mfail(TITAN_ECUDA, std::string("titan_mlp_train: ") + cudaGetErrorString(e));
+    if (gemm_error_take()) return mfail(TITAN_ETIMEOUT, "titan_mlp_train: a tensor-core wait ran out");
     if (loss_per_epoch)
         for (int ep = 0; ep < o->epochs; ++ep) loss_per_epoch[ep] = el[ep] / (float)(nb > 0 ? nb : 1);
     return TITAN_OK;

@@ -1,5 +1,6 @@
-// Training of the charge-exchange closure on the GPU: BF16 tensor-core GEMMs
-// with FP32 accumulation (mma.sync m16n8k16 tiles fed by ldmatrix), the SiLU
+// Training of the charge-exchange closure on the GPU: BF16 GEMMs on the
+// 5th-generation tensor cores (tcgen05.mma, FP32 accumulator in tensor
+// memory, operands staged in shared memory), the SiLU
 // forward/backward, bias gradients, the weighted MSE loss and Adam, all in
 // this file's kernels. Layer-wise, for a batch of rows:
 //   forward   Z_l = A_{l-1} W_l + b_l, A_l = SiLU(Z_l) (bf16), Y = A_4 W_5 + b_5
@@ -14,104 +15,148 @@
 #include <cstdint>
 
 #include "closure.h"
+#include "tcgen05.cuh"
 
 namespace titan {
 namespace train {
 
-constexpr int BM = 64, BN = 64, BK = 32, PAD = 8;
+using namespace tc;
 
-__device__ __forceinline__ void ldmatrix_x4(uint32_t* r, const void* p) {
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
+// Tiles of the training GEMM: 128 rows (the tcgen05 M) by up to 64 columns,
+// K staged 32 at a time, two stages in flight.
+constexpr int TM = 128, TK = 32, TN = 64;
+
+// Set when a bounded wait of a training GEMM ran out (read by the host API).
+__device__ int g_gemm_error;
+
+// Copies the [rows x TK] K-chunk at k0 of op(X) into shared memory in the
+// canonical K-major layout (R rows, canon_index), zero outside rows x K.
+// op(X)[r][k] = X[r * ld + k] (K contiguous: 16-byte copies of 8 elements),
+// or X[k * ld + r] when TR (rows contiguous: element copies, consecutive
+// threads along r so the loads coalesce).
+template <bool TR>
+__device__ __forceinline__ void stage_chunk(__nv_bfloat16* dst, int R, const __nv_bfloat16* __restrict__ X, int ld,
+                                            int r0, int rows, int k0, int K) {
+    if (!TR) {
+        // K and ld are multiples of 8 here (the layer widths), so a 16-byte
+        // unit is either wholly inside K or wholly past it
+        for (int u = threadIdx.x; u < R * (TK / 8); u += blockDim.x) {
+            const int r = u / (TK / 8), k = (u % (TK / 8)) * 8;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (r0 + r < rows && k0 + k < K) v = *reinterpret_cast<const uint4*>(X + (size_t)(r0 + r) * ld + k0 + k);
+            *reinterpret_cast<uint4*>(dst + canon_index(r, k, R)) = v;
+        }
+    } else {
+        const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+        for (int e = threadIdx.x; e < R * TK; e += blockDim.x) {
+            const int r = e % R, k = e / R;
+            __nv_bfloat16 v = zero;
+            if (r0 + r < rows && k0 + k < K) v = X[(size_t)(k0 + k) * ld + r0 + r];
+            dst[canon_index(r, k, R)] = v;
+        }
+    }
 }
 
-__device__ __forceinline__ void ldmatrix_x2(uint32_t* r, const void* p) {
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
-}
-
-__device__ __forceinline__ void mma16816(float* c, const uint32_t* a, const uint32_t* b) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// C[M][N] (+)= op(A) op(B); op(A) = A (row-major, lda) or A^T; op(B) = B
-// (row-major [K][N], ldb) or B^T (B stored [N][K]). 128 threads, 64x64 tile,
-// four warps of 32x32; K split across gridDim.z when `atomic` (C += partial).
+// C[M][N] (+)= op(A) op(B) on the tensor cores (tcgen05.mma, kind::f16, FP32
+// accumulator in tensor memory). op(A) = A (row-major [M][K], lda) or A^T (A
+// stored [K][M]); op(B) = B (row-major [K][N], ldb) or B^T (B stored [N][K]).
+// One CTA of 128 threads per tile of 128 rows by 64 columns; K split over
+// gridDim.z when `atomic` (C += the slice's partial sum). Each K-chunk
+// is staged by all threads into one of two buffers; one thread issues its
+// K = 16 steps and commits them to that buffer's mbarrier, which the threads
+// wait on before they refill the buffer two chunks later. The epilogue reads
+// the accumulator with tcgen05.ld (warp w owns rows 32w .. 32w+31).
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(128) gemm_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda,
                                                    const __nv_bfloat16* __restrict__ B, int ldb, float* __restrict__ C,
                                                    int ldc, int atomic) {
-    __shared__ __align__(16) __nv_bfloat16 As[BM][BK + PAD];
-    __shared__ __align__(16) __nv_bfloat16 Bs[BN][BK + PAD];
+    __shared__ __align__(128) __nv_bfloat16 As[2][TM * TK];
+    __shared__ __align__(128) __nv_bfloat16 Bs[2][TN * TK];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int kchunks = (K + BK - 1) / BK;
+    const int n0 = blockIdx.x * TN;
+    const int NP = (min(TN, N - n0) + 15) & ~15;  // this tile's columns, padded to the MMA's granularity
+    const int m0 = blockIdx.y * TM;
+    const int kchunks = (K + TK - 1) / TK;
     const int per = (kchunks + gridDim.z - 1) / gridDim.z;
     const int kc0 = blockIdx.z * per, kc1 = min(kchunks, kc0 + per);
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0f;
-    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-    for (int kc = kc0; kc < kc1; ++kc) {
-        const int k0 = kc * BK;
-        // staging runs along the operand's contiguous dimension in memory, so
-        // that a warp's loads coalesce (m for A^T, k for A; n for B, k for B^T)
-        for (int i = tid; i < BM * BK; i += 128) {
-            const int mm = TA ? i % BM : i / BK, kk = TA ? i / BM : i % BK;
-            const int gm = m0 + mm, gk = k0 + kk;
-            __nv_bfloat16 v = zero;
-            if (gm < M && gk < K) v = TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
-            As[mm][kk] = v;
-        }
-        for (int i = tid; i < BN * BK; i += 128) {
-            const int nn = TB ? i / BK : i % BN, kk = TB ? i % BK : i / BN;
-            const int gn = n0 + nn, gk = k0 + kk;
-            __nv_bfloat16 v = zero;
-            if (gn < N && gk < K) v = TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
-            Bs[nn][kk] = v;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int ks = 0; ks < BK; ks += 16) {
-            uint32_t af[2][4], bf[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) ldmatrix_x4(af[i], &As[wm + i * 16 + (lane & 15)][ks + 8 * (lane >> 4)]);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) ldmatrix_x2(bf[j], &Bs[wn + j * 8 + (lane & 7)][ks + 8 * ((lane >> 3) & 1)]);
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) mma16816(acc[i][j], af[i], bf[j]);
-        }
-        __syncthreads();
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(TN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tm = tmem_base;
+    const uint32_t idesc = instr_desc(TM, NP);
+    bool ok = true;
+    int n_chunks = 0;
+    for (int kc = kc0; kc < kc1; ++kc, ++n_chunks) {
+        const int buf = n_chunks & 1;
+        // the MMAs that read this buffer two chunks ago must have finished;
+        // the whole block stops if any thread's wait ran out
+        const bool w = n_chunks < 2 || mbar_sleep_wait(smem_u32(&mbar[buf]), ((n_chunks >> 1) - 1) & 1);
+        if (!__syncthreads_and(w)) {
+            ok = false;
+            break;
+        }
+        const int k0 = kc * TK;
+        stage_chunk<TA>(As[buf], TM, A, lda, m0, M, k0, K);
+        stage_chunk<!TB>(Bs[buf], NP, B, ldb, n0, N, k0, K);
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        if (tid == 0) {
+            const int ksteps = (min(TK, K - k0) + 15) / 16;
+            const uint32_t a0 = smem_u32(As[buf]), b0 = smem_u32(Bs[buf]);
+            for (int s = 0; s < ksteps; ++s)
+                mma_bf16(tm, smem_desc(a0 + s * 2 * TM * 16, TM * 16, 128), smem_desc(b0 + s * 2 * NP * 16, NP * 16, 128),
+                         idesc, (n_chunks > 0 || s > 0) ? 1u : 0u);
+            commit(smem_u32(&mbar[buf]));
+        }
+    }
+    // the last commit covers every MMA before it (after a wait that ran out,
+    // one more bounded wait, so tensor memory is not freed under running MMAs)
+    bool w = true;
+    if (n_chunks > 0) {
+        const int last = n_chunks - 1;
+        w = mbar_sleep_wait(smem_u32(&mbar[last & 1]), (last >> 1) & 1);
+        if (!w) mbar_sleep_wait(smem_u32(&mbar[last & 1]), (last >> 1) & 1);
+    }
+    ok = __syncthreads_and(ok && w) != 0;
+    if (!ok && tid == 0) atomicExch(&g_gemm_error, 1);
+    fence_after();
+    if (ok && n_chunks > 0) {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t taddr = tm + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < NP; c0 += 16) {
+            float v[16];
+            tmem_ld16(taddr + (uint32_t)c0, v);
+            tmem_wait_ld();
+            if (row < M) {
+                float* dst = C + (size_t)row * ldc + n0 + c0;
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int gm = m0 + wm + i * 16 + (lane >> 2) + (e >= 2 ? 8 : 0);
-                const int gn = n0 + wn + j * 8 + 2 * (lane & 3) + (e & 1);
-                if (gm < M && gn < N) {
-                    float* dst = C + (size_t)gm * ldc + gn;
+                for (int j = 0; j < 16; ++j) {
+                    if (n0 + c0 + j >= N) break;
                     if (atomic)
-                        atomicAdd(dst, acc[i][j][e]);
+                        atomicAdd(dst + j, v[j]);
                     else
-                        *dst = acc[i][j][e];
+                        dst[j] = v[j];
                 }
             }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(TN));
 }
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
@@ -318,7 +363,9 @@ __global__ void pack_kernel(const float* P, __nv_bfloat16* out) {
 
 cudaError_t launch_gemm(bool ta, bool tb, int M, int N, int K, const void* A, int lda, const void* B, int ldb,
                         float* C, int ldc, int splitk, cudaStream_t s) {
-    dim3 grid((N + train::BN - 1) / train::BN, (M + train::BM - 1) / train::BM, splitk);
+    // a K-contiguous operand needs K and its leading dimension in multiples of 8
+    if ((!ta && (K % 8 || lda % 8)) || (tb && (K % 8 || ldb % 8))) return cudaErrorInvalidValue;
+    dim3 grid((N + train::TN - 1) / train::TN, (M + train::TM - 1) / train::TM, splitk);
     const int atomic = splitk > 1 ? 1 : 0;
     auto a = static_cast<const __nv_bfloat16*>(A);
     auto b = static_cast<const __nv_bfloat16*>(B);
@@ -391,6 +438,17 @@ cudaError_t launch_input(const float* X, const float* mean, const float* istd, v
     train::input_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(X, mean, istd, static_cast<__nv_bfloat16*>(X0),
                                                                       rows);
     return cudaGetLastError();
+}
+
+// 1 when a training GEMM's bounded wait ran out since the last call (and clears it).
+int gemm_error_take() {
+    int e = 0;
+    cudaMemcpyFromSymbol(&e, train::g_gemm_error, sizeof(int));
+    if (e) {
+        const int z = 0;
+        cudaMemcpyToSymbol(train::g_gemm_error, &z, sizeof(int));
+    }
+    return e;
 }
 
 cudaError_t launch_pack(const float* P, void* out, cudaStream_t s) {

@@ -571,7 +571,42 @@ def run_large(pkg, args, barrier, dev):
                     "step_roofline": step_roofline(m, True, net, ms, list(r["kt"])),
                     "kernel_ms_per_step": {k: v[0] / v[1] for k, v in r["kt"].items()}}
     out["speedup_vs_plain_fp64"] = out["plain_fp64"]["ms_per_step"] / out["mixed_mlp"]["ms_per_step"]
+    out["coupled"] = run_coupled_loop(pkg, m, p, st, closure, args, barrier, dev)
     return out
+
+
+COUPLED_STEPS, COUPLED_MC_EVERY = 300, 100
+COUPLED_MC = dict(n_H=0.18, u_H=(-2.6, 0.0, 0.0), cp_H=float(np.sqrt(2.0 * (0.06 * 1.3 ** 2 / (5.0 / 3.0)) / 0.06)),
+                  n_particles=10_000_000)
+
+
+def run_coupled_loop(pkg, m, p, st, closure, args, barrier, dev, steps=COUPLED_STEPS):
+    """The large configuration's coupled loop (closure.run_coupled): the mixed
+    step with MLP sources every step and, every 100 steps, a Monte-Carlo pass
+    (1e7 neutrals) through the current plasma whose sources the cells outside
+    the closure's training envelope take; timed with CUDA events on the
+    context's stream around the whole loop, passes included."""
+    import torch
+
+    C = m["cell_nodes"].shape[0]
+    step, tuning = make_step(pkg, m, p, st, 32, args.tuning, closure)
+    step.go(max(args.warmup, 3))
+    stream = torch.cuda.ExternalStream(step.stream())
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(dev) as clk:
+        ev0.record(stream)
+        r = pkg.closure.run_coupled(step, closure, steps, mc_every=COUPLED_MC_EVERY, **COUPLED_MC)
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    step.close()
+    return {"steps": steps, "mc_every": COUPLED_MC_EVERY, "mc_passes": r["mc_passes"],
+            "mc_particles": COUPLED_MC["n_particles"], "value": C * steps / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / steps, "clocks": clk.summary(),
+            "cells_outside_envelope": r["outside_last_step"],
+            "note": "device time of the whole loop, the Monte-Carlo passes and their fallback hand-over included"}
 
 
 def cpu_baseline(args, m, p, st, steps=None):

@@ -11,7 +11,12 @@ TITAN/source/Setka_MK.cpp:1225-1575, AMR_f.cpp:4-96, AMR_cell.cpp:273-326).
   analytic launch's velocity moments: without charge exchange a neutral's end
   velocity is its start velocity, so the mean velocity and mean speed squared
   of the two launches agree within sampling and discretisation error.
-* Bad tables are refused before anything runs.
+* Outgoing tallies (titan_set_mc_face_tally: AMR_f::Add_particle and
+  Normir_velocity_volume, AMR_f.cpp:240-336) on an interior sphere of faces
+  against the oracle's restatement, and the zone coupling they make with the
+  tabulated launch: a second pass launched from the first pass's tallies
+  reproduces the inner zone's neutral content of one uncoupled pass.
+* Bad tables and tallies are refused before anything runs.
 """
 import numpy as np
 import pytest

@@ -163,7 +163,9 @@ typedef struct titan_surface_params {
     int32_t null_bn_on_HP;                        /* Phys_param::null_bn_on_HP: the HP cells and face
                                                      states lose their normal B first */
     int32_t sglag_TS, sglag_HP, sglag_BS;         /* Phys_param::sglag_*: surface smoothing (above) */
-    int32_t pad;
+    int32_t hp_tail;                              /* 1: HP nodes with x < 0 move along (0, y, z) instead
+                                                     of x / |x|, the reference's rule for its heliotail
+                                                     (Setka_move.cpp:1237-1247) */
     double sglag_TS_k_sphere, sglag_HP_k_sphere;  /* Phys_param::sglag_TS_k_sphere / sglag_HP_k_sphere */
     double sglag_BS_k;                            /* Phys_param::sglag_BS_k */
 } titan_surface_params;

@@ -113,7 +113,8 @@ struct OParams {
     int32_t null_bn_on_HP;  // Phys_param::null_bn_on_HP
     int32_t pad2;
     double velocity_TS, velocity_HP, velocity_BS;  // Phys_param::velocity_TS / _HP / _BS
-    int32_t sglag_TS, sglag_HP, sglag_BS, pad3;     // Phys_param::sglag_*: surface smoothing
+    int32_t sglag_TS, sglag_HP, sglag_BS;           // Phys_param::sglag_*: surface smoothing
+    int32_t hp_tail;      // HP nodes with x < 0 move along (0, y, z) (Setka_move.cpp:1237-1247)
     double sglag_TS_k_sphere, sglag_HP_k_sphere, sglag_BS_k;
 };
 
@@ -1945,8 +1946,21 @@ static int o_surface_motion(const OMesh* M, const OParams* P, double* st, const 
         }
         if (cnt > 0)
             for (double& c : v) c /= cnt;
-        const double an = std::sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
-        const double B[3] = {A[0] / an, A[1] / an, A[2] / an};
+        // along x / |x|; an HP node of the heliotail (x < 0) along (0, y, z)
+        // with hp_tail (Setka_move.cpp:1237-1247), the zero vector (no motion)
+        // for a node on the x axis, as Eigen's normalize() leaves it
+        double B[3];
+        if (P->hp_tail && s == 2 && A[0] < 0.0) {
+            const double bn = std::sqrt(A[1] * A[1] + A[2] * A[2]);
+            B[0] = 0.0;
+            B[1] = bn > 0.0 ? A[1] / bn : 0.0;
+            B[2] = bn > 0.0 ? A[2] / bn : 0.0;
+        } else {
+            const double an = std::sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+            B[0] = A[0] / an;
+            B[1] = A[1] / an;
+            B[2] = A[2] / an;
+        }
         const double vb = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];
         for (int k = 0; k < 3; ++k) xyz2[3 * i + k] = A[k] + vb * time * B[k];
     }

@@ -63,13 +63,13 @@ class OParams(ctypes.Structure):
         ("null_bn_on_HP", ctypes.c_int32), ("pad2", ctypes.c_int32),
         ("velocity_TS", ctypes.c_double), ("velocity_HP", ctypes.c_double), ("velocity_BS", ctypes.c_double),
         ("sglag_TS", ctypes.c_int32), ("sglag_HP", ctypes.c_int32), ("sglag_BS", ctypes.c_int32),
-        ("pad3", ctypes.c_int32), ("sglag_TS_k_sphere", ctypes.c_double), ("sglag_HP_k_sphere", ctypes.c_double),
+        ("hp_tail", ctypes.c_int32), ("sglag_TS_k_sphere", ctypes.c_double), ("sglag_HP_k_sphere", ctypes.c_double),
         ("sglag_BS_k", ctypes.c_double),
     ]
 
 # The surface-tracking fields of OParams (titan_surface_params on the library side).
 SURFACE_KEYS = ("move_TS", "move_HP", "move_BS", "null_bn_on_HP", "velocity_TS", "velocity_HP", "velocity_BS",
-                "sglag_TS", "sglag_HP", "sglag_BS", "sglag_TS_k_sphere", "sglag_HP_k_sphere", "sglag_BS_k")
+                "sglag_TS", "sglag_HP", "sglag_BS", "sglag_TS_k_sphere", "sglag_HP_k_sphere", "sglag_BS_k", "hp_tail")
 
 
 class OStepInfo(ctypes.Structure):
@@ -271,7 +271,7 @@ class OracleRun:
         self.mesh = m
         p = OParams()
         for k, _ in OParams._fields_:
-            if k not in ("pad2", "pad3", "surface_motion") + SURFACE_KEYS:
+            if k not in ("pad2", "surface_motion") + SURFACE_KEYS:
                 setattr(p, k, params[k])
         if surface is not None:
             p.surface_motion = 1

@@ -32,6 +32,7 @@ def _surface_shell(T, **kw):
     dict(ragged=True),
     dict(surface=dict(sglag_TS=1, sglag_HP=1, sglag_BS=1, sglag_TS_k_sphere=0.3, sglag_HP_k_sphere=0.3,
                       sglag_BS_k=0.3, null_bn_on_HP=1)),
+    dict(surface=dict(hp_tail=1)),
 ])
 def test_surface_tracking_steps_match_oracle(titan, oracle_lib, variant):
     m, p, st, rays = _surface_shell(titan, **variant.get("shell", {}))
@@ -64,6 +65,11 @@ def test_surface_tracking_steps_match_oracle(titan, oracle_lib, variant):
     assert np.array_equal(x[rays[:, 0]], x0[rays[:, 0]])
     full = rays[:, -1] >= 0
     assert np.array_equal(x[rays[full, -1]], x0[rays[full, -1]])
+    if surf.get("hp_tail"):
+        # the heliotail's HP nodes move across the x axis only
+        hp = rays[:, 9]
+        tail = x0[hp, 0] < 0
+        assert tail.any() and np.array_equal(x[hp[tail], 0], x0[hp[tail], 0])
     gpu.close()
 
 

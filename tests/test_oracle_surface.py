@@ -270,3 +270,26 @@ def test_a_luch_law_places_ray_nodes_from_the_moved_surfaces(titan, oracle_lib):
     d0 = x0[rays[:, 0]] / np.linalg.norm(x0[rays[:, 0]], axis=1)[:, None]
     u = run.xyz[rays] / r[:, :, None]
     assert np.abs(u - d0[:, None, :]).max() <= 1e-12
+
+
+def test_hp_tail_nodes_move_across_the_axis_only(titan, oracle_lib):
+    """With hp_tail (Setka_move.cpp:1237-1247) an HP node with x < 0 moves
+    along (0, y, z): its x stays, its distance from the x axis changes; HP
+    nodes with x >= 0 still move along their own direction."""
+    m, p, st = _shell(titan)
+    titan.mesh.mark_shell_surface(m, 6, 2)
+    rays = titan.mesh.shell_rays(m)
+    surf = dict(SURF, move_TS=0, move_BS=0, hp_tail=1)
+    run = ol.OracleRun(m, p, surface=surf, rays=rays)
+    x0 = run.xyz.copy()
+    assert run.go(np.ascontiguousarray(st.copy()), 2).err_code == 0
+    hp = rays[:, 6]
+    tail = x0[hp, 0] < 0
+    assert tail.any() and (~tail).any()
+    assert np.array_equal(run.xyz[hp[tail], 0], x0[hp[tail], 0])
+    assert np.abs(np.hypot(run.xyz[hp[tail], 1], run.xyz[hp[tail], 2]) -
+                  np.hypot(x0[hp[tail], 1], x0[hp[tail], 2])).max() > 0
+    head = hp[~tail]
+    u0 = x0[head] / np.linalg.norm(x0[head], axis=1)[:, None]
+    u1 = run.xyz[head] / np.linalg.norm(run.xyz[head], axis=1)[:, None]
+    assert np.abs(u1 - u0).max() < 1e-12

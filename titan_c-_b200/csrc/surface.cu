@@ -12,7 +12,8 @@
 //     neighbours are left out of the list (:192).
 //  2. One thread per surface node: the mean of its faces' contributions,
 //     summed in ascending original face order, and the move
-//     x' = x + (V . x/|x|) dt x/|x| (:1213-1265).
+//     x' = x + (V . x/|x|) dt x/|x| (:1213-1265); with hp_tail an HP node
+//     with x < 0 moves along (0, y, z) instead (:1237-1247).
 //  3. One thread per ray node: every node between two anchors (the ray's ends
 //     and its surface nodes) keeps its initial fraction of that segment, on
 //     the ray's direction; or, with the A_Luch law (Luch.cpp:9-152), takes the
@@ -175,8 +176,22 @@ __global__ void node_kernel(FaceArgs a, SurfaceDev S) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) v[k] /= num;
     }
-    const double an = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
-    const double B[3] = {A[0] / an, A[1] / an, A[2] / an};
+    // the direction of motion: x / |x|, or (0, y, z) normalised for an HP node
+    // of the heliotail (x < 0) with hp_tail (Setka_move.cpp:1237-1247); a node
+    // on the x axis keeps the zero vector, as Eigen's normalize() leaves it,
+    // and stays
+    double B[3];
+    if (S.node_tail && S.node_tail[i] && A[0] < 0.0) {
+        const double bn = sqrt(A[1] * A[1] + A[2] * A[2]);
+        B[0] = 0.0;
+        B[1] = bn > 0.0 ? A[1] / bn : 0.0;
+        B[2] = bn > 0.0 ? A[2] / bn : 0.0;
+    } else {
+        const double an = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+        B[0] = A[0] / an;
+        B[1] = A[1] / an;
+        B[2] = A[2] / an;
+    }
     const double vb = v[0] * B[0] + v[1] * B[1] + v[2] * B[2];
     double* x2 = const_cast<double*>(a.xyz2);
 #pragma unroll

@@ -55,6 +55,8 @@ struct SurfaceDev {
     const double* sm_centre;      // [3][n_node]
     const int* nb_ptr;            // [n_node + 1]
     const int* nb_id;             // device node ids
+    // [n_node] 1: an HP node that moves along (0, y, z) where x < 0 (hp_tail), or null
+    const signed char* node_tail;
 };
 
 // xyz2 of `fa` from xyz of fa.L1 by surface tracking, with the step's dt from

@@ -133,7 +133,7 @@ struct titan_ctx {
     SurfaceDev surf{};
     std::vector<int32_t> h_ray_nodes;  // the rays of surf (device node ids, -1 padding)
     std::vector<int8_t> h_node_surf;   // per device node: the surface (1 TS, 2 HP, 3 BS) it lies on, or 0
-    void* surf_buf[14] = {};  // face_list, vf, node_id, node_ptr, node_face, ray_nodes, ray_r0, ray_dir, ray_seg,
+    void* surf_buf[15] = {};  // face_list, vf, node_id, node_ptr, node_face, ray_nodes, ray_r0, ray_dir, ray_seg,
                               // sm_kind, sm_coef, sm_centre, nb_ptr, nb_id
 
     // Monte-Carlo pass buffers (titan_mc_sources), allocated by the first pass
@@ -1852,6 +1852,11 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     if (!e) e = upload_vec(&ctx->surf_buf[11], sm_centre);
     if (!e) e = upload_vec(&ctx->surf_buf[12], nb_ptr);
     if (!e) e = upload_vec(&ctx->surf_buf[13], nb_id);
+    if (!e && sp->hp_tail) {
+        std::vector<signed char> tail(S.n_node);
+        for (int i = 0; i < S.n_node; ++i) tail[i] = node_surf[node_id[i]] == 2 ? 1 : 0;
+        e = upload_vec(&ctx->surf_buf[14], tail);
+    }
     if (e) {
         drop_surface(ctx);
         return fail(TITAN_ECUDA, std::string("surface tables: ") + cudaGetErrorString(e));
@@ -1870,6 +1875,7 @@ int titan_set_surface_motion(titan_ctx* ctx, const titan_surface_params* sp, int
     S.sm_centre = (const double*)ctx->surf_buf[11];
     S.nb_ptr = (const int*)ctx->surf_buf[12];
     S.nb_id = (const int*)ctx->surf_buf[13];
+    S.node_tail = (const signed char*)ctx->surf_buf[14];
     ctx->surf = S;
     ctx->use_surface = true;
     ctx->h_ray_nodes = std::move(rn);

@@ -67,7 +67,7 @@ class TitanSurfaceParams(ctypes.Structure):
     _fields_ = [("velocity_TS", ctypes.c_double), ("velocity_HP", ctypes.c_double), ("velocity_BS", ctypes.c_double),
                 ("move_TS", ctypes.c_int32), ("move_HP", ctypes.c_int32), ("move_BS", ctypes.c_int32),
                 ("null_bn_on_HP", ctypes.c_int32), ("sglag_TS", ctypes.c_int32), ("sglag_HP", ctypes.c_int32),
-                ("sglag_BS", ctypes.c_int32), ("pad", ctypes.c_int32), ("sglag_TS_k_sphere", ctypes.c_double),
+                ("sglag_BS", ctypes.c_int32), ("hp_tail", ctypes.c_int32), ("sglag_TS_k_sphere", ctypes.c_double),
                 ("sglag_HP_k_sphere", ctypes.c_double), ("sglag_BS_k", ctypes.c_double)]
 
 

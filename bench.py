@@ -751,8 +751,8 @@ def main():
                     help="split one mesh over the GPUs (strong scaling) instead of N replicas")
     args = ap.parse_args()
     if args.impl == "reference":
-        # a bounded sample of the workload: a full step is about 0.35 s on 16
-        # host threads, so up to 100 steps (the line states the count it ran)
+        # a bounded sample of the workload: a full step takes about 0.12 s on
+        # 16 host threads, so up to 100 steps (the line states the count it ran)
         args.steps = min(args.steps, 100)
         args.warmup = min(args.warmup, 3)
 

@@ -2133,9 +2133,21 @@ void oracle_sources(const OMesh* M, const OParams* P, const double* st, const do
 int oracle_go(const OMesh* M, const OParams* P, double* state, double* xyz, const double* H, const double* S_ext,
               int64_t nsteps, double* clock, OStepInfo* info) {
     const int64_t nc = M->ncell, nf = M->nface, nn = M->nnode;
-    std::vector<double> st2(NV * nc), xyz2(3 * nn), fl(11 * nf);
-    std::vector<double> cc1(3 * nc), vol1(nc), fc1(3 * nf), fn1(3 * nf), fa1(nf);
-    std::vector<double> cc2(3 * nc), vol2(nc), fc2(3 * nf), fn2(3 * nf), fa2(nf);
+    // Scratch kept between calls (every element a step reads is written
+    // earlier in the same call), so a call's cost is its steps, not the
+    // allocation and first touch of its arrays.
+    static thread_local struct {
+        std::vector<double> st2, xyz2, fl, cc1, vol1, fc1, fn1, fa1, cc2, vol2, fc2, fn2, fa2;
+    } W;
+    auto sized = [](std::vector<double>& v, int64_t n) -> std::vector<double>& {
+        if ((int64_t)v.size() != n) v.resize(n);
+        return v;
+    };
+    std::vector<double>&st2 = sized(W.st2, NV * nc), &xyz2 = sized(W.xyz2, 3 * nn), &fl = sized(W.fl, 11 * nf);
+    std::vector<double>&cc1 = sized(W.cc1, 3 * nc), &vol1 = sized(W.vol1, nc), &fc1 = sized(W.fc1, 3 * nf),
+    &fn1 = sized(W.fn1, 3 * nf), &fa1 = sized(W.fa1, nf);
+    std::vector<double>&cc2 = sized(W.cc2, 3 * nc), &vol2 = sized(W.vol2, nc), &fc2 = sized(W.fc2, 3 * nf),
+    &fn2 = sized(W.fn2, 3 * nf), &fa2 = sized(W.fa2, nf);
     double time = clock[0], tphys = clock[1];
     info->err_code = 0;
     info->n_rho_floor = 0;

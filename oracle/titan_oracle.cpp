@@ -1561,8 +1561,9 @@ void oracle_move_nodes(const OMesh* M, const OParams* P, const double* xyz1, dou
 //  * Each node sums its faces' contributions in ascending face order (the
 //    reference sums under a mutex in thread order), divides by their number
 //    and moves along its own direction: x' = x + (V . x/|x|) dt x/|x|
-//    (:1213-1265; the reference's heliotail rays are parallel to the x axis
-//    and move HP nodes with x < 0 along (0, y, z); these rays are all radial).
+//    (:1213-1265); with hp_tail an HP node with x < 0 moves along (0, y, z)
+//    instead, the rule of the reference's heliotail, whose rays lie in planes
+//    of constant x (:1237-1247).
 //    With sglag_TS / sglag_HP a TS / HP node's mean also takes a term toward
 //    the sphere fitted through it and its neighbours (centres from
 //    oracle_surface_centres); with sglag_BS a BS node with more than five

@@ -475,11 +475,13 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
             // then the face speed from the node displacement (Gran::culc_velosity)
             const int nn = M.nnode;
             int nid[4];
-            double P[4][3];
+            double P[4][3], Q[4][3];
+            // both layers' nodes in one batch of loads, ahead of the arithmetic
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 nid[k] = M.face_nodes[k * nf + f];
                 load_node(a.L1.xyz, nn, nid[k], P[k]);
+                load_node(a.xyz2, nn, nid[k], Q[k]);
             }
             double cA[3], cB[3];
             load_cc(a.L1.cc, nc, c0, cA);
@@ -496,10 +498,9 @@ __global__ void __launch_bounds__(BS, MINB) face_flux_kernel(FaceArgs a) {
             double ddot = 0.0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const int i = nid[k];
-                const double dx = a.xyz2[i] - P[k][0];
-                const double dy = a.xyz2[nn + i] - P[k][1];
-                const double dz = a.xyz2[2 * nn + i] - P[k][2];
+                const double dx = Q[k][0] - P[k][0];
+                const double dy = Q[k][1] - P[k][1];
+                const double dz = Q[k][2] - P[k][2];
                 ddot = ddot + (dx * n[0] + dy * n[1] + dz * n[2]);
             }
             w = ddot / 4.0 / time;

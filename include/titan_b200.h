@@ -139,7 +139,8 @@ int titan_set_face_method(titan_ctx* ctx, const int8_t* n_state);
  * face loop, the faces of each moving surface (face_surf 1 = TS, 2 = HP,
  * 3 = BS; HP faces with fewer than four surface neighbours are skipped) solve
  * their Riemann problem at w = 0 on the step's state; each surface node moves
- * along its direction by dt times the mean of velocity_X * ds * n over its
+ * along its direction (x / |x|; with hp_tail, (0, y, z) for an HP node with
+ * x < 0) by dt times the mean of velocity_X * ds * n over its
  * faces (ds = dsl on TS, dsc on HP, dsr on BS; with bn_in_p_on_hp the HP
  * faces use the exact gas-dynamic solver). The other nodes of each ray keep
  * their fraction of the segment between the surface nodes and the ray's

@@ -11,6 +11,10 @@ construction with one table face and no other inflow:
 * the leaves are hit in proportion to their weights, and within a leaf the
   normal component follows the flux-weighted law x = sqrt(xL^2 + r (xR^2 -
   xL^2)) (its mean is 2 (xR^3 - xL^3) / (3 (xR^2 - xL^2))).
+
+And the outgoing tallies (AMR_f::Add_particle, Normir_velocity_volume):
+every neutral stopped on a tallied face is accounted for in its leaves and
+moments.
 """
 import numpy as np
 
@@ -57,3 +61,38 @@ def test_single_table_face_launch(titan, oracle_lib):
         xs = loc[leaf == k, 0]
         mean = 2.0 * (b[1] ** 3 - b[0] ** 3) / (3.0 * (b[1] ** 2 - b[0] ** 2))
         assert abs(xs.mean() - mean) < 0.02 * (b[1] - b[0]) + 4.0 * xs.std() / np.sqrt(len(xs))
+
+
+def test_outgoing_tallies_account_for_every_stopped_neutral(titan, oracle_lib):
+    """Tallies (AMR_f::Add_particle and Normir_velocity_volume, AMR_f.cpp:240-336)
+    on an interior sphere of faces: per face, the normalised leaves give back
+    the stopped weight (sum of f * box volume * area * box-centre x = Smu *
+    area), and the faces together hold mu times the neutrals whose trace ends
+    with kind 3 (stopped on a tallied face)."""
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=6, nlayer=8, move=False)
+    p = dict(p, par_Kn=3.0)
+    geo = ol.OracleRun(m, p).geometry()
+    on = np.all(m["node_layer"][m["face_nodes"]] == 5, axis=1) & (m["face_cells"][:, 1] >= 0)
+    faces = np.nonzero(on)[0]
+    cc = m["node_xyz"][m["cell_nodes"]].mean(axis=1)
+    fc = m["face_cells"][faces]
+    side = (np.linalg.norm(cc[fc[:, 1]], axis=1) > np.linalg.norm(cc[fc[:, 0]], axis=1)).astype(np.int8)
+    frame = np.array([_frame(geo["face_normal"][f] * (1.0 if s == 0 else -1.0)) for f, s in zip(faces, side)])
+    xe, ye = np.linspace(0.0, 8.0, 5), np.linspace(-6.0, 6.0, 4)
+    i, j, k = [a.ravel() for a in np.meshgrid(np.arange(4), np.arange(3), np.arange(3), indexing="ij")]
+    b = np.stack([xe[i], xe[i + 1], ye[j], ye[j + 1], ye[k], ye[k + 1]], axis=1)
+    ft = dict(face=faces, side=side, frame=frame, leaf_ptr=np.arange(len(faces) + 1) * len(b),
+              leaf_box=np.tile(b, (len(faces), 1)))
+    n = 40000
+    _, trace, total, lost = ol.mc_pass(m, st, p, n_particles=n, seed=4, face_tally=ft, **MC)
+    mu = total / n
+    stopped = int(np.sum(trace[:, 7] % 4 == 3))
+    assert stopped > 0 and ft["unplaced"] == 0
+    area = geo["face_area"][faces]
+    V = (b[:, 1] - b[:, 0]) * (b[:, 3] - b[:, 2]) * (b[:, 5] - b[:, 4])
+    cx = (b[:, 0] + b[:, 1]) / 2.0
+    f = ft["leaf_f"].reshape(len(faces), len(b))
+    per_face = (f * V[None, :] * cx[None, :]).sum(axis=1) * area
+    smu = ft["moments"][:, 1] * area
+    assert np.allclose(per_face, smu, rtol=1e-12, atol=1e-12 * smu.max())
+    assert abs(smu.sum() - mu * stopped) <= 1e-9 * mu * stopped

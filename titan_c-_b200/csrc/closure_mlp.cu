@@ -121,6 +121,9 @@ __device__ __forceinline__ void silu_pair(float h0, float h1, uint32_t& hi, uint
 // tensor core; the other turns the outputs into sources.
 constexpr int kPairs = 2;
 constexpr int kThreads = 256 * kPairs;
+// Registers per thread: 16 warps x 88 leave a third of the register file, so
+// blocks of another kernel (the face flux of the same step) can share the SM.
+constexpr int kMaxRegs = 88;
 // TMEM columns of one pair: its FP32 accumulator (128 columns), then its
 // activations as the next layer's A operand (128 rows in the lanes, two bf16
 // per column along K: columns 0..63 the hi halves of K = 0..127, columns
@@ -170,7 +173,7 @@ __device__ __forceinline__ void input_words(const MlpArgs& args, const Smem& S, 
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1) mlp_forward_tc(MlpArgs args) {
+__global__ void __maxnreg__(kMaxRegs) mlp_forward_tc(MlpArgs args) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -254,14 +257,14 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_forward_tc(MlpArgs args) {
             fence_after();
             // h -> SiLU -> this half's columns of the next layer's A operand
             {
-                float v[64];
-                tmem_ld64(acc + lane + 64 * h, v);
-                tmem_wait_ld();
+                float v[32];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {  // stored in two halves to keep fewer words live
+                for (int q = 0; q < 2; ++q) {  // 32 columns at a time, so few registers stay live
+                    tmem_ld32(acc + lane + 64 * h + 32 * q, v);
+                    tmem_wait_ld();
                     uint32_t hi[16], lo[16];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) silu_pair(v[32 * q + 2 * j], v[32 * q + 2 * j + 1], hi[j], lo[j]);
+                    for (int j = 0; j < 16; ++j) silu_pair(v[2 * j], v[2 * j + 1], hi[j], lo[j]);
                     tmem_st16(act + lane + 32 * h + 16 * q, hi);
                     tmem_st16(act + lane + kActLoCols + 32 * h + 16 * q, lo);
                 }

@@ -485,6 +485,11 @@ int titan_closure_outside(titan_ctx* ctx, int64_t* n_outside);
  * err_kind 21 and the step returns TITAN_ETIMEOUT. */
 int titan_autotune(titan_ctx* ctx, int32_t reps, const char* cache_path);
 int titan_set_tuning(titan_ctx* ctx, int32_t face_variant, int32_t cell_variant);
+/* With the closure installed, run its network on a stream of its own beside
+ * the face kernel (both read only the step's state; the cell update waits for
+ * both), 1, or before it on the context's stream, 0. Results are the same
+ * either way. */
+int titan_set_closure_overlap(titan_ctx* ctx, int32_t on);
 int titan_get_tuning(titan_ctx* ctx, int32_t* face_variant, int32_t* cell_variant, int32_t* face_block,
                      int32_t* face_min_blocks, int32_t* cell_block);
 

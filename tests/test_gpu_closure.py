@@ -277,3 +277,25 @@ def test_fallback_from_a_device_pass_equals_the_host_table(titan):
     g.close()
     for k in range(8):
         np.testing.assert_allclose(b[k], a[k], rtol=1e-9, atol=1e-13 * np.abs(a[k]).max())
+
+
+def test_closure_beside_the_face_kernel_gives_the_same_steps(titan):
+    """titan_set_closure_overlap: the network on its own stream beside the face
+    kernel, or before it; both read only the step's state and the cell update
+    waits for both, so the states are identical (graph and single steps)."""
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=10, nlayer=8, move=True, flux_precision=32)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    net = titan.closure.Closure.load(os.path.join(root, "titan_c-_b200", "data", "closure_shell.npz"))
+    outs = []
+    for on in (False, True):
+        for chunks in ([4], [1, 1, 1, 1]):
+            g = titan.PlasmaStep(m, p)
+            g.upload_state(st)
+            net.install(g)
+            g.set_closure_overlap(on)
+            for k in chunks:
+                g.go(k)
+            outs.append(g.download_state())
+            g.close()
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])

@@ -73,6 +73,11 @@ struct titan_ctx {
     int ns = 8;  // state fields stored on the device (8 + npassive)
     bool fp32 = false;
     cudaStream_t stream = nullptr;
+    // the closure's own stream (the greatest priority), forked from and joined
+    // back into `stream` so the network runs beside the face kernel
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    bool overlap_closure = true;
     int64_t dev_bytes = 0;
 
     Renumbering R;
@@ -248,6 +253,7 @@ int step_source_mode(const titan_ctx* ctx) {
 cudaError_t enqueue_step(titan_ctx* ctx) {
     const MeshView M = ctx->view();
     const bool move = ctx->prm.move != 0;
+    const bool overlap = ctx->use_closure && ctx->overlap_closure && !ctx->profiling;
     const int nxt = ctx->cur ^ 1;
     cudaError_t e = cudaSuccess;
     if (move && ctx->use_surface) {
@@ -289,7 +295,17 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
             e = cudaMemsetAsync(ctx->d_n_outside, 0, sizeof(unsigned long long), ctx->stream);
             if (e) return e;
         }
-        e = timed(ctx, "closure_mlp", [&] { return launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->stream); });
+        if (overlap) {
+            // beside the face kernel: both read only this step's state; the
+            // cell update waits for both (kernel-time profiling keeps them in turn)
+            e = cudaEventRecord(ctx->fork_ev, ctx->stream);
+            if (!e) e = cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0);
+            if (!e) e = launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->side);
+            if (!e) e = cudaEventRecord(ctx->join_ev, ctx->side);
+        } else {
+            e = timed(ctx, "closure_mlp",
+                      [&] { return launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->stream); });
+        }
         if (e) return e;
     }
     FaceArgs fa;
@@ -302,6 +318,7 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     fa.st = ctx->d_status;
     const int nk = ctx->prm.npassive;
     e = timed(ctx, face_kernel_name(ctx), [&] { return face_launch(ctx, fa, nk, move, ctx->face_variant, ctx->stream); });
+    if (!e && overlap) e = cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0);
     if (e) return e;
     CellArgs ca;
     ca.M = M;
@@ -582,6 +599,9 @@ int titan_destroy(titan_ctx* ctx) {
     for (auto& e : ctx->xev)
         if (e) cudaEventDestroy(e);
     if (ctx->xfer) cudaStreamDestroy(ctx->xfer);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return TITAN_OK;
@@ -633,6 +653,14 @@ int titan_create(const titan_mesh* m, const titan_params* p, titan_ctx** out) {
     cudaEventCreate(&ctx->ev[1]);
     e = cudaStreamCreateWithFlags(&ctx->xfer, cudaStreamNonBlocking);
     if (e) return bail(fail(TITAN_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)));
+    {
+        int lo = 0, hi = 0;
+        e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        if (!e) e = cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, hi);
+        if (!e) e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
+        if (!e) e = cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming);
+        if (e) return bail(fail(TITAN_ECUDA, std::string("closure stream: ") + cudaGetErrorString(e)));
+    }
     for (auto& x : ctx->xev) {
         e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
         if (e) return bail(fail(TITAN_ECUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(e)));
@@ -1929,6 +1957,13 @@ int titan_set_ray_law(titan_ctx* ctx, const titan_ray_law* law) {
             }
         }
     ctx->surf.law = g;
+    return TITAN_OK;
+}
+
+int titan_set_closure_overlap(titan_ctx* ctx, int32_t on) {
+    if (!ctx) return fail(TITAN_EINVAL, "null argument");
+    ctx->overlap_closure = on != 0;
+    drop_graph(ctx);
     return TITAN_OK;
 }
 

@@ -171,6 +171,7 @@ SIGNATURES = {
     "titan_unpack_halo": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "titan_autotune": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p], ctypes.c_int),
     "titan_set_tuning": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
+    "titan_set_closure_overlap": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "titan_get_tuning": ([ctypes.c_void_p, I32, I32, I32, I32, I32], ctypes.c_int),
     "titan_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "titan_set_profiling": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),

@@ -345,6 +345,10 @@ class PlasmaStep:
         N.check(self._lib.titan_autotune(self._ctx, int(reps), cache.encode() if cache else None))
         return self.tuning()
 
+    def set_closure_overlap(self, on: bool):
+        """Run the closure beside the face kernel (titan_set_closure_overlap)."""
+        N.check(self._lib.titan_set_closure_overlap(self._ctx, int(bool(on))))
+
     def set_tuning(self, face_variant: int, cell_variant: int):
         N.check(self._lib.titan_set_tuning(self._ctx, int(face_variant), int(cell_variant)))
 

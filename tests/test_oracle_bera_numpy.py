@@ -15,6 +15,7 @@ oracle's restatement of this part of the step beyond its invariants."""
 import ctypes
 
 import numpy as np
+import pytest
 
 import oracle_lib as ol
 
@@ -109,3 +110,23 @@ def test_bera_sources_agree_with_a_second_restatement(titan, oracle_lib):
     for k in range(4):
         scale = np.abs(S_n[k]).max()
         assert np.abs(S_o[:, k] - S_n[k]).max() <= 1e-12 * scale, k
+
+
+@pytest.mark.skipif(not ol.ref_available(), reason="reference solver not built (no reference tree)")
+def test_thermal_protons_match_the_compiled_reference(oracle_lib):
+    """rho_Th and T_Th of the restatement above (and of the oracle, which agrees
+    with it) against the reference's own compiled Phys_param::Plasma_components_1
+    (Phys_param.cpp:628-665), for the 0-based zones 0-3 it is called with."""
+    rng = np.random.default_rng(3)
+    L = ol.ref()
+    out = np.zeros(3)
+    for zone_ in range(4):
+        al = 2.0 if zone_ <= 2 else 1.0
+        for _ in range(200):
+            rho = 0.01 + 2.0 * rng.random()
+            p = 1e-3 + rng.random()
+            rho_He = rho * 0.2 * rng.random()
+            L.titan_ref_plasma_components_1(zone_, rho, p, rho_He, ol._p(out))
+            rho_p = -(ME_DMP * al * rho_He + 4.0 * (-rho + rho_He)) / (4.0 * (1.0 + ME_DMP))
+            T_p = 8.0 * (1.0 + ME_DMP) * p / (8.0 * rho - (7.0 - al + (-1.0 + al) * ME_DMP) * rho_He)
+            assert out[0] == rho_p and out[2] == T_p

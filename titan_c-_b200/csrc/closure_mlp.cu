@@ -45,34 +45,6 @@ namespace titan {
 namespace mlp {
 using namespace tc;
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%"
-        "20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-#pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// 64 consecutive 32-bit columns of this thread's TMEM lane (one instruction, one wait)
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
-    uint32_t r[64];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-                 : "r"(taddr));
-#pragma unroll
-    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* r) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
-                 : "memory");
-}
-
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // D (TMEM) += A (TMEM, M=128 rows in lanes, 2 bf16 per column along K) . B (shared memory)
@@ -85,15 +57,7 @@ __device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, ui
         "r"(tmem_a), "l"(bd), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
-// 16 / 8 consecutive 32-bit columns of this thread's TMEM lane
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
-            taddr),
-        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
-        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
-        : "memory");
-}
+// 8 consecutive 32-bit columns of this thread's TMEM lane
 __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* r) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
                  "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
@@ -121,9 +85,11 @@ __device__ __forceinline__ void silu_pair(float h0, float h1, uint32_t& hi, uint
 // tensor core; the other turns the outputs into sources.
 constexpr int kPairs = 2;
 constexpr int kThreads = 256 * kPairs;
-// Registers per thread: 16 warps x 88 leave a third of the register file, so
-// blocks of another kernel (the face flux of the same step) can share the SM.
-constexpr int kMaxRegs = 88;
+// Registers per thread: 16 warps x 56 take 28,672 of the SM's 65,536, so
+// blocks of another kernel (the face flux of the same step: three blocks of
+// 128 threads at 96 registers) share the SM with a closure CTA. The epilogue
+// works 16 accumulator columns at a time to fit.
+constexpr int kMaxRegs = 56;
 // TMEM columns of one pair: its FP32 accumulator (128 columns), then its
 // activations as the next layer's A operand (128 rows in the lanes, two bf16
 // per column along K: columns 0..63 the hi halves of K = 0..127, columns
@@ -257,16 +223,16 @@ __global__ void __maxnreg__(kMaxRegs) mlp_forward_tc(MlpArgs args) {
             fence_after();
             // h -> SiLU -> this half's columns of the next layer's A operand
             {
-                float v[32];
+                float v[16];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {  // 32 columns at a time, so few registers stay live
-                    tmem_ld32(acc + lane + 64 * h + 32 * q, v);
+                for (int q = 0; q < 4; ++q) {  // 16 columns at a time, so few registers stay live
+                    tmem_ld16(acc + lane + 64 * h + 16 * q, v);
                     tmem_wait_ld();
-                    uint32_t hi[16], lo[16];
+                    uint32_t hi[8], lo[8];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) silu_pair(v[2 * j], v[2 * j + 1], hi[j], lo[j]);
-                    tmem_st16(act + lane + 32 * h + 16 * q, hi);
-                    tmem_st16(act + lane + kActLoCols + 32 * h + 16 * q, lo);
+                    for (int j = 0; j < 8; ++j) silu_pair(v[2 * j], v[2 * j + 1], hi[j], lo[j]);
+                    tmem_st8(act + lane + 32 * h + 8 * q, hi);
+                    tmem_st8(act + lane + kActLoCols + 32 * h + 8 * q, lo);
                 }
                 tmem_wait_st();
             }

@@ -256,6 +256,34 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
     const bool overlap = ctx->use_closure && ctx->overlap_closure && !ctx->profiling;
     const int nxt = ctx->cur ^ 1;
     cudaError_t e = cudaSuccess;
+    if (ctx->use_closure) {
+        // the network on this step's inputs (formed by the previous cell update);
+        // the cell update turns its outputs into sources. It reads neither the
+        // nodes nor the state, so it starts before the node motion.
+        MlpArgs ma{};
+        ma.net = ctx->closure.view();
+        ma.n = (int)ctx->ncell;
+        ma.ncell = (int)ctx->ncell;
+        ma.in_words = ctx->d_cl_in;
+        ma.y_out = ctx->d_cl_y;
+        ma.error = ctx->closure.error;
+        if (ctx->d_n_outside) {
+            e = cudaMemsetAsync(ctx->d_n_outside, 0, sizeof(unsigned long long), ctx->stream);
+            if (e) return e;
+        }
+        if (overlap) {
+            // beside the node motion and the face kernel; the cell update waits
+            // for it (kernel-time profiling keeps the kernels in turn)
+            e = cudaEventRecord(ctx->fork_ev, ctx->stream);
+            if (!e) e = cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0);
+            if (!e) e = launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->side);
+            if (!e) e = cudaEventRecord(ctx->join_ev, ctx->side);
+        } else {
+            e = timed(ctx, "closure_mlp",
+                      [&] { return launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->stream); });
+        }
+        if (e) return e;
+    }
     if (move && ctx->use_surface) {
         // nodes follow the TS / HP / BS surfaces (Setka::Culc_Velocity_surface,
         // Luch::dvigenie) on this state; null_bn_on_HP may edit the HP cells' B
@@ -279,33 +307,6 @@ cudaError_t enqueue_step(titan_ctx* ctx) {
             return launch_move_nodes(M, ctx->P, ctx->layer[ctx->cur].xyz, ctx->layer[nxt].xyz, ctx->d_status,
                                      ctx->stream);
         });
-        if (e) return e;
-    }
-    if (ctx->use_closure) {
-        // the network on this step's inputs (formed by the previous cell update);
-        // the cell update turns its outputs into sources
-        MlpArgs ma{};
-        ma.net = ctx->closure.view();
-        ma.n = (int)ctx->ncell;
-        ma.ncell = (int)ctx->ncell;
-        ma.in_words = ctx->d_cl_in;
-        ma.y_out = ctx->d_cl_y;
-        ma.error = ctx->closure.error;
-        if (ctx->d_n_outside) {
-            e = cudaMemsetAsync(ctx->d_n_outside, 0, sizeof(unsigned long long), ctx->stream);
-            if (e) return e;
-        }
-        if (overlap) {
-            // beside the face kernel: both read only this step's state; the
-            // cell update waits for both (kernel-time profiling keeps them in turn)
-            e = cudaEventRecord(ctx->fork_ev, ctx->stream);
-            if (!e) e = cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0);
-            if (!e) e = launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->side);
-            if (!e) e = cudaEventRecord(ctx->join_ev, ctx->side);
-        } else {
-            e = timed(ctx, "closure_mlp",
-                      [&] { return launch_mlp_forward(ma, kModeSources, ctx->sm_count, ctx->stream); });
-        }
         if (e) return e;
     }
     FaceArgs fa;

@@ -108,6 +108,16 @@ def test_create_rejects_inconsistent_mesh_before_touching_the_device(built_lib, 
     assert e.value.code == -2
 
 
+def test_create_rejects_an_empty_mesh(built_lib, titan):
+    m, p, _, _ = titan.problems.brio_wu_box(1, 1, 1)
+    no_cells = dict(m, **{k: m[k][:0] for k in ("cell_nodes", "cell_faces", "cell_type", "cell_tvd")})
+    no_faces = dict(m, **{k: m[k][:0] for k in ("face_nodes", "face_cells", "face_type", "face_surf", "face_bc")})
+    for bad in (no_cells, no_faces, dict(m, node_xyz=m["node_xyz"][:0])):
+        with pytest.raises(titan.TitanError) as e:
+            titan.PlasmaStep(bad, p)
+        assert e.value.code == -2 and "empty" in str(e.value)
+
+
 def test_riemann_batch_argument_checks(built_lib, titan):
     N = titan.native
     rc = N.lib().titan_riemann_batch(0, None, None, None, None, None, 0, 64, 5.0 / 3.0, None, None, None)

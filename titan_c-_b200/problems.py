@@ -39,7 +39,13 @@ def params(**over) -> dict:
 
 def brio_wu_cube(n: int = 32):
     """(mesh, params, state [10, C], face_method [F])."""
-    m = _mesh.cube_mesh(n)
+    return brio_wu_box(n, n, n)
+
+
+def brio_wu_box(nx: int, ny: int, nz: int):
+    """The Brio-Wu problem of brio_wu_cube on the unit box cut into nx x ny x nz
+    hexahedra: (mesh, params, state [10, C], face_method [F])."""
+    m = _mesh.box_mesh(nx, ny, nz)
     cc = m["node_xyz"][m["cell_nodes"]].mean(axis=1)
     nrm = np.array([1.0, 1.0, 0.0]) / np.sqrt(2.0)
     tng = np.array([-1.0, 1.0, 0.0]) / np.sqrt(2.0)

@@ -78,16 +78,22 @@ def peak_tflops():
 
 
 # DRAM bytes (read + write) per launch, per kernel, from one ncu capture of
-# each kernel on the 6x96x96x40 shell itself (the workload of this benchmark;
-# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum, one launch each).
-# Keyed by (kernel, cells, sources in the step); other sizes report no traffic.
+# each kernel on the shells themselves (6x96x96x40, the workload of this
+# benchmark, and 6x192x192x40, its large shell; ncu --metrics
+# dram__bytes_read.sum,dram__bytes_write.sum, one launch each, the launch
+# shapes the autotuner picks). Keyed by (kernel, cells, sources in the step);
+# other sizes report no traffic.
 TRAFFIC = {
     # the mixed step (FP32 Riemann arithmetic, closure sources)
-    ("move_nodes", 2211840, True): 107.85e6, ("closure_mlp", 2211840, True): 81.21e6,
-    ("face_flux_fp32", 2211840, True): 1066.71e6, ("cell_update", 2211840, True): 1433.49e6,
+    ("move_nodes", 2211840, True): 107.86e6, ("closure_mlp", 2211840, True): 83.66e6,
+    ("face_flux_fp32", 2211840, True): 1039.27e6, ("cell_update", 2211840, True): 1450.35e6,
+    ("move_nodes", 8847360, True): 540.41e6, ("closure_mlp", 8847360, True): 427.86e6,
+    ("face_flux_fp32", 8847360, True): 4257.45e6, ("cell_update", 8847360, True): 5988.45e6,
     # the plain FP64 step
-    ("move_nodes", 2211840, False): 110.73e6, ("face_flux_fp64", 2211840, False): 1045.15e6,
-    ("cell_update", 2211840, False): 1164.85e6,
+    ("move_nodes", 2211840, False): 111.87e6, ("face_flux_fp64", 2211840, False): 1045.05e6,
+    ("cell_update", 2211840, False): 1163.66e6,
+    ("move_nodes", 8847360, False): 543.15e6, ("face_flux_fp64", 8847360, False): 4278.31e6,
+    ("cell_update", 8847360, False): 4772.92e6,
 }
 
 

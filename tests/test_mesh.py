@@ -58,6 +58,27 @@ def test_cube_geometry_invariants(titan, oracle_lib):
     assert np.allclose(g["face_area"], 1.0 / 64)
 
 
+@pytest.mark.parametrize("dims", [(1, 1, 1), (1, 40, 1), (3, 1, 2), (5, 7, 3), (33, 2, 5)])
+def test_ragged_box_counts_and_invariants(titan, oracle_lib, dims):
+    """The boxes of the size and shape edge cases: counts, the invariants
+    above, and volumes and areas of the unit box cut nx x ny x nz."""
+    nx, ny, nz = dims
+    m = titan.mesh.box_mesh(nx, ny, nz)
+    assert m["cell_nodes"].shape[0] == nx * ny * nz
+    assert m["node_xyz"].shape[0] == (nx + 1) * (ny + 1) * (nz + 1)
+    assert m["face_nodes"].shape[0] == (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+    assert int((m["face_cells"][:, 1] < 0).sum()) == 2 * (ny * nz + nx * nz + nx * ny)
+    g = ol.OracleRun(m, titan.problems.params()).geometry()
+    _invariants(m, g)
+    assert abs(g["cell_volume"].sum() - 1.0) < 1e-12
+    assert np.allclose(g["cell_volume"], 1.0 / (nx * ny * nz), rtol=1e-12)
+    n = np.abs(g["face_normal"])
+    for axis, area in ((0, 1.0 / (ny * nz)), (1, 1.0 / (nx * nz)), (2, 1.0 / (nx * ny))):
+        along = n[:, axis] > 0.5
+        assert int(along.sum()) == ((nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1))[axis]
+        assert np.allclose(g["face_area"][along], area, rtol=1e-12)
+
+
 def test_shell_geometry_invariants(titan, oracle_lib):
     m = titan.mesh.shell_mesh(6, 5)
     run = ol.OracleRun(m, titan.problems.params())

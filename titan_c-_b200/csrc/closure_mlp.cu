@@ -5,17 +5,17 @@
 //
 // Inference (every step) runs on the 5th-generation tensor cores. A CTA holds
 // the layer weights in shared memory for the whole kernel, in the canonical
-// K-major "interleave" layout (8x16-byte core matrices), and runs two
-// warpgroups, each with its own tile of 128 cells in flight. A warpgroup's
+// K-major "interleave" layout (8x16-byte core matrices), and runs two pairs
+// of warpgroups, each pair with its own tile of 128 cells in flight. A tile's
 // activations live in tensor memory next to its accumulator and are the A
 // operand of the next layer's tcgen05.mma (the TMEM-A form), so shared memory
-// holds only the weights: while one warpgroup turns its accumulator into the
-// next layer's activations (tcgen05.ld, SiLU, tcgen05.st), the tensor core
-// works on the other warpgroup's layer. One thread of the warpgroup issues
-// the M=128 x N x K=16 instructions; completion goes through the warpgroup's
-// mbarrier; waiting threads sleep (try_wait with a suspend hint) and the waits
-// are bounded: a wait that runs out records an error and the warpgroup stops
-// issuing work; the CTA releases TMEM and returns.
+// holds only the weights: while one pair turns its accumulator into the next
+// layer's activations (tcgen05.ld, SiLU, tcgen05.st), the tensor core works on
+// the other pair's layer. One thread of the pair issues the M=128 x N x K=16
+// instructions; completion goes through the pair's mbarrier; waiting threads
+// sleep (try_wait with a suspend hint) and the waits are bounded: a wait that
+// runs out records an error and the pair stops issuing work; the CTA releases
+// TMEM and returns.
 //
 // Precision: the network must be a smooth function of the cell state. Two
 // runs whose states differ at rounding level (the FP64 step and the mixed

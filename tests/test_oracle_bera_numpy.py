@@ -11,7 +11,10 @@ separate restatement in numpy, written from the reference's text:
   (:988-1000), scaled by n_H / Kn (:1236-1240).
 
 Two transcriptions that agree to rounding on seeded cells of every zone pin the
-oracle's restatement of this part of the step beyond its invariants."""
+oracle's restatement of this part of the step beyond its invariants; the
+thermal-proton split is also pinned bit for bit to the reference's compiled
+code, live where the reference tree is built and through a golden file it
+generated everywhere."""
 import ctypes
 
 import numpy as np
@@ -130,3 +133,21 @@ def test_thermal_protons_match_the_compiled_reference(oracle_lib):
             rho_p = -(ME_DMP * al * rho_He + 4.0 * (-rho + rho_He)) / (4.0 * (1.0 + ME_DMP))
             T_p = 8.0 * (1.0 + ME_DMP) * p / (8.0 * rho - (7.0 - al + (-1.0 + al) * ME_DMP) * rho_He)
             assert out[0] == rho_p and out[2] == T_p
+
+
+def test_thermal_protons_match_the_reference_golden():
+    """The same split against tests/golden/plasma_components_golden.npz, made
+    by the compiled reference (make_plasma_golden.py): rho_Th, p_Th and T_Th
+    bit for bit over zones 0-3, helium-rich cells included. Needs no reference
+    tree."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "plasma_components_golden.npz"))
+    rho, p, rho_He = g["rho"], g["p"], g["rho_he"]
+    al = np.where(g["zone"] <= 2, 2.0, 1.0)
+    rho_p = -(ME_DMP * al * rho_He + 4.0 * (-rho + rho_He)) / (4.0 * (1.0 + ME_DMP))
+    p_p = p * (4.0 * rho - (4.0 + al * ME_DMP) * rho_He) / (8.0 * rho + (-7.0 + al + (1.0 - al) * ME_DMP) * rho_He)
+    T_p = 8.0 * (1.0 + ME_DMP) * p / (8.0 * rho - (7.0 - al + (-1.0 + al) * ME_DMP) * rho_He)
+    assert len(rho) == 1600 and np.any(g["out"][:, 0] <= 0.0)
+    np.testing.assert_array_equal(g["out"][:, 0], rho_p)
+    np.testing.assert_array_equal(g["out"][:, 1], p_p)
+    np.testing.assert_array_equal(g["out"][:, 2], T_p)

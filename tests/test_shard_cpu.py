@@ -174,3 +174,49 @@ def test_two_gloo_ranks_match_the_single_domain_step(titan, oracle_lib):
     assert full.go(ref, 3).err_code == 0
     assert np.array_equal(got[:8], ref[:8])
     assert dt == full.clock[0]
+
+
+def _gloo_rank_that_may_fail(rank, world, port, out, fail_rank):
+    """Rank `fail_rank` leaves after the set-up barrier, between steps, with none
+    of its exchanges in flight; the others must end their next step with an
+    error within the process group's timeout instead of waiting for good."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    import importlib
+    import sys
+    import time
+
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    torch.distributed.init_process_group("gloo", rank=rank, world_size=world,
+                                         timeout=datetime.timedelta(seconds=10))
+    titan = importlib.import_module("titan_c-_b200")
+    m, p, st = _problem(titan)
+    ss = titan.shard.ShardedStep(titan, m, p, rank, world, torch.device("cpu"), stepper=OracleStepper)
+    ss.upload_state(st)
+    if rank == fail_rank:
+        os._exit(3)  # the rank dies between steps
+    t0 = time.monotonic()
+    try:
+        ss.go(3)
+        out.put((rank, "no error", time.monotonic() - t0))
+    except Exception as e:  # noqa: BLE001 - any error the collective raises
+        out.put((rank, type(e).__name__, time.monotonic() - t0))
+    out.close()
+    out.join_thread()  # the queue's feeder thread has written the result
+    os._exit(0)
+
+
+def test_a_rank_that_dies_between_steps_ends_the_others_with_an_error(titan):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gloo_rank_that_may_fail, args=(r, 2, port, q, 1)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    rank, what, waited = q.get(timeout=240)
+    for pr in procs:
+        pr.join(timeout=60)
+    assert rank == 0 and what != "no error"
+    assert waited < 60.0
+    assert procs[1].exitcode == 3 and procs[0].exitcode == 0

@@ -72,3 +72,18 @@ def test_step_roofline_is_bytes_over_time(bench):
     assert r["achieved"] == pytest.approx(801574752.0 / 1e-3 / 1e9)
     assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
     assert r["traffic_over_algorithmic"] == pytest.approx(r["traffic_per_step"] / r["algorithmic_bytes_per_step"])
+
+
+def test_reference_arm_line_on_a_small_shell(bench, oracle_lib):
+    """`bench.py --impl reference` on a small shell: the oracle times its FP64
+    step on the host and prints the line the driver reads (rank 0 only)."""
+    import argparse
+    args = argparse.Namespace(nq=6, nlayer=6, mode="mixed-mlp", steps=2, warmup=1)
+    line = bench.run_reference(args, 0, 1)
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "cell-updates/s"
+    assert line["config"]["cells"] == 6 * 6 * 6 * 6
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert bench.run_reference(args, 1, 2) is None   # other ranks do no work

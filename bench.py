@@ -615,22 +615,38 @@ def run_coupled_loop(pkg, m, p, st, closure, args, barrier, dev, steps=COUPLED_S
             "note": "device time of the whole loop, the Monte-Carlo passes and their fallback hand-over included"}
 
 
-def cpu_baseline(args, m, p, st, steps=None):
-    """The oracle (OpenMP restatement of Setka::Go's plasma loop) on the same
-    mesh, a bounded number of steps."""
+def timed_oracle(m, p, st, steps, warmup=1):
+    """Seconds for `steps` oracle steps of the workload (after `warmup`), with
+    the reference's own compiled Phys_param::chlld solving every face where
+    oracle/_ref holds it (the Riemann solves are most of the step's host time;
+    the results are identical to the oracle's restatement). Returns
+    (seconds, threads, where the Riemann solver came from)."""
     import oracle_lib as ol
 
     run = ol.OracleRun(m, p)
     s = np.ascontiguousarray(st.copy())
+    used_ref = ol.use_reference_riemann(p["gamma"])
+    try:
+        run.go(s, max(warmup, 1))  # first touch / geometry warm-up
+        t0 = time.perf_counter()
+        run.go(s, steps)
+        dt = time.perf_counter() - t0
+    finally:
+        ol.use_reference_riemann(None)
+    solver = ("the reference's own compiled Phys_param::chlld on every face" if used_ref
+              else "the oracle's restatement of chlld (the reference's was not built)")
+    return dt, int(ol.oracle().oracle_num_threads()), solver
+
+
+def cpu_baseline(args, m, p, st, steps=None):
+    """The oracle (OpenMP restatement of Setka::Go's plasma loop) on the same
+    mesh, a bounded number of steps."""
     steps = steps or args.cpu_steps
-    run.go(s, 1)  # first touch / geometry warm-up
-    t0 = time.perf_counter()
-    run.go(s, steps)
-    dt = time.perf_counter() - t0
+    dt, cores, solver = timed_oracle(m, p, st, steps)
     C = m["cell_nodes"].shape[0]
-    return {"value": C * steps / dt, "unit": UNIT, "cores": int(ol.oracle().oracle_num_threads()),
+    return {"value": C * steps / dt, "unit": UNIT, "cores": cores,
             "kind": "port", "sample": f"{steps} steps of the full {C}-cell workload "
-                                      f"({dt:.1f} s), oracle/titan_oracle.cpp with OpenMP"}
+                                      f"({dt:.1f} s), oracle/titan_oracle.cpp with OpenMP, {solver}"}
 
 
 def run_sharded(args, rank, world):
@@ -717,16 +733,8 @@ def run_reference(args, rank, world):
         return None
     pkg, m, p, st = build_problem(args)
     C = m["cell_nodes"].shape[0]
-    import oracle_lib as ol
-
-    run = ol.OracleRun(m, p)
-    s = np.ascontiguousarray(st.copy())
-    run.go(s, max(args.warmup, 1))
-    t0 = time.perf_counter()
-    run.go(s, args.steps)
-    dt = time.perf_counter() - t0
+    dt, cores, solver = timed_oracle(m, p, st, args.steps, args.warmup)
     v = C * args.steps / dt
-    cores = int(ol.oracle().oracle_num_threads())
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -734,7 +742,8 @@ def run_reference(args, rank, world):
             "config": {"workload": f"heliosphere shell 6x{args.nq}x{args.nq}x{args.nlayer} = {C} cells, ALE, "
                                    "HLLD/HLLC, FP64", "cells": C},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} steps of the full workload after {args.warmup} warm-up"},
+                             "sample": f"{args.steps} steps of the full workload after {args.warmup} warm-up, "
+                                       f"oracle/titan_oracle.cpp with OpenMP, {solver}"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -757,8 +766,8 @@ def main():
                     help="split one mesh over the GPUs (strong scaling) instead of N replicas")
     args = ap.parse_args()
     if args.impl == "reference":
-        # a bounded sample of the workload: a full step takes about 0.12 s on
-        # 16 host threads, so up to 100 steps (the line states the count it ran)
+        # a bounded sample of the workload: a full step takes about 0.12-0.2 s
+        # on 16 host threads, so up to 100 steps (the line states the count it ran)
         args.steps = min(args.steps, 100)
         args.warmup = min(args.warmup, 3)
 

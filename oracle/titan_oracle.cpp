@@ -154,6 +154,17 @@ static void o_bazis(const double n[3], double t[3], double m[3]) {
     m[2] = n[0] * t[1] - n[1] * t[0];
 }
 
+// An optional stand-in for o_chlld in the step's face loop: the reference's own
+// Phys_param::chlld, compiled unmodified into oracle/_ref behind its C wrapper
+// (titan_ref_chlld: the arguments of o_chlld without gamma, which the reference
+// holds itself). The CPU-baseline timing installs it so that the Riemann solves,
+// most of the step's host time, are the reference's code; results are
+// identical (the restatement is bit-exact against it). It reports no status:
+// the reference exits on inputs it cannot solve.
+using RefRiemann = void (*)(int, const double*, double, const double*, const double*, int, int, int,
+                            const double*, const double*, double*, double*, double*, int, int);
+static RefRiemann g_ref_riemann = nullptr;
+
 // ---------------------------------------------------------------------------
 // Riemann solver family, restating Phys_param::chlld
 // (TITAN/source/Phys_param.cpp:882-1878): n_state 0 Lax, 1 HLL, 2 HLLC,
@@ -1335,6 +1346,9 @@ static double o_face(const OMesh* M, const OParams* P, const double* st, const d
         ds[1] = gds[1];
         ds[2] = gds[2];
         bn_sum = 0.0;
+    } else if (g_ref_riemann) {
+        // the reference's own solver (CPU-baseline timing; it exits on errors)
+        g_ref_riemann(method, n, w, L, R, 0, 0, nk, L + 8, R + 8, q, kq, ds, left_ydar, contact);
     } else {
         const int rc = o_chlld(method, n, w, L, R, 0, 0, nk, L + 8, R + 8, q, kq, ds, left_ydar, contact, P->gamma);
         if (rc) *err = 10 + rc;
@@ -2243,6 +2257,8 @@ int oracle_godunov(const double* nrm, double w, const double* q1, const double* 
                    double* out, double* ds) {
     return o_godunov(nrm, w, q1, q2, contact, gamma, out, ds);
 }
+
+void oracle_set_reference_riemann(void* fn) { g_ref_riemann = reinterpret_cast<RefRiemann>(fn); }
 
 int oracle_num_threads(void) {
 #ifdef _OPENMP

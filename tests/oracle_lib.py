@@ -109,6 +109,7 @@ def oracle():
         lib.oracle_move_nodes.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D,
                                           ctypes.c_double, ctypes.c_double]
         lib.oracle_num_threads.restype = ctypes.c_int
+        lib.oracle_set_reference_riemann.argtypes = [ctypes.c_void_p]
         lib.oracle_tvd_neighbours.argtypes = [ctypes.POINTER(OMesh), D, I32]
         lib.oracle_ray_geometry.argtypes = [ctypes.POINTER(OMesh), D, D, D]
         lib.oracle_surface_centres.argtypes = [ctypes.POINTER(OMesh), D, D]
@@ -117,6 +118,24 @@ def oracle():
         lib.oracle_face_states.argtypes = [ctypes.POINTER(OMesh), ctypes.POINTER(OParams), D, D, D, I8]
         _oracle = lib
     return _oracle
+
+
+def use_reference_riemann(gamma: float | None) -> bool:
+    """Installs the reference's own compiled Phys_param::chlld as the oracle
+    step's Riemann solver (gamma: the step's adiabatic index), or removes it
+    (None). Returns whether the reference solver is in use."""
+    lib = oracle()
+    if gamma is None or not ref_available():
+        lib.oracle_set_reference_riemann(None)
+        return False
+    try:
+        r = ref()
+    except (OSError, RuntimeError):  # a reference build that does not load here
+        lib.oracle_set_reference_riemann(None)
+        return False
+    r.titan_ref_set_gamma(float(gamma))
+    lib.oracle_set_reference_riemann(ctypes.cast(r.titan_ref_chlld, ctypes.c_void_p).value)
+    return True
 
 
 def ref_available() -> bool:

@@ -70,3 +70,26 @@ def test_oracle_chlld_vs_golden(oracle_lib):
         np.testing.assert_array_equal(out, g["flux"][i])
         np.testing.assert_array_equal(kout, g["kout"][i, :nk])
         np.testing.assert_array_equal(ds, g["ds"][i])
+
+
+@pytest.mark.skipif(not ol.ref_available(), reason="reference solver not built (no reference tree)")
+@pytest.mark.parametrize("kw", [dict(), dict(zones=True, npassive=2, nh=2)])
+def test_oracle_step_with_the_reference_solver_is_identical(titan, oracle_lib, kw):
+    """The oracle step with the reference's own compiled chlld on every face
+    (the CPU baseline's timed form) against the oracle step with its
+    restatement: the same states, dt and time, bit for bit."""
+    m, p, st, hf = titan.problems.heliosphere_shell(nq=6, nlayer=6, move=True, **kw)
+    out = []
+    for use_ref in (False, True):
+        run = ol.OracleRun(m, p)
+        if hf is not None:
+            run.hf = np.ascontiguousarray(hf)
+        s = np.ascontiguousarray(st.copy())
+        try:
+            assert ol.use_reference_riemann(p["gamma"] if use_ref else None) == use_ref
+            assert run.go(s, 4).err_code == 0
+        finally:
+            ol.use_reference_riemann(None)
+        out.append((s, run.clock.copy()))
+    assert np.array_equal(out[0][0].view(np.uint64), out[1][0].view(np.uint64))
+    assert np.array_equal(out[0][1], out[1][1])

@@ -87,3 +87,16 @@ def test_reference_arm_line_on_a_small_shell(bench, oracle_lib):
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert bench.run_reference(args, 1, 2) is None   # other ranks do no work
+
+
+def test_cpu_timing_names_the_riemann_solver_it_ran(bench, oracle_lib, titan, monkeypatch):
+    """The CPU baseline uses the reference's compiled solver where oracle/_ref
+    holds it and says so; without it, the oracle's restatement, also said."""
+    import oracle_lib as ol
+    m, p, st, _ = titan.problems.heliosphere_shell(nq=6, nlayer=6, move=True)
+    dt, cores, solver = bench.timed_oracle(m, p, st, 1)
+    assert dt > 0 and cores >= 1
+    assert ("reference's own compiled" in solver) == ol.ref_available()
+    monkeypatch.setattr(ol, "ref_available", lambda: False)
+    _, _, solver = bench.timed_oracle(m, p, st, 1)
+    assert "restatement" in solver
